@@ -1,0 +1,405 @@
+"""Benchmark: ESP particle-steps/s on the mixed batch of 256 rock-salt systems.
+
+One step = one request round for every system of the batch: neighbour
+list build (cell list, r_list = r_c + 0.4), one evaluation, then 10
+velocity-Verlet NVE steps at dt = 0.002, each with a full ESP evaluation
+(mesh + pair), the 10 steps replayed from a CUDA graph. A step therefore
+advances sum(N) particles by 10 MD steps (particle-steps = 10 sum N).
+
+Reported beside the batched number: the plain path (the same systems, one
+system per launch sequence), the end-to-end number through the C ABI with
+pinned host buffers copied in and results copied out every step, the
+roofline of the dominant kernel (CUDA events on the launching stream), and
+the CPU baseline (the FP64 oracle port on the host cores).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s at <=1e-5 rel RMS force err, batched vs plain; p50/p99 latency"
+UNIT = "particle-steps/s"
+N_SYS = 256
+SEED = 1004
+RCUT = 3.0
+SKIN = 0.4
+CAP = 256
+DT = 0.002
+MD_STEPS = 10
+# kernels per launch group (used to count launches in the timed region)
+K_EVAL = 13      # bin, scan, scatter, tile_sort, spread, 5 FFT passes, interp, pair, finalize
+K_NLIST = 6      # cell_bin, scan, scatter, cell_sort, fill_slot_cell, nlist
+K_NVE = 2
+
+
+def _env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def _systems(rank: int):
+    from esp_hoomd_b200 import systems
+    rng = np.random.default_rng(SEED + 7919 * rank)
+    evens = np.arange(8, 41, 2)
+    ns = rng.choice(evens, size=N_SYS)
+    return [systems.rocksalt(int(n), seed=SEED * 100000 + rank * N_SYS + i) for i, n in enumerate(ns)]
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _peak_gbs():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def _traffic_from_profiles(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
+    try:
+        with open(p) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 2 and parts[0] == kernel:
+                    return float(parts[1])
+    except OSError:
+        pass
+    return None
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+def _cpu_eval(args):
+    """One FP64 oracle evaluation + NVE update of one system (worker)."""
+    n, seed = args
+    sys.path.insert(0, ROOT)
+    from esp_hoomd_b200 import systems, tables
+    from oracle import esp_ref as R
+    s = systems.rocksalt(n, seed=seed)
+    mesh = tables.smooth235(int(math.ceil(s.box[0] / (math.pi * RCUT / 18.5))))
+    c = round(2 * 0.93 * math.pi * RCUT / (s.box[0] / mesh)) * 0.5
+    prm = tables.ESPParams(mesh=(mesh,) * 3, box=s.box, rcut=RCUT, split=tables.split_cached(c),
+                           window=tables.window_cached(8, 17.6, 10))
+    G = R.influence(prm)  # per-box table, built outside the timed part
+    t0 = time.perf_counter()
+    nl = R.neighbor_list(s.pos, s.box, RCUT + SKIN)
+    rho = R.spread(s.pos, s.q, prm)
+    phi, _ = R.mesh_potential(rho, G)
+    _, fm = R.interpolate(s.pos, s.q, phi, prm)
+    fp, _, _ = R.pair_forces(s.pos, s.q, s.box, prm.split, RCUT, *nl)
+    v = s.vel + DT * (fm + fp)
+    _ = s.pos + DT * v
+    return s.N, time.perf_counter() - t0
+
+
+def cpu_baseline(sample_ns, seeds, procs: int):
+    import multiprocessing as mp
+    work = list(zip(sample_ns, seeds))
+    t0 = time.perf_counter()
+    if procs > 1:
+        with mp.get_context("spawn").Pool(procs) as pool:
+            res = pool.map(_cpu_eval, work)
+    else:
+        res = [_cpu_eval(w) for w in work]
+    wall = time.perf_counter() - t0
+    n_tot = sum(r[0] for r in res)
+    return n_tot, wall, sum(r[1] for r in res)
+
+
+def run_reference(args):
+    rank, world, _ = _env_rank()
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    ns = [8, 16, 24, 32]
+    seeds = [SEED * 100000 + i for i in range(len(ns))]
+    for _ in range(args.warmup):
+        cpu_baseline(ns, seeds, min(cores, len(ns)))
+    times = []
+    n_tot = 0
+    for _ in range(args.steps):
+        n_tot, wall, _ = cpu_baseline(ns, seeds, min(cores, len(ns)))
+        times.append(wall)
+    t = sum(times) / len(times)
+    value = n_tot / t
+    sample = "oracle FP64 evaluation + NVE update of rock-salt n=%s (%d particles) per step, %d processes" % (
+        ns, n_tot, min(cores, len(ns)))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "batched256 rock-salt (CPU sample)", "rcut": RCUT, "order": 8},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": min(cores, len(ns)), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from esp_hoomd_b200 import native
+    from esp_hoomd_b200._lib import ESP_ALL
+
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", rank=rank, world_size=world,
+                                timeout=__import__("datetime").timedelta(seconds=600))
+    sl = _systems(rank)
+    N = np.array([s.N for s in sl])
+    tot = int(N.sum())
+    params = native.make_params(order=8, rcut=RCUT, target_error=1e-5)
+    b = native.Batch(params, N, [s.box for s in sl])
+    pos_h = np.zeros((tot, 4), np.float32)
+    pos_h[:, :3] = np.concatenate([s.pos for s in sl])
+    vel_h = np.zeros((tot, 4), np.float32)
+    vel_h[:, :3] = np.concatenate([s.vel for s in sl])
+    vel_h[:, 3] = 1.0
+    q_h = np.concatenate([s.q for s in sl]).astype(np.float32)
+    pos0 = torch.tensor(pos_h, device=dev)
+    vel0 = torch.tensor(vel_h, device=dev)
+    q = torch.tensor(q_h, device=dev)
+    pos = pos0.clone()
+    vel = vel0.clone()
+    head = torch.zeros(tot, dtype=torch.int32, device=dev)
+    nn = torch.zeros_like(head)
+    nl = torch.zeros(tot * CAP, dtype=torch.int32, device=dev)
+    force = torch.zeros((tot, 4), dtype=torch.float32, device=dev)
+    energy = torch.zeros(N.size, dtype=torch.float64, device=dev)
+    virial = torch.zeros(6 * N.size, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def request(bb, p, v, use_graph=True):
+        bb.build_nlist(p, RCUT + SKIN, CAP, head, nn, nl)
+        bb.compute(p, q, force, energy, virial, nlist=(head, nn, nl), flags=ESP_ALL)
+        bb.md_run(p, v, q, force, energy, virial, (head, nn, nl), MD_STEPS, DT, use_graph=use_graph)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(max(3, args.warmup)):
+        request(b, pos, vel)
+    barrier()
+    st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        st.record(stream)
+        for _ in range(args.steps):
+            request(b, pos, vel)
+        en.record(stream)
+        barrier()
+    ms = st.elapsed_time(en) / args.steps
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * tot * MD_STEPS / (ms_max * 1e-3)
+
+    # -- stage timing (live CUDA events on the launching stream, same workload, no graph)
+    b.set_timing(True)
+    for _ in range(2):
+        request(b, pos, vel, use_graph=False)
+    stt = b.stage_times()
+    b.set_timing(False)
+    stage_ms = {k: v[0] / max(v[1], 1) for k, v in stt.items() if v[1] > 0}
+    stage_total = {k: v[0] for k, v in stt.items() if v[1] > 0}
+    dom = max(stage_total, key=stage_total.get)
+    mean_nn = float(nn.double().mean().item())
+    M = sum(b.info(i)["nx"] * b.info(i)["ny"] * b.info(i)["nz"] for i in range(N.size))
+    # algorithmic bytes per launch of each stage (FP32 storage)
+    alg = {"pair": 4.0 * tot * mean_nn + 16.0 * tot + 16.0 * tot,
+           "spread": 20.0 * tot + 4.0 * M,
+           "interp": 20.0 * tot + 4.0 * M + 16.0 * tot,
+           "fft": 5 * 2 * 8.0 * M / 2,
+           "sort": 40.0 * tot,
+           "bin": 40.0 * tot,
+           "nlist": 16.0 * tot + 4.0 * tot * mean_nn,
+           "nve": 48.0 * tot}
+    kname = {"pair": "k_pair", "spread": "k_spread", "interp": "k_interp", "fft": "k_fft", "nlist": "k_nlist",
+             "sort": "k_tile_sort", "bin": "k_bin", "nve": "k_nve"}
+    peak, peak_kind = _peak_gbs()
+    ach = alg[dom] / (stage_ms[dom] * 1e-3) / 1e9
+    roof = {"kernel": kname.get(dom, dom), "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+            "frac": ach / peak, "peak_kind": peak_kind, "traffic": _traffic_from_profiles(kname.get(dom, dom)),
+            "stage_ms_per_launch": stage_ms,
+            "algorithmic_bytes_per_launch": alg[dom]}
+
+    # -- plain path: one system per launch sequence (separate contexts, no graph)
+    plain_value = None
+    if rank == 0 and not args.no_plain:
+        ctxs = [native.Batch(params, [int(n)], [s.box]) for n, s in zip(N, sl)]
+        offs = np.concatenate([[0], np.cumsum(N)])
+        pos_p = pos0.clone()
+        vel_p = vel0.clone()
+        views = [(pos_p[offs[i]:offs[i + 1]], vel_p[offs[i]:offs[i + 1]], q[offs[i]:offs[i + 1]],
+                  head[offs[i]:offs[i + 1]], nn[offs[i]:offs[i + 1]], nl[offs[i] * CAP:offs[i + 1] * CAP],
+                  force[offs[i]:offs[i + 1]], energy[i:i + 1], virial[6 * i:6 * i + 6]) for i in range(N.size)]
+
+        def plain_round():
+            for c, (p, v, qq, h, n_, l_, f, e, w) in zip(ctxs, views):
+                c.build_nlist(p, RCUT + SKIN, CAP, h, n_, l_)
+                c.compute(p, qq, f, e, w, nlist=(h, n_, l_), flags=ESP_ALL)
+                c.md_run(p, v, qq, f, e, w, (h, n_, l_), MD_STEPS, DT, use_graph=False)
+
+        plain_round()
+        torch.cuda.synchronize(dev)
+        st.record(stream)
+        for _ in range(args.plain_steps):
+            plain_round()
+        en.record(stream)
+        torch.cuda.synchronize(dev)
+        plain_ms = st.elapsed_time(en) / args.plain_steps
+        plain_value = tot * MD_STEPS / (plain_ms * 1e-3)
+        del ctxs
+
+    # -- end to end through the public API with host buffers
+    pin_pos = torch.from_numpy(pos_h).pin_memory()
+    pin_vel = torch.from_numpy(vel_h).pin_memory()
+    pin_q = torch.from_numpy(q_h).pin_memory()
+    out_pos = torch.empty_like(pin_pos).pin_memory()
+    out_vel = torch.empty_like(pin_vel).pin_memory()
+    out_e = torch.empty(N.size, dtype=torch.float64).pin_memory()
+    h2d = pin_pos.numel() * 4 + pin_vel.numel() * 4 + pin_q.numel() * 4
+    d2h = out_pos.numel() * 4 + out_vel.numel() * 4 + out_e.numel() * 8
+
+    def e2e_step():
+        pos.copy_(pin_pos, non_blocking=True)
+        vel.copy_(pin_vel, non_blocking=True)
+        q.copy_(pin_q, non_blocking=True)
+        request(b, pos, vel)
+        out_pos.copy_(pos, non_blocking=True)
+        out_vel.copy_(vel, non_blocking=True)
+        out_e.copy_(energy, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    barrier()
+    st.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    en.record(stream)
+    barrier()
+    e2e_ms = st.elapsed_time(en) / args.steps
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * tot * MD_STEPS / (float(t.item()) * 1e-3)
+
+    if rank == 0:
+        cores = os.cpu_count() or 1
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": max(3, args.warmup), "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "batched256: 256 rock-salt systems n^3, n even ~U{8..40} (seed 1004), "
+                                       "1 nlist + 1 eval + 10 NVE steps per system per step",
+                           "systems_per_gpu": int(N.size), "particles_per_gpu": tot, "order": 8, "rcut": RCUT,
+                           "mesh_rule": "smallest 2/3/5-smooth >= L/h, h = pi r_c / 18.5 (1e-5 target)",
+                           "mesh_points_per_gpu": int(M), "mean_neighbours": mean_nn, "dt": DT,
+                           "l2": "inputs larger than L2 (neighbour lists %.1f GB)" % (tot * mean_nn * 4 / 1e9),
+                           "parallelism": "replicas over systems (dp%d)" % world},
+                "plain": {"value": plain_value, "unit": UNIT,
+                          "desc": "same systems, one system per launch sequence, no graph"},
+                "batched_over_plain": (value / world / plain_value) if plain_value else None,
+                "roofline": roof,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                        "d2h_bytes_per_step": int(d2h)},
+                "gpu_launches": int(args.steps * (K_NLIST + K_EVAL + MD_STEPS * (K_EVAL + K_NVE))),
+                "clocks": clk.summary()}
+        if not args.no_cpu:
+            ns = [int(N[i]) for i in np.argsort(N)[::64]]
+            ns = [round(x ** (1 / 3)) for x in ns]
+            n_tot, wall, _ = cpu_baseline(ns, [SEED * 100000 + i for i in range(len(ns))], 1)
+            line["cpu_baseline"] = {"value": n_tot / wall, "unit": UNIT, "cores": 1, "kind": "port",
+                                    "sample": "FP64 oracle evaluation + NVE update of rock-salt n=%s (%d particles)"
+                                              % (ns, n_tot)}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--plain-steps", type=int, default=1)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1008 @@
+// Host orchestration and C ABI (include/esp_b200.h).
+//
+// A batch plans N independent systems: it resolves each system's mesh and
+// PSWF parameters, builds the tables (host FP64 for the 1D pieces, GPU FP64
+// for the influence function), lays out all particle / mesh / spectrum
+// arrays back to back, and precomputes the work-item lists every stage
+// launches over. A single-system context (esp_ctx) is a batch of one: the
+// reference's ESPForceComputeGPU (src/ESPForceComputeGPU.cc:47-448) maps to
+// esp_create + esp_compute.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "esp_b200.h"
+#include "esp_kernels.h"
+#include "esp_md.h"
+#include "esp_tables.h"
+
+using namespace espb;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define ESPB_CK(x)                                                                                  \
+    do {                                                                                            \
+        cudaError_t e_ = (x);                                                                       \
+        if (e_ != cudaSuccess) return fail(ESP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Required k-space resolution kappa_N = pi r_c / h for a relative RMS force
+// target (measured against FP64 Ewald on rock-salt lattices, P = 8..12).
+double kappa_required(double target) {
+    const double lt[] = {-3, -4, -5, -6, -7, -8};
+    const double kv[] = {11.5, 14.0, 18.5, 22.0, 26.0, 30.0};
+    double l = std::log10(std::max(1e-9, std::min(1e-2, target)));
+    if (l >= lt[0]) return kv[0];
+    for (int i = 0; i < 5; ++i)
+        if (l >= lt[i + 1]) {
+            double f = (l - lt[i]) / (lt[i + 1] - lt[i]);
+            return kv[i] + f * (kv[i + 1] - kv[i]);
+        }
+    return kv[5];
+}
+
+uint32_t radix_plan(int n) {
+    std::vector<int> r;
+    int m = n;
+    int twos = 0;
+    while (m % 2 == 0) {
+        m /= 2;
+        ++twos;
+    }
+    while (twos >= 2) {
+        r.push_back(4);
+        twos -= 2;
+    }
+    if (twos) r.push_back(2);
+    while (m % 3 == 0) {
+        r.push_back(3);
+        m /= 3;
+    }
+    while (m % 5 == 0) {
+        r.push_back(5);
+        m /= 5;
+    }
+    if (m != 1 || r.size() > 8) return 0;
+    uint32_t code = 0;
+    for (size_t i = 0; i < r.size(); ++i) code |= (uint32_t)r[i] << (4 * i);
+    return code;
+}
+
+// (PX, PP) pitches of the interpolation tile with few bank conflicts for the
+// lane pattern b = lane % P, cg = lane / P.
+void choose_pitch(int P, int E, int& PX, int& PP) {
+    int best = 1 << 30;
+    PX = E;
+    PP = E * E;
+    const int ncg = 32 / P;
+    for (int px = E; px <= E + 8; ++px)
+        for (int pp = px * E; pp <= px * E + 32; ++pp) {
+            int cnt[32] = {0};
+            int worst = 0;
+            for (int l = 0; l < ncg * P; ++l) {
+                int bank = ((l / P) * pp + (l % P) * px) & 31;
+                worst = std::max(worst, ++cnt[bank]);
+            }
+            const int score = worst * 100000 + pp * E;
+            if (score < best) {
+                best = score;
+                PX = px;
+                PP = pp;
+            }
+        }
+}
+
+struct DevAlloc {
+    std::vector<void*> ptrs;
+    long long bytes = 0;
+    template <class T>
+    int get(T*& p, size_t n) {
+        p = nullptr;
+        if (n == 0) n = 1;
+        cudaError_t e = cudaMalloc((void**)&p, n * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(ESP_ERR_ALLOC, std::string("cudaMalloc of ") + std::to_string(n * sizeof(T)) +
+                                           " bytes failed: " + cudaGetErrorString(e));
+        }
+        ptrs.push_back(p);
+        bytes += (long long)(n * sizeof(T));
+        return 0;
+    }
+    void release() {
+        for (void* p : ptrs) cudaFree(p);
+        ptrs.clear();
+        bytes = 0;
+    }
+    ~DevAlloc() { release(); }
+};
+
+struct PsetHost {
+    Split split;
+    Window win;
+    double rcut = 0;
+};
+
+// Per-stage CUDA-event timing on the launching stream. Records are queued
+// without synchronising; read() synchronises once and sums the elapsed
+// times (used by benchmarks to time kernels inside their timed region).
+struct StageTimer {
+    bool on = false;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> stage;
+    int used = 0;
+    double ms[ESP_N_STAGES] = {0};
+    long long count[ESP_N_STAGES] = {0};
+    int cur = -1;
+    ~StageTimer() {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+    void collect() {
+        if (used == 0) return;
+        cudaEventSynchronize(ev[2 * used - 1]);
+        for (int i = 0; i < used; ++i) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]) == cudaSuccess) {
+                ms[stage[i]] += t;
+                count[stage[i]] += 1;
+            }
+        }
+        used = 0;
+    }
+    void begin(int id, cudaStream_t st) {
+        if (!on) return;
+        if (used * 2 + 2 > (int)ev.size()) {
+            if (ev.size() >= 8192) {
+                collect();
+            } else {
+                for (int k = 0; k < 256; ++k) {
+                    cudaEvent_t e;
+                    cudaEventCreate(&e);
+                    ev.push_back(e);
+                }
+                stage.resize(ev.size() / 2);
+            }
+        }
+        cur = id;
+        cudaEventRecord(ev[2 * used], st);
+    }
+    void end(cudaStream_t st) {
+        if (!on || cur < 0) return;
+        cudaEventRecord(ev[2 * used + 1], st);
+        stage[used] = cur;
+        ++used;
+        cur = -1;
+    }
+    void reset() {
+        for (int k = 0; k < ESP_N_STAGES; ++k) {
+            ms[k] = 0;
+            count[k] = 0;
+        }
+    }
+};
+
+}  // namespace
+
+struct esp_batch {
+    esp_params prm{};
+    int P = 8, T = 8, D = 10, tpp = 8, PX = 0, PP = 0;
+    int nsys = 0, totN = 0, n_tiles = 0;
+    std::vector<int> N;
+    std::vector<double> box;
+    std::vector<int> mesh;
+    std::vector<SysDev> sd;
+    std::vector<PsetHost> psh;
+    std::vector<ParamSet> psd;
+    std::vector<double> c_split, c_win;
+    int n_chunks = 0, n_pchunks = 0, n_x = 0, n_y = 0, n_z = 0;
+    DevAlloc mem;
+    // device
+    SysDev* d_sys = nullptr;
+    ParamSet* d_pset = nullptr;
+    int2 *d_chunks = nullptr, *d_pchunks = nullptr;
+    int* d_tile_sys = nullptr;
+    uint32_t *d_tcount = nullptr, *d_tstart = nullptr;
+    float4 *d_posq = nullptr, *d_trec = nullptr, *d_srec = nullptr;
+    uint32_t *d_rel = nullptr, *d_key = nullptr, *d_perm_u = nullptr, *d_perm = nullptr, *d_srel = nullptr;
+    double* d_rho = nullptr;
+    float2 *d_spec = nullptr, *d_gtab = nullptr, *d_tw = nullptr;
+    float* d_phi = nullptr;
+    int4 *d_x = nullptr, *d_y = nullptr, *d_z = nullptr;
+    double *d_acc = nullptr, *d_energy = nullptr, *d_virial = nullptr;
+    // neighbour-list harness (allocated on first use)
+    DevAlloc nlmem;
+    double nl_rlist = -1;
+    int n_cells = 0;
+    CellDev* d_cells = nullptr;
+    int* d_cell_sys = nullptr;
+    uint32_t *d_ckey = nullptr, *d_ccount = nullptr, *d_cstart = nullptr, *d_cperm = nullptr, *d_slot_cell = nullptr;
+    float4 *d_wpos = nullptr, *d_cpos = nullptr;
+    int* d_overflow = nullptr;
+
+    StageTimer timer;
+    struct GraphKey {
+        const void *pos, *vel, *q, *head, *nn, *nl, *force, *energy, *virial;
+        double dt;
+        bool operator==(const GraphKey& o) const {
+            return pos == o.pos && vel == o.vel && q == o.q && head == o.head && nn == o.nn && nl == o.nl &&
+                   force == o.force && energy == o.energy && virial == o.virial && dt == o.dt;
+        }
+    } graph_key{};
+    cudaGraphExec_t graph_exec = nullptr;
+    ~esp_batch() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    }
+
+    LaunchArgs args() const;
+    int plan(const esp_params& p, int ns, const int* N_, const double* boxes, const int* mesh_);
+    int md_run(cudaStream_t st, float* pos4, float* vel4, const float* q, const unsigned* head, const unsigned* nn,
+               const unsigned* nl, float* force4, double* energy, double* virial, int nsteps, double dt,
+               int use_graph);
+    int compute(cudaStream_t st, const float* pos4, const float* q, const unsigned* head, const unsigned* nn,
+                const unsigned* nl, float* force4, double* energy, double* virial, int flags);
+    int spread_only(cudaStream_t st, const float* pos4, const float* q, double* rho_out);
+    int build_nlist(cudaStream_t st, const float* pos4, double rlist, int cap, unsigned* head, unsigned* nn,
+                    unsigned* nl);
+    int info(int s, esp_info* out) const;
+};
+
+int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* boxes, const int* mesh_) {
+    mem.release();
+    nlmem.release();
+    nl_rlist = -1;
+    prm = p;
+    if (ns <= 0) return fail(ESP_ERR_INVALID, "number of systems must be positive");
+    if (p.order < 2 || p.order > MAX_P) return fail(ESP_ERR_UNSUPPORTED, "order must be in [2, 12]");
+    if (!(p.rcut > 0)) return fail(ESP_ERR_INVALID, "rcut must be positive");
+    if (p.alpha != 0.0) return fail(ESP_ERR_UNSUPPORTED, "Debye screening (alpha != 0) is not supported");
+    if (p.kappa < 0 || p.window_c < 0) return fail(ESP_ERR_INVALID, "kappa and window_c must be >= 0");
+    P = p.order;
+    nsys = ns;
+    N.assign(N_, N_ + ns);
+    box.assign(boxes, boxes + 3 * ns);
+    mesh.assign(3 * ns, 0);
+    tpp = p.threads_per_particle ? p.threads_per_particle : 8;
+    if (tpp != 4 && tpp != 8 && tpp != 16 && tpp != 32)
+        return fail(ESP_ERR_UNSUPPORTED, "threads_per_particle must be 4, 8, 16 or 32");
+    const double target = p.target_error > 0 ? p.target_error : 1e-5;
+    const double kreq = kappa_required(target);
+    T = p.tile > 0 ? p.tile : P;
+    if (T > 64) return fail(ESP_ERR_UNSUPPORTED, "tile edge must be <= 64");
+    totN = 0;
+    for (int s = 0; s < ns; ++s) {
+        if (N[s] < 0) return fail(ESP_ERR_INVALID, "negative particle count");
+        for (int d = 0; d < 3; ++d) {
+            const double L = box[3 * s + d];
+            if (!(L > 0)) return fail(ESP_ERR_INVALID, "box lengths must be positive");
+            if (2.0 * p.rcut > L) return fail(ESP_ERR_INVALID, "rcut must not exceed half the box");
+            int n = mesh_ ? mesh_[3 * s + d] : 0;
+            if (n <= 0 && d == 0 && p.nx > 0) n = p.nx;
+            if (n <= 0 && d == 1 && p.ny > 0) n = p.ny;
+            if (n <= 0 && d == 2 && p.nz > 0) n = p.nz;
+            if (n <= 0) {
+                const double h = M_PI * p.rcut / kreq;
+                n = smooth235(std::max(P, (int)std::ceil(L / h)));
+            }
+            if (n < P || n < 4 || n > FFT_MAX_N || radix_plan(n) == 0)
+                return fail(ESP_ERR_UNSUPPORTED, "mesh size " + std::to_string(n) +
+                                                     " must be 2/3/5-smooth, >= order and <= 256");
+            if (T > n) T = n;
+            mesh[3 * s + d] = n;
+        }
+        totN += N[s];
+    }
+    D = p.window_degree > 0 ? p.window_degree : std::max(P + 2, 9);
+    if (D > MAX_D) return fail(ESP_ERR_UNSUPPORTED, "window degree must be <= 15");
+    // parameter sets
+    std::map<std::tuple<double, double>, int> pmap;
+    psh.clear();
+    psd.clear();
+    c_split.assign(ns, 0);
+    c_win.assign(ns, 0);
+    std::vector<int> sys_pset(ns);
+    // One split per batch: the coarsest mesh sets c, so every system shares
+    // the pair-term polynomial (kernel-parameter resident) and the finer
+    // meshes are only more accurate.
+    double hmax_all = 0;
+    for (int s = 0; s < ns; ++s)
+        for (int d = 0; d < 3; ++d) hmax_all = std::max(hmax_all, box[3 * s + d] / mesh[3 * s + d]);
+    for (int s = 0; s < ns; ++s) {
+        double c;
+        if (p.kappa > 0) {
+            c = p.kappa * p.rcut;
+        } else {
+            // 0.93 kappa_N (kappa_N = pi r_c / h), rounded to 0.5: the
+            // measured optimum against FP64 Ewald at P = 8, h = r_c / 6
+            c = std::round(2.0 * 0.93 * M_PI * p.rcut / hmax_all) * 0.5;
+        }
+        c = std::max(2.0, std::min(60.0, c));
+        const double cw = p.window_c > 0 ? p.window_c : 2.2 * P;
+        c_split[s] = c;
+        c_win[s] = cw;
+        auto key = std::make_tuple(c, cw);
+        auto it = pmap.find(key);
+        if (it == pmap.end()) {
+            PsetHost h;
+            try {
+                h.split.build(c);
+                h.win.build(P, cw, D);
+            } catch (const std::exception& ex) {
+                return fail(ESP_ERR_INVALID, ex.what());
+            }
+            h.rcut = p.rcut;
+            if (h.split.qv.size() > (size_t)MAX_QC)
+                return fail(ESP_ERR_UNSUPPORTED, "split polynomial needs more than 32 coefficients");
+            ParamSet d{};
+            for (int a = 0; a < P; ++a)
+                for (int j = 0; j <= D; ++j) d.wcoef[a * (MAX_D + 1) + j] = (float)h.win.coef[(size_t)a * (D + 1) + j];
+            d.nq = (int)h.split.qv.size();
+            for (int j = 0; j < d.nq; ++j) d.qv[j] = (float)h.split.qv[j];
+            for (int j = 1; j < d.nq; ++j) d.dqv[j - 1] = (float)(2.0 * j * h.split.qv[j]);
+            d.rcut = (float)p.rcut;
+            d.rcut2 = (float)(p.rcut * p.rcut);
+            d.inv_rcut = (float)(1.0 / p.rcut);
+            d.two_inv_rcut3 = (float)(2.0 / (p.rcut * p.rcut * p.rcut));
+            d.self_coef = -0.5 * h.split.lambda0 * INV_4PI_D / p.rcut;
+            d.bg_coef = -0.25 * p.rcut * p.rcut * h.split.m2;
+            it = pmap.emplace(key, (int)psh.size()).first;
+            psh.push_back(std::move(h));
+            psd.push_back(d);
+        }
+        sys_pset[s] = it->second;
+    }
+    // twiddles
+    std::map<int, int> twoff;
+    std::vector<float2> tw;
+    auto twid = [&](int n) {
+        auto it = twoff.find(n);
+        if (it != twoff.end()) return it->second;
+        const int off = (int)tw.size();
+        for (int t = 0; t < n; ++t) {
+            const double a = -2.0 * M_PI * t / n;
+            tw.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+        }
+        twoff[n] = off;
+        return off;
+    };
+    // system descriptors, influence-table sharing
+    sd.assign(ns, SysDev{});
+    std::map<std::tuple<int, double, double, double, int, int, int>, long long> gmap;
+    long long m_off = 0, s_off = 0, g_off = 0;
+    int p_off = 0, t_off = 0;
+    std::vector<int> g_first;  // system that owns each distinct table
+    for (int s = 0; s < ns; ++s) {
+        SysDev& S = sd[s];
+        S.N = N[s];
+        S.p_off = p_off;
+        S.nx = mesh[3 * s];
+        S.ny = mesh[3 * s + 1];
+        S.nz = mesh[3 * s + 2];
+        S.nxh = S.nx / 2 + 1;
+        S.m_off = m_off;
+        S.s_off = s_off;
+        S.ntx = (S.nx + T - 1) / T;
+        S.nty = (S.ny + T - 1) / T;
+        S.ntz = (S.nz + T - 1) / T;
+        S.t_off = t_off;
+        S.Lx = (float)box[3 * s];
+        S.Ly = (float)box[3 * s + 1];
+        S.Lz = (float)box[3 * s + 2];
+        S.inv_Lx = 1.0f / S.Lx;
+        S.inv_Ly = 1.0f / S.Ly;
+        S.inv_Lz = 1.0f / S.Lz;
+        S.gxd = S.nx / box[3 * s];
+        S.gyd = S.ny / box[3 * s + 1];
+        S.gzd = S.nz / box[3 * s + 2];
+        S.V = box[3 * s] * box[3 * s + 1] * box[3 * s + 2];
+        S.pset = sys_pset[s];
+        S.twx = twid(S.nx);
+        S.twy = twid(S.ny);
+        S.twz = twid(S.nz);
+        S.radx = radix_plan(S.nx);
+        S.rady = radix_plan(S.ny);
+        S.radz = radix_plan(S.nz);
+        auto gk = std::make_tuple(S.pset, box[3 * s], box[3 * s + 1], box[3 * s + 2], S.nx, S.ny, S.nz);
+        auto it = gmap.find(gk);
+        if (it == gmap.end()) {
+            it = gmap.emplace(gk, g_off).first;
+            g_first.push_back(s);
+            g_off += (long long)S.nz * S.ny * S.nxh;
+        }
+        S.g_off = it->second;
+        p_off += N[s];
+        m_off += (long long)S.nx * S.ny * S.nz;
+        s_off += (long long)S.nz * S.ny * S.nxh;
+        t_off += S.ntx * S.nty * S.ntz;
+    }
+    n_tiles = t_off;
+    // work lists
+    std::vector<int2> chunks, pchunks;
+    const int ppb = 256 / tpp;
+    std::vector<int> tile_sys(n_tiles);
+    std::vector<int4> xi, yi, zi;
+    for (int s = 0; s < ns; ++s) {
+        const SysDev& S = sd[s];
+        for (int i = 0; i < S.N; i += 256) chunks.push_back(make_int2(s, S.p_off + i));
+        for (int i = 0; i < S.N; i += ppb) pchunks.push_back(make_int2(s, S.p_off + i));
+        for (int t = 0; t < S.ntx * S.nty * S.ntz; ++t) tile_sys[S.t_off + t] = s;
+        for (int z = 0; z < S.nz; ++z)
+            for (int y0 = 0; y0 < S.ny; y0 += 2 * FFT_B_X) xi.push_back(make_int4(s, z, y0, 0));
+        for (int z = 0; z < S.nz; ++z)
+            for (int k0 = 0; k0 < S.nxh; k0 += FFT_B_YZ) yi.push_back(make_int4(s, z, k0, 0));
+        for (int y = 0; y < S.ny; ++y)
+            for (int k0 = 0; k0 < S.nxh; k0 += FFT_B_YZ) zi.push_back(make_int4(s, y, k0, 0));
+    }
+    n_chunks = (int)chunks.size();
+    n_pchunks = (int)pchunks.size();
+    n_x = (int)xi.size();
+    n_y = (int)yi.size();
+    n_z = (int)zi.size();
+    choose_pitch(P, T + P - 1, PX, PP);
+    // allocate
+    int rc = 0;
+    if ((rc = mem.get(d_sys, ns)) || (rc = mem.get(d_pset, psd.size())) || (rc = mem.get(d_chunks, chunks.size())) ||
+        (rc = mem.get(d_pchunks, pchunks.size())) || (rc = mem.get(d_tile_sys, n_tiles)) ||
+        (rc = mem.get(d_tcount, n_tiles)) || (rc = mem.get(d_tstart, n_tiles + 1)) || (rc = mem.get(d_posq, totN)) ||
+        (rc = mem.get(d_trec, totN)) || (rc = mem.get(d_srec, totN)) || (rc = mem.get(d_rel, totN)) ||
+        (rc = mem.get(d_key, totN)) || (rc = mem.get(d_perm_u, totN)) || (rc = mem.get(d_perm, totN)) ||
+        (rc = mem.get(d_srel, totN)) || (rc = mem.get(d_rho, m_off)) || (rc = mem.get(d_phi, m_off)) ||
+        (rc = mem.get(d_spec, s_off)) || (rc = mem.get(d_gtab, g_off)) || (rc = mem.get(d_tw, tw.size())) ||
+        (rc = mem.get(d_x, xi.size())) || (rc = mem.get(d_y, yi.size())) || (rc = mem.get(d_z, zi.size())) ||
+        (rc = mem.get(d_acc, (size_t)ns * ACC_STRIDE)) || (rc = mem.get(d_energy, ns)) ||
+        (rc = mem.get(d_virial, (size_t)ns * 6)))
+        return rc;
+    ESPB_CK(cudaMemcpy(d_sys, sd.data(), ns * sizeof(SysDev), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(d_pset, psd.data(), psd.size() * sizeof(ParamSet), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(d_chunks, chunks.data(), chunks.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(d_pchunks, pchunks.data(), pchunks.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(d_tile_sys, tile_sys.data(), n_tiles * sizeof(int), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(d_x, xi.data(), xi.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(d_y, yi.data(), yi.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(d_z, zi.data(), zi.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemset(d_tcount, 0, n_tiles * sizeof(uint32_t)));
+    ESPB_CK(cudaMemset(d_rho, 0, (size_t)std::max<long long>(m_off, 1) * sizeof(double)));
+    if (graph_exec) {
+        cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+    }
+    {
+        // kernel attributes are set here, outside any stream capture
+        LaunchArgs a = args();
+        a.configure_only = 1;
+        ESPB_CK(launch_spread(a, 0));
+        ESPB_CK(launch_interp(a, 0));
+        ESPB_CK(launch_fft(a, 0));
+    }
+    // influence tables (FP64 on the GPU)
+    for (int s : g_first) {
+        const SysDev& S = sd[s];
+        const PsetHost& h = psh[S.pset];
+        std::vector<double> w1d(S.nx + S.ny + S.nz);
+        const int nn[3] = {S.nx, S.ny, S.nz};
+        int o = 0;
+        for (int d = 0; d < 3; ++d)
+            for (int i = 0; i < nn[d]; ++i) {
+                const int f = (i < (nn[d] + 1) / 2) ? i : nn[d] - i;
+                w1d[o++] = h.win.fourier(2.0 * M_PI * f / nn[d]);
+            }
+        double kmax2 = 0;
+        for (int d = 0; d < 3; ++d) {
+            const double k = M_PI * nn[d] / box[3 * s + d];
+            kmax2 += k * k;
+        }
+        const double kap_max = std::sqrt(kmax2) * p.rcut;
+        const int nq = std::max(48, std::min(320, (int)(0.6 * kap_max) + 40));
+        std::vector<double> tq, wq;
+        gauss_legendre01(nq, tq, wq);
+        for (int j = 0; j < nq; ++j) wq[j] *= h.split.pro.psi(tq[j]) / h.split.pro.int01;
+        double *d_w1d = nullptr, *d_tq = nullptr, *d_wq = nullptr;
+        ESPB_CK(cudaMalloc(&d_w1d, w1d.size() * sizeof(double)));
+        ESPB_CK(cudaMalloc(&d_tq, nq * sizeof(double)));
+        ESPB_CK(cudaMalloc(&d_wq, nq * sizeof(double)));
+        ESPB_CK(cudaMemcpy(d_w1d, w1d.data(), w1d.size() * sizeof(double), cudaMemcpyHostToDevice));
+        ESPB_CK(cudaMemcpy(d_tq, tq.data(), nq * sizeof(double), cudaMemcpyHostToDevice));
+        ESPB_CK(cudaMemcpy(d_wq, wq.data(), nq * sizeof(double), cudaMemcpyHostToDevice));
+        cudaError_t e = launch_influence(S, d_w1d, d_tq, d_wq, nq, p.rcut, 1e-14, d_gtab, 0);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        cudaFree(d_w1d);
+        cudaFree(d_tq);
+        cudaFree(d_wq);
+        if (e != cudaSuccess) return fail(ESP_ERR_CUDA, std::string("influence build: ") + cudaGetErrorString(e));
+    }
+    return 0;
+}
+
+LaunchArgs esp_batch::args() const {
+    LaunchArgs a;
+    a.sys = d_sys;
+    a.psets = d_pset;
+    a.nsys = nsys;
+    a.P = P;
+    a.T = T;
+    a.D = D;
+    a.PX = PX;
+    a.PP = PP;
+    a.tpp = tpp;
+    // one split per batch (plan() guarantees a single parameter set)
+    a.nq = psd[0].nq;
+    for (int c = 0; c < MAX_QC; ++c) {
+        a.pc.q[c] = c < psd[0].nq ? psd[0].qv[c] : 0.f;
+        a.pc.d[c] = c < psd[0].nq - 1 ? psd[0].dqv[c] : 0.f;
+    }
+    a.chunks = d_chunks;
+    a.n_chunks = n_chunks;
+    a.pchunks = d_pchunks;
+    a.n_pchunks = n_pchunks;
+    a.tile_sys = d_tile_sys;
+    a.n_tiles = n_tiles;
+    a.tile_count = d_tcount;
+    a.tile_start = d_tstart;
+    a.posq = d_posq;
+    a.trec = d_trec;
+    a.rel = d_rel;
+    a.key = d_key;
+    a.perm_u = d_perm_u;
+    a.perm = d_perm;
+    a.srec = d_srec;
+    a.srel = d_srel;
+    a.rho = d_rho;
+    a.spec = d_spec;
+    a.phi = d_phi;
+    a.gtab = d_gtab;
+    a.tw = d_tw;
+    a.xitems = d_x;
+    a.n_xitems = n_x;
+    a.yitems = d_y;
+    a.n_yitems = n_y;
+    a.zitems = d_z;
+    a.n_zitems = n_z;
+    a.acc = d_acc;
+    a.energy = d_energy;
+    a.virial = d_virial;
+    return a;
+}
+
+int esp_batch::compute(cudaStream_t st, const float* pos4, const float* q, const unsigned* head, const unsigned* nn,
+                       const unsigned* nl, float* force4, double* energy, double* virial, int flags) {
+    if (!pos4 || !q || !force4) return fail(ESP_ERR_INVALID, "null position, charge or force pointer");
+    if (!(flags & ESP_ALL)) return fail(ESP_ERR_INVALID, "flags select no term");
+    if ((flags & ESP_SHORT_RANGE) && (!head || !nn || !nl))
+        return fail(ESP_ERR_INVALID, "short-range term needs the neighbour list");
+    LaunchArgs a = args();
+    a.pos_in = reinterpret_cast<const float4*>(pos4);
+    a.q_in = q;
+    a.force = reinterpret_cast<float4*>(force4);
+    if (energy) a.energy = energy;
+    if (virial) a.virial = virial;
+    a.nl_head = head;
+    a.nl_n = nn;
+    a.nl_list = nl;
+    const bool lr = flags & ESP_LONG_RANGE, sr = flags & ESP_SHORT_RANGE;
+    a.accumulate = lr ? 1 : 0;
+    a.add_bg = lr ? 1 : 0;
+    ESPB_CK(cudaMemsetAsync(d_acc, 0, (size_t)nsys * ACC_STRIDE * sizeof(double), st));
+    timer.begin(ESP_STAGE_BIN, st);
+    ESPB_CK(launch_bin(a, st));
+    timer.end(st);
+    if (lr) {
+        timer.begin(ESP_STAGE_SORT, st);
+        ESPB_CK(launch_sort(a, st));
+        timer.end(st);
+        timer.begin(ESP_STAGE_SPREAD, st);
+        ESPB_CK(launch_spread(a, st));
+        timer.end(st);
+        timer.begin(ESP_STAGE_FFT, st);
+        ESPB_CK(launch_fft(a, st));
+        timer.end(st);
+        timer.begin(ESP_STAGE_INTERP, st);
+        ESPB_CK(launch_interp(a, st));
+        timer.end(st);
+    } else {
+        // bin counted particles per tile; clear the histogram for the next call
+        ESPB_CK(cudaMemsetAsync(d_tcount, 0, (size_t)n_tiles * sizeof(uint32_t), st));
+    }
+    if (sr) {
+        timer.begin(ESP_STAGE_PAIR, st);
+        ESPB_CK(launch_pair(a, st));
+        timer.end(st);
+    }
+    ESPB_CK(launch_finalize(a, st));
+    return 0;
+}
+
+int esp_batch::md_run(cudaStream_t st, float* pos4, float* vel4, const float* q, const unsigned* head,
+                      const unsigned* nn, const unsigned* nl, float* force4, double* energy, double* virial, int nsteps,
+                      double dt, int use_graph) {
+    if (nsteps < 0) return fail(ESP_ERR_INVALID, "negative step count");
+    if (!pos4 || !vel4 || !q || !force4 || !head || !nn || !nl) return fail(ESP_ERR_INVALID, "null pointer");
+    auto step = [&]() -> int {
+        timer.begin(ESP_STAGE_NVE, st);
+        ESPB_CK(launch_nve1(d_chunks, n_chunks, d_sys, reinterpret_cast<float4*>(pos4),
+                            reinterpret_cast<float4*>(vel4), reinterpret_cast<const float4*>(force4), (float)dt, st));
+        timer.end(st);
+        int rc = compute(st, pos4, q, head, nn, nl, force4, energy, virial, ESP_ALL);
+        if (rc) return rc;
+        timer.begin(ESP_STAGE_NVE, st);
+        ESPB_CK(launch_nve2(d_chunks, n_chunks, d_sys, reinterpret_cast<float4*>(vel4),
+                            reinterpret_cast<const float4*>(force4), (float)dt, st));
+        timer.end(st);
+        return 0;
+    };
+    if (!use_graph || timer.on) {
+        for (int k = 0; k < nsteps; ++k) {
+            int rc = step();
+            if (rc) return rc;
+        }
+        return 0;
+    }
+    const GraphKey key{pos4, vel4, q, head, nn, nl, force4, energy, virial, dt};
+    if (!graph_exec || !(key == graph_key)) {
+        if (graph_exec) {
+            cudaGraphExecDestroy(graph_exec);
+            graph_exec = nullptr;
+        }
+        cudaStream_t cs = nullptr;
+        ESPB_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        int rc = 0;
+        if (e == cudaSuccess) {
+            cudaStream_t saved = st;
+            st = cs;
+            rc = step();
+            st = saved;
+            cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+            if (e == cudaSuccess) e = e2;
+        }
+        cudaStreamDestroy(cs);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&graph_exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(ESP_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        graph_key = key;
+    }
+    for (int k = 0; k < nsteps; ++k) ESPB_CK(cudaGraphLaunch(graph_exec, st));
+    return 0;
+}
+
+int esp_batch::spread_only(cudaStream_t st, const float* pos4, const float* q, double* rho_out) {
+    if (!pos4 || !q || !rho_out) return fail(ESP_ERR_INVALID, "null pointer");
+    long long M = 0;
+    for (const SysDev& S : sd) M += (long long)S.nx * S.ny * S.nz;
+    ESPB_CK(cudaMemsetAsync(rho_out, 0, (size_t)M * sizeof(double), st));
+    ESPB_CK(cudaMemsetAsync(d_acc, 0, (size_t)nsys * ACC_STRIDE * sizeof(double), st));
+    LaunchArgs a = args();
+    a.pos_in = reinterpret_cast<const float4*>(pos4);
+    a.q_in = q;
+    a.rho = rho_out;
+    ESPB_CK(launch_bin(a, st));
+    ESPB_CK(launch_sort(a, st));
+    ESPB_CK(launch_spread(a, st));
+    return 0;
+}
+
+int esp_batch::build_nlist(cudaStream_t st, const float* pos4, double rlist, int cap, unsigned* head, unsigned* nn,
+                           unsigned* nl) {
+    if (!(rlist > 0) || cap <= 0) return fail(ESP_ERR_INVALID, "rlist and cap must be positive");
+    if (!pos4 || !head || !nn || !nl) return fail(ESP_ERR_INVALID, "null pointer");
+    if (rlist != nl_rlist) {
+        nlmem.release();
+        std::vector<CellDev> cells(nsys);
+        std::vector<int> cell_sys;
+        int c_off = 0;
+        long long nl_off = 0;
+        for (int s = 0; s < nsys; ++s) {
+            CellDev& C = cells[s];
+            int nc[3];
+            for (int d = 0; d < 3; ++d) {
+                if (2.0 * rlist > box[3 * s + d]) return fail(ESP_ERR_INVALID, "rlist must not exceed half the box");
+                nc[d] = std::max(1, (int)std::floor(box[3 * s + d] / rlist));
+            }
+            C.ncx = nc[0];
+            C.ncy = nc[1];
+            C.ncz = nc[2];
+            C.inv_wx = (float)(nc[0] / box[3 * s]);
+            C.inv_wy = (float)(nc[1] / box[3 * s + 1]);
+            C.inv_wz = (float)(nc[2] / box[3 * s + 2]);
+            C.c_off = c_off;
+            C.nl_off = nl_off;
+            for (int c = 0; c < nc[0] * nc[1] * nc[2]; ++c) cell_sys.push_back(s);
+            c_off += nc[0] * nc[1] * nc[2];
+            nl_off += (long long)N[s] * cap;
+        }
+        n_cells = c_off;
+        int rc = 0;
+        if ((rc = nlmem.get(d_cells, nsys)) || (rc = nlmem.get(d_cell_sys, n_cells)) ||
+            (rc = nlmem.get(d_ckey, totN)) || (rc = nlmem.get(d_ccount, n_cells)) ||
+            (rc = nlmem.get(d_cstart, n_cells + 1)) || (rc = nlmem.get(d_cperm, totN)) ||
+            (rc = nlmem.get(d_slot_cell, totN)) || (rc = nlmem.get(d_wpos, totN)) || (rc = nlmem.get(d_cpos, totN)) ||
+            (rc = nlmem.get(d_overflow, 1)))
+            return rc;
+        ESPB_CK(cudaMemcpy(d_cells, cells.data(), nsys * sizeof(CellDev), cudaMemcpyHostToDevice));
+        ESPB_CK(cudaMemcpy(d_cell_sys, cell_sys.data(), n_cells * sizeof(int), cudaMemcpyHostToDevice));
+        ESPB_CK(cudaMemset(d_ccount, 0, n_cells * sizeof(uint32_t)));
+        nl_rlist = rlist;
+    }
+    NlistArgs a;
+    a.chunks = d_chunks;
+    a.n_chunks = n_chunks;
+    a.sys = d_sys;
+    a.cells = d_cells;
+    a.cell_sys = d_cell_sys;
+    a.n_cells = n_cells;
+    a.total = totN;
+    a.pos = reinterpret_cast<const float4*>(pos4);
+    a.ckey = d_ckey;
+    a.ccount = d_ccount;
+    a.cstart = d_cstart;
+    a.perm_u = d_cperm;
+    a.wpos = d_wpos;
+    a.cpos = d_cpos;
+    a.slot_cell = d_slot_cell;
+    a.rlist2 = (float)(rlist * rlist);
+    a.cap = cap;
+    a.head = head;
+    a.nn = nn;
+    a.nl = nl;
+    a.overflow = d_overflow;
+    timer.begin(ESP_STAGE_NLIST, st);
+    ESPB_CK(launch_nlist(a, st));
+    timer.end(st);
+    int ovf = 0;
+    ESPB_CK(cudaMemcpyAsync(&ovf, d_overflow, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ESPB_CK(cudaStreamSynchronize(st));
+    if (ovf) return fail(ESP_ERR_OVERFLOW, "neighbour-list row capacity exceeded; n_neigh holds the needed counts");
+    return 0;
+}
+
+int esp_batch::info(int s, esp_info* out) const {
+    if (!out || s < 0 || s >= nsys) return fail(ESP_ERR_INVALID, "bad system index or null info");
+    const SysDev& S = sd[s];
+    const PsetHost& h = psh[S.pset];
+    out->nx = S.nx;
+    out->ny = S.ny;
+    out->nz = S.nz;
+    out->order = P;
+    out->tile = T;
+    out->window_degree = D;
+    out->c_split = c_split[s];
+    out->c_window = c_win[s];
+    out->rcut = h.rcut;
+    out->lambda0 = h.split.lambda0;
+    out->m2 = h.split.m2;
+    out->split_fit_err = h.split.fit_err;
+    out->window_fit_err = h.win.fit_err;
+    out->device_bytes = mem.bytes + nlmem.bytes;
+    return 0;
+}
+
+struct esp_ctx {
+    esp_params prm{};
+    double L[3] = {0, 0, 0};
+    int N = -1;
+    bool dirty = true;
+    esp_batch b;
+};
+
+extern "C" {
+
+int esp_params_default(esp_params* p) {
+    if (!p) return fail(ESP_ERR_INVALID, "null params");
+    std::memset(p, 0, sizeof(*p));
+    p->order = 8;
+    p->rcut = 3.0;
+    p->n_table = 512;
+    p->target_error = 1e-5;
+    return 0;
+}
+
+const char* esp_last_error(void) { return g_err.c_str(); }
+
+int esp_create(const esp_params* p, double Lx, double Ly, double Lz, int N, esp_ctx** out) {
+    if (!p || !out) return fail(ESP_ERR_INVALID, "null argument");
+    *out = nullptr;
+    esp_ctx* c = new esp_ctx();
+    c->prm = *p;
+    c->L[0] = Lx;
+    c->L[1] = Ly;
+    c->L[2] = Lz;
+    c->N = N;
+    int rc = c->b.plan(c->prm, 1, &c->N, c->L, nullptr);
+    if (rc) {
+        delete c;
+        return rc;
+    }
+    c->dirty = false;
+    *out = c;
+    return 0;
+}
+
+int esp_set_params(esp_ctx* c, const esp_params* p) {
+    if (!c || !p) return fail(ESP_ERR_INVALID, "null argument");
+    c->prm = *p;
+    c->dirty = true;
+    return 0;
+}
+
+int esp_set_box(esp_ctx* c, double Lx, double Ly, double Lz) {
+    if (!c) return fail(ESP_ERR_INVALID, "null context");
+    c->L[0] = Lx;
+    c->L[1] = Ly;
+    c->L[2] = Lz;
+    c->dirty = true;
+    return 0;
+}
+
+int esp_invalidate(esp_ctx* c) {
+    if (!c) return fail(ESP_ERR_INVALID, "null context");
+    c->dirty = true;
+    return 0;
+}
+
+int esp_compute(esp_ctx* c, void* stream, const float* pos4, const float* charge, int N, const unsigned* head,
+                const unsigned* n_neigh, const unsigned* nlist, float* force4, double* energy, double* virial6,
+                int flags) {
+    if (!c) return fail(ESP_ERR_INVALID, "null context");
+    if (N < 0) return fail(ESP_ERR_INVALID, "negative particle count");
+    if (N != c->N || c->dirty) {
+        c->N = N;
+        int rc = c->b.plan(c->prm, 1, &c->N, c->L, nullptr);
+        if (rc) return rc;
+        c->dirty = false;
+    }
+    if (N == 0) {
+        cudaStream_t st = (cudaStream_t)stream;
+        if (energy) ESPB_CK(cudaMemsetAsync(energy, 0, sizeof(double), st));
+        if (virial6) ESPB_CK(cudaMemsetAsync(virial6, 0, 6 * sizeof(double), st));
+        return 0;
+    }
+    return c->b.compute((cudaStream_t)stream, pos4, charge, head, n_neigh, nlist, force4, energy, virial6, flags);
+}
+
+int esp_get_info(const esp_ctx* c, esp_info* info) {
+    if (!c) return fail(ESP_ERR_INVALID, "null context");
+    return c->b.info(0, info);
+}
+
+int esp_destroy(esp_ctx* c) {
+    delete c;
+    return 0;
+}
+
+int esp_spread(esp_ctx* c, void* stream, const float* pos4, const float* charge, int N, double* rho) {
+    if (!c) return fail(ESP_ERR_INVALID, "null context");
+    if (N <= 0) return fail(ESP_ERR_INVALID, "particle count must be positive");
+    if (N != c->N || c->dirty) {
+        c->N = N;
+        int rc = c->b.plan(c->prm, 1, &c->N, c->L, nullptr);
+        if (rc) return rc;
+        c->dirty = false;
+    }
+    return c->b.spread_only((cudaStream_t)stream, pos4, charge, rho);
+}
+
+int esp_get_sort(const esp_ctx* c, void* stream, unsigned* key, unsigned* perm) {
+    if (!c || !key || !perm) return fail(ESP_ERR_INVALID, "null argument");
+    const int N = c->b.totN;
+    cudaStream_t st = (cudaStream_t)stream;
+    ESPB_CK(cudaMemcpyAsync(key, c->b.d_key, N * sizeof(unsigned), cudaMemcpyDeviceToDevice, st));
+    ESPB_CK(cudaMemcpyAsync(perm, c->b.d_perm, N * sizeof(unsigned), cudaMemcpyDeviceToDevice, st));
+    return 0;
+}
+
+int esp_get_potential(const esp_ctx* c, void* stream, float* phi) {
+    if (!c || !phi) return fail(ESP_ERR_INVALID, "null argument");
+    const SysDev& S = c->b.sd[0];
+    ESPB_CK(cudaMemcpyAsync(phi, c->b.d_phi, (size_t)S.nx * S.ny * S.nz * sizeof(float), cudaMemcpyDeviceToDevice,
+                            (cudaStream_t)stream));
+    return 0;
+}
+
+int esp_batch_create(const esp_params* p, int nsys, const int* N, const double* boxes, const int* mesh,
+                     esp_batch** out) {
+    if (!p || !N || !boxes || !out) return fail(ESP_ERR_INVALID, "null argument");
+    *out = nullptr;
+    esp_batch* b = new esp_batch();
+    int rc = b->plan(*p, nsys, N, boxes, mesh);
+    if (rc) {
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return 0;
+}
+
+int esp_batch_compute(esp_batch* b, void* stream, const float* pos4, const float* charge, const unsigned* head,
+                      const unsigned* n_neigh, const unsigned* nlist, float* force4, double* energy, double* virial6,
+                      int flags) {
+    if (!b) return fail(ESP_ERR_INVALID, "null batch");
+    return b->compute((cudaStream_t)stream, pos4, charge, head, n_neigh, nlist, force4, energy, virial6, flags);
+}
+
+int esp_batch_get_info(const esp_batch* b, int sys, esp_info* info) {
+    if (!b) return fail(ESP_ERR_INVALID, "null batch");
+    return b->info(sys, info);
+}
+
+int esp_batch_total_particles(const esp_batch* b) { return b ? b->totN : -1; }
+
+int esp_batch_destroy(esp_batch* b) {
+    delete b;
+    return 0;
+}
+
+int esp_batch_md_run(esp_batch* b, void* stream, float* pos4, float* vel4, const float* charge, const unsigned* head,
+                     const unsigned* n_neigh, const unsigned* nlist, float* force4, double* energy, double* virial6,
+                     int nsteps, double dt, int use_graph) {
+    if (!b) return fail(ESP_ERR_INVALID, "null batch");
+    return b->md_run((cudaStream_t)stream, pos4, vel4, charge, head, n_neigh, nlist, force4, energy, virial6, nsteps,
+                     dt, use_graph);
+}
+
+int esp_batch_set_timing(esp_batch* b, int on) {
+    if (!b) return fail(ESP_ERR_INVALID, "null batch");
+    b->timer.collect();
+    b->timer.reset();
+    b->timer.on = on != 0;
+    return 0;
+}
+
+int esp_batch_stage_times(esp_batch* b, double* ms, long long* counts) {
+    if (!b || !ms) return fail(ESP_ERR_INVALID, "null argument");
+    b->timer.collect();
+    for (int k = 0; k < ESP_N_STAGES; ++k) {
+        ms[k] = b->timer.ms[k];
+        if (counts) counts[k] = b->timer.count[k];
+    }
+    b->timer.reset();
+    return 0;
+}
+
+int esp_pswf_eval_pairs(void* stream, int n, const double* rsq, const double* qiqj, double rcut, int n_segs,
+                        const double* screen, const double* dscreen, const double* r_lo, const double* dr_inv,
+                        double* force_divr, double* pair_eng, int* evaluated) {
+    if (n < 0 || n_segs <= 0) return fail(ESP_ERR_INVALID, "bad sizes");
+    if (n > 0 && (!rsq || !qiqj || !screen || !dscreen || !r_lo || !dr_inv || !force_divr || !pair_eng || !evaluated))
+        return fail(ESP_ERR_INVALID, "null pointer");
+    ESPB_CK(launch_pswf_eval_pairs(n, rsq, qiqj, rcut, n_segs, screen, dscreen, r_lo, dr_inv, force_divr, pair_eng,
+                                   evaluated, (cudaStream_t)stream));
+    return 0;
+}
+
+int esp_batch_build_nlist(esp_batch* b, void* stream, const float* pos4, double rlist, int cap, unsigned* head,
+                          unsigned* n_neigh, unsigned* nlist) {
+    if (!b) return fail(ESP_ERR_INVALID, "null batch");
+    return b->build_nlist((cudaStream_t)stream, pos4, rlist, cap, head, n_neigh, nlist);
+}
+
+int esp_batch_nve_step1(esp_batch* b, void* stream, float* pos4, float* vel4, const float* force4, double dt) {
+    if (!b || !pos4 || !vel4 || !force4) return fail(ESP_ERR_INVALID, "null argument");
+    ESPB_CK(launch_nve1(b->d_chunks, b->n_chunks, b->d_sys, reinterpret_cast<float4*>(pos4),
+                        reinterpret_cast<float4*>(vel4), reinterpret_cast<const float4*>(force4), (float)dt,
+                        (cudaStream_t)stream));
+    return 0;
+}
+
+int esp_batch_nve_step2(esp_batch* b, void* stream, float* vel4, const float* force4, double dt) {
+    if (!b || !vel4 || !force4) return fail(ESP_ERR_INVALID, "null argument");
+    ESPB_CK(launch_nve2(b->d_chunks, b->n_chunks, b->d_sys, reinterpret_cast<float4*>(vel4),
+                        reinterpret_cast<const float4*>(force4), (float)dt, (cudaStream_t)stream));
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,1048 @@
+// ESP hot-path kernels for sm_100a.
+//
+// Stage map to the reference (slweng0321/ESP_HOOMD):
+//   k_bin / k_scan / k_scatter / k_tile_sort : new particle binning + stable
+//       sort (nearest reference code: makeFraction+floorf in
+//       src/ESPForceComputeGPU.cu:228-236)
+//   k_spread   : charge assignment, src/ESPForceComputeGPU.cu:206-272 (K2)
+//   k_fftx_fwd / k_ffty<false> : forward FFT, src/ESPForceComputeGPU.cc:254-265 (K3)
+//   k_fftz_conv : influence multiply fused into the z pass,
+//       src/ESPForceComputeGPU.cu:277-287 (K4), plus the k-space energy and
+//       virial (stubs in src/ESPForceCompute.cc:236-248)
+//   k_ffty<true> / k_fftx_inv : inverse FFT (missing in the reference,
+//       src/ESPForceCompute.cc:225-232)
+//   k_interp   : force interpolation, src/ESPForceComputeGPU.cu:292-373 (K6)
+//   k_pair     : EvaluatorPairPSWF over a neighbour list,
+//       src/EvaluatorPairPSWF.h:274-295 with the HOOMD PotentialPair loop
+//   k_influence: influence-function build (K1), src/ESPForceComputeGPU.cu:157-201
+#include "esp_common.cuh"
+#include "esp_kernels.h"
+
+namespace espb {
+
+// ============================================================================
+// a1: bin + stable sort
+// ============================================================================
+
+__global__ void k_bin(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, int P, int T,
+                      const float4* __restrict__ pos_in, const float* __restrict__ q_in,
+                      float4* __restrict__ posq, float4* __restrict__ trec, uint32_t* __restrict__ rel,
+                      uint32_t* __restrict__ key, uint32_t* __restrict__ tile_count, double* __restrict__ acc) {
+    __shared__ double red[32 * 2];
+    const int2 ch = chunks[blockIdx.x];
+    const SysDev& S = sys[ch.x];
+    const int i = ch.y + threadIdx.x;
+    double qs[2] = {0.0, 0.0};
+    if (i < S.p_off + S.N) {
+        const float4 p = pos_in[i];
+        const float q = q_in[i];
+        float x = p.x - S.Lx * floorf(p.x * S.inv_Lx);
+        float y = p.y - S.Ly * floorf(p.y * S.inv_Ly);
+        float z = p.z - S.Lz * floorf(p.z * S.inv_Lz);
+        if (x >= S.Lx) x -= S.Lx;
+        if (y >= S.Ly) y -= S.Ly;
+        if (z >= S.Lz) z -= S.Lz;
+        if (x < 0.f) x += S.Lx;
+        if (y < 0.f) y += S.Ly;
+        if (z < 0.f) z += S.Lz;
+        // grid coordinate and stencil origin in FP64 (exact product of the
+        // FP32 position), so t carries no position-rounding amplification
+        const double hp = 0.5 * P;
+        double g[3] = {(double)x * S.gxd, (double)y * S.gyd, (double)z * S.gzd};
+        const int n[3] = {S.nx, S.ny, S.nz};
+        int i0m[3];
+        float tt[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (g[d] >= n[d]) g[d] -= n[d];
+            const int i0 = (int)floor(g[d] - hp) + 1;
+            tt[d] = (float)((double)i0 + hp - g[d]);
+            i0m[d] = i0 < 0 ? i0 + n[d] : (i0 >= n[d] ? i0 - n[d] : i0);
+        }
+        const int tx = i0m[0] / T, ty = i0m[1] / T, tz = i0m[2] / T;
+        const uint32_t k = (uint32_t)(S.t_off + (tz * S.nty + ty) * S.ntx + tx);
+        key[i] = k;
+        atomicAdd(&tile_count[k], 1u);
+        posq[i] = make_float4(x, y, z, q);
+        trec[i] = make_float4(tt[0], tt[1], tt[2], q);
+        rel[i] = (uint32_t)(i0m[0] - tx * T) | ((uint32_t)(i0m[1] - ty * T) << 8) |
+                 ((uint32_t)(i0m[2] - tz * T) << 16);
+        qs[0] = q;
+        qs[1] = (double)q * q;
+    }
+    block_sum_f64<2>(qs, red);
+    if (threadIdx.x == 0) {
+        atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_QSUM], qs[0]);
+        atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_Q2SUM], qs[1]);
+    }
+}
+
+// Exclusive scan of n counts (single CTA of 1024 threads); start[n] = total.
+__global__ void k_scan(const uint32_t* __restrict__ cnt, uint32_t* __restrict__ start, int n) {
+    __shared__ uint32_t wsum[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t carry = 0;
+    for (int base = 0; base < n; base += 1024) {
+        const int i = base + threadIdx.x;
+        const uint32_t v = i < n ? cnt[i] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            uint32_t w = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            wsum[lane] = w;
+        }
+        __syncthreads();
+        const uint32_t pre = wid > 0 ? wsum[wid - 1] : 0u;
+        if (i < n) start[i] = carry + pre + x - v;
+        const uint32_t total = wsum[31];
+        __syncthreads();
+        carry += total;
+    }
+    if (threadIdx.x == 0) start[n] = carry;
+}
+
+// Slot of each particle inside its tile; leaves tile_count at zero so the
+// next step's histogram needs no memset.
+__global__ void k_scatter(const int2* __restrict__ chunks, const SysDev* __restrict__ sys,
+                          const uint32_t* __restrict__ key, const uint32_t* __restrict__ start,
+                          uint32_t* __restrict__ cnt, uint32_t* __restrict__ perm_u) {
+    const int2 ch = chunks[blockIdx.x];
+    const SysDev& S = sys[ch.x];
+    const int i = ch.y + threadIdx.x;
+    if (i >= S.p_off + S.N) return;
+    const uint32_t k = key[i];
+    const uint32_t slot = start[k] + atomicSub(&cnt[k], 1u) - 1u;
+    perm_u[slot] = (uint32_t)i;
+}
+
+// Deterministic per-tile order: particles of one tile sorted by index, so
+// the permutation equals a stable sort on (key, index). Also gathers the
+// sorted particle records.
+__global__ void k_tile_sort(const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm_u,
+                            uint32_t* __restrict__ perm, const float4* __restrict__ trec,
+                            const uint32_t* __restrict__ rel, float4* __restrict__ srec,
+                            uint32_t* __restrict__ srel) {
+    __shared__ uint32_t sm[SORT_CAP];
+    const uint32_t s0 = start[blockIdx.x];
+    const uint32_t n = start[blockIdx.x + 1] - s0;
+    if (n == 0) return;
+    const bool cached = n <= (uint32_t)SORT_CAP;
+    if (cached)
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sm[i] = perm_u[s0 + i];
+    __syncthreads();
+    const uint32_t* src = cached ? sm : perm_u + s0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint32_t v = src[i];
+        uint32_t r = 0;
+        for (uint32_t j = 0; j < n; ++j) r += (src[j] < v) ? 1u : 0u;
+        perm[s0 + r] = v;
+        srec[s0 + r] = trec[v];
+        srel[s0 + r] = rel[v];
+    }
+}
+
+// ============================================================================
+// a3: spreading. One CTA per tile; shared-memory accumulators with residue
+// ownership: location X of the tile's extended region [0, T+P-1)^3 is owned
+// by the threads whose residue is X mod P, so every (particle, stencil
+// point) update has a single writer and is Kahan-compensated without atomics
+// (sum and compensation interleaved: one 64-bit shared load and store per
+// tap). Thread (rx, ry, zg) handles, for each particle, the CZ = P/ZS stencil
+// points of its x/y residue in its block of z residues. Each tile is flushed
+// once to the FP64 mesh (sum - comp, one atomic per footprint point).
+// ============================================================================
+
+template <int P>
+struct SpreadCfg {
+    static constexpr int P2 = P * P;
+    static constexpr int P3 = P * P * P;
+    // z-residue groups: the largest divisor of P with P^2 * ZS <= 160 threads
+    static constexpr int zs(int d) { return d <= 1 ? 1 : ((P % d == 0 && P2 * d <= 160) ? d : zs(d - 1)); }
+    static constexpr int ZS = zs(P);
+    static constexpr int CZ = P / ZS;  // stencil points per particle per thread
+    static constexpr int THREADS = P2 * ZS;
+    static constexpr int CH = 32;  // particles staged per round
+};
+
+template <int P>
+__global__ void __launch_bounds__(SpreadCfg<P>::THREADS)
+    k_spread(const int* __restrict__ tile_sys, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
+             int T, int D, const uint32_t* __restrict__ start, const float4* __restrict__ srec,
+             const uint32_t* __restrict__ srel, double* __restrict__ rho) {
+    using C = SpreadCfg<P>;
+    extern __shared__ float4 smem4[];
+    const int t = blockIdx.x;
+    const uint32_t s0 = start[t];
+    const int np = (int)(start[t + 1] - s0);
+    if (np == 0) return;
+    const int si = tile_sys[t];
+    const SysDev& S = sys[si];
+    const ParamSet& ps = psets[S.pset];
+    const int E = T + P - 1;
+    const int nb = (E + P - 1) / P;
+    const int NL = nb * nb * nb * C::P3;
+    float2* accc = reinterpret_cast<float2*>(smem4);       // [NL] (sum, comp)
+    float* pwx = reinterpret_cast<float*>(accc + NL);       // [CH][P] x weights * q
+    float* pwy = pwx + C::CH * P;                           // [CH][P]
+    float* pwz = pwy + C::CH * P;                           // [CH][P] by z residue
+    int* pzo = reinterpret_cast<int*>(pwz + C::CH * P);     // [CH][P] z slot offsets
+    int* pxy = pzo + C::CH * P;                             // [CH] packed x/y origins
+    float* wc = reinterpret_cast<float*>(pxy + C::CH);      // [P][D+1]
+    const int tid = threadIdx.x;
+    for (int i = tid; i < NL; i += C::THREADS) accc[i] = make_float2(0.f, 0.f);
+    for (int i = tid; i < P * (D + 1); i += C::THREADS)
+        wc[i] = ps.wcoef[(i / (D + 1)) * (MAX_D + 1) + (i % (D + 1))];
+    __syncthreads();
+    const int rx = tid % P, ry = (tid / P) % P, zg = tid / C::P2;
+    const int nbP3 = nb * nb * C::P3;
+    for (int base = 0; base < np; base += C::CH) {
+        const int nc = min(C::CH, np - base);
+        for (int k = tid; k < nc * 3 * P; k += C::THREADS) {
+            const int p = k / (3 * P), r = k - p * 3 * P, ax = r / P, a = r - ax * P;
+            const float4 rec = srec[s0 + base + p];
+            const uint32_t rl = srel[s0 + base + p];
+            const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
+            const float w = horner_w(&wc[a * (D + 1)], D, tt);
+            if (ax == 0) {
+                pwx[p * P + a] = w * rec.w;
+            } else if (ax == 1) {
+                pwy[p * P + a] = w;
+            } else {
+                const int Z = (int)((rl >> 16) & 255u) + a, rz = Z % P, bz = Z / P;
+                pwz[p * P + rz] = w;
+                pzo[p * P + rz] = bz * nbP3 + rz * C::P2;
+            }
+            if (r == 0) {
+                const int ox = (int)(rl & 255u), oy = (int)((rl >> 8) & 255u);
+                pxy[p] = ox | ((ox % P) << 8) | (oy << 16) | ((oy % P) << 24);
+            }
+        }
+        __syncthreads();
+        for (int p = 0; p < nc; ++p) {
+            const int pk = pxy[p];
+            const int ox = pk & 255, oy = (pk >> 16) & 255;
+            int a = rx - ((pk >> 8) & 255);
+            a += a < 0 ? P : 0;
+            int b = ry - ((pk >> 24) & 255);
+            b += b < 0 ? P : 0;
+            const int bx = (ox + a) / P, by = (oy + b) / P;
+            const float wxy = pwx[p * P + a] * pwy[p * P + b];
+            const int bs = (by * nb + bx) * C::P3 + ry * P + rx;
+            const float* wz = pwz + p * P + zg * C::CZ;
+            const int* zo = pzo + p * P + zg * C::CZ;
+#pragma unroll
+            for (int k = 0; k < C::CZ; ++k) {
+                const int sl = bs + zo[k];
+                const float tap = wxy * wz[k];
+                float2 v = accc[sl];
+                const float y = __fsub_rn(tap, v.y);
+                const float tsum = __fadd_rn(v.x, y);
+                v.y = __fsub_rn(__fsub_rn(tsum, v.x), y);
+                v.x = tsum;
+                accc[sl] = v;
+            }
+        }
+        __syncthreads();
+    }
+    // flush: one FP64 atomic per footprint point (region slots that wrap
+    // onto the same mesh point are summed first)
+    const int lt = t - S.t_off;
+    const int X0 = (lt % S.ntx) * T, Y0 = ((lt / S.ntx) % S.nty) * T, Z0 = (lt / (S.ntx * S.nty)) * T;
+    const int Ex = min(E, S.nx), Ey = min(E, S.ny), Ez = min(E, S.nz);
+    for (int i = tid; i < Ex * Ey * Ez; i += C::THREADS) {
+        const int X = i % Ex, Y = (i / Ex) % Ey, Z = i / (Ex * Ey);
+        double v = 0.0;
+        for (int Zs = Z; Zs < E; Zs += S.nz)
+            for (int Ys = Y; Ys < E; Ys += S.ny)
+                for (int Xs = X; Xs < E; Xs += S.nx) {
+                    const int sl = ((Zs / P * nb + Ys / P) * nb + Xs / P) * C::P3 +
+                                   ((Zs % P) * P + Ys % P) * P + Xs % P;
+                    const float2 a2 = accc[sl];
+                    v += (double)a2.x - (double)a2.y;
+                }
+        if (v != 0.0) {
+            int gx = X0 + X, gy = Y0 + Y, gz = Z0 + Z;
+            gx -= gx >= S.nx ? S.nx : 0;
+            gy -= gy >= S.ny ? S.ny : 0;
+            gz -= gz >= S.nz ? S.nz : 0;
+            atomicAdd(&rho[S.m_off + ((long long)gz * S.ny + gy) * S.nx + gx], v);
+        }
+    }
+}
+
+// ============================================================================
+// a4-a6: FFT passes. Batched mixed-radix (2,3,4,5) Stockham transforms in
+// shared memory; lines stored element-major s[i*B + b].
+// ============================================================================
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft_small(float2 (&v)[R]) {
+    if constexpr (R == 2) {
+        const float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (R == 3) {
+        const float s1 = INV ? -0.86602540378443865f : 0.86602540378443865f;
+        const float2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+        const float2 m = make_float2(v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y);
+        v[0] = cadd(v[0], t1);
+        // -i s1 t2 = (s1 t2.y, -s1 t2.x)
+        v[1] = make_float2(m.x + s1 * t2.y, m.y - s1 * t2.x);
+        v[2] = make_float2(m.x - s1 * t2.y, m.y + s1 * t2.x);
+    } else if constexpr (R == 4) {
+        const float2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
+        const float2 c = cadd(v[1], v[3]), d = csub(v[1], v[3]);
+        v[0] = cadd(a, c);
+        v[2] = csub(a, c);
+        if (INV) {
+            v[1] = make_float2(b.x - d.y, b.y + d.x);
+            v[3] = make_float2(b.x + d.y, b.y - d.x);
+        } else {
+            v[1] = make_float2(b.x + d.y, b.y - d.x);
+            v[3] = make_float2(b.x - d.y, b.y + d.x);
+        }
+    } else if constexpr (R == 5) {
+        const float c1 = 0.30901699437494742f, c2 = -0.80901699437494742f;
+        const float s1 = INV ? -0.95105651629515357f : 0.95105651629515357f;
+        const float s2 = INV ? -0.58778525229247313f : 0.58778525229247313f;
+        const float2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+        const float2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+        const float2 a1 = make_float2(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+        const float2 a2 = make_float2(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+        const float2 b1 = make_float2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y);
+        const float2 b2 = make_float2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y);
+        v[0] = cadd(v[0], cadd(t1, t2));
+        // a -/+ i b
+        v[1] = make_float2(a1.x + b1.y, a1.y - b1.x);
+        v[4] = make_float2(a1.x - b1.y, a1.y + b1.x);
+        v[2] = make_float2(a2.x + b2.y, a2.y - b2.x);
+        v[3] = make_float2(a2.x - b2.y, a2.y + b2.x);
+    }
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void fft_stage(const float2* __restrict__ src, float2* __restrict__ dst, int n, int B,
+                                          int SB, int Ns, const float2* __restrict__ tw) {
+    const int m = n / R;
+    const int stride = n / (Ns * R);
+    for (int idx = threadIdx.x; idx < m * B; idx += blockDim.x) {
+        const int b = idx % B, j = idx / B, k = j % Ns;
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = src[(j + r * m) * SB + b];
+        if (Ns > 1) {
+            const int ts = k * stride;
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                float2 w = __ldg(&tw[ts * r]);
+                if (INV) w.y = -w.y;
+                v[r] = cmul(v[r], w);
+            }
+        }
+        dft_small<R, INV>(v);
+        const int o = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) dst[(o + r * Ns) * SB + b] = v[r];
+    }
+}
+
+// Runs all stages; returns the buffer that holds the result.
+template <bool INV>
+__device__ float2* fft_lines(float2* s0, float2* s1, int n, int B, int SB, const float2* __restrict__ tw,
+                             uint32_t plan) {
+    int Ns = 1;
+    for (int s = 0; s < 8; ++s) {
+        const int R = (int)((plan >> (4 * s)) & 15u);
+        if (R == 0) break;
+        switch (R) {
+            case 2: fft_stage<2, INV>(s0, s1, n, B, SB, Ns, tw); break;
+            case 3: fft_stage<3, INV>(s0, s1, n, B, SB, Ns, tw); break;
+            case 4: fft_stage<4, INV>(s0, s1, n, B, SB, Ns, tw); break;
+            case 5: fft_stage<5, INV>(s0, s1, n, B, SB, Ns, tw); break;
+        }
+        __syncthreads();
+        float2* tmp = s0;
+        s0 = s1;
+        s1 = tmp;
+        Ns *= R;
+    }
+    return s0;
+}
+
+// Forward x pass: real rows (FP64 mesh, read and cleared) -> half spectrum.
+// Two real rows form one complex line; the half spectra are separated with
+// A_k = (Z_k + conj Z_{n-k})/2, B_k = (Z_k - conj Z_{n-k})/(2i).
+__global__ void k_fftx_fwd(const int4* __restrict__ items, const SysDev* __restrict__ sys,
+                           const float2* __restrict__ tw, double* __restrict__ rho, float2* __restrict__ spec) {
+    extern __shared__ float2 sb[];
+    const int4 it = items[blockIdx.x];
+    const SysDev& S = sys[it.x];
+    const int z = it.y, y0 = it.z, n = S.nx;
+    constexpr int B = FFT_B_X, SB = FFT_SB_X;  // padded line stride: conflict-free row access
+    float2* s0 = sb;
+    float2* s1 = sb + FFT_MAX_N * SB;
+    for (int idx = threadIdx.x; idx < B * n; idx += blockDim.x) {
+        const int b = idx / n, i = idx - b * n, y = y0 + 2 * b;
+        float2 v = make_float2(0.f, 0.f);
+        if (y < S.ny) {
+            const long long g = S.m_off + ((long long)z * S.ny + y) * n + i;
+            v.x = (float)rho[g];
+            rho[g] = 0.0;
+            if (y + 1 < S.ny) {
+                v.y = (float)rho[g + n];
+                rho[g + n] = 0.0;
+            }
+        }
+        s0[i * SB + b] = v;
+    }
+    __syncthreads();
+    const float2* r = fft_lines<false>(s0, s1, n, B, SB, tw + S.twx, S.radx);
+    for (int idx = threadIdx.x; idx < B * S.nxh; idx += blockDim.x) {
+        const int b = idx / S.nxh, k = idx - b * S.nxh;
+        const float2 zk = r[k * SB + b], zn = r[((n - k) % n) * SB + b];
+        const int y = y0 + 2 * b;
+        if (y < S.ny)
+            spec[S.s_off + ((long long)z * S.ny + y) * S.nxh + k] =
+                make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+        if (y + 1 < S.ny)
+            spec[S.s_off + ((long long)z * S.ny + y + 1) * S.nxh + k] =
+                make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+    }
+}
+
+// y pass (C2C), forward or inverse, in place on the half spectrum.
+template <bool INV>
+__global__ void k_ffty(const int4* __restrict__ items, const SysDev* __restrict__ sys,
+                       const float2* __restrict__ tw, float2* __restrict__ spec) {
+    extern __shared__ float2 sb[];
+    const int4 it = items[blockIdx.x];
+    const SysDev& S = sys[it.x];
+    const int z = it.y, kx0 = it.z, n = S.ny;
+    constexpr int B = FFT_B_YZ;
+    float2* s0 = sb;
+    float2* s1 = sb + FFT_MAX_N * B;
+    for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
+        const int y = idx / B, b = idx - y * B, kx = kx0 + b;
+        s0[idx] = kx < S.nxh ? spec[S.s_off + ((long long)z * S.ny + y) * S.nxh + kx] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const float2* r = fft_lines<INV>(s0, s1, n, B, B, tw + S.twy, S.rady);
+    for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
+        const int y = idx / B, b = idx - y * B, kx = kx0 + b;
+        if (kx < S.nxh) spec[S.s_off + ((long long)z * S.ny + y) * S.nxh + kx] = r[idx];
+    }
+}
+
+// z pass: forward transform, k-space energy and virial (FP64), influence
+// multiply, inverse transform -- the only pass that holds whole k-columns.
+__global__ void k_fftz_conv(const int4* __restrict__ items, const SysDev* __restrict__ sys,
+                            const float2* __restrict__ tw, const float2* __restrict__ gtab,
+                            float2* __restrict__ spec, double* __restrict__ acc) {
+    extern __shared__ float2 sb[];
+    __shared__ double red[32 * 7];
+    const int4 it = items[blockIdx.x];
+    const SysDev& S = sys[it.x];
+    const int y = it.y, kx0 = it.z, n = S.nz;
+    constexpr int B = FFT_B_YZ;
+    float2* s0 = sb;
+    float2* s1 = sb + FFT_MAX_N * B;
+    const long long rowstride = (long long)S.ny * S.nxh;
+    for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
+        const int z = idx / B, b = idx - z * B, kx = kx0 + b;
+        s0[idx] = kx < S.nxh ? spec[S.s_off + z * rowstride + (long long)y * S.nxh + kx] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float2* r = fft_lines<false>(s0, s1, n, B, B, tw + S.twz, S.radz);
+    float2* other = (r == s0) ? s1 : s0;
+    const double twopi = 6.283185307179586;
+    const int fy = (y < (S.ny + 1) / 2) ? y : y - S.ny;
+    const double kyv = twopi * fy / (double)S.Ly;
+    double e[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
+        const int z = idx / B, b = idx - z * B, kx = kx0 + b;
+        if (kx >= S.nxh) {
+            r[idx] = make_float2(0.f, 0.f);
+            continue;
+        }
+        const float2 gb = gtab[S.g_off + z * rowstride + (long long)y * S.nxh + kx];
+        const float2 d = r[idx];
+        const double p2 = (double)d.x * d.x + (double)d.y * d.y;
+        const double mult = (kx == 0 || 2 * kx == S.nx) ? 0.5 : 1.0;
+        const double ek = mult * (double)gb.x * p2, eb = mult * (double)gb.y * p2;
+        const int fz = (z < (n + 1) / 2) ? z : z - n;
+        const double kxv = twopi * kx / (double)S.Lx, kzv = twopi * fz / (double)S.Lz;
+        e[0] += ek;
+        e[1] += ek + eb * kxv * kxv;
+        e[2] += eb * kxv * kyv;
+        e[3] += eb * kxv * kzv;
+        e[4] += ek + eb * kyv * kyv;
+        e[5] += eb * kyv * kzv;
+        e[6] += ek + eb * kzv * kzv;
+        r[idx] = make_float2(d.x * gb.x, d.y * gb.x);
+    }
+    __syncthreads();
+    const float2* o = fft_lines<true>(r, other, n, B, B, tw + S.twz, S.radz);
+    for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
+        const int z = idx / B, b = idx - z * B, kx = kx0 + b;
+        if (kx < S.nxh) spec[S.s_off + z * rowstride + (long long)y * S.nxh + kx] = o[idx];
+    }
+    block_sum_f64<7>(e, red);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < 7; ++k) atomicAdd(&acc[it.x * ACC_STRIDE + ACC_EK + k], e[k]);
+}
+
+// Inverse x pass (C2R): two Hermitian half-spectrum rows A, B are extended
+// and combined as Z = A + iB; the inverse transform returns row A in the
+// real part and row B in the imaginary part.
+__global__ void k_fftx_inv(const int4* __restrict__ items, const SysDev* __restrict__ sys,
+                           const float2* __restrict__ tw, const float2* __restrict__ spec, float* __restrict__ phi) {
+    extern __shared__ float2 sb[];
+    const int4 it = items[blockIdx.x];
+    const SysDev& S = sys[it.x];
+    const int z = it.y, y0 = it.z, n = S.nx;
+    constexpr int B = FFT_B_X, SB = FFT_SB_X;
+    float2* s0 = sb;
+    float2* s1 = sb + FFT_MAX_N * SB;
+    for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
+        const int b = idx / n, k = idx - b * n, ya = y0 + 2 * b, yb = ya + 1;
+        const bool up = k >= S.nxh;
+        const int kk = up ? n - k : k;
+        float2 A = ya < S.ny ? spec[S.s_off + ((long long)z * S.ny + ya) * S.nxh + kk] : make_float2(0.f, 0.f);
+        float2 Bv = yb < S.ny ? spec[S.s_off + ((long long)z * S.ny + yb) * S.nxh + kk] : make_float2(0.f, 0.f);
+        if (up) {
+            A.y = -A.y;
+            Bv.y = -Bv.y;
+        }
+        if (k == 0 || 2 * k == n) {
+            A.y = 0.f;
+            Bv.y = 0.f;
+        }
+        s0[k * SB + b] = make_float2(A.x - Bv.y, A.y + Bv.x);
+    }
+    __syncthreads();
+    const float2* r = fft_lines<true>(s0, s1, n, B, SB, tw + S.twx, S.radx);
+    for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
+        const int b = idx / n, i = idx - b * n, y = y0 + 2 * b;
+        if (y < S.ny) {
+            const float2 v = r[i * SB + b];
+            const long long g = S.m_off + ((long long)z * S.ny + y) * n + i;
+            phi[g] = v.x;
+            if (y + 1 < S.ny) phi[g + n] = v.y;
+        }
+    }
+}
+
+// ============================================================================
+// a5 (build): influence table {G, G*B} over the half spectrum, in FP64.
+//   G  = Psi(|k| r_c) / (k^2 V w_x^2 w_y^2 w_z^2)
+//   GB = (-2 Psi / k^2 + r_c Psi'(|k| r_c) / |k|) / (k^2 V w^2)
+// Psi by Gauss-Legendre quadrature of the prolate (weights pre-scaled).
+// ============================================================================
+__global__ void k_influence(SysDev S, const double* __restrict__ w1d, const double* __restrict__ tq,
+                            const double* __restrict__ wq, int nq, double rcut, double psi_floor,
+                            float2* __restrict__ gtab) {
+    const long long total = (long long)S.nz * S.ny * S.nxh;
+    const double twopi = 6.283185307179586;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int kx = (int)(idx % S.nxh);
+        const int y = (int)((idx / S.nxh) % S.ny);
+        const int z = (int)(idx / ((long long)S.nxh * S.ny));
+        const int fy = (y < (S.ny + 1) / 2) ? y : y - S.ny;
+        const int fz = (z < (S.nz + 1) / 2) ? z : z - S.nz;
+        const double kxv = twopi * kx / (double)S.Lx, kyv = twopi * fy / (double)S.Ly,
+                     kzv = twopi * fz / (double)S.Lz;
+        const double k2 = kxv * kxv + kyv * kyv + kzv * kzv;
+        float2 out = make_float2(0.f, 0.f);
+        // Nyquist planes of even meshes are dropped: there Psi(kappa_N) is
+        // at the split's truncation level while 1/w^2 amplifies aliasing
+        // and round-off the most
+        const bool nyq = (2 * kx == S.nx) || (2 * y == S.ny) || (2 * z == S.nz);
+        if (k2 > 0.0 && !nyq) {
+            const double kk = sqrt(k2), kap = kk * rcut;
+            double psi = 0.0, dpsi = 0.0;
+            for (int j = 0; j < nq; ++j) {
+                double s, c;
+                sincos(kap * tq[j], &s, &c);
+                psi += wq[j] * c;
+                dpsi -= wq[j] * tq[j] * s;
+            }
+            if (psi > psi_floor) {
+                const double w = w1d[kx] * w1d[S.nx + y] * w1d[S.nx + S.ny + z];
+                const double den = k2 * S.V * w * w;
+                out.x = (float)(psi / den);
+                out.y = (float)((-2.0 * psi / k2 + rcut * dpsi / kk) / den);
+            }
+        }
+        gtab[S.g_off + idx] = out;
+    }
+}
+
+// ============================================================================
+// a7: interpolation. One CTA per tile stages the potential of the tile's
+// extended region in shared memory; one warp per particle gathers the P^3
+// stencil with analytic differentiation of the window. The 3P weights and
+// derivatives are computed by lanes and shared by warp shuffles.
+// ============================================================================
+template <int P>
+__global__ void __launch_bounds__(128)
+    k_interp(const int* __restrict__ tile_sys, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
+             int T, int D, int PX, int PP, const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
+             const float4* __restrict__ srec, const uint32_t* __restrict__ srel, const float* __restrict__ phi,
+             float4* __restrict__ force, double* __restrict__ acc) {
+    extern __shared__ float sm[];
+    __shared__ double red[32];
+    const int t = blockIdx.x;
+    const uint32_t s0 = start[t];
+    const int np = (int)(start[t + 1] - s0);
+    if (np == 0) return;
+    const int si = tile_sys[t];
+    const SysDev& S = sys[si];
+    const ParamSet& ps = psets[S.pset];
+    const int E = T + P - 1;
+    float* wc = sm + E * PP;
+    const int lt = t - S.t_off;
+    const int X0 = (lt % S.ntx) * T, Y0 = ((lt / S.ntx) % S.nty) * T, Z0 = (lt / (S.ntx * S.nty)) * T;
+    // stage the extended region row by row (x fastest: coalesced rows)
+    for (int row = threadIdx.x >> 5; row < E * E; row += blockDim.x >> 5) {
+        const int Y = row % E, Z = row / E;
+        int gy = Y0 + Y, gz = Z0 + Z;
+        while (gy >= S.ny) gy -= S.ny;
+        while (gz >= S.nz) gz -= S.nz;
+        const float* src = phi + S.m_off + ((long long)gz * S.ny + gy) * S.nx;
+        for (int X = threadIdx.x & 31; X < E; X += 32) {
+            int gx = X0 + X;
+            while (gx >= S.nx) gx -= S.nx;
+            sm[Z * PP + Y * PX + X] = __ldg(&src[gx]);
+        }
+    }
+    for (int i = threadIdx.x; i < P * (D + 1); i += blockDim.x)
+        wc[i] = ps.wcoef[(i / (D + 1)) * (MAX_D + 1) + (i % (D + 1))];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    constexpr int NCG = 32 / P;              // c-groups of lanes
+    constexpr int NCI = (P + NCG - 1) / NCG; // rows (c values) per lane
+    const int b = lane % P, cg = lane / P;
+    const float gxs = (float)S.gxd, gys = (float)S.gyd, gzs = (float)S.gzd;
+    double esum = 0.0;
+    for (int p = warp; p < np; p += nw) {
+        const float4 rec = srec[s0 + p];
+        const uint32_t rl = srel[s0 + p];
+        const int ox = (int)(rl & 255u), oy = (int)((rl >> 8) & 255u), oz = (int)((rl >> 16) & 255u);
+        // lane e computes entry e of [x0..xP-1, y0.., z0..]; entries >= 32 in w1
+        float w0 = 0.f, d0 = 0.f, w1 = 0.f, d1 = 0.f;
+        {
+            const int e = lane;
+            if (e < 3 * P) {
+                const int ax = e / P, a = e - ax * P;
+                const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
+                w0 = horner_w(&wc[a * (D + 1)], D, tt);
+                d0 = horner_dw(&wc[a * (D + 1)], D, tt);
+            }
+            if (3 * P > 32 && e + 32 < 3 * P) {
+                const int ax = (e + 32) / P, a = e + 32 - ax * P;
+                const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
+                w1 = horner_w(&wc[a * (D + 1)], D, tt);
+                d1 = horner_dw(&wc[a * (D + 1)], D, tt);
+            }
+        }
+        float wx[P], dwx[P];
+#pragma unroll
+        for (int a = 0; a < P; ++a) {
+            wx[a] = __shfl_sync(0xffffffffu, w0, a);
+            dwx[a] = __shfl_sync(0xffffffffu, d0, a);
+        }
+        const float wyb = __shfl_sync(0xffffffffu, w0, P + b);
+        const float dwyb = __shfl_sync(0xffffffffu, d0, P + b);
+        float pot = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+#pragma unroll
+        for (int ci = 0; ci < NCI; ++ci) {
+            const int c = cg + ci * NCG;
+            const int src = 2 * P + c;
+            float wzc, dwzc;
+            if (3 * P > 32) {
+                const float a0 = __shfl_sync(0xffffffffu, w0, src & 31), a1 = __shfl_sync(0xffffffffu, w1, src & 31);
+                const float e0 = __shfl_sync(0xffffffffu, d0, src & 31), e1 = __shfl_sync(0xffffffffu, d1, src & 31);
+                wzc = src < 32 ? a0 : a1;
+                dwzc = src < 32 ? e0 : e1;
+            } else {
+                wzc = __shfl_sync(0xffffffffu, w0, src & 31);
+                dwzc = __shfl_sync(0xffffffffu, d0, src & 31);
+            }
+            if (lane < NCG * P && c < P) {
+                const float* row = &sm[(oz + c) * PP + (oy + b) * PX + ox];
+                float s = 0.f, d = 0.f;
+#pragma unroll
+                for (int a = 0; a < P; ++a) {
+                    const float v = row[a];
+                    s = fmaf(v, wx[a], s);
+                    d = fmaf(v, dwx[a], d);
+                }
+                const float wyz = wyb * wzc;
+                pot = fmaf(s, wyz, pot);
+                gx = fmaf(d, wyz, gx);
+                gy = fmaf(s, dwyb * wzc, gy);
+                gz = fmaf(s, wyb * dwzc, gz);
+            }
+        }
+        pot = warp_sum(pot);
+        gx = warp_sum(gx);
+        gy = warp_sum(gy);
+        gz = warp_sum(gz);
+        if (lane == 0) {
+            const float q = rec.w;
+            const double e_i = 0.5 * (double)q * pot + ps.self_coef * (double)q * q;
+            force[perm[s0 + p]] = make_float4(q * gxs * gx, q * gys * gy, q * gzs * gz, (float)e_i);
+            esum += e_i;
+        }
+    }
+    double ev[1] = {esum};
+    block_sum_f64<1>(ev, red);
+    if (threadIdx.x == 0) atomicAdd(&acc[si * ACC_STRIDE + ACC_E], ev[0]);
+}
+
+// ============================================================================
+// a8: short-range pair term over a HOOMD-layout neighbour list
+// (neighbours of i: nlist[head[i] + k], k < n_neigh[i], local indices).
+// TPP lanes cooperate on one particle; per pair
+//   pair_eng = qiqj/(4 pi) (1/r - Q(u)/r_c),  u = r^2/r_c^2
+//   force_divr = qiqj/(4 pi) (1/r^3 + 2 Q'(u)/r_c^3)
+// (the split form of EvaluatorPairPSWF::evalForceAndEnergy).
+// ============================================================================
+template <int NQ>
+struct PairEval {
+    const PairCoef& pc;  // the kernel parameter: constant-bank operands
+    float rc2, irc2, irc, tirc3, Lx, Ly, Lz, iLx, iLy, iLz;
+    float fx = 0.f, fy = 0.f, fz = 0.f, en = 0.f;
+    float vxx = 0.f, vxy = 0.f, vxz = 0.f, vyy = 0.f, vyz = 0.f, vzz = 0.f;
+    __device__ __forceinline__ void pair(const float4& pi, const float4& pj) {
+        float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        dx -= Lx * rintf(dx * iLx);
+        dy -= Ly * rintf(dy * iLy);
+        dz -= Lz * rintf(dz * iLz);
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 < rc2 && r2 > 0.f) {
+            float ri = rsqrtf(r2);
+            ri = ri * fmaf(-0.5f * r2 * ri, ri, 1.5f);  // one Newton step: ~1 ulp
+            const float v = fmaf(2.f * irc2, r2, -1.f);
+            float qv = pc.q[NQ - 1], dq = pc.d[NQ - 2];
+#pragma unroll
+            for (int c = NQ - 2; c >= 0; --c) qv = fmaf(qv, v, pc.q[c]);
+#pragma unroll
+            for (int c = NQ - 3; c >= 0; --c) dq = fmaf(dq, v, pc.d[c]);
+            const float qq = pi.w * pj.w * INV_4PI_F;
+            const float fdr = qq * fmaf(tirc3, dq, ri * ri * ri);
+            en = fmaf(qq, ri - qv * irc, en);
+            fx = fmaf(fdr, dx, fx);
+            fy = fmaf(fdr, dy, fy);
+            fz = fmaf(fdr, dz, fz);
+            vxx = fmaf(fdr * dx, dx, vxx);
+            vxy = fmaf(fdr * dx, dy, vxy);
+            vxz = fmaf(fdr * dx, dz, vxz);
+            vyy = fmaf(fdr * dy, dy, vyy);
+            vyz = fmaf(fdr * dy, dz, vyz);
+            vzz = fmaf(fdr * dz, dz, vzz);
+        }
+    }
+};
+
+template <int TPP, int NQ>
+__global__ void __launch_bounds__(256)
+    k_pair(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
+           const float4* __restrict__ posq, const uint32_t* __restrict__ head, const uint32_t* __restrict__ nn,
+           const uint32_t* __restrict__ nlist, float4* __restrict__ force, double* __restrict__ acc, int accumulate,
+           const PairCoef pc) {
+    __shared__ double red[32 * 7];
+    const int2 ch = chunks[blockIdx.x];
+    const SysDev& S = sys[ch.x];
+    const ParamSet& ps = psets[S.pset];
+    PairEval<NQ> ev{pc};
+    ev.rc2 = ps.rcut2;
+    ev.irc = ps.inv_rcut;
+    ev.irc2 = ps.inv_rcut * ps.inv_rcut;
+    ev.tirc3 = ps.two_inv_rcut3;
+    ev.Lx = S.Lx;
+    ev.Ly = S.Ly;
+    ev.Lz = S.Lz;
+    ev.iLx = S.inv_Lx;
+    ev.iLy = S.inv_Ly;
+    ev.iLz = S.inv_Lz;
+    const int i = ch.y + threadIdx.x / TPP;
+    const int sub = threadIdx.x % TPP;
+    const bool valid = i < S.p_off + S.N;
+    if (valid) {
+        const float4 pi = posq[i];
+        const uint32_t n = nn[i], h = head[i];
+        const int po = S.p_off;
+        uint32_t k0 = 0;
+        if ((h & 3u) == 0u) {
+            // 16-byte row segments: each lane streams 4 neighbour indices
+            const uint4* row = reinterpret_cast<const uint4*>(nlist + h);
+            const uint32_t n4 = n >> 2;
+            for (uint32_t k4 = sub; k4 < n4; k4 += TPP) {
+                const uint4 jj = __ldg(&row[k4]);
+                const float4 p0 = __ldg(&posq[po + (int)jj.x]);
+                const float4 p1 = __ldg(&posq[po + (int)jj.y]);
+                const float4 p2 = __ldg(&posq[po + (int)jj.z]);
+                const float4 p3 = __ldg(&posq[po + (int)jj.w]);
+                ev.pair(pi, p0);
+                ev.pair(pi, p1);
+                ev.pair(pi, p2);
+                ev.pair(pi, p3);
+            }
+            k0 = n4 << 2;
+        }
+        for (uint32_t k = k0 + sub; k < n; k += TPP) ev.pair(pi, __ldg(&posq[po + (int)__ldg(&nlist[h + k])]));
+    }
+    float fx = ev.fx, fy = ev.fy, fz = ev.fz, en = ev.en;
+#pragma unroll
+    for (int o = TPP / 2; o > 0; o >>= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+        en += __shfl_xor_sync(0xffffffffu, en, o);
+    }
+    if (valid && sub == 0) {
+        float4 f = accumulate ? force[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        f.x += fx;
+        f.y += fy;
+        f.z += fz;
+        f.w += 0.5f * en;
+        force[i] = f;
+    }
+    double e[7] = {sub == 0 ? 0.5 * (double)en : 0.0, 0.5 * (double)ev.vxx, 0.5 * (double)ev.vxy,
+                   0.5 * (double)ev.vxz, 0.5 * (double)ev.vyy, 0.5 * (double)ev.vyz, 0.5 * (double)ev.vzz};
+    block_sum_f64<7>(e, red);
+    if (threadIdx.x == 0) {
+        atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_E], e[0]);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_WP + k], e[1 + k]);
+    }
+}
+
+// Energy and virial per system: E = sum_i e_i + E_bg; W = W_k + W_pair + E_bg I.
+__global__ void k_finalize(const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets, int nsys,
+                           const double* __restrict__ acc, double* __restrict__ energy, double* __restrict__ virial,
+                           int add_bg) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    const SysDev& S = sys[s];
+    const double* a = acc + s * ACC_STRIDE;
+    const double Q = a[ACC_QSUM];
+    const double ebg = add_bg ? psets[S.pset].bg_coef * Q * Q / S.V : 0.0;
+    if (energy) energy[s] = a[ACC_E] + ebg;
+    if (virial) {
+        const int diag[6] = {1, 0, 0, 1, 0, 1};
+        for (int k = 0; k < 6; ++k) virial[s * 6 + k] = a[ACC_WK + k] + a[ACC_WP + k] + (diag[k] ? ebg : 0.0);
+    }
+}
+
+// ============================================================================
+// Reference-format evaluator: detail::pswf_eval_L + evalForceAndEnergy of
+// src/EvaluatorPairPSWF.h:113-143, 274-295, reading a PSWF_Coeffs.h-layout
+// segment table. Rounding is pinned (_rn intrinsics, no FMA contraction)
+// so the FP64 instance reproduces a host compile of the reference.
+// ============================================================================
+__device__ __forceinline__ double seg_horner5(const double* __restrict__ c, double t) {
+    double v = c[4];
+    v = __dadd_rn(c[3], __dmul_rn(t, v));
+    v = __dadd_rn(c[2], __dmul_rn(t, v));
+    v = __dadd_rn(c[1], __dmul_rn(t, v));
+    v = __dadd_rn(c[0], __dmul_rn(t, v));
+    return v;
+}
+
+__global__ void k_pswf_eval_pairs(int n, const double* __restrict__ rsq, const double* __restrict__ qiqj,
+                                  double rcut, double rcutsq, int n_segs, const double* __restrict__ screen,
+                                  const double* __restrict__ dscreen, const double* __restrict__ r_lo,
+                                  const double* __restrict__ dr_inv, double* __restrict__ force_divr,
+                                  double* __restrict__ pair_eng, int* __restrict__ evaluated) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double r2 = rsq[i], qq = qiqj[i];
+    double fd = 0.0, pe = 0.0;
+    int ok = 0;
+    if (!(r2 >= rcutsq || qq == 0.0 || rcut < 1.0e-12)) {
+        ok = 1;
+        // the reference calls sqrtf() on a double (FP32 square root)
+        const double r = (double)sqrtf((float)r2);
+        const double rinv = 1.0 / r;
+        double L = 0.0, negdLdr = 0.0;
+        if (!(r < 1.0e-12 || r > rcut)) {
+            double s = r / rcut;
+            s = s < 0.0 ? 0.0 : (s > 1.0 - 1.0e-9 ? 1.0 - 1.0e-9 : s);
+            unsigned int seg = (unsigned int)(s * (double)n_segs);
+            seg = seg >= (unsigned int)n_segs ? (unsigned int)n_segs - 1u : seg;
+            const double t = __dmul_rn(__dsub_rn(r, r_lo[seg]), dr_inv[seg]);
+            const double S = seg_horner5(screen + (size_t)seg * 5, t);
+            const double dS = seg_horner5(dscreen + (size_t)seg * 5, t);
+            const double i4r = INV_4PI_D / r;
+            const double i4r2 = i4r / r;
+            L = __dmul_rn(S, i4r);
+            negdLdr = __dsub_rn(__dmul_rn(S, i4r2), __dmul_rn(dS, i4r));
+        }
+        pe = __dmul_rn(qq, L);
+        fd = __dmul_rn(__dmul_rn(qq, negdLdr), rinv);
+    }
+    force_divr[i] = fd;
+    pair_eng[i] = pe;
+    evaluated[i] = ok;
+}
+
+// ============================================================================
+// host launch wrappers
+// ============================================================================
+template <int P>
+static cudaError_t launch_spread_p(const LaunchArgs& a, cudaStream_t st) {
+    using C = SpreadCfg<P>;
+    const int nb = (a.T + 2 * P - 2) / P;
+    const size_t NL = (size_t)nb * nb * nb * C::P3;
+    const size_t smem = NL * sizeof(float2) + (size_t)C::CH * P * 4 * 4 + C::CH * 4 + P * (MAX_D + 1) * 4;
+    if (a.configure_only)
+        return cudaFuncSetAttribute(k_spread<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (a.n_tiles == 0) return cudaSuccess;
+    k_spread<P><<<a.n_tiles, C::THREADS, smem, st>>>(a.tile_sys, a.sys, a.psets, a.T, a.D, a.tile_start, a.srec,
+                                                       a.srel, a.rho);
+    return cudaGetLastError();
+}
+
+template <int P>
+static cudaError_t launch_interp_p(const LaunchArgs& a, cudaStream_t st) {
+    const int E = a.T + P - 1;
+    const size_t smem = ((size_t)E * a.PP + P * (MAX_D + 1)) * 4;
+    if (a.configure_only)
+        return cudaFuncSetAttribute(k_interp<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (a.n_tiles == 0) return cudaSuccess;
+    k_interp<P><<<a.n_tiles, 128, smem, st>>>(a.tile_sys, a.sys, a.psets, a.T, a.D, a.PX, a.PP, a.tile_start,
+                                                a.perm, a.srec, a.srel, a.phi, a.force, a.acc);
+    return cudaGetLastError();
+}
+
+#define ESPB_DISPATCH_P(FN, P_, ...)                 \
+    switch (P_) {                                    \
+        case 2: return FN<2>(__VA_ARGS__);           \
+        case 3: return FN<3>(__VA_ARGS__);           \
+        case 4: return FN<4>(__VA_ARGS__);           \
+        case 5: return FN<5>(__VA_ARGS__);           \
+        case 6: return FN<6>(__VA_ARGS__);           \
+        case 7: return FN<7>(__VA_ARGS__);           \
+        case 8: return FN<8>(__VA_ARGS__);           \
+        case 9: return FN<9>(__VA_ARGS__);           \
+        case 10: return FN<10>(__VA_ARGS__);         \
+        case 11: return FN<11>(__VA_ARGS__);         \
+        case 12: return FN<12>(__VA_ARGS__);         \
+        default: return cudaErrorInvalidValue;       \
+    }
+
+cudaError_t launch_scan(const uint32_t* cnt, uint32_t* start, int n, cudaStream_t st) {
+    k_scan<<<1, 1024, 0, st>>>(cnt, start, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter(const int2* chunks, int n_chunks, const SysDev* sys, const uint32_t* key,
+                           const uint32_t* start, uint32_t* cnt, uint32_t* perm_u, cudaStream_t st) {
+    if (n_chunks) k_scatter<<<n_chunks, 256, 0, st>>>(chunks, sys, key, start, cnt, perm_u);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bin(const LaunchArgs& a, cudaStream_t st) {
+    if (a.n_chunks == 0) return cudaSuccess;
+    k_bin<<<a.n_chunks, 256, 0, st>>>(a.chunks, a.sys, a.P, a.T, a.pos_in, a.q_in, a.posq, a.trec, a.rel, a.key,
+                                      a.tile_count, a.acc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sort(const LaunchArgs& a, cudaStream_t st) {
+    k_scan<<<1, 1024, 0, st>>>(a.tile_count, a.tile_start, a.n_tiles);
+    if (a.n_chunks) k_scatter<<<a.n_chunks, 256, 0, st>>>(a.chunks, a.sys, a.key, a.tile_start, a.tile_count, a.perm_u);
+    if (a.n_tiles) k_tile_sort<<<a.n_tiles, 256, 0, st>>>(a.tile_start, a.perm_u, a.perm, a.trec, a.rel, a.srec, a.srel);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_spread(const LaunchArgs& a, cudaStream_t st) { ESPB_DISPATCH_P(launch_spread_p, a.P, a, st); }
+
+cudaError_t launch_interp(const LaunchArgs& a, cudaStream_t st) { ESPB_DISPATCH_P(launch_interp_p, a.P, a, st); }
+
+cudaError_t launch_fft(const LaunchArgs& a, cudaStream_t st) {
+    const size_t smx = 2 * FFT_MAX_N * FFT_SB_X * sizeof(float2);
+    const size_t smyz = 2 * FFT_MAX_N * FFT_B_YZ * sizeof(float2);
+    if (a.configure_only) {
+        cudaError_t e;
+        if ((e = cudaFuncSetAttribute(k_fftx_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx))) return e;
+        if ((e = cudaFuncSetAttribute(k_fftx_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx))) return e;
+        if ((e = cudaFuncSetAttribute(k_ffty<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz))) return e;
+        if ((e = cudaFuncSetAttribute(k_ffty<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz))) return e;
+        return cudaFuncSetAttribute(k_fftz_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz);
+    }
+    if (a.n_xitems) k_fftx_fwd<<<a.n_xitems, 256, smx, st>>>(a.xitems, a.sys, a.tw, a.rho, a.spec);
+    if (a.n_yitems) k_ffty<false><<<a.n_yitems, 256, smyz, st>>>(a.yitems, a.sys, a.tw, a.spec);
+    if (a.n_zitems) k_fftz_conv<<<a.n_zitems, 256, smyz, st>>>(a.zitems, a.sys, a.tw, a.gtab, a.spec, a.acc);
+    if (a.n_yitems) k_ffty<true><<<a.n_yitems, 256, smyz, st>>>(a.yitems, a.sys, a.tw, a.spec);
+    if (a.n_xitems) k_fftx_inv<<<a.n_xitems, 256, smx, st>>>(a.xitems, a.sys, a.tw, a.spec, a.phi);
+    return cudaGetLastError();
+}
+
+template <int TPP>
+static cudaError_t launch_pair_t(const LaunchArgs& a, cudaStream_t st) {
+#define ESPB_PAIR(NQ)                                                                                         \
+    k_pair<TPP, NQ><<<a.n_pchunks, 256, 0, st>>>(a.pchunks, a.sys, a.psets, a.posq, a.nl_head, a.nl_n, a.nl_list, \
+                                                 a.force, a.acc, a.accumulate, a.pc)
+    if (a.nq <= 8) ESPB_PAIR(8);
+    else if (a.nq <= 10) ESPB_PAIR(10);
+    else if (a.nq <= 12) ESPB_PAIR(12);
+    else if (a.nq <= 14) ESPB_PAIR(14);
+    else if (a.nq <= 16) ESPB_PAIR(16);
+    else if (a.nq <= 20) ESPB_PAIR(20);
+    else if (a.nq <= 24) ESPB_PAIR(24);
+    else ESPB_PAIR(32);
+#undef ESPB_PAIR
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pair(const LaunchArgs& a, cudaStream_t st) {
+    if (a.n_pchunks == 0) return cudaSuccess;
+    switch (a.tpp) {
+        case 4: return launch_pair_t<4>(a, st);
+        case 8: return launch_pair_t<8>(a, st);
+        case 16: return launch_pair_t<16>(a, st);
+        case 32: return launch_pair_t<32>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_finalize(const LaunchArgs& a, cudaStream_t st) {
+    k_finalize<<<(a.nsys + 127) / 128, 128, 0, st>>>(a.sys, a.psets, a.nsys, a.acc, a.energy, a.virial, a.add_bg);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_influence(const SysDev& S, const double* w1d, const double* tq, const double* wq, int nq,
+                             double rcut, double psi_floor, float2* gtab, cudaStream_t st) {
+    const long long total = (long long)S.nz * S.ny * S.nxh;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+    k_influence<<<blocks, 256, 0, st>>>(S, w1d, tq, wq, nq, rcut, psi_floor, gtab);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pswf_eval_pairs(int n, const double* rsq, const double* qiqj, double rcut, int n_segs,
+                                   const double* screen, const double* dscreen, const double* r_lo,
+                                   const double* dr_inv, double* force_divr, double* pair_eng, int* evaluated,
+                                   cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    k_pswf_eval_pairs<<<(n + 255) / 256, 256, 0, st>>>(n, rsq, qiqj, rcut, rcut * rcut, n_segs, screen, dscreen,
+                                                        r_lo, dr_inv, force_divr, pair_eng, evaluated);
+    return cudaGetLastError();
+}
+
+}  // namespace espb

@@ -1,0 +1,85 @@
+// Internal launch interface between the host orchestration (esp_host.cu)
+// and the kernels (esp_kernels.cu, esp_md.cu). Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "esp_common.cuh"
+
+namespace espb {
+
+constexpr int SORT_CAP = 2048;  // particles per tile sorted in shared memory
+
+// Split-polynomial coefficients of a batch, passed by value so the pair
+// kernel's FMAs read them from the kernel-parameter constant bank.
+struct PairCoef {
+    float q[MAX_QC];  // Q(v)
+    float d[MAX_QC];  // dQ/du in v
+};
+
+struct LaunchArgs {
+    PairCoef pc{};
+    const SysDev* sys = nullptr;
+    const ParamSet* psets = nullptr;
+    int nsys = 0, P = 8, T = 8, D = 10, PX = 0, PP = 0, tpp = 8, accumulate = 0, nq = 16;
+    const int2* chunks = nullptr;   // {sys, first particle}, 256 particles each
+    int n_chunks = 0;
+    const int2* pchunks = nullptr;  // {sys, first particle}, 256/tpp particles each
+    int n_pchunks = 0;
+    const int* tile_sys = nullptr;
+    int n_tiles = 0;
+    uint32_t* tile_count = nullptr;
+    uint32_t* tile_start = nullptr;
+    const float4* pos_in = nullptr;
+    const float* q_in = nullptr;
+    float4* posq = nullptr;
+    float4* trec = nullptr;
+    uint32_t* rel = nullptr;
+    uint32_t* key = nullptr;
+    uint32_t* perm_u = nullptr;
+    uint32_t* perm = nullptr;
+    float4* srec = nullptr;
+    uint32_t* srel = nullptr;
+    double* rho = nullptr;
+    float2* spec = nullptr;
+    float* phi = nullptr;
+    const float2* gtab = nullptr;
+    const float2* tw = nullptr;
+    const int4* xitems = nullptr;
+    int n_xitems = 0;
+    const int4* yitems = nullptr;
+    int n_yitems = 0;
+    const int4* zitems = nullptr;
+    int n_zitems = 0;
+    float4* force = nullptr;
+    double* acc = nullptr;
+    double* energy = nullptr;
+    double* virial = nullptr;
+    int add_bg = 1;
+    int configure_only = 0;  // set kernel attributes (plan time) instead of launching
+    const uint32_t* nl_head = nullptr;
+    const uint32_t* nl_n = nullptr;
+    const uint32_t* nl_list = nullptr;
+};
+
+cudaError_t launch_scan(const uint32_t* cnt, uint32_t* start, int n, cudaStream_t st);
+cudaError_t launch_scatter(const int2* chunks, int n_chunks, const SysDev* sys, const uint32_t* key,
+                           const uint32_t* start, uint32_t* cnt, uint32_t* perm_u, cudaStream_t st);
+cudaError_t launch_bin(const LaunchArgs& a, cudaStream_t st);
+cudaError_t launch_sort(const LaunchArgs& a, cudaStream_t st);
+cudaError_t launch_spread(const LaunchArgs& a, cudaStream_t st);
+cudaError_t launch_fft(const LaunchArgs& a, cudaStream_t st);
+cudaError_t launch_interp(const LaunchArgs& a, cudaStream_t st);
+cudaError_t launch_pair(const LaunchArgs& a, cudaStream_t st);
+cudaError_t launch_finalize(const LaunchArgs& a, cudaStream_t st);
+cudaError_t launch_influence(const SysDev& S, const double* w1d, const double* tq, const double* wq, int nq,
+                             double rcut, double psi_floor, float2* gtab, cudaStream_t st);
+cudaError_t launch_pswf_eval_pairs(int n, const double* rsq, const double* qiqj, double rcut, int n_segs,
+                                   const double* screen, const double* dscreen, const double* r_lo,
+                                   const double* dr_inv, double* force_divr, double* pair_eng, int* evaluated,
+                                   cudaStream_t st);
+
+}  // namespace espb

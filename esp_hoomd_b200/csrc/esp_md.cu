@@ -1,0 +1,190 @@
+// MD harness kernels: cell-list neighbour list and velocity-Verlet halves.
+// These stand in for the HOOMD-blue pieces the reference relies on
+// (NeighborList and the integrator; not vendored in the reference) so the
+// ESP path can run standalone.
+#include "esp_common.cuh"
+#include "esp_kernels.h"
+#include "esp_md.h"
+
+namespace espb {
+
+// Cell of each particle (cells of edge >= rlist, at least 3 per axis).
+__global__ void k_cell_bin(const int2* __restrict__ chunks, const SysDev* __restrict__ sys,
+                           const CellDev* __restrict__ cells, const float4* __restrict__ pos,
+                           uint32_t* __restrict__ ckey, uint32_t* __restrict__ ccount, float4* __restrict__ wpos) {
+    const int2 ch = chunks[blockIdx.x];
+    const SysDev& S = sys[ch.x];
+    const CellDev& C = cells[ch.x];
+    const int i = ch.y + threadIdx.x;
+    if (i >= S.p_off + S.N) return;
+    const float4 p = pos[i];
+    float x = p.x - S.Lx * floorf(p.x * S.inv_Lx);
+    float y = p.y - S.Ly * floorf(p.y * S.inv_Ly);
+    float z = p.z - S.Lz * floorf(p.z * S.inv_Lz);
+    if (x >= S.Lx) x -= S.Lx;
+    if (y >= S.Ly) y -= S.Ly;
+    if (z >= S.Lz) z -= S.Lz;
+    int cx = min((int)(x * C.inv_wx), C.ncx - 1), cy = min((int)(y * C.inv_wy), C.ncy - 1),
+        cz = min((int)(z * C.inv_wz), C.ncz - 1);
+    cx = max(cx, 0);
+    cy = max(cy, 0);
+    cz = max(cz, 0);
+    const uint32_t k = (uint32_t)(C.c_off + (cz * C.ncy + cy) * C.ncx + cx);
+    ckey[i] = k;
+    atomicAdd(&ccount[k], 1u);
+    wpos[i] = make_float4(x, y, z, __int_as_float(i));
+}
+
+// Deterministic order inside each cell (ascending particle index) and the
+// cell-sorted positions.
+__global__ void k_cell_sort(const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm_u,
+                            const float4* __restrict__ wpos, float4* __restrict__ cpos) {
+    __shared__ uint32_t sm[1024];
+    const uint32_t s0 = start[blockIdx.x];
+    const uint32_t n = start[blockIdx.x + 1] - s0;
+    if (n == 0) return;
+    const bool cached = n <= 1024u;
+    if (cached)
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sm[i] = perm_u[s0 + i];
+    __syncthreads();
+    const uint32_t* src = cached ? sm : perm_u + s0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint32_t v = src[i];
+        uint32_t r = 0;
+        for (uint32_t j = 0; j < n; ++j) r += (src[j] < v) ? 1u : 0u;
+        cpos[s0 + r] = wpos[v];
+    }
+}
+
+// One thread per particle, visited in cell order; scans the 27 surrounding
+// cells in a fixed order, so every row is deterministic.
+__global__ void k_nlist(const int* __restrict__ cell_sys, int n_cells_total, const SysDev* __restrict__ sys,
+                        const CellDev* __restrict__ cells, const uint32_t* __restrict__ cstart,
+                        const float4* __restrict__ cpos, float rlist2, int cap, uint32_t* __restrict__ head,
+                        uint32_t* __restrict__ nn, uint32_t* __restrict__ nl, int* __restrict__ overflow,
+                        const uint32_t* __restrict__ slot_cell, int total) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= total) return;
+    const uint32_t cidx = slot_cell[slot];
+    const int si = cell_sys[cidx];
+    const SysDev& S = sys[si];
+    const CellDev& C = cells[si];
+    const float4 pi = cpos[slot];
+    const int i = __float_as_int(pi.w);
+    const int lc = (int)cidx - C.c_off;
+    const int cx = lc % C.ncx, cy = (lc / C.ncx) % C.ncy, cz = lc / (C.ncx * C.ncy);
+    const long long hrow = (long long)C.nl_off + (long long)(i - S.p_off) * cap;
+    uint32_t cnt = 0;
+    // with fewer than 3 cells on an axis the -1/+1 neighbours coincide:
+    // visit each distinct cell once (offsets {0,1} for 2 cells, {0} for 1)
+    const int z0 = C.ncz >= 3 ? -1 : 0, z1 = C.ncz >= 3 ? 1 : C.ncz - 1;
+    const int y0 = C.ncy >= 3 ? -1 : 0, y1 = C.ncy >= 3 ? 1 : C.ncy - 1;
+    const int x0 = C.ncx >= 3 ? -1 : 0, x1 = C.ncx >= 3 ? 1 : C.ncx - 1;
+    for (int dz = z0; dz <= z1; ++dz) {
+        const int zz = (cz + dz + C.ncz) % C.ncz;
+        for (int dy = y0; dy <= y1; ++dy) {
+            const int yy = (cy + dy + C.ncy) % C.ncy;
+            for (int dx = x0; dx <= x1; ++dx) {
+                const int xx = (cx + dx + C.ncx) % C.ncx;
+                const uint32_t c = (uint32_t)(C.c_off + (zz * C.ncy + yy) * C.ncx + xx);
+                const uint32_t b = cstart[c], e = cstart[c + 1];
+                for (uint32_t s = b; s < e; ++s) {
+                    const float4 pj = cpos[s];
+                    const int j = __float_as_int(pj.w);
+                    if (j == i) continue;
+                    float ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
+                    ddx -= S.Lx * rintf(ddx * S.inv_Lx);
+                    ddy -= S.Ly * rintf(ddy * S.inv_Ly);
+                    ddz -= S.Lz * rintf(ddz * S.inv_Lz);
+                    if (ddx * ddx + ddy * ddy + ddz * ddz < rlist2) {
+                        if (cnt < (uint32_t)cap) nl[hrow + cnt] = (uint32_t)(j - S.p_off);
+                        ++cnt;
+                    }
+                }
+            }
+        }
+    }
+    head[i] = (uint32_t)hrow;
+    nn[i] = cnt;
+    if (cnt > (uint32_t)cap) atomicOr(overflow, 1);
+}
+
+__global__ void k_fill_slot_cell(const uint32_t* __restrict__ cstart, int n_cells, uint32_t* __restrict__ slot_cell) {
+    const int c = blockIdx.x;
+    if (c >= n_cells) return;
+    const uint32_t b = cstart[c], e = cstart[c + 1];
+    for (uint32_t s = b + threadIdx.x; s < e; s += blockDim.x) slot_cell[s] = (uint32_t)c;
+}
+
+__global__ void k_nve1(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, float4* __restrict__ pos,
+                       float4* __restrict__ vel, const float4* __restrict__ force, float dt) {
+    const int2 ch = chunks[blockIdx.x];
+    const SysDev& S = sys[ch.x];
+    const int i = ch.y + threadIdx.x;
+    if (i >= S.p_off + S.N) return;
+    float4 v = vel[i];
+    const float4 f = force[i];
+    const float h = 0.5f * dt / v.w;
+    v.x += h * f.x;
+    v.y += h * f.y;
+    v.z += h * f.z;
+    float4 p = pos[i];
+    p.x += dt * v.x;
+    p.y += dt * v.y;
+    p.z += dt * v.z;
+    p.x -= S.Lx * floorf(p.x * S.inv_Lx);
+    p.y -= S.Ly * floorf(p.y * S.inv_Ly);
+    p.z -= S.Lz * floorf(p.z * S.inv_Lz);
+    if (p.x >= S.Lx) p.x -= S.Lx;
+    if (p.y >= S.Ly) p.y -= S.Ly;
+    if (p.z >= S.Lz) p.z -= S.Lz;
+    pos[i] = p;
+    vel[i] = v;
+}
+
+__global__ void k_nve2(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, float4* __restrict__ vel,
+                       const float4* __restrict__ force, float dt) {
+    const int2 ch = chunks[blockIdx.x];
+    const SysDev& S = sys[ch.x];
+    const int i = ch.y + threadIdx.x;
+    if (i >= S.p_off + S.N) return;
+    float4 v = vel[i];
+    const float4 f = force[i];
+    const float h = 0.5f * dt / v.w;
+    v.x += h * f.x;
+    v.y += h * f.y;
+    v.z += h * f.z;
+    vel[i] = v;
+}
+
+cudaError_t launch_nlist(const NlistArgs& a, cudaStream_t st) {
+    if (a.n_chunks == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(a.overflow, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    k_cell_bin<<<a.n_chunks, 256, 0, st>>>(a.chunks, a.sys, a.cells, a.pos, a.ckey, a.ccount, a.wpos);
+    if ((e = launch_scan(a.ccount, a.cstart, a.n_cells, st)) != cudaSuccess) return e;
+    if ((e = launch_scatter(a.chunks, a.n_chunks, a.sys, a.ckey, a.cstart, a.ccount, a.perm_u, st)) != cudaSuccess)
+        return e;
+    k_cell_sort<<<a.n_cells, 256, 0, st>>>(a.cstart, a.perm_u, a.wpos, a.cpos);
+    k_fill_slot_cell<<<a.n_cells, 64, 0, st>>>(a.cstart, a.n_cells, a.slot_cell);
+    k_nlist<<<(a.total + 127) / 128, 128, 0, st>>>(a.cell_sys, a.n_cells, a.sys, a.cells, a.cstart, a.cpos,
+                                                   a.rlist2, a.cap, a.head, a.nn, a.nl, a.overflow, a.slot_cell,
+                                                   a.total);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_nve1(const int2* chunks, int n_chunks, const SysDev* sys, float4* pos, float4* vel,
+                        const float4* force, float dt, cudaStream_t st) {
+    if (n_chunks == 0) return cudaSuccess;
+    k_nve1<<<n_chunks, 256, 0, st>>>(chunks, sys, pos, vel, force, dt);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_nve2(const int2* chunks, int n_chunks, const SysDev* sys, float4* vel, const float4* force,
+                        float dt, cudaStream_t st) {
+    if (n_chunks == 0) return cudaSuccess;
+    k_nve2<<<n_chunks, 256, 0, st>>>(chunks, sys, vel, force, dt);
+    return cudaGetLastError();
+}
+
+}  // namespace espb

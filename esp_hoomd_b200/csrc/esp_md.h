@@ -1,0 +1,47 @@
+// Internal launch interface of the MD harness kernels (esp_md.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "esp_common.cuh"
+
+namespace espb {
+
+struct CellDev {
+    int ncx, ncy, ncz, c_off;  // cell grid and first cell
+    float inv_wx, inv_wy, inv_wz;
+    long long nl_off;          // first neighbour-list entry of this system
+};
+
+struct NlistArgs {
+    const int2* chunks = nullptr;
+    int n_chunks = 0;
+    const SysDev* sys = nullptr;
+    const CellDev* cells = nullptr;
+    const int* cell_sys = nullptr;
+    int n_cells = 0;
+    int total = 0;
+    const float4* pos = nullptr;
+    uint32_t* ckey = nullptr;
+    uint32_t* ccount = nullptr;
+    uint32_t* cstart = nullptr;
+    uint32_t* perm_u = nullptr;
+    float4* wpos = nullptr;
+    float4* cpos = nullptr;
+    uint32_t* slot_cell = nullptr;
+    float rlist2 = 0.f;
+    int cap = 0;
+    uint32_t* head = nullptr;
+    uint32_t* nn = nullptr;
+    uint32_t* nl = nullptr;
+    int* overflow = nullptr;
+};
+
+cudaError_t launch_nlist(const NlistArgs& a, cudaStream_t st);
+cudaError_t launch_nve1(const int2* chunks, int n_chunks, const SysDev* sys, float4* pos, float4* vel,
+                        const float4* force, float dt, cudaStream_t st);
+cudaError_t launch_nve2(const int2* chunks, int n_chunks, const SysDev* sys, float4* vel, const float4* force,
+                        float dt, cudaStream_t st);
+
+}  // namespace espb

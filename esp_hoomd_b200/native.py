@@ -1,0 +1,213 @@
+"""Python handles over the native ESP contexts (device buffers are torch
+CUDA tensors; torch is only the allocator and stream provider here)."""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import EspInfo, EspParams, check, get_lib
+
+
+def make_params(order: int = 8, rcut: float = 3.0, kappa: float = 0.0, mesh: Optional[Sequence[int]] = None,
+                target_error: float = 1e-5, window_c: float = 0.0, window_degree: int = 0, tile: int = 0,
+                threads_per_particle: int = 0, alpha: float = 0.0, n_table: int = 512) -> EspParams:
+    p = EspParams()
+    check(get_lib().esp_params_default(ctypes.byref(p)), "esp_params_default")
+    p.order = int(order)
+    p.rcut = float(rcut)
+    p.kappa = float(kappa)
+    p.alpha = float(alpha)
+    p.n_table = int(n_table)
+    if mesh is not None:
+        p.nx, p.ny, p.nz = (int(m) for m in mesh)
+    p.target_error = float(target_error)
+    p.window_c = float(window_c)
+    p.window_degree = int(window_degree)
+    p.tile = int(tile)
+    p.threads_per_particle = int(threads_per_particle)
+    return p
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("device tensor expected")
+    if not t.is_contiguous():
+        raise ValueError("contiguous tensor expected")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def info_dict(inf: EspInfo) -> dict:
+    return {f[0]: getattr(inf, f[0]) for f in EspInfo._fields_}
+
+
+class Context:
+    """One system (plain path): wraps esp_create / esp_compute."""
+
+    def __init__(self, params: EspParams, box: Sequence[float], N: int):
+        self._lib = get_lib()
+        self._h = ctypes.c_void_p()
+        self.params = params
+        self.box = tuple(float(b) for b in box)
+        check(self._lib.esp_create(ctypes.byref(params), *self.box, int(N), ctypes.byref(self._h)), "esp_create")
+
+    def compute(self, pos4: torch.Tensor, q: torch.Tensor, force4: torch.Tensor, energy: Optional[torch.Tensor] = None,
+                virial: Optional[torch.Tensor] = None, nlist=None, flags: int = _lib.ESP_ALL, stream=None) -> None:
+        head, nn, nl = nlist if nlist is not None else (None, None, None)
+        check(self._lib.esp_compute(self._h, _stream(stream), _ptr(pos4), _ptr(q), int(pos4.shape[0]), _ptr(head),
+                                    _ptr(nn), _ptr(nl), _ptr(force4), _ptr(energy), _ptr(virial), int(flags)),
+              "esp_compute")
+
+    def spread(self, pos4: torch.Tensor, q: torch.Tensor, stream=None) -> torch.Tensor:
+        """Charge mesh rho[nz, ny, nx] (float64) of the bin+sort+spread stages."""
+        inf = self.info()
+        rho = torch.empty((inf["nz"], inf["ny"], inf["nx"]), dtype=torch.float64, device=pos4.device)
+        check(self._lib.esp_spread(self._h, _stream(stream), _ptr(pos4), _ptr(q), int(pos4.shape[0]), _ptr(rho)),
+              "esp_spread")
+        return rho
+
+    def sort_state(self, N: int, device="cuda", stream=None):
+        """(key[N], perm[N]) of the last call (uint32 stored in int32 tensors)."""
+        key = torch.empty(N, dtype=torch.int32, device=device)
+        perm = torch.empty(N, dtype=torch.int32, device=device)
+        check(self._lib.esp_get_sort(self._h, _stream(stream), _ptr(key), _ptr(perm)), "esp_get_sort")
+        return key, perm
+
+    def potential(self, stream=None) -> torch.Tensor:
+        inf = self.info()
+        phi = torch.empty((inf["nz"], inf["ny"], inf["nx"]), dtype=torch.float32, device="cuda")
+        check(self._lib.esp_get_potential(self._h, _stream(stream), _ptr(phi)), "esp_get_potential")
+        return phi
+
+    def set_params(self, params: EspParams) -> None:
+        self.params = params
+        check(self._lib.esp_set_params(self._h, ctypes.byref(params)), "esp_set_params")
+
+    def set_box(self, box: Sequence[float]) -> None:
+        self.box = tuple(float(b) for b in box)
+        check(self._lib.esp_set_box(self._h, *self.box), "esp_set_box")
+
+    def invalidate(self) -> None:
+        check(self._lib.esp_invalidate(self._h), "esp_invalidate")
+
+    def info(self) -> dict:
+        inf = EspInfo()
+        check(self._lib.esp_get_info(self._h, ctypes.byref(inf)), "esp_get_info")
+        return info_dict(inf)
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.esp_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many independent systems evaluated by one launch per stage."""
+
+    def __init__(self, params: EspParams, N: Sequence[int], boxes: Sequence[Sequence[float]],
+                 meshes: Optional[Sequence[Sequence[int]]] = None):
+        self._lib = get_lib()
+        self._h = ctypes.c_void_p()
+        self.N = np.asarray(N, dtype=np.int32)
+        self.boxes = np.asarray(boxes, dtype=np.float64).reshape(-1, 3)
+        self.offsets = np.concatenate([[0], np.cumsum(self.N)]).astype(np.int64)
+        m = None if meshes is None else np.ascontiguousarray(np.asarray(meshes, dtype=np.int32).reshape(-1, 3))
+        self._m = m
+        check(self._lib.esp_batch_create(ctypes.byref(params), int(self.N.size),
+                                         self.N.ctypes.data_as(ctypes.c_void_p),
+                                         self.boxes.ctypes.data_as(ctypes.c_void_p),
+                                         None if m is None else m.ctypes.data_as(ctypes.c_void_p),
+                                         ctypes.byref(self._h)), "esp_batch_create")
+
+    @property
+    def nsys(self) -> int:
+        return int(self.N.size)
+
+    @property
+    def total(self) -> int:
+        return int(self.offsets[-1])
+
+    def compute(self, pos4, q, force4, energy=None, virial=None, nlist=None, flags: int = _lib.ESP_ALL,
+                stream=None) -> None:
+        head, nn, nl = nlist if nlist is not None else (None, None, None)
+        check(self._lib.esp_batch_compute(self._h, _stream(stream), _ptr(pos4), _ptr(q), _ptr(head), _ptr(nn),
+                                          _ptr(nl), _ptr(force4), _ptr(energy), _ptr(virial), int(flags)),
+              "esp_batch_compute")
+
+    def build_nlist(self, pos4, rlist: float, cap: int, head, nn, nl, stream=None) -> None:
+        check(self._lib.esp_batch_build_nlist(self._h, _stream(stream), _ptr(pos4), float(rlist), int(cap),
+                                              _ptr(head), _ptr(nn), _ptr(nl)), "esp_batch_build_nlist")
+
+    def nve_step1(self, pos4, vel4, force4, dt: float, stream=None) -> None:
+        check(self._lib.esp_batch_nve_step1(self._h, _stream(stream), _ptr(pos4), _ptr(vel4), _ptr(force4),
+                                            float(dt)), "esp_batch_nve_step1")
+
+    def nve_step2(self, vel4, force4, dt: float, stream=None) -> None:
+        check(self._lib.esp_batch_nve_step2(self._h, _stream(stream), _ptr(vel4), _ptr(force4), float(dt)),
+              "esp_batch_nve_step2")
+
+    def md_run(self, pos4, vel4, q, force4, energy, virial, nlist, nsteps: int, dt: float, use_graph: bool = True,
+               stream=None) -> None:
+        head, nn, nl = nlist
+        check(self._lib.esp_batch_md_run(self._h, _stream(stream), _ptr(pos4), _ptr(vel4), _ptr(q), _ptr(head),
+                                         _ptr(nn), _ptr(nl), _ptr(force4), _ptr(energy), _ptr(virial), int(nsteps),
+                                         float(dt), int(bool(use_graph))), "esp_batch_md_run")
+
+    def set_timing(self, on: bool) -> None:
+        check(self._lib.esp_batch_set_timing(self._h, int(bool(on))), "esp_batch_set_timing")
+
+    def stage_times(self) -> dict:
+        """{stage: (total ms, launches)} since timing was enabled or last read."""
+        ms = np.zeros(len(_lib.STAGES), dtype=np.float64)
+        cnt = np.zeros(len(_lib.STAGES), dtype=np.int64)
+        check(self._lib.esp_batch_stage_times(self._h, ms.ctypes.data_as(ctypes.c_void_p),
+                                              cnt.ctypes.data_as(ctypes.c_void_p)), "esp_batch_stage_times")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_lib.STAGES)}
+
+    def info(self, s: int) -> dict:
+        inf = EspInfo()
+        check(self._lib.esp_batch_get_info(self._h, int(s), ctypes.byref(inf)), "esp_batch_get_info")
+        return info_dict(inf)
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.esp_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pswf_eval_pairs(rsq: torch.Tensor, qiqj: torch.Tensor, rcut: float, table, stream=None):
+    """Reference-format evaluator over n pairs on the GPU (FP64).
+
+    ``table`` holds device float64 tensors screen, dscreen, r_lo, dr_inv.
+    Returns (force_divr, pair_eng, evaluated)."""
+    n = int(rsq.numel())
+    fd = torch.empty(n, dtype=torch.float64, device=rsq.device)
+    pe = torch.empty_like(fd)
+    ev = torch.empty(n, dtype=torch.int32, device=rsq.device)
+    screen, dscreen, r_lo, dr_inv = table
+    check(get_lib().esp_pswf_eval_pairs(_stream(stream), n, _ptr(rsq), _ptr(qiqj), float(rcut), int(r_lo.numel()),
+                                        _ptr(screen), _ptr(dscreen), _ptr(r_lo), _ptr(dr_inv), _ptr(fd), _ptr(pe),
+                                        _ptr(ev)), "esp_pswf_eval_pairs")
+    return fd, pe, ev

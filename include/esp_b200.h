@@ -1,0 +1,201 @@
+/*
+ * esp_b200.h -- C ABI of the Blackwell (sm_100a) ESP electrostatics path.
+ *
+ * ESP = Ewald Summation with Prolates: the long-range Coulomb part on a
+ * mesh (PSWF spreading, 3D FFT, influence multiply, inverse FFT,
+ * interpolation) plus the short-range EvaluatorPairPSWF term over a
+ * neighbour list. Units follow the reference: E = q_i q_j / (4 pi r).
+ *
+ * Conventions (all entry points):
+ *  - plain pointers and sizes only; device pointers are CUDA device memory
+ *    owned by the caller; `stream` is a cudaStream_t passed as void*;
+ *  - positions are float4 per particle laid out as 4 floats (x, y, z, w),
+ *    w ignored (HOOMD keeps the type there), any periodic image;
+ *  - forces are written as 4 floats per particle: fx, fy, fz, per-particle
+ *    energy (the Scalar4 output contract of HOOMD's ForceCompute::m_force);
+ *  - neighbour lists use HOOMD's layout: the neighbours of particle i are
+ *    nlist[head[i] + k], k < n_neigh[i], full (both i-j and j-i) lists;
+ *  - virial: 6 doubles xx, xy, xz, yy, yz, zz with W_ab = -dE/d eps_ab;
+ *  - every call returns 0 on success or a negative ESP_ERR_* code and
+ *    throws nothing; esp_last_error() gives the message. Calls are
+ *    asynchronous on `stream` and not thread-safe per context.
+ *
+ * The reference interfaces each entry point replaces are cited per call
+ * (paths relative to the reference repository slweng0321/ESP_HOOMD).
+ */
+#ifndef ESP_B200_H_
+#define ESP_B200_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ESP_OK 0
+#define ESP_ERR_INVALID (-1)     /* bad argument */
+#define ESP_ERR_CUDA (-2)        /* CUDA runtime error */
+#define ESP_ERR_ALLOC (-3)       /* device allocation failed */
+#define ESP_ERR_UNSUPPORTED (-4) /* parameter outside the supported set */
+#define ESP_ERR_OVERFLOW (-5)    /* neighbour list capacity exceeded */
+
+/* compute flags */
+#define ESP_LONG_RANGE 1  /* mesh part + self + background (esp.Spectral) */
+#define ESP_SHORT_RANGE 2 /* pair part over the neighbour list (esp.Local) */
+#define ESP_ALL 3
+
+typedef struct esp_ctx esp_ctx;
+typedef struct esp_batch esp_batch;
+
+/* Parameters. Mirrors ESPForceCompute::setParams(nx, ny, nz, order, kappa,
+ * rcut, alpha, n_table) of src/ESPForceCompute.h:99-106, plus the knobs of
+ * the runtime table generator that replaces src/PSWF_Coeffs.h:24-27. */
+typedef struct esp_params {
+    int nx, ny, nz;      /* mesh; 0 = chosen from target_error */
+    int order;           /* PSWF support P in grid points, 2..12 */
+    double kappa;        /* split bandwidth in 1/length: c = kappa * rcut; 0 = auto */
+    double rcut;         /* real-space cutoff r_c (> 0) */
+    double alpha;        /* Debye screening; only 0 is supported */
+    int n_table;         /* segments of the introspection table */
+    double target_error; /* relative RMS force error the auto choices aim at */
+    double window_c;     /* window bandwidth c_w; 0 = auto */
+    int window_degree;   /* window polynomial degree; 0 = auto */
+    int tile;            /* tile edge in mesh cells; 0 = auto */
+    int threads_per_particle; /* pair kernel lanes per particle: 4, 8, 16, 32; 0 = auto */
+} esp_params;
+
+/* Resolved configuration of a context or of one system of a batch. */
+typedef struct esp_info {
+    int nx, ny, nz, order, tile, window_degree;
+    double c_split, c_window, rcut;
+    double lambda0, m2;      /* Q(0) and int_0^1 psi t^2 / int_0^1 psi */
+    double split_fit_err, window_fit_err;
+    long long device_bytes;  /* device memory held by the context */
+} esp_info;
+
+/* Fill `p` with defaults (order 8, rcut 3.0, target 1e-5, everything else auto). */
+int esp_params_default(esp_params* p);
+
+/* Message of the last failed call on this thread (ctx may be NULL). */
+const char* esp_last_error(void);
+
+/* ---------------------------------------------------------------- single system
+ * Replaces ESPForceComputeGPU (src/ESPForceComputeGPU.h:55-131): the
+ * constructor + initializeFFT() + setupCoeffs() (src/ESPForceComputeGPU.cc:47-214,
+ * src/ESPForceCompute.cc:179-198). Orthorhombic box Lx, Ly, Lz. */
+int esp_create(const esp_params* p, double Lx, double Ly, double Lz, int N, esp_ctx** out);
+
+/* ESPForceCompute::setParams (src/ESPForceCompute.cc:71-89): new parameters,
+ * tables rebuilt on the next compute. */
+int esp_set_params(esp_ctx* ctx, const esp_params* p);
+
+/* Box change (HOOMD box resize); re-plans the influence table. */
+int esp_set_box(esp_ctx* ctx, double Lx, double Ly, double Lz);
+
+/* ESPForceCompute::invalidate (src/ESPForceCompute.h:120): rebuild all
+ * tables on the next compute. */
+int esp_invalidate(esp_ctx* ctx);
+
+/* One evaluation: ESPForceCompute::computeForces (src/ESPForceCompute.cc:96-127)
+ * with its GPU stages (src/ESPForceComputeGPU.cu:206-373) when
+ * flags & ESP_LONG_RANGE, and PotentialPairGPU<EvaluatorPairPSWF>
+ * (src/module.cc:79, src/EvaluatorPairPSWF.h:274-295) when
+ * flags & ESP_SHORT_RANGE. Overwrites force[4N]; writes energy[1] and
+ * virial[6] (device doubles, may be NULL). The neighbour-list pointers may
+ * be NULL without ESP_SHORT_RANGE. */
+int esp_compute(esp_ctx* ctx, void* stream, const float* pos4, const float* charge, int N,
+                const unsigned* head, const unsigned* n_neigh, const unsigned* nlist,
+                float* force4, double* energy, double* virial6, int flags);
+
+int esp_get_info(const esp_ctx* ctx, esp_info* info);
+int esp_destroy(esp_ctx* ctx);
+
+/* Stage outputs, for validation of single stages (no reference
+ * counterpart: the reference exposes only the final forces).
+ * esp_spread: bin + sort + spreading of (pos4, charge) into the caller's
+ * FP64 charge mesh rho[nz*ny*nx] (x fastest; zeroed first), the charge
+ * assignment of src/ESPForceComputeGPU.cu:206-272.
+ * esp_get_sort: tile key of every particle (key[N], input order) and the
+ * stable permutation (perm[N], sorted slot -> particle) of the last call.
+ * esp_get_potential: the potential mesh phi[nz*ny*nx] of the last
+ * long-range evaluation. */
+int esp_spread(esp_ctx* ctx, void* stream, const float* pos4, const float* charge, int N, double* rho);
+int esp_get_sort(const esp_ctx* ctx, void* stream, unsigned* key, unsigned* perm);
+int esp_get_potential(const esp_ctx* ctx, void* stream, float* phi);
+
+/* ---------------------------------------------------------------- batches
+ * Many independent systems evaluated by one launch per stage (no reference
+ * counterpart; the reference evaluates one HOOMD system per ForceCompute).
+ * System s holds N[s] particles at offset sum_{r<s} N[r] of the
+ * concatenated arrays; boxes[3s..3s+2] its box; mesh[3s..] its mesh or
+ * NULL for automatic meshes. Neighbour indices are local to each system;
+ * head[] values index the concatenated nlist array. energy[nsys],
+ * virial[6*nsys]. */
+int esp_batch_create(const esp_params* p, int nsys, const int* N, const double* boxes, const int* mesh,
+                     esp_batch** out);
+int esp_batch_compute(esp_batch* b, void* stream, const float* pos4, const float* charge, const unsigned* head,
+                      const unsigned* n_neigh, const unsigned* nlist, float* force4, double* energy,
+                      double* virial6, int flags);
+int esp_batch_get_info(const esp_batch* b, int sys, esp_info* info);
+int esp_batch_total_particles(const esp_batch* b);
+int esp_batch_destroy(esp_batch* b);
+
+/* ---------------------------------------------------------------- evaluator
+ * EvaluatorPairPSWF::evalForceAndEnergy (src/EvaluatorPairPSWF.h:274-295)
+ * with detail::pswf_eval_L (src/EvaluatorPairPSWF.h:113-143) over n pairs,
+ * reading a PSWF_Coeffs.h-layout segment table (src/PSWF_Coeffs.h:29-30,
+ * 4130, 8229, 8915): screen/dscreen [5*n_segs], r_lo/dr_inv [n_segs]. All
+ * arrays are device doubles; evaluated[i] is the evaluator's return value.
+ * energy_shift is not applied (the reference's V_cut is 0). */
+int esp_pswf_eval_pairs(void* stream, int n, const double* rsq, const double* qiqj, double rcut, int n_segs,
+                        const double* screen, const double* dscreen, const double* r_lo, const double* dr_inv,
+                        double* force_divr, double* pair_eng, int* evaluated);
+
+/* ---------------------------------------------------------------- MD harness
+ * The pieces HOOMD would supply (neighbour list, NVE integrator), for
+ * standalone runs and benchmarks. Neighbour list: cell list from the
+ * particle positions, full list of all pairs with r < rlist, fixed row
+ * capacity `cap` (head[i] = offset of system s + local i * cap); returns
+ * ESP_ERR_OVERFLOW when a row exceeds cap (n_neigh then holds the true
+ * counts). Synchronises `stream` to read the overflow flag. */
+int esp_batch_build_nlist(esp_batch* b, void* stream, const float* pos4, double rlist, int cap, unsigned* head,
+                          unsigned* n_neigh, unsigned* nlist);
+
+/* Velocity-Verlet halves on the concatenated arrays: vel4 = (vx, vy, vz,
+ * mass). step1: v += dt/2 F/m; x += dt v (wrapped into the box).
+ * step2: v += dt/2 F/m. */
+int esp_batch_nve_step1(esp_batch* b, void* stream, float* pos4, float* vel4, const float* force4, double dt);
+int esp_batch_nve_step2(esp_batch* b, void* stream, float* vel4, const float* force4, double dt);
+
+/* nsteps velocity-Verlet steps of every system of the batch: per step
+ * step1, a full evaluation (ESP_ALL) at the new positions into force4 /
+ * energy / virial, step2. force4 must hold the forces of the current
+ * positions on entry. With use_graph != 0 one step is captured in a CUDA
+ * graph on first use (and whenever a pointer or dt changes) and replayed.
+ * The neighbour list is used as given (no rebuild). */
+int esp_batch_md_run(esp_batch* b, void* stream, float* pos4, float* vel4, const float* charge, const unsigned* head,
+                     const unsigned* n_neigh, const unsigned* nlist, float* force4, double* energy, double* virial6,
+                     int nsteps, double dt, int use_graph);
+
+/* ---------------------------------------------------------------- timing
+ * Per-stage CUDA-event timing on the launching stream (no counterpart in
+ * the reference, whose Autotuner times kernels for block-size selection,
+ * src/ESPForceComputeGPU.cc:52-61). Enabling resets the totals; events are
+ * recorded without synchronising; esp_batch_stage_times synchronises once,
+ * returns total milliseconds and launch counts per stage, and resets.
+ * Graph replays are not timed per stage. */
+#define ESP_STAGE_BIN 0
+#define ESP_STAGE_SORT 1
+#define ESP_STAGE_SPREAD 2
+#define ESP_STAGE_FFT 3
+#define ESP_STAGE_INTERP 4
+#define ESP_STAGE_PAIR 5
+#define ESP_STAGE_NLIST 6
+#define ESP_STAGE_NVE 7
+#define ESP_N_STAGES 8
+int esp_batch_set_timing(esp_batch* b, int on);
+int esp_batch_stage_times(esp_batch* b, double* ms, long long* counts);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ESP_B200_H_ */

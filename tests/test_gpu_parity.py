@@ -1,0 +1,203 @@
+"""GPU parity: every stage of the sm_100a path, called through the C ABI,
+against the FP64 oracle on the same seeded inputs.
+
+Tolerances (FP32 bulk arithmetic, FP64 reductions):
+* sort keys and permutation: bit-exact;
+* charge mesh: max |d rho| <= 2e-6 max |rho|;
+* potential mesh: max |d phi| <= 5e-6 max |phi|;
+* forces: relative RMS difference <= 5e-6; energy relative <= 2e-6;
+  virial max abs <= 1e-5 max |W|;
+* physics: relative RMS force error vs FP64 Ewald <= 1e-5 at the default
+  target (the north-star accuracy bar).
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from esp_hoomd_b200 import native, systems, tables  # noqa: E402
+from esp_hoomd_b200._lib import ESP_LONG_RANGE, ESP_SHORT_RANGE, ESP_ALL, EspError  # noqa: E402
+from oracle import esp_ref as R  # noqa: E402
+from oracle.ewald import ewald  # noqa: E402
+
+
+def _dev(a, dtype):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device="cuda")
+
+
+def _upload(sysm):
+    pos4 = np.zeros((sysm.N, 4), dtype=np.float32)
+    pos4[:, :3] = sysm.pos
+    return _dev(pos4, torch.float32), _dev(sysm.q, torch.float32)
+
+
+def _oracle_params(info, box):
+    return tables.ESPParams(mesh=(info["nx"], info["ny"], info["nz"]), box=tuple(box), rcut=info["rcut"],
+                            split=tables.split_cached(info["c_split"]),
+                            window=tables.window_cached(info["order"], info["c_window"], info["window_degree"]))
+
+
+def _nlist_dev(head, cnt, lst):
+    return (_dev(head.astype(np.int32), torch.int32), _dev(cnt.astype(np.int32), torch.int32),
+            _dev(lst.astype(np.int32), torch.int32))
+
+
+@pytest.fixture(scope="module")
+def rs8():
+    s = systems.rocksalt(8, seed=1001)
+    s.pos = s.pos.astype(np.float32).astype(np.float64)  # the device sees float32 positions
+    return s
+
+
+def test_sort_bit_exact(rs8):
+    ctx = native.Context(native.make_params(), rs8.box, rs8.N)
+    pos4, q = _upload(rs8)
+    ctx.spread(pos4, q)
+    key, perm = ctx.sort_state(rs8.N)
+    torch.cuda.synchronize()
+    inf = ctx.info()
+    k_ref, p_ref = R.bin_sort(rs8.pos, rs8.box, (inf["nx"], inf["ny"], inf["nz"]), inf["order"], inf["tile"])
+    assert np.array_equal(key.cpu().numpy().astype(np.uint32), k_ref)
+    assert np.array_equal(perm.cpu().numpy().astype(np.uint32), p_ref)
+
+
+def test_spread_matches_oracle(rs8):
+    ctx = native.Context(native.make_params(), rs8.box, rs8.N)
+    pos4, q = _upload(rs8)
+    rho = ctx.spread(pos4, q).cpu().numpy()
+    prm = _oracle_params(ctx.info(), rs8.box)
+    ref = R.spread(rs8.pos, rs8.q, prm)
+    assert np.abs(rho - ref).max() <= 2e-6 * np.abs(ref).max()
+    # spreading conserves charge up to the window normalisation
+    assert abs(rho.sum() - ref.sum()) <= 1e-6 * np.abs(ref).sum()
+
+
+def test_potential_and_forces_match_oracle(rs8):
+    ctx = native.Context(native.make_params(), rs8.box, rs8.N)
+    pos4, q = _upload(rs8)
+    head, cnt, lst = R.neighbor_list(rs8.pos, rs8.box, ctx.info()["rcut"])
+    nl = _nlist_dev(head, cnt, lst)
+    force = torch.zeros((rs8.N, 4), dtype=torch.float32, device="cuda")
+    energy = torch.zeros(1, dtype=torch.float64, device="cuda")
+    virial = torch.zeros(6, dtype=torch.float64, device="cuda")
+    ctx.compute(pos4, q, force, energy, virial, nlist=nl)
+    phi = ctx.potential().cpu().numpy()
+    torch.cuda.synchronize()
+    prm = _oracle_params(ctx.info(), rs8.box)
+    E, F, W, parts = R.esp(rs8.pos, rs8.q, prm, nlist=(head, cnt, lst), return_parts=True)
+    assert np.abs(phi - parts["phi"]).max() <= 5e-6 * np.abs(parts["phi"]).max()
+    f = force.cpu().numpy()
+    assert R.rel_rms(f[:, :3].astype(np.float64), F) <= 5e-6
+    assert abs(energy.item() - E) <= 2e-6 * abs(E)
+    assert np.abs(virial.cpu().numpy() - W).max() <= 1e-5 * np.abs(W).max()
+    # per-particle energies sum to the total minus the background term
+    assert abs(f[:, 3].astype(np.float64).sum() - (E - parts["E_bg"])) <= 5e-6 * abs(E)
+
+
+def test_accuracy_vs_ewald(rs8):
+    ctx = native.Context(native.make_params(target_error=1e-5), rs8.box, rs8.N)
+    pos4, q = _upload(rs8)
+    head, cnt, lst = R.neighbor_list(rs8.pos, rs8.box, 3.0)
+    force = torch.zeros((rs8.N, 4), dtype=torch.float32, device="cuda")
+    energy = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ctx.compute(pos4, q, force, energy, nlist=_nlist_dev(head, cnt, lst))
+    E0, F0, _ = ewald(rs8.pos, rs8.q, rs8.box)
+    f = force.cpu().numpy()[:, :3].astype(np.float64)
+    assert R.rel_rms(f, F0) <= 1e-5
+    assert abs(energy.item() - E0) <= 1e-5 * abs(E0)
+
+
+def test_long_plus_short_equals_all(rs8):
+    ctx = native.Context(native.make_params(), rs8.box, rs8.N)
+    pos4, q = _upload(rs8)
+    nl = _nlist_dev(*R.neighbor_list(rs8.pos, rs8.box, 3.0))
+    out = {}
+    for flags in (ESP_LONG_RANGE, ESP_SHORT_RANGE, ESP_ALL):
+        f = torch.zeros((rs8.N, 4), dtype=torch.float32, device="cuda")
+        e = torch.zeros(1, dtype=torch.float64, device="cuda")
+        ctx.compute(pos4, q, f, e, nlist=nl, flags=flags)
+        out[flags] = (f.cpu().numpy().astype(np.float64), e.item())
+    fl, el = out[ESP_LONG_RANGE]
+    fs, es = out[ESP_SHORT_RANGE]
+    fa, ea = out[ESP_ALL]
+    assert np.abs(fl + fs - fa).max() <= 1e-6 * np.abs(fa).max() + 1e-7
+    assert abs(el + es - ea) <= 1e-9 * abs(ea)
+
+
+def test_reference_evaluator_bit_exact(golden_dir):
+    g = np.load(golden_dir + "/pswf_eval_golden.npz")
+    t = np.load(golden_dir + "/pswf_coeffs_shipped.npz")
+    table = tuple(_dev(t[k], torch.float64) for k in ("screen", "dscreen", "r_lo", "dr_inv"))
+    fd, pe, ev = native.pswf_eval_pairs(_dev(g["rsq"], torch.float64), _dev(g["qiqj"], torch.float64),
+                                        float(g["rcut"]), table)
+    torch.cuda.synchronize()
+    assert np.array_equal(ev.cpu().numpy(), g["evaluated"])
+    # r = 0 gives the reference's own NaN (0 * inf), compared as equal
+    assert np.array_equal(fd.cpu().numpy(), g["force_divr"], equal_nan=True)
+    assert np.array_equal(pe.cpu().numpy(), g["pair_eng"], equal_nan=True)
+
+
+def test_batch_alone_equals_in_mix():
+    sys_list = [systems.rocksalt(n, seed=300 + n) for n in (8, 10, 12)]
+    params = native.make_params()
+    N = [s.N for s in sys_list]
+    boxes = [s.box for s in sys_list]
+    b = native.Batch(params, N, boxes)
+    pos4 = np.zeros((sum(N), 4), dtype=np.float32)
+    pos4[:, :3] = np.concatenate([s.pos for s in sys_list])
+    q = np.concatenate([s.q for s in sys_list])
+    nls = [R.neighbor_list(s.pos.astype(np.float32).astype(np.float64), s.box, 3.0) for s in sys_list]
+    heads, cnts, lsts, off = [], [], [], 0
+    for h, c, l in nls:
+        heads.append(h.astype(np.int64) + off)
+        cnts.append(c)
+        lsts.append(l)
+        off += l.size
+    nl = _nlist_dev(np.concatenate(heads), np.concatenate(cnts), np.concatenate(lsts))
+    fb = torch.zeros((sum(N), 4), dtype=torch.float32, device="cuda")
+    eb = torch.zeros(len(N), dtype=torch.float64, device="cuda")
+    vb = torch.zeros(6 * len(N), dtype=torch.float64, device="cuda")
+    b.compute(_dev(pos4, torch.float32), _dev(q, torch.float32), fb, eb, vb, nlist=nl)
+    fb = fb.cpu().numpy()
+    for i, s in enumerate(sys_list):
+        ctx = native.Context(params, s.box, s.N)
+        p4, qq = _upload(s)
+        f = torch.zeros((s.N, 4), dtype=torch.float32, device="cuda")
+        e = torch.zeros(1, dtype=torch.float64, device="cuda")
+        v = torch.zeros(6, dtype=torch.float64, device="cuda")
+        ctx.compute(p4, qq, f, e, v, nlist=_nlist_dev(*nls[i]))
+        a, z = b.offsets[i], b.offsets[i + 1]
+        fa = f.cpu().numpy()
+        assert np.abs(fa - fb[a:z]).max() <= 1e-6 * np.abs(fa).max()
+        assert abs(e.item() - eb[i].item()) <= 1e-9 * abs(e.item())
+        # the FP64 charge-mesh flush is atomic, so mesh sums may round in a
+        # different order: agreement to 1e-6 of the largest component
+        va, vbi = v.cpu().numpy(), vb[6 * i:6 * i + 6].cpu().numpy()
+        assert np.abs(va - vbi).max() <= 1e-6 * np.abs(va).max()
+
+
+def test_gpu_nlist_matches_oracle():
+    s = systems.rocksalt(10, seed=77)
+    b = native.Batch(native.make_params(), [s.N], [s.box])
+    pos4 = np.zeros((s.N, 4), dtype=np.float32)
+    pos4[:, :3] = s.pos
+    cap = 256
+    head = torch.zeros(s.N, dtype=torch.int32, device="cuda")
+    nn = torch.zeros(s.N, dtype=torch.int32, device="cuda")
+    nl = torch.zeros(s.N * cap, dtype=torch.int32, device="cuda")
+    b.build_nlist(_dev(pos4, torch.float32), 3.4, cap, head, nn, nl)
+    h, c, l = head.cpu().numpy(), nn.cpu().numpy(), nl.cpu().numpy()
+    rh, rc, rl = R.neighbor_list(s.pos.astype(np.float32).astype(np.float64), s.box, 3.4)
+    assert np.array_equal(c, rc.astype(np.int32))
+    for i in range(s.N):
+        assert set(l[h[i]:h[i] + c[i]].tolist()) == set(rl[rh[i]:rh[i] + rc[i]].tolist())
+
+
+def test_errors_are_reported():
+    with pytest.raises(EspError):
+        native.Context(native.make_params(order=13), (10, 10, 10), 10)
+    with pytest.raises(EspError):
+        native.Context(native.make_params(alpha=0.5), (10, 10, 10), 10)
+    with pytest.raises(EspError):
+        native.Context(native.make_params(mesh=(14, 14, 14)), (10, 10, 10), 10)  # 14 is not 2/3/5-smooth
