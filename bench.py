@@ -236,9 +236,11 @@ def run_ours(args):
     stream = torch.cuda.current_stream(dev)
 
     def request(bb, p, v, use_graph=True):
+        # the first evaluation reports energy and virial; the NVE steps need
+        # forces and energies only
         bb.build_nlist(p, RCUT + SKIN, CAP, head, nn, nl)
         bb.compute(p, q, force, energy, virial, nlist=(head, nn, nl), flags=ESP_ALL)
-        bb.md_run(p, v, q, force, energy, virial, (head, nn, nl), MD_STEPS, DT, use_graph=use_graph)
+        bb.md_run(p, v, q, force, energy, None, (head, nn, nl), MD_STEPS, DT, use_graph=use_graph)
 
     def barrier():
         if world > 1:
@@ -306,7 +308,7 @@ def run_ours(args):
             for c, (p, v, qq, h, n_, l_, f, e, w) in zip(ctxs, views):
                 c.build_nlist(p, RCUT + SKIN, CAP, h, n_, l_)
                 c.compute(p, qq, f, e, w, nlist=(h, n_, l_), flags=ESP_ALL)
-                c.md_run(p, v, qq, f, e, w, (h, n_, l_), MD_STEPS, DT, use_graph=False)
+                c.md_run(p, v, qq, f, e, None, (h, n_, l_), MD_STEPS, DT, use_graph=False)
 
         plain_round()
         torch.cuda.synchronize(dev)

@@ -119,4 +119,37 @@ __device__ __forceinline__ float horner_dw(const float* c, int D, float t) {
     return v;
 }
 
+// Default window degree for support P (what the planner picks when the
+// degree is not set): the staging kernels unroll this case fully.
+template <int P>
+constexpr int default_window_degree() {
+    return P + 2 > 9 ? P + 2 : 9;
+}
+
+// One window segment held in registers by the thread that evaluates it
+// (degree DD at compile time, or a runtime degree through shared memory).
+template <int DD>
+struct SegPoly {
+    float c[DD + 1];  // w(t)  = sum_j c[j] t^j
+    float d[DD];      // w'(t) = sum_j d[j] t^j, d[j] = (j+1) c[j+1]
+    __device__ __forceinline__ void load(const float* wc_seg) {
+#pragma unroll
+        for (int j = 0; j <= DD; ++j) c[j] = wc_seg[j];
+#pragma unroll
+        for (int j = 0; j < DD; ++j) d[j] = (float)(j + 1) * c[j + 1];
+    }
+    __device__ __forceinline__ float w(float t) const {
+        float v = c[DD];
+#pragma unroll
+        for (int j = DD - 1; j >= 0; --j) v = fmaf(v, t, c[j]);
+        return v;
+    }
+    __device__ __forceinline__ float dw(float t) const {
+        float v = d[DD - 1];
+#pragma unroll
+        for (int j = DD - 2; j >= 0; --j) v = fmaf(v, t, d[j]);
+        return v;
+    }
+};
+
 }  // namespace espb

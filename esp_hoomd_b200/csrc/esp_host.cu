@@ -79,28 +79,23 @@ uint32_t radix_plan(int n) {
     return code;
 }
 
-// (PX, PP) pitches of the interpolation tile with few bank conflicts for the
-// lane pattern b = lane % P, cg = lane / P.
+// (PX, PP) pitches of the interpolation tile: the lanes of one particle
+// group read the stencil planes oz + c (c < P) at a common (x, y), so the
+// plane pitch spreads c * PP over distinct banks.
 void choose_pitch(int P, int E, int& PX, int& PP) {
-    int best = 1 << 30;
     PX = E;
     PP = E * E;
-    const int ncg = 32 / P;
-    for (int px = E; px <= E + 8; ++px)
-        for (int pp = px * E; pp <= px * E + 32; ++pp) {
-            int cnt[32] = {0};
-            int worst = 0;
-            for (int l = 0; l < ncg * P; ++l) {
-                int bank = ((l / P) * pp + (l % P) * px) & 31;
-                worst = std::max(worst, ++cnt[bank]);
-            }
-            const int score = worst * 100000 + pp * E;
-            if (score < best) {
-                best = score;
-                PX = px;
-                PP = pp;
-            }
+    int best = 1 << 30;
+    for (int pp = E * E; pp <= E * E + 32; ++pp) {
+        int cnt[32] = {0};
+        int worst = 0;
+        for (int c = 0; c < P; ++c) worst = std::max(worst, ++cnt[(c * pp) & 31]);
+        const int score = worst * 1000 + (pp - E * E);
+        if (score < best) {
+            best = score;
+            PP = pp;
         }
+    }
 }
 
 struct DevAlloc {
@@ -219,6 +214,8 @@ struct esp_batch {
     float2 *d_spec = nullptr, *d_gtab = nullptr, *d_tw = nullptr;
     float* d_phi = nullptr;
     int4 *d_x = nullptr, *d_y = nullptr, *d_z = nullptr;
+    int2 *d_p = nullptr, *d_s = nullptr;
+    int n_p = 0, n_s = 0, smem_plane = 0, smem_slab = 0;
     double *d_acc = nullptr, *d_energy = nullptr, *d_virial = nullptr;
     // neighbour-list harness (allocated on first use)
     DevAlloc nlmem;
@@ -277,7 +274,9 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         return fail(ESP_ERR_UNSUPPORTED, "threads_per_particle must be 4, 8, 16 or 32");
     const double target = p.target_error > 0 ? p.target_error : 1e-5;
     const double kreq = kappa_required(target);
-    T = p.tile > 0 ? p.tile : P;
+    // default tile: extended region E = T + P - 1 = 16 (the dense spreading
+    // kernel's register column and a 16^3 interpolation tile)
+    T = p.tile > 0 ? p.tile : std::max(1, 17 - P);
     if (T > 64) return fail(ESP_ERR_UNSUPPORTED, "tile edge must be <= 64");
     totN = 0;
     for (int s = 0; s < ns; ++s) {
@@ -431,18 +430,35 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
     const int ppb = 256 / tpp;
     std::vector<int> tile_sys(n_tiles);
     std::vector<int4> xi, yi, zi;
+    std::vector<int2> pi, si;
+    smem_plane = 0;
+    smem_slab = 0;
     for (int s = 0; s < ns; ++s) {
         const SysDev& S = sd[s];
         for (int i = 0; i < S.N; i += 256) chunks.push_back(make_int2(s, S.p_off + i));
         for (int i = 0; i < S.N; i += ppb) pchunks.push_back(make_int2(s, S.p_off + i));
         for (int t = 0; t < S.ntx * S.nty * S.ntz; ++t) tile_sys[S.t_off + t] = s;
-        for (int z = 0; z < S.nz; ++z)
-            for (int y0 = 0; y0 < S.ny; y0 += 2 * FFT_B_X) xi.push_back(make_int4(s, z, y0, 0));
-        for (int z = 0; z < S.nz; ++z)
-            for (int k0 = 0; k0 < S.nxh; k0 += FFT_B_YZ) yi.push_back(make_int4(s, z, k0, 0));
-        for (int y = 0; y < S.ny; ++y)
-            for (int k0 = 0; k0 < S.nxh; k0 += FFT_B_YZ) zi.push_back(make_int4(s, y, k0, 0));
+        // whole planes / slabs in shared memory when they fit, else per-line passes
+        const int sp = fft_plane_smem(S.nx, S.ny), ss = fft_slab_smem(S.nx, S.nz);
+        if (sp <= FFT_SMEM_MAX) {
+            smem_plane = std::max(smem_plane, sp);
+            for (int z = 0; z < S.nz; ++z) pi.push_back(make_int2(s, z));
+        } else {
+            for (int z = 0; z < S.nz; ++z)
+                for (int y0 = 0; y0 < S.ny; y0 += 2 * FFT_B_X) xi.push_back(make_int4(s, z, y0, 0));
+            for (int z = 0; z < S.nz; ++z)
+                for (int k0 = 0; k0 < S.nxh; k0 += FFT_B_YZ) yi.push_back(make_int4(s, z, k0, 0));
+        }
+        if (ss <= FFT_SMEM_MAX) {
+            smem_slab = std::max(smem_slab, ss);
+            for (int y = 0; y < S.ny; ++y) si.push_back(make_int2(s, y));
+        } else {
+            for (int y = 0; y < S.ny; ++y)
+                for (int k0 = 0; k0 < S.nxh; k0 += FFT_B_YZ) zi.push_back(make_int4(s, y, k0, 0));
+        }
     }
+    n_p = (int)pi.size();
+    n_s = (int)si.size();
     n_chunks = (int)chunks.size();
     n_pchunks = (int)pchunks.size();
     n_x = (int)xi.size();
@@ -459,6 +475,7 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         (rc = mem.get(d_srel, totN)) || (rc = mem.get(d_rho, m_off)) || (rc = mem.get(d_phi, m_off)) ||
         (rc = mem.get(d_spec, s_off)) || (rc = mem.get(d_gtab, g_off)) || (rc = mem.get(d_tw, tw.size())) ||
         (rc = mem.get(d_x, xi.size())) || (rc = mem.get(d_y, yi.size())) || (rc = mem.get(d_z, zi.size())) ||
+        (rc = mem.get(d_p, pi.size())) || (rc = mem.get(d_s, si.size())) ||
         (rc = mem.get(d_acc, (size_t)ns * ACC_STRIDE)) || (rc = mem.get(d_energy, ns)) ||
         (rc = mem.get(d_virial, (size_t)ns * 6)))
         return rc;
@@ -471,6 +488,8 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
     ESPB_CK(cudaMemcpy(d_x, xi.data(), xi.size() * sizeof(int4), cudaMemcpyHostToDevice));
     ESPB_CK(cudaMemcpy(d_y, yi.data(), yi.size() * sizeof(int4), cudaMemcpyHostToDevice));
     ESPB_CK(cudaMemcpy(d_z, zi.data(), zi.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    if (!pi.empty()) ESPB_CK(cudaMemcpy(d_p, pi.data(), pi.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    if (!si.empty()) ESPB_CK(cudaMemcpy(d_s, si.data(), si.size() * sizeof(int2), cudaMemcpyHostToDevice));
     ESPB_CK(cudaMemset(d_tcount, 0, n_tiles * sizeof(uint32_t)));
     ESPB_CK(cudaMemset(d_rho, 0, (size_t)std::max<long long>(m_off, 1) * sizeof(double)));
     if (graph_exec) {
@@ -568,9 +587,21 @@ LaunchArgs esp_batch::args() const {
     a.n_yitems = n_y;
     a.zitems = d_z;
     a.n_zitems = n_z;
+    a.pitems = d_p;
+    a.n_pitems = n_p;
+    a.sitems = d_s;
+    a.n_sitems = n_s;
+    a.smem_plane = smem_plane;
+    a.smem_slab = smem_slab;
     a.acc = d_acc;
     a.energy = d_energy;
     a.virial = d_virial;
+    a.nmax_x = a.nmax_y = a.nmax_z = 1;
+    for (const SysDev& S : sd) {
+        a.nmax_x = std::max(a.nmax_x, S.nx);
+        a.nmax_y = std::max(a.nmax_y, S.ny);
+        a.nmax_z = std::max(a.nmax_z, S.nz);
+    }
     return a;
 }
 
@@ -586,6 +617,7 @@ int esp_batch::compute(cudaStream_t st, const float* pos4, const float* q, const
     a.force = reinterpret_cast<float4*>(force4);
     if (energy) a.energy = energy;
     if (virial) a.virial = virial;
+    a.want_virial = virial != nullptr;
     a.nl_head = head;
     a.nl_n = nn;
     a.nl_list = nl;

@@ -30,7 +30,7 @@ __global__ void k_bin(const int2* __restrict__ chunks, const SysDev* __restrict_
                       uint32_t* __restrict__ key, uint32_t* __restrict__ tile_count, double* __restrict__ acc) {
     __shared__ double red[32 * 2];
     const int2 ch = chunks[blockIdx.x];
-    const SysDev& S = sys[ch.x];
+    const SysDev S = sys[ch.x];
     const int i = ch.y + threadIdx.x;
     double qs[2] = {0.0, 0.0};
     if (i < S.p_off + S.N) {
@@ -118,7 +118,7 @@ __global__ void k_scatter(const int2* __restrict__ chunks, const SysDev* __restr
                           const uint32_t* __restrict__ key, const uint32_t* __restrict__ start,
                           uint32_t* __restrict__ cnt, uint32_t* __restrict__ perm_u) {
     const int2 ch = chunks[blockIdx.x];
-    const SysDev& S = sys[ch.x];
+    const SysDev S = sys[ch.x];
     const int i = ch.y + threadIdx.x;
     if (i >= S.p_off + S.N) return;
     const uint32_t k = key[i];
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(SpreadCfg<P>::THREADS)
     const int np = (int)(start[t + 1] - s0);
     if (np == 0) return;
     const int si = tile_sys[t];
-    const SysDev& S = sys[si];
+    const SysDev S = sys[si];
     const ParamSet& ps = psets[S.pset];
     const int E = T + P - 1;
     const int nb = (E + P - 1) / P;
@@ -278,6 +278,308 @@ __global__ void __launch_bounds__(SpreadCfg<P>::THREADS)
             gz -= gz >= S.nz ? S.nz : 0;
             atomicAdd(&rho[S.m_off + ((long long)gz * S.ny + gy) * S.nx + gx], v);
         }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Dense spreading (tiles with E = T + P - 1 <= 16): thread (X, Y) owns the
+// whole z-column (X, Y, 0..E-1) of the tile's extended region in
+// registers. For each particle it adds wx[X-ox] wy[Y-oy] wz_shift[Z] into
+// all E registers (wz_shift = the particle's z weights placed at oz, zero
+// elsewhere; read as broadcast 128-bit loads) -- no per-tap shared-memory
+// traffic and no per-tap index arithmetic. Sums are compensated blockwise:
+// each block of SPREAD_KC particles is summed in FP32 and Kahan-merged into
+// the column's (sum, comp) registers. Flush: one FP64 atomic per column
+// point.
+// ----------------------------------------------------------------------------
+constexpr int SPREAD_EM = 16;   // z registers per column (E <= 16)
+constexpr int SPREAD_KC = 16;   // particles per compensated block
+constexpr int SPREAD_CHD = 64;  // particles staged per round
+
+template <int P>
+__global__ void __launch_bounds__(256)
+    k_spread_dense(const int* __restrict__ tile_sys, const SysDev* __restrict__ sys,
+                   const ParamSet* __restrict__ psets, int T, int D, const uint32_t* __restrict__ start,
+                   const float4* __restrict__ srec, const uint32_t* __restrict__ srel, double* __restrict__ rho) {
+    extern __shared__ float4 smd4[];
+    const int t = blockIdx.x;
+    const uint32_t s0 = start[t];
+    const int np = (int)(start[t + 1] - s0);
+    if (np == 0) return;
+    const int si = tile_sys[t];
+    const SysDev S = sys[si];
+    const ParamSet& ps = psets[S.pset];
+    const int E = T + P - 1;
+    float4* wzs = smd4;                                          // [CH][4] shifted z weights
+    float* pwx = reinterpret_cast<float*>(wzs + SPREAD_CHD * 4);  // [CH][P] x weights * q
+    float* pwy = pwx + SPREAD_CHD * P;                           // [CH][P]
+    int* pxy = reinterpret_cast<int*>(pwy + SPREAD_CHD * P);     // [CH] origins
+    float* wc = reinterpret_cast<float*>(pxy + SPREAD_CHD);      // [P][D+1]
+    const int tid = threadIdx.x;
+    for (int i = tid; i < P * (D + 1); i += blockDim.x) wc[i] = ps.wcoef[(i / (D + 1)) * (MAX_D + 1) + (i % (D + 1))];
+    const int X = tid % E, Y = tid / E;
+    const bool owner = tid < E * E;
+    float cs[SPREAD_EM], sum[SPREAD_EM], comp[SPREAD_EM];
+#pragma unroll
+    for (int z = 0; z < SPREAD_EM; ++z) {
+        cs[z] = 0.f;
+        sum[z] = 0.f;
+        comp[z] = 0.f;
+    }
+    int inblk = 0;
+    for (int base = 0; base < np; base += SPREAD_CHD) {
+        const int nc = min(SPREAD_CHD, np - base);
+        __syncthreads();  // coefficients loaded; previous chunk consumed
+        for (int k = tid; k < nc * 16; k += blockDim.x) reinterpret_cast<float*>(wzs)[k] = 0.f;
+        __syncthreads();
+        for (int k = tid; k < nc * 3 * P; k += blockDim.x) {
+            const int p = k / (3 * P), r = k - p * 3 * P, ax = r / P, a = r - ax * P;
+            const float4 rec = srec[s0 + base + p];
+            const uint32_t rl = srel[s0 + base + p];
+            const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
+            const float w = horner_w(&wc[a * (D + 1)], D, tt);
+            if (ax == 0) {
+                pwx[p * P + a] = w * rec.w;
+            } else if (ax == 1) {
+                pwy[p * P + a] = w;
+            } else {
+                reinterpret_cast<float*>(wzs)[p * 16 + (int)((rl >> 16) & 255u) + a] = w;
+            }
+            if (r == 0) pxy[p] = (int)(rl & 0xffffu);
+        }
+        __syncthreads();
+        for (int p = 0; p < nc; ++p) {
+            const int pk = pxy[p];
+            const int a = X - (pk & 255), b = Y - ((pk >> 8) & 255);
+            if (owner && (unsigned)a < (unsigned)P && (unsigned)b < (unsigned)P) {
+                const float wxy = pwx[p * P + a] * pwy[p * P + b];
+                const float4 z0 = wzs[p * 4 + 0], z1 = wzs[p * 4 + 1], z2 = wzs[p * 4 + 2], z3 = wzs[p * 4 + 3];
+                const float wz[16] = {z0.x, z0.y, z0.z, z0.w, z1.x, z1.y, z1.z, z1.w,
+                                      z2.x, z2.y, z2.z, z2.w, z3.x, z3.y, z3.z, z3.w};
+#pragma unroll
+                for (int z = 0; z < SPREAD_EM; ++z) cs[z] = fmaf(wxy, wz[z], cs[z]);
+            }
+            if (++inblk == SPREAD_KC) {
+                inblk = 0;
+#pragma unroll
+                for (int z = 0; z < SPREAD_EM; ++z) {
+                    const float y = __fsub_rn(cs[z], comp[z]);
+                    const float ts = __fadd_rn(sum[z], y);
+                    comp[z] = __fsub_rn(__fsub_rn(ts, sum[z]), y);
+                    sum[z] = ts;
+                    cs[z] = 0.f;
+                }
+            }
+        }
+    }
+    if (!owner) return;
+    const int lt = t - S.t_off;
+    int gx = (lt % S.ntx) * T + X, gy = ((lt / S.ntx) % S.nty) * T + Y;
+    const int Z0 = (lt / (S.ntx * S.nty)) * T;
+    while (gx >= S.nx) gx -= S.nx;
+    while (gy >= S.ny) gy -= S.ny;
+    double* col = rho + S.m_off + (long long)gy * S.nx + gx;
+    const long long zstride = (long long)S.ny * S.nx;
+#pragma unroll
+    for (int z = 0; z < SPREAD_EM; ++z) {
+        if (z < E) {
+            const double v = ((double)sum[z] - (double)comp[z]) + (double)cs[z];
+            if (v != 0.0) {
+                int gz = Z0 + z;
+                while (gz >= S.nz) gz -= S.nz;
+                atomicAdd(col + gz * zstride, v);
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Tensor-core spreading (tiles with E = T + P - 1 = 16). The tile's
+// extended region is a dense contraction over the tile's particles,
+//   rho[(X,Y), Z] = sum_p  (q wx_p[X-ox_p] wy_p[Y-oy_p]) * wz_p[Z-oz_p],
+// i.e. a (256 x K) x (K x 16) product with K = particles (zero weights
+// outside each stencil). Warp w owns rows Y = 2w, 2w+1 (two m16 tiles, X =
+// 0..15) and both n8 tiles of Z; each k-step of 8 particles issues
+// mma.sync m16n8k8 TF32 with 3xTF32 operand splitting (hi*hi + hi*lo +
+// lo*hi: FP32-level products). Per k-step the A fragments are built from
+// the staged 1D weights, B fragments are the particles' shifted z weights.
+// Every four k-steps (32 particles) the FP32 block accumulators are
+// Kahan-merged into (sum, comp) registers; the tile is flushed with one
+// FP64 atomic per point.
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t f2tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+    hi = f2tf32(x);
+    lo = f2tf32(x - __uint_as_float(hi));
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+constexpr int SPREAD_CHM = 64;  // particles staged per round (multiple of 8)
+
+template <int P>
+__global__ void __launch_bounds__(256)
+    k_spread_mma(const int* __restrict__ tile_sys, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
+                 int T, int D, const uint32_t* __restrict__ start, const float4* __restrict__ srec,
+                 const uint32_t* __restrict__ srel, double* __restrict__ rho) {
+    extern __shared__ float4 smm4[];
+    const int t = blockIdx.x;
+    const uint32_t s0 = start[t];
+    const int np = (int)(start[t + 1] - s0);
+    if (np == 0) return;
+    const int si = tile_sys[t];
+    const SysDev S = sys[si];
+    const ParamSet& ps = psets[S.pset];
+    float* wzs = reinterpret_cast<float*>(smm4);   // [CH][16] shifted z weights
+    float* pwx = wzs + SPREAD_CHM * 16;            // [CH][P] x weights * q
+    float* pwy = pwx + SPREAD_CHM * P;             // [CH][P]
+    int* pxy = reinterpret_cast<int*>(pwy + SPREAD_CHM * P);  // [CH] origins
+    float* wc = reinterpret_cast<float*>(pxy + SPREAD_CHM);   // [P][D+1]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, tg = lane & 3;
+    for (int i = tid; i < P * (D + 1); i += blockDim.x) wc[i] = ps.wcoef[(i / (D + 1)) * (MAX_D + 1) + (i % (D + 1))];
+    float acc[2][2][4], sum[2][2][4], cmp[2][2][4];
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+        for (int n = 0; n < 2; ++n)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                acc[m][n][i] = 0.f;
+                sum[m][n][i] = 0.f;
+                cmp[m][n][i] = 0.f;
+            }
+    int ksteps = 0;
+    for (int base = 0; base < np; base += SPREAD_CHM) {
+        const int nc = min(SPREAD_CHM, np - base);
+        const int ncp = (nc + 7) & ~7;  // padded to whole k-steps (zero weights)
+        __syncthreads();
+        for (int k = tid; k < ncp * 16; k += blockDim.x) wzs[k] = 0.f;
+        for (int k = tid; k < ncp * P; k += blockDim.x) {
+            pwx[k] = 0.f;
+            pwy[k] = 0.f;
+        }
+        if (tid < ncp) pxy[tid] = 0;
+        __syncthreads();
+        {
+            // thread (a, j0) evaluates window segment a for items j0, j0 + nla, ...
+            constexpr int DD = default_window_degree<P>();
+            const int nla = blockDim.x / P, a = tid % P, j0 = tid / P;
+            if (j0 < nla) {
+                SegPoly<DD> sp;
+                if (D == DD) sp.load(&wc[a * (D + 1)]);
+                for (int j = j0; j < nc * 3; j += nla) {
+                    const int p = j / 3, ax = j - 3 * p;
+                    const float4 rec = srec[s0 + base + p];
+                    const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
+                    const float w = D == DD ? sp.w(tt) : horner_w(&wc[a * (D + 1)], D, tt);
+                    if (ax == 0)
+                        pwx[p * P + a] = w * rec.w;
+                    else if (ax == 1)
+                        pwy[p * P + a] = w;
+                    else
+                        wzs[p * 16 + (int)((srel[s0 + base + p] >> 16) & 255u) + a] = w;
+                }
+            }
+            for (int p = tid; p < nc; p += blockDim.x) pxy[p] = (int)(srel[s0 + base + p] & 0xffffu);
+        }
+        __syncthreads();
+        for (int k0 = 0; k0 < ncp; k0 += 8) {
+            const int p1 = k0 + tg, p2 = k0 + tg + 4;
+            // B fragments: b0 = wz_{p1}[Z], b1 = wz_{p2}[Z], Z = 8 nt + g
+            uint32_t bh[2][2], bl[2][2];
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) {
+                split_tf32(wzs[p1 * 16 + 8 * nt + g], bh[nt][0], bl[nt][0]);
+                split_tf32(wzs[p2 * 16 + 8 * nt + g], bh[nt][1], bl[nt][1]);
+            }
+            const int o1 = pxy[p1], o2 = pxy[p2];
+            const int ox1 = o1 & 255, oy1 = (o1 >> 8) & 255, ox2 = o2 & 255, oy2 = (o2 >> 8) & 255;
+            const int ax1 = g - ox1, ax1b = g + 8 - ox1, ax2 = g - ox2, ax2b = g + 8 - ox2;
+            const float wx1 = (unsigned)ax1 < (unsigned)P ? pwx[p1 * P + ax1] : 0.f;
+            const float wx1b = (unsigned)ax1b < (unsigned)P ? pwx[p1 * P + ax1b] : 0.f;
+            const float wx2 = (unsigned)ax2 < (unsigned)P ? pwx[p2 * P + ax2] : 0.f;
+            const float wx2b = (unsigned)ax2b < (unsigned)P ? pwx[p2 * P + ax2b] : 0.f;
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+                const int Y = 2 * warp + mt;
+                const int ay1 = Y - oy1, ay2 = Y - oy2;
+                const float wy1 = (unsigned)ay1 < (unsigned)P ? pwy[p1 * P + ay1] : 0.f;
+                const float wy2 = (unsigned)ay2 < (unsigned)P ? pwy[p2 * P + ay2] : 0.f;
+                uint32_t ah0, al0, ah1, al1, ah2, al2, ah3, al3;
+                split_tf32(wx1 * wy1, ah0, al0);   // row X = g,     particle p1
+                split_tf32(wx1b * wy1, ah1, al1);  // row X = g + 8, particle p1
+                split_tf32(wx2 * wy2, ah2, al2);   // row X = g,     particle p2
+                split_tf32(wx2b * wy2, ah3, al3);  // row X = g + 8, particle p2
+#pragma unroll
+                for (int nt = 0; nt < 2; ++nt) {
+                    mma_tf32(acc[mt][nt], al0, al1, al2, al3, bh[nt][0], bh[nt][1]);
+                    mma_tf32(acc[mt][nt], ah0, ah1, ah2, ah3, bl[nt][0], bl[nt][1]);
+                    mma_tf32(acc[mt][nt], ah0, ah1, ah2, ah3, bh[nt][0], bh[nt][1]);
+                }
+            }
+            if (++ksteps == 4) {
+                ksteps = 0;
+#pragma unroll
+                for (int m = 0; m < 2; ++m)
+#pragma unroll
+                    for (int n = 0; n < 2; ++n)
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            const float y = __fsub_rn(acc[m][n][i], cmp[m][n][i]);
+                            const float ts = __fadd_rn(sum[m][n][i], y);
+                            cmp[m][n][i] = __fsub_rn(__fsub_rn(ts, sum[m][n][i]), y);
+                            sum[m][n][i] = ts;
+                            acc[m][n][i] = 0.f;
+                        }
+            }
+        }
+    }
+    // flush: C fragment element i of (mt, nt) is point X = g + 8 (i >> 1), Y = 2 warp + mt,
+    // Z = 8 nt + 2 tg + (i & 1)
+    const int lt = t - S.t_off;
+    const int X0 = (lt % S.ntx) * T, Y0 = ((lt / S.ntx) % S.nty) * T, Z0 = (lt / (S.ntx * S.nty)) * T;
+    const long long zstride = (long long)S.ny * S.nx;
+    long long xo[2], zo[2][2];  // wrapped x offsets (X = g, g + 8), z offsets (Z = 8 nt + 2 tg + e)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        int gx = X0 + g + 8 * h;
+        while (gx >= S.nx) gx -= S.nx;
+        xo[h] = gx;
+    }
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            int gz = Z0 + 8 * nt + 2 * tg + e;
+            while (gz >= S.nz) gz -= S.nz;
+            zo[nt][e] = gz * zstride;
+        }
+    double* rb = rho + S.m_off;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+        int gy = Y0 + 2 * warp + mt;
+        while (gy >= S.ny) gy -= S.ny;
+        const long long yo = (long long)gy * S.nx;
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const float rest = acc[mt][nt][i] - cmp[mt][nt][i];
+                const double v = (double)sum[mt][nt][i] + (double)rest;
+                if (v != 0.0) atomicAdd(rb + zo[nt][i & 1] + yo + xo[i >> 1], v);
+            }
     }
 }
 
@@ -384,25 +686,21 @@ __device__ float2* fft_lines(float2* s0, float2* s1, int n, int B, int SB, const
 // Two real rows form one complex line; the half spectra are separated with
 // A_k = (Z_k + conj Z_{n-k})/2, B_k = (Z_k - conj Z_{n-k})/(2i).
 __global__ void k_fftx_fwd(const int4* __restrict__ items, const SysDev* __restrict__ sys,
-                           const float2* __restrict__ tw, double* __restrict__ rho, float2* __restrict__ spec) {
+                           const float2* __restrict__ tw, const double* __restrict__ rho, float2* __restrict__ spec) {
     extern __shared__ float2 sb[];
     const int4 it = items[blockIdx.x];
-    const SysDev& S = sys[it.x];
+    const SysDev S = sys[it.x];
     const int z = it.y, y0 = it.z, n = S.nx;
     constexpr int B = FFT_B_X, SB = FFT_SB_X;  // padded line stride: conflict-free row access
     float2* s0 = sb;
-    float2* s1 = sb + FFT_MAX_N * SB;
+    float2* s1 = sb + n * SB;
     for (int idx = threadIdx.x; idx < B * n; idx += blockDim.x) {
         const int b = idx / n, i = idx - b * n, y = y0 + 2 * b;
         float2 v = make_float2(0.f, 0.f);
         if (y < S.ny) {
             const long long g = S.m_off + ((long long)z * S.ny + y) * n + i;
             v.x = (float)rho[g];
-            rho[g] = 0.0;
-            if (y + 1 < S.ny) {
-                v.y = (float)rho[g + n];
-                rho[g + n] = 0.0;
-            }
+            if (y + 1 < S.ny) v.y = (float)rho[g + n];
         }
         s0[i * SB + b] = v;
     }
@@ -427,11 +725,11 @@ __global__ void k_ffty(const int4* __restrict__ items, const SysDev* __restrict_
                        const float2* __restrict__ tw, float2* __restrict__ spec) {
     extern __shared__ float2 sb[];
     const int4 it = items[blockIdx.x];
-    const SysDev& S = sys[it.x];
+    const SysDev S = sys[it.x];
     const int z = it.y, kx0 = it.z, n = S.ny;
     constexpr int B = FFT_B_YZ;
     float2* s0 = sb;
-    float2* s1 = sb + FFT_MAX_N * B;
+    float2* s1 = sb + n * B;
     for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
         const int y = idx / B, b = idx - y * B, kx = kx0 + b;
         s0[idx] = kx < S.nxh ? spec[S.s_off + ((long long)z * S.ny + y) * S.nxh + kx] : make_float2(0.f, 0.f);
@@ -452,11 +750,11 @@ __global__ void k_fftz_conv(const int4* __restrict__ items, const SysDev* __rest
     extern __shared__ float2 sb[];
     __shared__ double red[32 * 7];
     const int4 it = items[blockIdx.x];
-    const SysDev& S = sys[it.x];
+    const SysDev S = sys[it.x];
     const int y = it.y, kx0 = it.z, n = S.nz;
     constexpr int B = FFT_B_YZ;
     float2* s0 = sb;
-    float2* s1 = sb + FFT_MAX_N * B;
+    float2* s1 = sb + n * B;
     const long long rowstride = (long long)S.ny * S.nxh;
     for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
         const int z = idx / B, b = idx - z * B, kx = kx0 + b;
@@ -507,14 +805,15 @@ __global__ void k_fftz_conv(const int4* __restrict__ items, const SysDev* __rest
 // and combined as Z = A + iB; the inverse transform returns row A in the
 // real part and row B in the imaginary part.
 __global__ void k_fftx_inv(const int4* __restrict__ items, const SysDev* __restrict__ sys,
-                           const float2* __restrict__ tw, const float2* __restrict__ spec, float* __restrict__ phi) {
+                           const float2* __restrict__ tw, const float2* __restrict__ spec, float* __restrict__ phi,
+                           double* __restrict__ rho) {
     extern __shared__ float2 sb[];
     const int4 it = items[blockIdx.x];
-    const SysDev& S = sys[it.x];
+    const SysDev S = sys[it.x];
     const int z = it.y, y0 = it.z, n = S.nx;
     constexpr int B = FFT_B_X, SB = FFT_SB_X;
     float2* s0 = sb;
-    float2* s1 = sb + FFT_MAX_N * SB;
+    float2* s1 = sb + n * SB;
     for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
         const int b = idx / n, k = idx - b * n, ya = y0 + 2 * b, yb = ya + 1;
         const bool up = k >= S.nxh;
@@ -539,9 +838,166 @@ __global__ void k_fftx_inv(const int4* __restrict__ items, const SysDev* __restr
             const float2 v = r[i * SB + b];
             const long long g = S.m_off + ((long long)z * S.ny + y) * n + i;
             phi[g] = v.x;
-            if (y + 1 < S.ny) phi[g + n] = v.y;
+            rho[g] = 0.0;  // clear the charge mesh for the next spread
+            if (y + 1 < S.ny) {
+                phi[g + n] = v.y;
+                rho[g + n] = 0.0;
+            }
         }
     }
+}
+
+// ----------------------------------------------------------------------------
+// Plane and slab passes (meshes whose planes fit in shared memory): one CTA
+// transforms a whole z-plane (x R2C + y C2C, and the inverse), or a whole
+// xz-slab for the z pass, so every CTA carries enough independent work to
+// hide memory latency. Line strides are odd so 64-bit shared accesses with
+// a stride of one line are bank-conflict free.
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ int odd_up(int v) { return v | 1; }
+
+__global__ void __launch_bounds__(512)
+    k_fft_plane_fwd(const int2* __restrict__ items, const SysDev* __restrict__ sys, const float2* __restrict__ tw,
+                    const double* __restrict__ rho, float2* __restrict__ spec) {
+    extern __shared__ float2 sb[];
+    const int2 it = items[blockIdx.x];
+    const SysDev S = sys[it.x];
+    const int z = it.y, nx = S.nx, ny = S.ny, nxh = S.nxh;
+    const int np = (ny + 1) / 2, SBx = odd_up(np), SBy = odd_up(nxh);
+    const int cap = max(nx * SBx, ny * SBy);
+    float2* s0 = sb;
+    float2* s1 = sb + cap;
+    const double* src = rho + S.m_off + (long long)z * ny * nx;
+    for (int idx = threadIdx.x; idx < np * nx; idx += blockDim.x) {
+        const int b = idx / nx, i = idx - b * nx, y = 2 * b;
+        float2 v;
+        v.x = (float)src[y * nx + i];
+        v.y = (y + 1 < ny) ? (float)src[(y + 1) * nx + i] : 0.f;
+        s0[i * SBx + b] = v;
+    }
+    __syncthreads();
+    float2* r = fft_lines<false>(s0, s1, nx, np, SBx, tw + S.twx, S.radx);
+    float2* o = (r == s0) ? s1 : s0;
+    for (int idx = threadIdx.x; idx < np * nxh; idx += blockDim.x) {
+        const int b = idx / nxh, k = idx - b * nxh;
+        const float2 zk = r[k * SBx + b], zn = r[((nx - k) % nx) * SBx + b];
+        o[(2 * b) * SBy + k] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+        if (2 * b + 1 < ny) o[(2 * b + 1) * SBy + k] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+    }
+    __syncthreads();
+    const float2* r2 = fft_lines<false>(o, r, ny, nxh, SBy, tw + S.twy, S.rady);
+    float2* dst = spec + S.s_off + (long long)z * ny * nxh;
+    for (int idx = threadIdx.x; idx < ny * nxh; idx += blockDim.x) {
+        const int y = idx / nxh, k = idx - y * nxh;
+        dst[idx] = r2[y * SBy + k];
+    }
+}
+
+__global__ void __launch_bounds__(512)
+    k_fft_plane_inv(const int2* __restrict__ items, const SysDev* __restrict__ sys, const float2* __restrict__ tw,
+                    const float2* __restrict__ spec, float* __restrict__ phi, double* __restrict__ rho) {
+    extern __shared__ float2 sb[];
+    const int2 it = items[blockIdx.x];
+    const SysDev S = sys[it.x];
+    const int z = it.y, nx = S.nx, ny = S.ny, nxh = S.nxh;
+    const int np = (ny + 1) / 2, SBx = odd_up(np), SBy = odd_up(nxh);
+    const int cap = max(nx * SBx, ny * SBy);
+    float2* s0 = sb;
+    float2* s1 = sb + cap;
+    const float2* src = spec + S.s_off + (long long)z * ny * nxh;
+    for (int idx = threadIdx.x; idx < ny * nxh; idx += blockDim.x) {
+        const int y = idx / nxh, k = idx - y * nxh;
+        s0[y * SBy + k] = src[idx];
+    }
+    __syncthreads();
+    float2* r = fft_lines<true>(s0, s1, ny, nxh, SBy, tw + S.twy, S.rady);
+    float2* o = (r == s0) ? s1 : s0;
+    for (int idx = threadIdx.x; idx < np * nx; idx += blockDim.x) {
+        const int b = idx / nx, k = idx - b * nx;
+        const bool up = k >= nxh;
+        const int kk = up ? nx - k : k;
+        float2 A = r[(2 * b) * SBy + kk];
+        float2 Bv = (2 * b + 1 < ny) ? r[(2 * b + 1) * SBy + kk] : make_float2(0.f, 0.f);
+        if (up) {
+            A.y = -A.y;
+            Bv.y = -Bv.y;
+        }
+        if (k == 0 || 2 * k == nx) {
+            A.y = 0.f;
+            Bv.y = 0.f;
+        }
+        o[k * SBx + b] = make_float2(A.x - Bv.y, A.y + Bv.x);
+    }
+    __syncthreads();
+    const float2* r2 = fft_lines<true>(o, r, nx, np, SBx, tw + S.twx, S.radx);
+    float* dst = phi + S.m_off + (long long)z * ny * nx;
+    double* rz = rho + S.m_off + (long long)z * ny * nx;
+    for (int idx = threadIdx.x; idx < np * nx; idx += blockDim.x) {
+        const int b = idx / nx, i = idx - b * nx;
+        const float2 v = r2[i * SBx + b];
+        dst[(2 * b) * nx + i] = v.x;
+        rz[(2 * b) * nx + i] = 0.0;  // clear the charge mesh for the next spread
+        if (2 * b + 1 < ny) {
+            dst[(2 * b + 1) * nx + i] = v.y;
+            rz[(2 * b + 1) * nx + i] = 0.0;
+        }
+    }
+}
+
+// z pass over a whole xz-slab (fixed y): forward, energy/virial, influence
+// multiply, inverse.
+__global__ void __launch_bounds__(512)
+    k_fft_slab_z(const int2* __restrict__ items, const SysDev* __restrict__ sys, const float2* __restrict__ tw,
+                 const float2* __restrict__ gtab, float2* __restrict__ spec, double* __restrict__ acc) {
+    extern __shared__ float2 sb[];
+    __shared__ double red[32 * 7];
+    const int2 it = items[blockIdx.x];
+    const SysDev S = sys[it.x];
+    const int y = it.y, nz = S.nz, nxh = S.nxh, SBz = odd_up(nxh);
+    float2* s0 = sb;
+    float2* s1 = sb + nz * SBz;
+    const long long rowstride = (long long)S.ny * nxh;
+    float2* base = spec + S.s_off + (long long)y * nxh;
+    const float2* gbase = gtab + S.g_off + (long long)y * nxh;
+    for (int idx = threadIdx.x; idx < nz * nxh; idx += blockDim.x) {
+        const int z = idx / nxh, k = idx - z * nxh;
+        s0[z * SBz + k] = base[z * rowstride + k];
+    }
+    __syncthreads();
+    float2* r = fft_lines<false>(s0, s1, nz, nxh, SBz, tw + S.twz, S.radz);
+    float2* other = (r == s0) ? s1 : s0;
+    const double twopi = 6.283185307179586;
+    const int fy = (y < (S.ny + 1) / 2) ? y : y - S.ny;
+    const double kyv = twopi * fy / (double)S.Ly;
+    double e[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int idx = threadIdx.x; idx < nz * nxh; idx += blockDim.x) {
+        const int z = idx / nxh, kx = idx - z * nxh;
+        const float2 gb = gbase[z * rowstride + kx];
+        float2& d = r[z * SBz + kx];
+        const double p2 = (double)d.x * d.x + (double)d.y * d.y;
+        const double mult = (kx == 0 || 2 * kx == S.nx) ? 0.5 : 1.0;
+        const double ek = mult * (double)gb.x * p2, eb = mult * (double)gb.y * p2;
+        const int fz = (z < (nz + 1) / 2) ? z : z - nz;
+        const double kxv = twopi * kx / (double)S.Lx, kzv = twopi * fz / (double)S.Lz;
+        e[0] += ek;
+        e[1] += ek + eb * kxv * kxv;
+        e[2] += eb * kxv * kyv;
+        e[3] += eb * kxv * kzv;
+        e[4] += ek + eb * kyv * kyv;
+        e[5] += eb * kyv * kzv;
+        e[6] += ek + eb * kzv * kzv;
+        d = make_float2(d.x * gb.x, d.y * gb.x);
+    }
+    __syncthreads();
+    const float2* o = fft_lines<true>(r, other, nz, nxh, SBz, tw + S.twz, S.radz);
+    for (int idx = threadIdx.x; idx < nz * nxh; idx += blockDim.x) {
+        const int z = idx / nxh, k = idx - z * nxh;
+        base[z * rowstride + k] = o[z * SBz + k];
+    }
+    block_sum_f64<7>(e, red);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < 7; ++k) atomicAdd(&acc[it.x * ACC_STRIDE + ACC_EK + k], e[k]);
 }
 
 // ============================================================================
@@ -592,120 +1048,167 @@ __global__ void k_influence(SysDev S, const double* __restrict__ w1d, const doub
 
 // ============================================================================
 // a7: interpolation. One CTA per tile stages the potential of the tile's
-// extended region in shared memory; one warp per particle gathers the P^3
-// stencil with analytic differentiation of the window. The 3P weights and
-// derivatives are computed by lanes and shared by warp shuffles.
+// extended region in shared memory and, per chunk of particles, the 3P
+// window weights and derivatives (computed once per particle by all
+// threads). A group of G lanes serves one particle: lane c owns stencil
+// plane z = oz + c and contracts it separably (x, then y) in registers;
+// the group sums its four partials (potential, gradient) with shuffles.
 // ============================================================================
+// words of the interpolation staging area: the per-chunk weights, or (before
+// the first chunk) the wrapped row offsets and x indices of the region
+__host__ __device__ inline int interp_stage_words(int P, int CH, int E) {
+    return CH * 6 * P > E * E + E ? CH * 6 * P : E * E + E;
+}
+
+template <int P>
+struct InterpCfg {
+    static constexpr int G = P <= 4 ? 4 : (P <= 8 ? 8 : 16);  // lanes per particle
+    static constexpr int THREADS = 128;
+    static constexpr int NG = THREADS / G;  // particles in flight per CTA
+    static constexpr int CH = 2 * NG;       // particles staged per round
+};
+
 template <int P>
 __global__ void __launch_bounds__(128)
     k_interp(const int* __restrict__ tile_sys, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
              int T, int D, int PX, int PP, const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
              const float4* __restrict__ srec, const uint32_t* __restrict__ srel, const float* __restrict__ phi,
              float4* __restrict__ force, double* __restrict__ acc) {
-    extern __shared__ float sm[];
+    using C = InterpCfg<P>;
+    extern __shared__ float4 sm4[];
     __shared__ double red[32];
     const int t = blockIdx.x;
     const uint32_t s0 = start[t];
     const int np = (int)(start[t + 1] - s0);
     if (np == 0) return;
     const int si = tile_sys[t];
-    const SysDev& S = sys[si];
+    const SysDev S = sys[si];
     const ParamSet& ps = psets[S.pset];
     const int E = T + P - 1;
-    float* wc = sm + E * PP;
+    float* sm = reinterpret_cast<float*>(sm4);     // [E*PP] potential
+    float* wts = sm + E * PP;                      // [CH][6P] wx dwx wy dwy wz dwz (index tables first)
+    float* qv = wts + interp_stage_words(P, C::CH, E);  // [CH] charges
+    int* org = reinterpret_cast<int*>(qv + C::CH); // [CH] packed origins
+    float* wc = reinterpret_cast<float*>(org + C::CH);  // [P][D+1]
     const int lt = t - S.t_off;
     const int X0 = (lt % S.ntx) * T, Y0 = ((lt / S.ntx) % S.nty) * T, Z0 = (lt / (S.ntx * S.nty)) * T;
-    // stage the extended region row by row (x fastest: coalesced rows)
-    for (int row = threadIdx.x >> 5; row < E * E; row += blockDim.x >> 5) {
-        const int Y = row % E, Z = row / E;
-        int gy = Y0 + Y, gz = Z0 + Z;
-        while (gy >= S.ny) gy -= S.ny;
-        while (gz >= S.nz) gz -= S.nz;
-        const float* src = phi + S.m_off + ((long long)gz * S.ny + gy) * S.nx;
-        for (int X = threadIdx.x & 31; X < E; X += 32) {
-            int gx = X0 + X;
-            while (gx >= S.nx) gx -= S.nx;
-            sm[Z * PP + Y * PX + X] = __ldg(&src[gx]);
+    // stage the extended region with asynchronous 4-byte copies (every
+    // thread keeps all its loads in flight; periodic wrap per axis)
+    {
+        // wrapped row offsets per (Y, Z) and x indices, then one 4-byte
+        // asynchronous copy per point (all of a thread's copies in flight)
+        int* rowo = reinterpret_cast<int*>(wts);  // the staging area holds the index tables first
+        int* xs = rowo + E * E;
+        for (int i = threadIdx.x; i < E * E; i += blockDim.x) {
+            int gy = Y0 + i % E, gz = Z0 + i / E;
+            while (gy >= S.ny) gy -= S.ny;
+            while (gz >= S.nz) gz -= S.nz;
+            rowo[i] = (gz * S.ny + gy) * S.nx;
         }
+        for (int i = threadIdx.x; i < E; i += blockDim.x) {
+            int gx = X0 + i;
+            while (gx >= S.nx) gx -= S.nx;
+            xs[i] = gx;
+        }
+        __syncthreads();
+        const float* base = phi + S.m_off;
+        for (int idx = threadIdx.x; idx < E * E * E; idx += blockDim.x) {
+            const int X = idx % E, r = idx / E;
+            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sm[(r / E) * PP + (r % E) * PX + X]);
+            const float* src = base + rowo[r] + xs[X];
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src));
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+        asm volatile("cp.async.wait_group 0;\n" ::);
     }
     for (int i = threadIdx.x; i < P * (D + 1); i += blockDim.x)
         wc[i] = ps.wcoef[(i / (D + 1)) * (MAX_D + 1) + (i % (D + 1))];
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    constexpr int NCG = 32 / P;              // c-groups of lanes
-    constexpr int NCI = (P + NCG - 1) / NCG; // rows (c values) per lane
-    const int b = lane % P, cg = lane / P;
+    const int grp = threadIdx.x / C::G, gl = threadIdx.x % C::G;
     const float gxs = (float)S.gxd, gys = (float)S.gyd, gzs = (float)S.gzd;
+    const double self_coef = ps.self_coef;
     double esum = 0.0;
-    for (int p = warp; p < np; p += nw) {
-        const float4 rec = srec[s0 + p];
-        const uint32_t rl = srel[s0 + p];
-        const int ox = (int)(rl & 255u), oy = (int)((rl >> 8) & 255u), oz = (int)((rl >> 16) & 255u);
-        // lane e computes entry e of [x0..xP-1, y0.., z0..]; entries >= 32 in w1
-        float w0 = 0.f, d0 = 0.f, w1 = 0.f, d1 = 0.f;
+    for (int base = 0; base < np; base += C::CH) {
+        const int nc = min(C::CH, np - base);
+        __syncthreads();  // region / coefficients staged; previous chunk consumed
         {
-            const int e = lane;
-            if (e < 3 * P) {
-                const int ax = e / P, a = e - ax * P;
-                const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
-                w0 = horner_w(&wc[a * (D + 1)], D, tt);
-                d0 = horner_dw(&wc[a * (D + 1)], D, tt);
-            }
-            if (3 * P > 32 && e + 32 < 3 * P) {
-                const int ax = (e + 32) / P, a = e + 32 - ax * P;
-                const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
-                w1 = horner_w(&wc[a * (D + 1)], D, tt);
-                d1 = horner_dw(&wc[a * (D + 1)], D, tt);
-            }
-        }
-        float wx[P], dwx[P];
-#pragma unroll
-        for (int a = 0; a < P; ++a) {
-            wx[a] = __shfl_sync(0xffffffffu, w0, a);
-            dwx[a] = __shfl_sync(0xffffffffu, d0, a);
-        }
-        const float wyb = __shfl_sync(0xffffffffu, w0, P + b);
-        const float dwyb = __shfl_sync(0xffffffffu, d0, P + b);
-        float pot = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-#pragma unroll
-        for (int ci = 0; ci < NCI; ++ci) {
-            const int c = cg + ci * NCG;
-            const int src = 2 * P + c;
-            float wzc, dwzc;
-            if (3 * P > 32) {
-                const float a0 = __shfl_sync(0xffffffffu, w0, src & 31), a1 = __shfl_sync(0xffffffffu, w1, src & 31);
-                const float e0 = __shfl_sync(0xffffffffu, d0, src & 31), e1 = __shfl_sync(0xffffffffu, d1, src & 31);
-                wzc = src < 32 ? a0 : a1;
-                dwzc = src < 32 ? e0 : e1;
-            } else {
-                wzc = __shfl_sync(0xffffffffu, w0, src & 31);
-                dwzc = __shfl_sync(0xffffffffu, d0, src & 31);
-            }
-            if (lane < NCG * P && c < P) {
-                const float* row = &sm[(oz + c) * PP + (oy + b) * PX + ox];
-                float s = 0.f, d = 0.f;
-#pragma unroll
-                for (int a = 0; a < P; ++a) {
-                    const float v = row[a];
-                    s = fmaf(v, wx[a], s);
-                    d = fmaf(v, dwx[a], d);
+            // thread (a, j0) evaluates window segment a (value and derivative)
+            constexpr int DD = default_window_degree<P>();
+            const int nla = blockDim.x / P, a2 = threadIdx.x % P, j0 = threadIdx.x / P;
+            if (j0 < nla) {
+                SegPoly<DD> sp;
+                if (D == DD) sp.load(&wc[a2 * (D + 1)]);
+                for (int j = j0; j < nc * 3; j += nla) {
+                    const int p = j / 3, ax = j - 3 * p;
+                    const float4 rec = srec[s0 + base + p];
+                    const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
+                    float w, dw;
+                    if (D == DD) {
+                        w = sp.w(tt);
+                        dw = sp.dw(tt);
+                    } else {
+                        w = horner_w(&wc[a2 * (D + 1)], D, tt);
+                        dw = horner_dw(&wc[a2 * (D + 1)], D, tt);
+                    }
+                    wts[p * 6 * P + ax * 2 * P + a2] = w;
+                    wts[p * 6 * P + ax * 2 * P + P + a2] = dw;
                 }
-                const float wyz = wyb * wzc;
-                pot = fmaf(s, wyz, pot);
-                gx = fmaf(d, wyz, gx);
-                gy = fmaf(s, dwyb * wzc, gy);
-                gz = fmaf(s, wyb * dwzc, gz);
+            }
+            for (int p = threadIdx.x; p < nc; p += blockDim.x) {
+                qv[p] = srec[s0 + base + p].w;
+                org[p] = (int)srel[s0 + base + p];
             }
         }
-        pot = warp_sum(pot);
-        gx = warp_sum(gx);
-        gy = warp_sum(gy);
-        gz = warp_sum(gz);
-        if (lane == 0) {
-            const float q = rec.w;
-            const double e_i = 0.5 * (double)q * pot + ps.self_coef * (double)q * q;
-            force[perm[s0 + p]] = make_float4(q * gxs * gx, q * gys * gy, q * gzs * gz, (float)e_i);
-            esum += e_i;
+        __syncthreads();
+        for (int pp = 0; pp < nc; pp += C::NG) {
+            const int p = pp + grp;
+            const bool act = p < nc && gl < P;
+            float pot = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+            if (act) {
+                const float* W = wts + p * 6 * P;
+                float wx[P], dwx[P];
+#pragma unroll
+                for (int a2 = 0; a2 < P; ++a2) {
+                    wx[a2] = W[a2];
+                    dwx[a2] = W[P + a2];
+                }
+                const int rl = org[p];
+                const int ox = rl & 255, oy = (rl >> 8) & 255, oz = (rl >> 16) & 255;
+                const float* plane = sm + (oz + gl) * PP + oy * PX + ox;
+                float Sv = 0.f, Dv = 0.f, Sy = 0.f;
+#pragma unroll
+                for (int b = 0; b < P; ++b) {
+                    const float* row = plane + b * PX;
+                    float sr = 0.f, dr = 0.f;
+#pragma unroll
+                    for (int a2 = 0; a2 < P; ++a2) {
+                        const float v = row[a2];
+                        sr = fmaf(v, wx[a2], sr);
+                        dr = fmaf(v, dwx[a2], dr);
+                    }
+                    const float wyb = W[2 * P + b], dwyb = W[3 * P + b];
+                    Sv = fmaf(sr, wyb, Sv);
+                    Dv = fmaf(dr, wyb, Dv);
+                    Sy = fmaf(sr, dwyb, Sy);
+                }
+                const float wzc = W[4 * P + gl], dwzc = W[5 * P + gl];
+                pot = Sv * wzc;
+                gx = Dv * wzc;
+                gy = Sy * wzc;
+                gz = Sv * dwzc;
+            }
+#pragma unroll
+            for (int o = C::G / 2; o > 0; o >>= 1) {
+                pot += __shfl_xor_sync(0xffffffffu, pot, o, C::G);
+                gx += __shfl_xor_sync(0xffffffffu, gx, o, C::G);
+                gy += __shfl_xor_sync(0xffffffffu, gy, o, C::G);
+                gz += __shfl_xor_sync(0xffffffffu, gz, o, C::G);
+            }
+            if (p < nc && gl == 0) {
+                const float q = qv[p];
+                const double e_i = 0.5 * (double)q * pot + self_coef * (double)q * q;
+                force[perm[s0 + base + p]] = make_float4(q * gxs * gx, q * gys * gy, q * gzs * gz, (float)e_i);
+                esum += e_i;
+            }
         }
     }
     double ev[1] = {esum};
@@ -721,7 +1224,7 @@ __global__ void __launch_bounds__(128)
 //   force_divr = qiqj/(4 pi) (1/r^3 + 2 Q'(u)/r_c^3)
 // (the split form of EvaluatorPairPSWF::evalForceAndEnergy).
 // ============================================================================
-template <int NQ>
+template <int NQ, bool VIR>
 struct PairEval {
     const PairCoef& pc;  // the kernel parameter: constant-bank operands
     float rc2, irc2, irc, tirc3, Lx, Ly, Lz, iLx, iLy, iLz;
@@ -748,17 +1251,19 @@ struct PairEval {
             fx = fmaf(fdr, dx, fx);
             fy = fmaf(fdr, dy, fy);
             fz = fmaf(fdr, dz, fz);
-            vxx = fmaf(fdr * dx, dx, vxx);
-            vxy = fmaf(fdr * dx, dy, vxy);
-            vxz = fmaf(fdr * dx, dz, vxz);
-            vyy = fmaf(fdr * dy, dy, vyy);
-            vyz = fmaf(fdr * dy, dz, vyz);
-            vzz = fmaf(fdr * dz, dz, vzz);
+            if (VIR) {
+                vxx = fmaf(fdr * dx, dx, vxx);
+                vxy = fmaf(fdr * dx, dy, vxy);
+                vxz = fmaf(fdr * dx, dz, vxz);
+                vyy = fmaf(fdr * dy, dy, vyy);
+                vyz = fmaf(fdr * dy, dz, vyz);
+                vzz = fmaf(fdr * dz, dz, vzz);
+            }
         }
     }
 };
 
-template <int TPP, int NQ>
+template <int TPP, int NQ, bool VIR>
 __global__ void __launch_bounds__(256)
     k_pair(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
            const float4* __restrict__ posq, const uint32_t* __restrict__ head, const uint32_t* __restrict__ nn,
@@ -766,9 +1271,9 @@ __global__ void __launch_bounds__(256)
            const PairCoef pc) {
     __shared__ double red[32 * 7];
     const int2 ch = chunks[blockIdx.x];
-    const SysDev& S = sys[ch.x];
+    const SysDev S = sys[ch.x];
     const ParamSet& ps = psets[S.pset];
-    PairEval<NQ> ev{pc};
+    PairEval<NQ, VIR> ev{pc};
     ev.rc2 = ps.rcut2;
     ev.irc = ps.inv_rcut;
     ev.irc2 = ps.inv_rcut * ps.inv_rcut;
@@ -822,13 +1327,19 @@ __global__ void __launch_bounds__(256)
         f.w += 0.5f * en;
         force[i] = f;
     }
-    double e[7] = {sub == 0 ? 0.5 * (double)en : 0.0, 0.5 * (double)ev.vxx, 0.5 * (double)ev.vxy,
-                   0.5 * (double)ev.vxz, 0.5 * (double)ev.vyy, 0.5 * (double)ev.vyz, 0.5 * (double)ev.vzz};
-    block_sum_f64<7>(e, red);
-    if (threadIdx.x == 0) {
-        atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_E], e[0]);
+    if (VIR) {
+        double e[7] = {sub == 0 ? 0.5 * (double)en : 0.0, 0.5 * (double)ev.vxx, 0.5 * (double)ev.vxy,
+                       0.5 * (double)ev.vxz, 0.5 * (double)ev.vyy, 0.5 * (double)ev.vyz, 0.5 * (double)ev.vzz};
+        block_sum_f64<7>(e, red);
+        if (threadIdx.x == 0) {
+            atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_E], e[0]);
 #pragma unroll
-        for (int k = 0; k < 6; ++k) atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_WP + k], e[1 + k]);
+            for (int k = 0; k < 6; ++k) atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_WP + k], e[1 + k]);
+        }
+    } else {
+        double e[1] = {sub == 0 ? 0.5 * (double)en : 0.0};
+        block_sum_f64<1>(e, red);
+        if (threadIdx.x == 0) atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_E], e[0]);
     }
 }
 
@@ -838,7 +1349,7 @@ __global__ void k_finalize(const SysDev* __restrict__ sys, const ParamSet* __res
                            int add_bg) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nsys) return;
-    const SysDev& S = sys[s];
+    const SysDev S = sys[s];
     const double* a = acc + s * ACC_STRIDE;
     const double Q = a[ACC_QSUM];
     const double ebg = add_bg ? psets[S.pset].bg_coef * Q * Q / S.V : 0.0;
@@ -907,26 +1418,43 @@ __global__ void k_pswf_eval_pairs(int n, const double* __restrict__ rsq, const d
 template <int P>
 static cudaError_t launch_spread_p(const LaunchArgs& a, cudaStream_t st) {
     using C = SpreadCfg<P>;
+    const bool mma = a.T + P - 1 == SPREAD_EM && a.spread_mode == 0;
+    const bool dense = a.T + P - 1 <= SPREAD_EM;
     const int nb = (a.T + 2 * P - 2) / P;
     const size_t NL = (size_t)nb * nb * nb * C::P3;
     const size_t smem = NL * sizeof(float2) + (size_t)C::CH * P * 4 * 4 + C::CH * 4 + P * (MAX_D + 1) * 4;
-    if (a.configure_only)
+    const size_t smem_d = (size_t)SPREAD_CHD * 16 * 4 + (size_t)SPREAD_CHD * (2 * P + 1) * 4 + P * (MAX_D + 1) * 4;
+    const size_t smem_m = (size_t)SPREAD_CHM * 16 * 4 + (size_t)SPREAD_CHM * (2 * P + 1) * 4 + P * (MAX_D + 1) * 4;
+    if (a.configure_only) {
+        cudaError_t e = cudaFuncSetAttribute(k_spread_mma<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(k_spread_dense<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_d);
+        if (e != cudaSuccess || dense) return e;
         return cudaFuncSetAttribute(k_spread<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    }
     if (a.n_tiles == 0) return cudaSuccess;
-    k_spread<P><<<a.n_tiles, C::THREADS, smem, st>>>(a.tile_sys, a.sys, a.psets, a.T, a.D, a.tile_start, a.srec,
-                                                       a.srel, a.rho);
+    if (mma)
+        k_spread_mma<P><<<a.n_tiles, 256, smem_m, st>>>(a.tile_sys, a.sys, a.psets, a.T, a.D, a.tile_start, a.srec,
+                                                        a.srel, a.rho);
+    else if (dense)
+        k_spread_dense<P><<<a.n_tiles, 256, smem_d, st>>>(a.tile_sys, a.sys, a.psets, a.T, a.D, a.tile_start, a.srec,
+                                                          a.srel, a.rho);
+    else
+        k_spread<P><<<a.n_tiles, C::THREADS, smem, st>>>(a.tile_sys, a.sys, a.psets, a.T, a.D, a.tile_start, a.srec,
+                                                          a.srel, a.rho);
     return cudaGetLastError();
 }
 
 template <int P>
 static cudaError_t launch_interp_p(const LaunchArgs& a, cudaStream_t st) {
+    using C = InterpCfg<P>;
     const int E = a.T + P - 1;
-    const size_t smem = ((size_t)E * a.PP + P * (MAX_D + 1)) * 4;
+    const size_t smem = ((size_t)E * a.PP + interp_stage_words(P, C::CH, E) + 2 * C::CH + P * (MAX_D + 1)) * 4;
     if (a.configure_only)
         return cudaFuncSetAttribute(k_interp<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (a.n_tiles == 0) return cudaSuccess;
-    k_interp<P><<<a.n_tiles, 128, smem, st>>>(a.tile_sys, a.sys, a.psets, a.T, a.D, a.PX, a.PP, a.tile_start,
-                                                a.perm, a.srec, a.srel, a.phi, a.force, a.acc);
+    k_interp<P><<<a.n_tiles, C::THREADS, smem, st>>>(a.tile_sys, a.sys, a.psets, a.T, a.D, a.PX, a.PP, a.tile_start,
+                                                       a.perm, a.srec, a.srel, a.phi, a.force, a.acc);
     return cudaGetLastError();
 }
 
@@ -976,29 +1504,41 @@ cudaError_t launch_spread(const LaunchArgs& a, cudaStream_t st) { ESPB_DISPATCH_
 cudaError_t launch_interp(const LaunchArgs& a, cudaStream_t st) { ESPB_DISPATCH_P(launch_interp_p, a.P, a, st); }
 
 cudaError_t launch_fft(const LaunchArgs& a, cudaStream_t st) {
-    const size_t smx = 2 * FFT_MAX_N * FFT_SB_X * sizeof(float2);
-    const size_t smyz = 2 * FFT_MAX_N * FFT_B_YZ * sizeof(float2);
+    // attributes allow the largest transform; launches request what the
+    // batch's longest line on that axis needs (occupancy for small meshes)
+    const size_t smx = 2 * (a.configure_only ? FFT_MAX_N : a.nmax_x) * FFT_SB_X * sizeof(float2);
+    const size_t smy = 2 * (a.configure_only ? FFT_MAX_N : a.nmax_y) * FFT_B_YZ * sizeof(float2);
+    const size_t smz = 2 * (a.configure_only ? FFT_MAX_N : a.nmax_z) * FFT_B_YZ * sizeof(float2);
+    const size_t smyz = smy > smz ? smy : smz;
     if (a.configure_only) {
         cudaError_t e;
         if ((e = cudaFuncSetAttribute(k_fftx_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx))) return e;
         if ((e = cudaFuncSetAttribute(k_fftx_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx))) return e;
         if ((e = cudaFuncSetAttribute(k_ffty<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz))) return e;
         if ((e = cudaFuncSetAttribute(k_ffty<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz))) return e;
-        return cudaFuncSetAttribute(k_fftz_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz);
+        if ((e = cudaFuncSetAttribute(k_fftz_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz))) return e;
+        if ((e = cudaFuncSetAttribute(k_fft_plane_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_MAX)))
+            return e;
+        if ((e = cudaFuncSetAttribute(k_fft_plane_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_MAX)))
+            return e;
+        return cudaFuncSetAttribute(k_fft_slab_z, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_MAX);
     }
+    if (a.n_pitems) k_fft_plane_fwd<<<a.n_pitems, 512, a.smem_plane, st>>>(a.pitems, a.sys, a.tw, a.rho, a.spec);
     if (a.n_xitems) k_fftx_fwd<<<a.n_xitems, 256, smx, st>>>(a.xitems, a.sys, a.tw, a.rho, a.spec);
-    if (a.n_yitems) k_ffty<false><<<a.n_yitems, 256, smyz, st>>>(a.yitems, a.sys, a.tw, a.spec);
-    if (a.n_zitems) k_fftz_conv<<<a.n_zitems, 256, smyz, st>>>(a.zitems, a.sys, a.tw, a.gtab, a.spec, a.acc);
-    if (a.n_yitems) k_ffty<true><<<a.n_yitems, 256, smyz, st>>>(a.yitems, a.sys, a.tw, a.spec);
-    if (a.n_xitems) k_fftx_inv<<<a.n_xitems, 256, smx, st>>>(a.xitems, a.sys, a.tw, a.spec, a.phi);
+    if (a.n_yitems) k_ffty<false><<<a.n_yitems, 256, smy, st>>>(a.yitems, a.sys, a.tw, a.spec);
+    if (a.n_sitems) k_fft_slab_z<<<a.n_sitems, 512, a.smem_slab, st>>>(a.sitems, a.sys, a.tw, a.gtab, a.spec, a.acc);
+    if (a.n_zitems) k_fftz_conv<<<a.n_zitems, 256, smz, st>>>(a.zitems, a.sys, a.tw, a.gtab, a.spec, a.acc);
+    if (a.n_yitems) k_ffty<true><<<a.n_yitems, 256, smy, st>>>(a.yitems, a.sys, a.tw, a.spec);
+    if (a.n_xitems) k_fftx_inv<<<a.n_xitems, 256, smx, st>>>(a.xitems, a.sys, a.tw, a.spec, a.phi, a.rho);
+    if (a.n_pitems) k_fft_plane_inv<<<a.n_pitems, 512, a.smem_plane, st>>>(a.pitems, a.sys, a.tw, a.spec, a.phi, a.rho);
     return cudaGetLastError();
 }
 
-template <int TPP>
+template <int TPP, bool VIR>
 static cudaError_t launch_pair_t(const LaunchArgs& a, cudaStream_t st) {
-#define ESPB_PAIR(NQ)                                                                                         \
-    k_pair<TPP, NQ><<<a.n_pchunks, 256, 0, st>>>(a.pchunks, a.sys, a.psets, a.posq, a.nl_head, a.nl_n, a.nl_list, \
-                                                 a.force, a.acc, a.accumulate, a.pc)
+#define ESPB_PAIR(NQ)                                                                                    \
+    k_pair<TPP, NQ, VIR><<<a.n_pchunks, 256, 0, st>>>(a.pchunks, a.sys, a.psets, a.posq, a.nl_head, a.nl_n, \
+                                                      a.nl_list, a.force, a.acc, a.accumulate, a.pc)
     if (a.nq <= 8) ESPB_PAIR(8);
     else if (a.nq <= 10) ESPB_PAIR(10);
     else if (a.nq <= 12) ESPB_PAIR(12);
@@ -1013,11 +1553,20 @@ static cudaError_t launch_pair_t(const LaunchArgs& a, cudaStream_t st) {
 
 cudaError_t launch_pair(const LaunchArgs& a, cudaStream_t st) {
     if (a.n_pchunks == 0) return cudaSuccess;
+    if (a.want_virial) {
+        switch (a.tpp) {
+            case 4: return launch_pair_t<4, true>(a, st);
+            case 8: return launch_pair_t<8, true>(a, st);
+            case 16: return launch_pair_t<16, true>(a, st);
+            case 32: return launch_pair_t<32, true>(a, st);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (a.tpp) {
-        case 4: return launch_pair_t<4>(a, st);
-        case 8: return launch_pair_t<8>(a, st);
-        case 16: return launch_pair_t<16>(a, st);
-        case 32: return launch_pair_t<32>(a, st);
+        case 4: return launch_pair_t<4, false>(a, st);
+        case 8: return launch_pair_t<8, false>(a, st);
+        case 16: return launch_pair_t<16, false>(a, st);
+        case 32: return launch_pair_t<32, false>(a, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -12,6 +12,16 @@
 namespace espb {
 
 constexpr int SORT_CAP = 2048;  // particles per tile sorted in shared memory
+constexpr int FFT_SMEM_MAX = 220 * 1024;  // shared memory of the plane / slab FFT passes
+
+// shared memory (bytes) of the plane pass of an nx x ny plane and of the z
+// pass of an nz x nxh slab; line strides are rounded up to odd numbers
+inline int fft_plane_smem(int nx, int ny) {
+    const int np = (ny + 1) / 2, nxh = nx / 2 + 1;
+    const int c = std::max(nx * (np | 1), ny * (nxh | 1));
+    return 2 * c * 8;
+}
+inline int fft_slab_smem(int nx, int nz) { return 2 * nz * ((nx / 2 + 1) | 1) * 8; }
 
 // Split-polynomial coefficients of a batch, passed by value so the pair
 // kernel's FMAs read them from the kernel-parameter constant bank.
@@ -54,12 +64,20 @@ struct LaunchArgs {
     int n_yitems = 0;
     const int4* zitems = nullptr;
     int n_zitems = 0;
+    const int2* pitems = nullptr;  // {sys, z}: whole-plane x/y passes
+    int n_pitems = 0;
+    const int2* sitems = nullptr;  // {sys, y}: whole-slab z pass
+    int n_sitems = 0;
+    int smem_plane = 0, smem_slab = 0;
     float4* force = nullptr;
     double* acc = nullptr;
     double* energy = nullptr;
     double* virial = nullptr;
     int add_bg = 1;
-    int configure_only = 0;  // set kernel attributes (plan time) instead of launching
+    int want_virial = 1;
+    int spread_mode = 0;  // 0: tensor-core spreading when E == 16; 1: CUDA-core kernels  // accumulate the pair virial (skipped when no virial is requested)
+    int configure_only = 0;
+    int nmax_x = FFT_MAX_N, nmax_y = FFT_MAX_N, nmax_z = FFT_MAX_N;  // longest line per axis  // set kernel attributes (plan time) instead of launching
     const uint32_t* nl_head = nullptr;
     const uint32_t* nl_n = nullptr;
     const uint32_t* nl_list = nullptr;

@@ -197,6 +197,11 @@ void Split::build(double c_, double tol) {
     };
     for (int deg = 6; deg <= 30; ++deg) {
         qv = cheb_interp_monomial([&](double v) { return qfun(0.5 * (v + 1.0)); }, deg);
+        // pin Q(1) = 1 (v = 1: sum of the coefficients), i.e. S(r_c) = 0, so
+        // the pair energy is continuous at the cutoff
+        double s1 = 0.0;
+        for (double c : qv) s1 += c;
+        qv[0] += 1.0 - s1;
         double err = 0.0;
         for (int i = 0; i <= 2000; ++i) {
             double u = i / 2000.0;

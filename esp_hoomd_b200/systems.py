@@ -29,20 +29,24 @@ class System:
         return int(self.pos.shape[0])
 
 
-def rocksalt(n: int, spacing: float = 1.0, jitter: float = 0.1, seed: int = 0, T: float = 1.0) -> System:
-    """n^3 simple-cubic lattice, q = (-1)^(ix+iy+iz), uniform jitter
-    U(-jitter, jitter) per axis, Maxwell velocities at temperature T with
-    the centre-of-mass momentum removed, mass 1."""
+def rocksalt(n: int, spacing: float = 1.0, jitter: float = 0.1, seed: int = 0, T: float = 1.0,
+             shape: Tuple[int, int, int] = None) -> System:
+    """n^3 (or shape[0] x shape[1] x shape[2]) simple-cubic lattice,
+    q = (-1)^(ix+iy+iz), uniform jitter U(-jitter, jitter) per axis, Maxwell
+    velocities at temperature T with the centre-of-mass momentum removed,
+    mass 1. Box edges = lattice counts x spacing."""
     rng = np.random.default_rng(seed)
-    ix, iy, iz = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    nx, ny, nz = shape if shape is not None else (n, n, n)
+    ix, iy, iz = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
     idx = np.stack([ix.ravel(), iy.ravel(), iz.ravel()], -1)
     pos = (idx + 0.5) * spacing + rng.uniform(-jitter, jitter, idx.shape)
-    L = n * spacing
+    L = np.array([nx, ny, nz], dtype=np.float64) * spacing
     pos = np.mod(pos, L)
     q = np.where(np.sum(idx, -1) % 2 == 0, 1.0, -1.0)
     vel = rng.normal(0.0, math.sqrt(T), idx.shape)
     vel -= vel.mean(0)
-    return System(pos=pos, q=q, vel=vel, mass=np.ones(pos.shape[0]), box=(L, L, L), name="rocksalt%d" % n)
+    return System(pos=pos, q=q, vel=vel, mass=np.ones(pos.shape[0]), box=tuple(float(v) for v in L),
+                  name="rocksalt%dx%dx%d" % (nx, ny, nz))
 
 
 def water(n_mol: int, density: float = 33.4, seed: int = 0, q_o: float = -0.8476, r_oh: float = 0.1,

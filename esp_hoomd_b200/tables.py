@@ -194,7 +194,9 @@ def make_split(c: float, degree: int = 0, tol: float = 1e-8) -> SplitTable:
     degs = [degree] if degree else range(6, 31)
     for d in degs:
         qv = _cheb_interp_monomial(lambda v: qfun(0.5 * (v + 1.0)), d)
-        err = float(np.max(np.abs(np.polynomial.polynomial.polyval(2 * uu - 1, qv) - qfun(uu))))
+        # pin Q(1) = 1, i.e. S(r_c) = 0: the pair energy is continuous at r_c
+        qv[0] += 1.0 - float(np.sum(qv))
+        err =float(np.max(np.abs(np.polynomial.polynomial.polyval(2 * uu - 1, qv) - qfun(uu))))
         if err < tol:
             break
     xg, wg = np.polynomial.legendre.leggauss(64)
@@ -472,6 +474,7 @@ def eval_segment_L(tab: SegmentTable, r, rcut: Optional[float] = None):
     S = horner(cs)
     dS = horner(cd)
     inv4pir = INV_4PI / r[ok]
+    inv4pir2 = inv4pir / r[ok]
     L[ok] = S * inv4pir
-    D[ok] = S * inv4pir / r[ok] - dS * inv4pir
+    D[ok] = S * inv4pir2 - dS * inv4pir
     return L, D

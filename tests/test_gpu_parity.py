@@ -95,6 +95,29 @@ def test_potential_and_forces_match_oracle(rs8):
     assert abs(f[:, 3].astype(np.float64).sum() - (E - parts["E_bg"])) <= 5e-6 * abs(E)
 
 
+@pytest.mark.parametrize("shape", [(22, 22, 22), (90, 90, 8), (90, 8, 90), (12, 10, 14)])
+def test_mesh_shapes_match_oracle(shape):
+    """Odd meshes (45), xy planes (180 x 180) and xz slabs (180 x 180)
+    too large for shared memory (the per-line FFT passes) and non-cubic
+    boxes, against the FP64 oracle."""
+    s = systems.rocksalt(0, seed=sum(shape), shape=shape)
+    s.pos = s.pos.astype(np.float32).astype(np.float64)
+    ctx = native.Context(native.make_params(), s.box, s.N)
+    pos4, q = _upload(s)
+    head, cnt, lst = R.neighbor_list(s.pos, s.box, 3.0)
+    force = torch.zeros((s.N, 4), dtype=torch.float32, device="cuda")
+    energy = torch.zeros(1, dtype=torch.float64, device="cuda")
+    virial = torch.zeros(6, dtype=torch.float64, device="cuda")
+    ctx.compute(pos4, q, force, energy, virial, nlist=_nlist_dev(head, cnt, lst))
+    torch.cuda.synchronize()
+    prm = _oracle_params(ctx.info(), s.box)
+    E, F, W = R.esp(s.pos, s.q, prm, nlist=(head, cnt, lst))
+    f = force.cpu().numpy()[:, :3].astype(np.float64)
+    assert R.rel_rms(f, F) <= 5e-6
+    assert abs(energy.item() - E) <= 2e-6 * abs(E)
+    assert np.abs(virial.cpu().numpy() - W).max() <= 1e-5 * np.abs(W).max()
+
+
 def test_accuracy_vs_ewald(rs8):
     ctx = native.Context(native.make_params(target_error=1e-5), rs8.box, rs8.N)
     pos4, q = _upload(rs8)

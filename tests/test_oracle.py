@@ -1,0 +1,181 @@
+"""CPU tests of the oracle and the table generator (no GPU needed).
+
+* the oracle's restatement of the reference pair evaluator is bit-exact
+  against the reference compiled from its own sources (golden fixtures);
+* the shipped PSWF_Coeffs.h known answers (S(0) = 1/2 etc., the reference's
+  defects, pinned as they are);
+* the prolate solver against scipy.special.pro_ang1 and the Fourier
+  eigen-relation; split and window fits;
+* the Ewald oracle against finite differences and its own parameter
+  independence;
+* the ESP oracle: forces are the exact gradient of its energy, and it
+  converges to Ewald at the default (1e-5) parameters.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from esp_hoomd_b200 import systems, tables
+from oracle import esp_ref as R
+from oracle import evaluator as EV
+from oracle.ewald import ewald
+
+
+@pytest.fixture(scope="module")
+def shipped(golden_dir):
+    t = np.load(golden_dir + "/pswf_coeffs_shipped.npz")
+    return (t["screen"], t["dscreen"], t["r_lo"], t["dr_inv"]), float(t["rcut"])
+
+
+def test_evaluator_restatement_bit_exact(golden_dir, shipped):
+    g = np.load(golden_dir + "/pswf_eval_golden.npz")
+    table, rcut = shipped
+    with np.errstate(divide="ignore", invalid="ignore"):
+        fd, pe, ok = EV.eval_force_energy(g["rsq"], g["qiqj"], rcut, table)
+    assert np.array_equal(ok, g["evaluated"])
+    assert np.array_equal(fd, g["force_divr"], equal_nan=True)
+    assert np.array_equal(pe, g["pair_eng"], equal_nan=True)
+    L, D = EV.pswf_eval_L(g["r"], rcut, *table)
+    assert np.array_equal(L, g["L"]) and np.array_equal(D, g["negdLdr"])
+
+
+def test_evaluator_known_answers(shipped):
+    # values of the reference evaluator compiled from its sources (r_c = 1)
+    table, rcut = shipped
+    L, D = EV.pswf_eval_L(np.array([0.1, 0.25, 0.5, 0.75]), rcut, *table)
+    assert L.tolist() == [0.2698302206310154, 0.04716774142484325, 0.002554122723247796, 3.573561155029599e-05]
+    assert D.tolist() == [3.9099951149259775, 0.5010553234185513, 0.034535829960987245, 0.0007858715534125451]
+    fd, pe, ok = EV.eval_force_energy(np.array([0.25]), np.array([-1.0]), rcut, table)
+    assert fd[0] == -0.06907165992197449 and pe[0] == -0.002554122723247796 and ok[0] == 1
+
+
+def test_shipped_table_is_not_a_coulomb_split(shipped):
+    # the reference screening starts at S(0) = 1/2 (CDF of psi^2 on [-1, 1])
+    (screen, dscreen, r_lo, dr_inv), rcut = shipped
+    assert screen[0] == 5.00000000000008993e-01
+    assert r_lo.size == 4096 and dr_inv[0] == 4096.0
+
+
+def test_segment_table_roundtrip(shipped):
+    (screen, dscreen, r_lo, dr_inv), rcut = shipped
+    tab = tables.SegmentTable(rcut=rcut, screen=screen, dscreen=dscreen, r_lo=r_lo, dr_inv=dr_inv)
+    text = tables.emit_pswf_coeffs_header(tab)
+    back = tables.parse_pswf_coeffs_header(text)
+    assert np.array_equal(back.screen, screen) and np.array_equal(back.r_lo, r_lo)
+    r = np.linspace(0.0, 1.1, 777)
+    L1, D1 = tables.eval_segment_L(tab, r)
+    L2, D2 = EV.pswf_eval_L(r, rcut, screen, dscreen, r_lo, dr_inv)
+    assert np.array_equal(L1, L2) and np.array_equal(D1, D2)
+
+
+@pytest.mark.parametrize("c", [6.0, 12.0, 18.0])
+def test_prolate_matches_scipy(c):
+    from scipy.special import pro_ang1
+
+    p = tables.Prolate(c)
+    x = np.linspace(-0.95, 0.95, 9)
+    ref, _ = pro_ang1(0, 0, c, x)
+    ratio = ref / p.psi(x)
+    assert np.ptp(ratio) < 1e-9 * abs(ratio.mean())
+    kap = np.array([0.0, 1.0, 0.5 * c, 0.9 * c])
+    assert np.allclose(p.fourier_ratio(kap), p.psi(kap / c) / p.psi0, rtol=1e-10, atol=1e-14)
+
+
+def test_split_properties():
+    sp = tables.make_split(17.5)
+    s = np.linspace(0, 1, 101)
+    assert abs(sp.S(np.array([0.0]))[0] - 1.0) < 1e-14
+    assert abs(sp.S(np.array([1.0 - 1e-12]))[0]) < 1e-9
+    # S(s) = 1 - s Q(s^2) with the fitted polynomial
+    assert np.max(np.abs(1.0 - s * sp.Q(s * s) - sp.S(s))) < 2e-8
+    # dQ/du is the derivative of Q
+    u = np.linspace(0.05, 0.95, 19)
+    h = 1e-6
+    assert np.allclose(sp.dQ(u), (sp.Q(u + h) - sp.Q(u - h)) / (2 * h), rtol=1e-6, atol=1e-8)
+    assert sp.fit_err < 1e-8
+
+
+def test_window_fit_and_fourier():
+    w = tables.make_window(8, 17.6)
+    assert w.fit_err < 1e-9
+    t = np.linspace(0.0, 1.0, 11)[:-1]  # t = 1 is the support edge (value() returns 0 there)
+    W = w.weights(t)
+    # weights at t and the continuous window at the stencil offsets agree
+    u = np.arange(8)[None, :] - 4.0 + t[:, None]
+    assert np.allclose(W, w.value(u), atol=1e-10)
+    # Fourier transform at 0 equals the integral of the window
+    xs = np.linspace(-4, 4, 40001)
+    assert abs(w.fourier(0.0)[0] - np.trapezoid(w.value(xs), xs)) < 1e-6
+
+
+def test_smooth235():
+    assert [tables.smooth235(n) for n in (1, 7, 14, 28, 44, 52, 77, 97)] == [1, 8, 15, 30, 45, 54, 80, 100]
+
+
+def test_ewald_forces_are_gradients():
+    rng = np.random.default_rng(3)
+    pos = rng.uniform(0, 4.0, (24, 3))
+    q = rng.choice([-1.0, 1.0], 24)
+    E, F, W = ewald(pos, q, (4.0, 4.0, 4.0))
+    h = 1e-5
+    for i, a in ((0, 0), (5, 2)):
+        p1, p2 = pos.copy(), pos.copy()
+        p1[i, a] += h
+        p2[i, a] -= h
+        fd = -(ewald(p1, q, (4.0, 4.0, 4.0))[0] - ewald(p2, q, (4.0, 4.0, 4.0))[0]) / (2 * h)
+        assert abs(fd - F[i, a]) < 1e-7
+    E2, F2, W2 = ewald(pos, q, (4.0, 4.0, 4.0), tol_exp=30.0)
+    assert abs(E - E2) < 1e-11 and np.abs(F - F2).max() < 1e-10 and np.abs(W - W2).max() < 1e-10
+
+
+def test_esp_oracle_gradient_and_accuracy():
+    s = systems.rocksalt(8, seed=11)
+    # the mesh stage sees float32 positions (as the device does): start from
+    # float32 values and step by an exactly representable h, with a fixed list
+    s.pos = s.pos.astype(np.float32).astype(np.float64)
+    prm = tables.ESPParams(mesh=(16, 16, 16), box=s.box, rcut=3.0, split=tables.split_cached(17.5),
+                           window=tables.window_cached(8, 17.6, 10))
+    nl = R.neighbor_list(s.pos, s.box, 3.3)
+    E, F, W = R.esp(s.pos, s.q, prm, nlist=nl)
+    h = 2.0 ** -12
+    for i, a in ((0, 0), (100, 1)):
+        p1, p2 = s.pos.copy(), s.pos.copy()
+        p1[i, a] += h
+        p2[i, a] -= h
+        fd = -(R.esp(p1, s.q, prm, nlist=nl)[0] - R.esp(p2, s.q, prm, nlist=nl)[0]) / (2 * h)
+        assert abs(fd - F[i, a]) < 2e-7
+    E0, F0, W0 = ewald(s.pos, s.q, s.box)
+    assert R.rel_rms(F, F0) < 1e-5
+    assert abs(E - E0) < 1e-6 * abs(E0)
+    assert np.abs(W - W0).max() < 1e-5 * np.abs(W0).max()
+
+
+def test_bin_sort_is_stable():
+    s = systems.rocksalt(6, seed=2)
+    key, perm = R.bin_sort(s.pos, s.box, (16, 16, 16), 8, 8)
+    assert np.all(np.diff(key[perm].astype(np.int64)) >= 0)
+    for k in np.unique(key):
+        idx = perm[key[perm] == k]
+        assert np.all(np.diff(idx.astype(np.int64)) > 0)
+
+
+def test_neighbor_list_matches_brute_force():
+    s = systems.rocksalt(6, seed=4)
+    head, cnt, lst = R.neighbor_list(s.pos, s.box, 2.5)
+    L = np.asarray(s.box)
+    d = s.pos[:, None, :] - s.pos[None, :, :]
+    d -= L * np.round(d / L)
+    r2 = np.sum(d * d, -1)
+    np.fill_diagonal(r2, np.inf)
+    for i in range(0, s.N, 17):
+        ref = np.nonzero(r2[i] < 2.5 ** 2)[0]
+        assert np.array_equal(np.sort(lst[head[i]:head[i] + cnt[i]]), ref)
+
+
+def test_water_system():
+    w = systems.water(27, seed=1)
+    assert w.N == 81
+    assert abs(w.q.sum()) < 1e-12
+    L = w.box[0]
+    assert abs(L - (27 / 33.4) ** (1 / 3)) < 1e-12
