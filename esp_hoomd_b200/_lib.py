@@ -25,7 +25,7 @@ EXPORTS = [
     "esp_compute", "esp_get_info", "esp_destroy", "esp_batch_create", "esp_batch_compute", "esp_batch_get_info",
     "esp_batch_total_particles", "esp_batch_destroy", "esp_pswf_eval_pairs", "esp_batch_build_nlist",
     "esp_batch_nve_step1", "esp_batch_nve_step2", "esp_spread", "esp_get_sort", "esp_get_potential",
-    "esp_batch_md_run", "esp_batch_set_timing", "esp_batch_stage_times",
+    "esp_batch_md_run", "esp_batch_set_timing", "esp_batch_stage_times", "esp_spread_noalloc",
 ]
 
 STAGES = ["bin", "sort", "spread", "fft", "interp", "pair", "nlist", "nve"]
@@ -91,6 +91,7 @@ def get_lib() -> ctypes.CDLL:
         lib.esp_batch_md_run.argtypes = [P, P, P, P, P, P, P, P, P, P, P, I, D, I]
         lib.esp_batch_set_timing.argtypes = [P, I]
         lib.esp_batch_stage_times.argtypes = [P, P, P]
+        lib.esp_spread_noalloc.argtypes = [P, ctypes.POINTER(EspParams), D, D, D, P, P, I, P]
         for name in EXPORTS:
             if name != "esp_last_error":
                 getattr(lib, name).restype = ctypes.c_int

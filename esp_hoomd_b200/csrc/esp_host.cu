@@ -1038,3 +1038,216 @@ int esp_batch_nve_step2(esp_batch* b, void* stream, float* vel4, const float* fo
 }
 
 }  // extern "C"
+
+// ============================================================================
+// No-allocation spreading (esp_spread_noalloc).
+//
+// For callers that cannot allocate device memory (an engine whose pool
+// allocator owns all of the device memory, or a step that must not call
+// cudaFree because it synchronises the device): bin + sort + spreading of
+// one system with every work array carved out of one file-scope scratch
+// array of fixed size. The kernels are the ones esp_spread launches; only
+// where their work arrays live differs.
+// ============================================================================
+#include <mutex>
+
+namespace {
+
+constexpr int NA_MAX_N = ESP_SPREAD_NOALLOC_MAX_N;
+constexpr int NA_MAX_TILES = ESP_SPREAD_NOALLOC_MAX_TILES;
+static_assert(NA_MAX_N % 256 == 0, "particle limit must be a whole number of 256-particle chunks");
+constexpr size_t na_round(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Byte offsets of the work arrays inside the scratch array (256-byte aligned).
+constexpr size_t NA_SYS = 0;
+constexpr size_t NA_PSET = NA_SYS + na_round(sizeof(SysDev));
+constexpr size_t NA_CHUNKS = NA_PSET + na_round(sizeof(ParamSet));
+constexpr size_t NA_TILE_SYS = NA_CHUNKS + na_round(sizeof(int2) * (NA_MAX_N / 256));
+constexpr size_t NA_TCOUNT = NA_TILE_SYS + na_round(sizeof(int) * NA_MAX_TILES);
+constexpr size_t NA_TSTART = NA_TCOUNT + na_round(sizeof(uint32_t) * NA_MAX_TILES);
+constexpr size_t NA_ACC = NA_TSTART + na_round(sizeof(uint32_t) * (NA_MAX_TILES + 1));
+constexpr size_t NA_POSQ = NA_ACC + na_round(sizeof(double) * ACC_STRIDE);
+constexpr size_t NA_TREC = NA_POSQ + sizeof(float4) * NA_MAX_N;
+constexpr size_t NA_SREC = NA_TREC + sizeof(float4) * NA_MAX_N;
+constexpr size_t NA_REL = NA_SREC + sizeof(float4) * NA_MAX_N;
+constexpr size_t NA_SREL = NA_REL + sizeof(uint32_t) * NA_MAX_N;
+constexpr size_t NA_KEY = NA_SREL + sizeof(uint32_t) * NA_MAX_N;
+constexpr size_t NA_PERM_U = NA_KEY + sizeof(uint32_t) * NA_MAX_N;
+constexpr size_t NA_PERM = NA_PERM_U + sizeof(uint32_t) * NA_MAX_N;
+constexpr size_t NA_BYTES = NA_PERM + sizeof(uint32_t) * NA_MAX_N;  // 2,280,448 bytes
+static_assert(NA_BYTES <= (size_t)3 << 20, "scratch must stay a few MB");
+
+// The scratch itself. In host code this name is only a handle for
+// cudaGetSymbolAddress, never a device address.
+static __device__ __align__(256) unsigned char g_na_scratch[NA_BYTES];
+
+constexpr int NA_MAX_DEVICES = 64;
+std::mutex g_na_mutex;
+unsigned char* g_na_base[NA_MAX_DEVICES] = {};
+
+// One-time set-up per device, with that device current: the scratch
+// array's device address and the spreading kernels' shared-memory limits.
+int na_setup(unsigned char** base) {
+    int dev = 0;
+    ESPB_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NA_MAX_DEVICES) return fail(ESP_ERR_UNSUPPORTED, "device index above 63");
+    std::lock_guard<std::mutex> lock(g_na_mutex);
+    if (!g_na_base[dev]) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_na_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(ESP_ERR_CUDA, std::string("cudaGetSymbolAddress of the spreading scratch: ") +
+                                          cudaGetErrorString(e));
+        for (int P = 2; P <= MAX_P; ++P) {
+            LaunchArgs a;
+            a.configure_only = 1;
+            a.P = P;
+            a.T = 17 - P;  // extended region of 16: the tensor-core and dense kernels
+            ESPB_CK(launch_spread(a, 0));
+        }
+        g_na_base[dev] = static_cast<unsigned char*>(ptr);
+    }
+    *base = g_na_base[dev];
+    return 0;
+}
+
+// Window coefficients per (P, c_w, D), built once on the host.
+int na_param_set(int P, double cw, int D, ParamSet* out) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, double, int>, ParamSet> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    const auto key = std::make_tuple(P, cw, D);
+    auto it = cache.find(key);
+    if (it == cache.end()) {
+        Window win;
+        try {
+            win.build(P, cw, D);
+        } catch (const std::exception& ex) {
+            return fail(ESP_ERR_INVALID, ex.what());
+        }
+        ParamSet d{};
+        for (int a = 0; a < P; ++a)
+            for (int j = 0; j <= D; ++j) d.wcoef[a * (MAX_D + 1) + j] = (float)win.coef[(size_t)a * (D + 1) + j];
+        it = cache.emplace(key, d).first;
+    }
+    *out = it->second;
+    return 0;
+}
+
+// Writes the system descriptor, window coefficients and work lists into the
+// scratch, and clears what the bin kernel accumulates into (tile counts and
+// the charge sums): the scratch keeps the previous call's contents.
+__global__ void k_na_prepare(SysDev S, ParamSet ps, SysDev* sys, ParamSet* pset, int2* chunks, int n_chunks,
+                             int* tile_sys, uint32_t* tile_count, int n_tiles, double* acc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        *sys = S;
+        *pset = ps;
+    }
+    if (i < n_chunks) chunks[i] = make_int2(0, 256 * i);
+    if (i < n_tiles) {
+        tile_sys[i] = 0;
+        tile_count[i] = 0u;
+    }
+    if (i < ACC_STRIDE) acc[i] = 0.0;
+}
+
+}  // namespace
+
+extern "C" int esp_spread_noalloc(void* stream, const esp_params* p, double Lx, double Ly, double Lz,
+                                  const float* pos4, const float* charge, int N, double* rho) {
+    if (!p || !pos4 || !charge || !rho) return fail(ESP_ERR_INVALID, "null argument");
+    if (N <= 0) return fail(ESP_ERR_INVALID, "particle count must be positive");
+    if (N > NA_MAX_N)
+        return fail(ESP_ERR_UNSUPPORTED, "esp_spread_noalloc: N = " + std::to_string(N) +
+                                             " exceeds its fixed scratch limit of " + std::to_string(NA_MAX_N) +
+                                             " particles (esp_spread has no such limit)");
+    const int P = p->order;
+    if (P < 2 || P > MAX_P) return fail(ESP_ERR_UNSUPPORTED, "order must be in [2, 12]");
+    const double L[3] = {Lx, Ly, Lz};
+    const int n[3] = {p->nx, p->ny, p->nz};
+    int T = p->tile > 0 ? p->tile : 17 - P;
+    for (int d = 0; d < 3; ++d) {
+        if (!(L[d] > 0)) return fail(ESP_ERR_INVALID, "box lengths must be positive");
+        if (n[d] <= 0) return fail(ESP_ERR_INVALID, "esp_spread_noalloc needs an explicit mesh (nx, ny, nz > 0)");
+        if (n[d] < std::max(P, 4) || n[d] > FFT_MAX_N)
+            return fail(ESP_ERR_UNSUPPORTED, "mesh size " + std::to_string(n[d]) + " must be in [max(order, 4), 256]");
+        T = std::min(T, n[d]);
+    }
+    if (T + P - 1 > 16) return fail(ESP_ERR_UNSUPPORTED, "esp_spread_noalloc needs tile + order - 1 <= 16");
+    const int nt[3] = {(n[0] + T - 1) / T, (n[1] + T - 1) / T, (n[2] + T - 1) / T};
+    const long long n_tiles = (long long)nt[0] * nt[1] * nt[2];
+    if (n_tiles > NA_MAX_TILES)
+        return fail(ESP_ERR_UNSUPPORTED, "esp_spread_noalloc: " + std::to_string(n_tiles) +
+                                             " tiles exceed its fixed scratch limit of " +
+                                             std::to_string(NA_MAX_TILES));
+    const int D = p->window_degree > 0 ? p->window_degree : std::max(P + 2, 9);
+    if (D > MAX_D) return fail(ESP_ERR_UNSUPPORTED, "window degree must be <= 15");
+    if (p->window_c < 0) return fail(ESP_ERR_INVALID, "window_c must be >= 0");
+    const double cw = p->window_c > 0 ? p->window_c : 2.2 * P;
+
+    ParamSet ps;
+    int rc = na_param_set(P, cw, D, &ps);
+    if (rc) return rc;
+    SysDev S{};
+    S.N = N;
+    S.nx = n[0];
+    S.ny = n[1];
+    S.nz = n[2];
+    S.nxh = n[0] / 2 + 1;
+    S.ntx = nt[0];
+    S.nty = nt[1];
+    S.ntz = nt[2];
+    S.Lx = (float)Lx;
+    S.Ly = (float)Ly;
+    S.Lz = (float)Lz;
+    S.inv_Lx = 1.0f / S.Lx;
+    S.inv_Ly = 1.0f / S.Ly;
+    S.inv_Lz = 1.0f / S.Lz;
+    S.gxd = n[0] / Lx;
+    S.gyd = n[1] / Ly;
+    S.gzd = n[2] / Lz;
+    S.V = Lx * Ly * Lz;
+
+    unsigned char* base = nullptr;
+    if ((rc = na_setup(&base))) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int n_chunks = (N + 255) / 256;
+    LaunchArgs a;
+    a.sys = reinterpret_cast<SysDev*>(base + NA_SYS);
+    a.psets = reinterpret_cast<ParamSet*>(base + NA_PSET);
+    a.nsys = 1;
+    a.P = P;
+    a.T = T;
+    a.D = D;
+    a.chunks = reinterpret_cast<int2*>(base + NA_CHUNKS);
+    a.n_chunks = n_chunks;
+    a.tile_sys = reinterpret_cast<int*>(base + NA_TILE_SYS);
+    a.n_tiles = (int)n_tiles;
+    a.tile_count = reinterpret_cast<uint32_t*>(base + NA_TCOUNT);
+    a.tile_start = reinterpret_cast<uint32_t*>(base + NA_TSTART);
+    a.acc = reinterpret_cast<double*>(base + NA_ACC);
+    a.posq = reinterpret_cast<float4*>(base + NA_POSQ);
+    a.trec = reinterpret_cast<float4*>(base + NA_TREC);
+    a.srec = reinterpret_cast<float4*>(base + NA_SREC);
+    a.rel = reinterpret_cast<uint32_t*>(base + NA_REL);
+    a.srel = reinterpret_cast<uint32_t*>(base + NA_SREL);
+    a.key = reinterpret_cast<uint32_t*>(base + NA_KEY);
+    a.perm_u = reinterpret_cast<uint32_t*>(base + NA_PERM_U);
+    a.perm = reinterpret_cast<uint32_t*>(base + NA_PERM);
+    a.pos_in = reinterpret_cast<const float4*>(pos4);
+    a.q_in = charge;
+    a.rho = rho;
+
+    const int n_prep = std::max(std::max(n_chunks, (int)n_tiles), (int)ACC_STRIDE);
+    ESPB_CK(cudaMemsetAsync(rho, 0, (size_t)n[0] * n[1] * n[2] * sizeof(double), st));
+    k_na_prepare<<<(n_prep + 255) / 256, 256, 0, st>>>(S, ps, const_cast<SysDev*>(a.sys),
+                                                       const_cast<ParamSet*>(a.psets), const_cast<int2*>(a.chunks),
+                                                       n_chunks, const_cast<int*>(a.tile_sys), a.tile_count,
+                                                       (int)n_tiles, a.acc);
+    ESPB_CK(cudaGetLastError());
+    ESPB_CK(launch_bin(a, st));
+    ESPB_CK(launch_sort(a, st));
+    ESPB_CK(launch_spread(a, st));
+    return 0;
+}

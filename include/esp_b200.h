@@ -121,6 +121,37 @@ int esp_spread(esp_ctx* ctx, void* stream, const float* pos4, const float* charg
 int esp_get_sort(const esp_ctx* ctx, void* stream, unsigned* key, unsigned* perm);
 int esp_get_potential(const esp_ctx* ctx, void* stream, float* phi);
 
+/* No-allocation charge spreading. No counterpart in the reference.
+ * Some callers cannot allocate device memory: an MD engine that hands all of
+ * its device memory to its own pool allocator, or a time step that must not
+ * call cudaFree (which synchronises the whole device) in the middle of a
+ * run. esp_create/esp_spread allocate their work arrays with cudaMalloc, so
+ * such callers cannot use them. esp_spread_noalloc does the same bin + sort +
+ * spreading into the caller's FP64 charge mesh rho[nz*ny*nx] (x fastest;
+ * zeroed first) with no context: its work arrays live in one fixed-size
+ * scratch array inside the library (2.2 MB, held on every GPU that
+ * loads the library until the process exits), and it calls no allocating
+ * CUDA or library routine.
+ *  - Limits: 1 <= N <= ESP_SPREAD_NOALLOC_MAX_N particles and at most
+ *    ESP_SPREAD_NOALLOC_MAX_TILES tiles; larger inputs are rejected with
+ *    ESP_ERR_UNSUPPORTED (use esp_spread for them).
+ *  - Parameters: p->order, p->window_c, p->window_degree and p->tile as in
+ *    esp_create; the mesh p->nx, p->ny, p->nz must be given (no automatic
+ *    choice), each in [max(order, 4), 256]; tile + order - 1 <= 16.
+ *  - The first call on a device (per device, with that device current) looks
+ *    up the scratch array's device address and sets the spreading kernels'
+ *    shared-memory limits; make that first call before any stream capture.
+ *  - Every call on a device shares the one scratch array: calls whose work
+ *    overlaps on the GPU (different streams, or different host threads,
+ *    without ordering between them) race and give wrong meshes. Calls
+ *    ordered on one stream are safe.
+ * Results equal esp_spread's for the same parameters and mesh, up to the
+ * order of FP64 atomic additions. */
+#define ESP_SPREAD_NOALLOC_MAX_N 32768
+#define ESP_SPREAD_NOALLOC_MAX_TILES 4096
+int esp_spread_noalloc(void* stream, const esp_params* p, double Lx, double Ly, double Lz, const float* pos4,
+                       const float* charge, int N, double* rho);
+
 /* ---------------------------------------------------------------- batches
  * Many independent systems evaluated by one launch per stage (no reference
  * counterpart; the reference evaluates one HOOMD system per ForceCompute).
