@@ -50,11 +50,12 @@ def _env_rank():
         int(os.environ.get("LOCAL_RANK", "0"))
 
 
-def _systems(rank: int):
+def _systems(rank: int, count: int = N_SYS):
+    """The first `count` systems of the rank's 256-system batch."""
     from esp_hoomd_b200 import systems
     rng = np.random.default_rng(SEED + 7919 * rank)
     evens = np.arange(8, 41, 2)
-    ns = rng.choice(evens, size=N_SYS)
+    ns = rng.choice(evens, size=N_SYS)[:count]
     return [systems.rocksalt(int(n), seed=SEED * 100000 + rank * N_SYS + i) for i, n in enumerate(ns)]
 
 
@@ -211,7 +212,7 @@ def run_ours(args):
     if world > 1:
         dist.init_process_group("nccl", init_method="env://", rank=rank, world_size=world,
                                 timeout=__import__("datetime").timedelta(seconds=600))
-    sl = _systems(rank)
+    sl = _systems(rank, args.systems)
     N = np.array([s.N for s in sl])
     tot = int(N.sum())
     params = native.make_params(order=8, rcut=RCUT, target_error=1e-5)
@@ -359,8 +360,8 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": max(3, args.warmup), "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "batched256: 256 rock-salt systems n^3, n even ~U{8..40} (seed 1004), "
-                                       "1 nlist + 1 eval + 10 NVE steps per system per step",
+                "config": {"workload": "batched%d: %d rock-salt systems n^3, n even ~U{8..40} (seed 1004), "
+                                       "1 nlist + 1 eval + 10 NVE steps per system per step" % (N.size, N.size),
                            "systems_per_gpu": int(N.size), "particles_per_gpu": tot, "order": 8, "rcut": RCUT,
                            "mesh_rule": "smallest 2/3/5-smooth >= L/h, h = pi r_c / 18.5 (1e-5 target)",
                            "mesh_points_per_gpu": int(M), "mean_neighbours": mean_nn, "dt": DT,
@@ -396,6 +397,8 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--systems", type=int, default=N_SYS,
+                    help="evaluate only the first S systems of the batch (small cases for profiling)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

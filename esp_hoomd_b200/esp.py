@@ -1,0 +1,538 @@
+"""ESP force objects with the Python API of the reference plugin.
+
+Mirrors ``hoomd_esp.esp`` (src/esp.py:137-701): ``Spectral`` (the long-range
+mesh force, ESPForceCompute), ``Local`` (the short-range EvaluatorPairPSWF
+pair force), ``make_esp_forces`` and the aliases ``Coulomb``/``Pair``, with
+the same constructor arguments, properties and validation errors
+(ValueError / TypeError / RuntimeError, src/esp.py:103-126, 225-241,
+355-359, 523-527). HOOMD-blue is not a dependency: the objects attach to the
+small standalone ``Simulation`` below (a stand-in for ``hoomd.Simulation``
+with a cell neighbour list and an NVE integrator), and every computation
+runs in the sm_100a library through ``native`` -- there is no CPU path.
+
+Differences from the reference, all deliberate:
+* ``MAX_ORDER`` is 12 (the reference's C++ limit, src/ESPForceCompute.h:63;
+  its Python says 8) and the smallest order is 2;
+* ``kappa`` is the split bandwidth in 1/length (prolate c = kappa * r_cut).
+  ``kappa=None`` lets the library choose c from the mesh spacing for a
+  1e-5 force error (the reference's 3.2 / r_cut heuristic belongs to its
+  Gaussian influence function and gives no usable ESP split);
+* ``alpha > 0`` (Debye screening) is rejected with ValueError: the library
+  computes unscreened Coulomb only.
+"""
+from __future__ import annotations
+
+import warnings
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+#: Largest PSWF support P in grid points (ESP_MAX_ORDER).
+MAX_ORDER: int = 12
+#: Smallest PSWF support the kernels accept.
+MIN_ORDER: int = 2
+#: Segments of the introspection table (src/esp.py:95).
+DEFAULT_TABLE_SEGMENTS: int = 512
+#: Smallest allowed introspection table (src/esp.py:98).
+MIN_TABLE_SEGMENTS: int = 16
+
+
+# ----------------------------------------------------------------------------- validation
+def _check_positive_int(val, name: str) -> None:
+    if isinstance(val, bool) or not isinstance(val, (int, np.integer)) or val <= 0:
+        raise ValueError(f"ESP: '{name}' must be a positive integer, got {val!r}.")
+
+
+def _check_positive_float(val, name: str) -> None:
+    if isinstance(val, bool) or not (isinstance(val, (int, float, np.integer, np.floating)) and val > 0):
+        raise ValueError(f"ESP: '{name}' must be a positive number, got {val!r}.")
+
+
+def _check_nonneg_float(val, name: str) -> None:
+    if isinstance(val, bool) or not (isinstance(val, (int, float, np.integer, np.floating)) and val >= 0):
+        raise ValueError(f"ESP: '{name}' must be >= 0, got {val!r}.")
+
+
+def _check_order(order) -> None:
+    if isinstance(order, bool) or not isinstance(order, (int, np.integer)) or not MIN_ORDER <= order <= MAX_ORDER:
+        raise ValueError(f"ESP: 'order' must be an integer in [{MIN_ORDER}, {MAX_ORDER}], got {order!r}.")
+
+
+def _check_alpha(alpha) -> None:
+    _check_nonneg_float(alpha, "alpha")
+    if alpha != 0:
+        raise ValueError("ESP: Debye screening (alpha > 0) is not supported; use alpha = 0.")
+
+
+def _check_n_table(n_table) -> None:
+    if isinstance(n_table, bool) or not isinstance(n_table, (int, np.integer)) or n_table < MIN_TABLE_SEGMENTS:
+        raise ValueError(f"ESP: 'n_table' must be an integer >= {MIN_TABLE_SEGMENTS}, got {n_table!r}.")
+
+
+def _validate_resolution(res: Sequence[int]) -> Tuple[int, int, int]:
+    res = tuple(res)
+    if len(res) != 3:
+        raise ValueError(f"ESP: 'resolution' must be a 3-tuple (Nx, Ny, Nz), got length {len(res)}.")
+    for i, (v, label) in enumerate(zip(res, ("Nx", "Ny", "Nz"))):
+        _check_positive_int(v, f"resolution[{i}] ({label})")
+    return tuple(int(v) for v in res)  # type: ignore[return-value]
+
+
+# ----------------------------------------------------------------------------- harness
+class NeighborList:
+    """Cell neighbour list (stand-in for ``hoomd.md.nlist.Cell(buffer)``).
+
+    Full lists of all pairs within r_cut + buffer, fixed row capacity; rebuilt
+    on the GPU when a particle has moved more than buffer / 2 since the last
+    build (or the box changed)."""
+
+    def __init__(self, buffer: float = 0.4, capacity: int = 256):
+        _check_nonneg_float(buffer, "buffer")
+        _check_positive_int(capacity, "capacity")
+        self.buffer = float(buffer)
+        self.capacity = int(capacity)
+        self.r_cut = 0.0
+        self._lists = None
+        self._ref_pos = None
+        self.builds = 0
+
+    def _require(self, r_cut: float) -> None:
+        if r_cut > self.r_cut:
+            self.r_cut = float(r_cut)
+            self._lists = None
+
+    def lists(self, sim: "Simulation", batch) -> Tuple:
+        import torch
+        st = sim.state
+        stale = self._lists is None or self._ref_pos is None
+        if not stale:
+            d = st.pos4[:, :3] - self._ref_pos
+            L = torch.as_tensor(st.box, dtype=d.dtype, device=d.device)
+            d = d - L * torch.round(d / L)
+            stale = bool((d * d).sum(1).max().item() > (0.5 * self.buffer) ** 2)
+        if stale:
+            N = st.N
+            if self._lists is None:
+                dev = st.pos4.device
+                self._lists = (torch.zeros(N, dtype=torch.int32, device=dev),
+                               torch.zeros(N, dtype=torch.int32, device=dev),
+                               torch.zeros(N * self.capacity, dtype=torch.int32, device=dev))
+            batch.build_nlist(st.pos4, self.r_cut + self.buffer, self.capacity, *self._lists)
+            self._ref_pos = st.pos4[:, :3].clone()
+            self.builds += 1
+        return self._lists
+
+
+class State:
+    """Particle data on the device: positions, charges, velocities, masses and
+    an orthorhombic box (stand-in for ``hoomd.State``)."""
+
+    def __init__(self, positions, charges, box: Sequence[float], velocities=None, masses=None,
+                 device: str = "cuda"):
+        import torch
+        pos = np.asarray(positions, dtype=np.float64).reshape(-1, 3)
+        N = pos.shape[0]
+        self.box = tuple(float(b) for b in box)
+        if len(self.box) != 3 or min(self.box) <= 0:
+            raise ValueError("ESP: 'box' must be three positive lengths.")
+        q = np.asarray(charges, dtype=np.float64).reshape(-1)
+        if q.shape[0] != N:
+            raise ValueError("ESP: one charge per particle expected.")
+        p4 = np.zeros((N, 4), np.float32)
+        p4[:, :3] = pos
+        v4 = np.zeros((N, 4), np.float32)
+        if velocities is not None:
+            v4[:, :3] = np.asarray(velocities, dtype=np.float64).reshape(-1, 3)
+        v4[:, 3] = 1.0 if masses is None else np.asarray(masses, dtype=np.float64).reshape(-1)
+        self.pos4 = torch.tensor(p4, device=device)
+        self.vel4 = torch.tensor(v4, device=device)
+        self.charge = torch.tensor(q.astype(np.float32), device=device)
+
+    @property
+    def N(self) -> int:
+        return int(self.pos4.shape[0])
+
+
+class Force:
+    """Minimal stand-in for ``hoomd.md.force.Force``: results of the last
+    compute as device buffers, read back on demand."""
+
+    def __init__(self) -> None:
+        self._simulation: Optional["Simulation"] = None
+        self._force = None   # [N, 4] float32: fx, fy, fz, per-particle energy
+        self._energy = None  # [1] float64
+        self._virial = None  # [6] float64
+
+    @property
+    def _attached(self) -> bool:
+        return self._simulation is not None
+
+    def _alloc(self, N: int, device) -> None:
+        import torch
+        self._force = torch.zeros((N, 4), dtype=torch.float32, device=device)
+        self._energy = torch.zeros(1, dtype=torch.float64, device=device)
+        self._virial = torch.zeros(6, dtype=torch.float64, device=device)
+
+    def _need_results(self) -> None:
+        if self._force is None:
+            raise RuntimeError("ESP: no results before the first compute.")
+
+    @property
+    def forces(self) -> np.ndarray:
+        self._need_results()
+        return self._force[:, :3].double().cpu().numpy()
+
+    @property
+    def energies(self) -> np.ndarray:
+        self._need_results()
+        return self._force[:, 3].double().cpu().numpy()
+
+    @property
+    def energy(self) -> float:
+        self._need_results()
+        return float(self._energy.item())
+
+    @property
+    def virial(self) -> np.ndarray:
+        """Total virial (xx, xy, xz, yy, yz, zz)."""
+        self._need_results()
+        return self._virial.cpu().numpy()
+
+
+class Simulation:
+    """Standalone stand-in for ``hoomd.Simulation`` + ``md.Integrator``
+    with an NVE method: attach forces, compute them, run velocity-Verlet
+    steps on the device."""
+
+    def __init__(self, state: State, nlist: Optional[NeighborList] = None, dt: float = 0.002):
+        _check_positive_float(dt, "dt")
+        self.state = state
+        self.nlist = nlist
+        self.dt = float(dt)
+        self.forces: List[Force] = []
+        self.timestep = 0
+        self._total = None
+
+    def add(self, *forces: Force) -> None:
+        for f in forces:
+            if f._attached:
+                raise RuntimeError("ESP: force is already attached to a simulation.")
+            f._simulation = self
+            try:
+                f._attach_hook()
+            except Exception:
+                f._simulation = None
+                raise
+            self.forces.append(f)
+
+    def remove(self, f: Force) -> None:
+        self.forces.remove(f)
+        f._detach_hook()
+        f._simulation = None
+
+    def compute(self) -> None:
+        import torch
+        for f in self.forces:
+            f._compute()
+        if self._total is None or self._total.shape[0] != self.state.N:
+            self._total = torch.zeros((self.state.N, 4), dtype=torch.float32, device=self.state.pos4.device)
+        self._total.zero_()
+        for f in self.forces:
+            self._total += f._force
+
+    def run(self, steps: int) -> None:
+        if not self.forces:
+            raise RuntimeError("ESP: no forces attached.")
+        batch = self.forces[0]._batch_handle()
+        if self.timestep == 0 or self._total is None:
+            self.compute()
+        for _ in range(int(steps)):
+            batch.nve_step1(self.state.pos4, self.state.vel4, self._total, self.dt)
+            self.compute()
+            batch.nve_step2(self.state.vel4, self._total, self.dt)
+            self.timestep += 1
+
+
+# ----------------------------------------------------------------------------- Spectral
+class Spectral(Force):
+    """Long-range Coulomb force by the ESP mesh method (the reference's
+    ``esp.Spectral``, src/esp.py:137-449): PSWF spreading, FFT, influence
+    multiply, inverse FFT and interpolation on the GPU, plus the self and
+    neutralising-background energies. Pair with :class:`Local`.
+
+    Parameters follow src/esp.py:208-217: ``nlist``, ``default_r_cut``,
+    ``resolution=(Nx, Ny, Nz)``, ``order`` (support P, 2..12), ``kappa``
+    (split bandwidth in 1/length, None = automatic), ``alpha`` (0 only),
+    ``n_table`` (introspection table segments, >= 16), ``nlist_buffer``
+    (default 0.1 r_cut).
+    """
+
+    def __init__(self, nlist: NeighborList, default_r_cut: float, resolution: Sequence[int] = (32, 32, 32),
+                 order: int = 6, kappa: Optional[float] = None, alpha: float = 0.0,
+                 n_table: int = DEFAULT_TABLE_SEGMENTS, nlist_buffer: Optional[float] = None) -> None:
+        super().__init__()
+        _check_positive_float(default_r_cut, "default_r_cut")
+        res = _validate_resolution(resolution)
+        _check_order(order)
+        if kappa is None:
+            warnings.warn("ESP: 'kappa' not specified; the split bandwidth is chosen from the mesh spacing "
+                          "for a 1e-5 relative RMS force error.", stacklevel=2)
+        else:
+            _check_positive_float(kappa, "kappa")
+        _check_alpha(alpha)
+        _check_n_table(n_table)
+        self._nlist = nlist
+        self._r_cut = float(default_r_cut)
+        self._resolution = res
+        self._order = int(order)
+        self._kappa = None if kappa is None else float(kappa)
+        self._alpha = float(alpha)
+        self._n_table = int(n_table)
+        self._nlist_buffer = 0.1 * self._r_cut if nlist_buffer is None else float(nlist_buffer)
+        self._batch = None
+        self._pair: Optional["Local"] = None
+
+    # -- properties (src/esp.py:266-313)
+    @property
+    def kappa(self) -> Optional[float]:
+        """Split bandwidth in use (1/length): c / r_cut. Before attachment the
+        constructor's value (None when automatic)."""
+        if self._batch is not None:
+            inf = self._batch.info(0)
+            return inf["c_split"] / inf["rcut"]
+        return self._kappa
+
+    @property
+    def resolution(self) -> Tuple[int, int, int]:
+        if self._batch is not None:
+            inf = self._batch.info(0)
+            return (inf["nx"], inf["ny"], inf["nz"])
+        return self._resolution
+
+    @property
+    def order(self) -> int:
+        return self._order
+
+    @property
+    def r_cut(self) -> float:
+        return self._r_cut
+
+    @property
+    def alpha(self) -> float:
+        return self._alpha
+
+    @property
+    def n_table(self) -> int:
+        return self._n_table
+
+    @property
+    def q_sum(self) -> float:
+        if not self._attached:
+            raise RuntimeError("ESP: q_sum not available before simulation attachment.")
+        return float(self._simulation.state.charge.double().sum().item())
+
+    @property
+    def q2_sum(self) -> float:
+        if not self._attached:
+            raise RuntimeError("ESP: q2_sum not available before simulation attachment.")
+        q = self._simulation.state.charge.double()
+        return float((q * q).sum().item())
+
+    # -- runtime parameter change (src/esp.py:319-393)
+    def set_params(self, *, resolution: Optional[Sequence[int]] = None, order: Optional[int] = None,
+                   kappa: Optional[float] = None, r_cut: Optional[float] = None, alpha: Optional[float] = None,
+                   n_table: Optional[int] = None) -> None:
+        """Update parameters; the tables are rebuilt before the next compute."""
+        if not self._attached:
+            raise RuntimeError("ESP: 'set_params()' called before the Simulation was attached. "
+                               "Pass initial values to the Spectral constructor instead.")
+        new = dict(resolution=self._resolution, order=self._order, kappa=self._kappa, r_cut=self._r_cut,
+                   alpha=self._alpha, n_table=self._n_table)
+        if resolution is not None:
+            new["resolution"] = _validate_resolution(resolution)
+        if order is not None:
+            _check_order(order)
+            new["order"] = int(order)
+        if kappa is not None:
+            _check_positive_float(kappa, "kappa")
+            new["kappa"] = float(kappa)
+        if r_cut is not None:
+            _check_positive_float(r_cut, "r_cut")
+            new["r_cut"] = float(r_cut)
+        if alpha is not None:
+            _check_alpha(alpha)
+            new["alpha"] = float(alpha)
+        if n_table is not None:
+            _check_n_table(n_table)
+            new["n_table"] = int(n_table)
+        self._resolution, self._order, self._kappa = new["resolution"], new["order"], new["kappa"]
+        self._r_cut, self._alpha, self._n_table = new["r_cut"], new["alpha"], new["n_table"]
+        self.invalidate()
+        if self._pair is not None:
+            self._pair._sync_params_from_spectral()
+
+    def invalidate(self) -> None:
+        """Rebuild every table on the next compute (src/esp.py:396-403)."""
+        if self._batch is not None:
+            self._batch.close()
+            self._batch = None
+
+    # -- lifecycle
+    def _params(self):
+        from . import native
+        return native.make_params(order=self._order, rcut=self._r_cut,
+                                  kappa=0.0 if self._kappa is None else self._kappa, mesh=self._resolution,
+                                  alpha=self._alpha, n_table=self._n_table)
+
+    def _batch_handle(self):
+        from . import native
+        if self._batch is None:
+            st = self._simulation.state
+            self._batch = native.Batch(self._params(), [st.N], [st.box])
+            self._nlist._require(self._r_cut)
+        return self._batch
+
+    def _attach_hook(self) -> None:
+        st = self._simulation.state
+        if 2.0 * self._r_cut > min(st.box):
+            raise ValueError("ESP: 'default_r_cut' must not exceed half the box.")
+        self._alloc(st.N, st.pos4.device)
+        self._nlist._require(self._r_cut)
+        self._batch_handle()
+
+    def _detach_hook(self) -> None:
+        self.invalidate()
+
+    def _compute(self, flags: Optional[int] = None) -> None:
+        from ._lib import ESP_LONG_RANGE
+        b = self._batch_handle()
+        st = self._simulation.state
+        b.compute(st.pos4, st.charge, self._force, self._energy, self._virial,
+                  flags=ESP_LONG_RANGE if flags is None else flags)
+
+    def __repr__(self) -> str:
+        k = "auto" if self._kappa is None else "%.4g" % self._kappa
+        return (f"esp.Spectral(resolution={self._resolution}, order={self._order}, kappa={k}, "
+                f"r_cut={self._r_cut}, alpha={self._alpha})")
+
+
+# ----------------------------------------------------------------------------- Local
+class Local(Force):
+    """Short-range real-space complement of :class:`Spectral` (the reference's
+    ``esp.Local`` over ``PotentialPair<EvaluatorPairPSWF>``, src/esp.py:456-625):
+    q_i q_j L(r) over the neighbour list with the split of the associated
+    Spectral. ``params[(a, b)]`` takes an empty dict (every parameter comes
+    from the Spectral object); ``r_cut[(a, b)]`` defaults to ``default_r_cut``.
+    """
+
+    _accepted_modes = ("none",)
+
+    def __init__(self, nlist: NeighborList, default_r_cut: float, spectral: Optional[Spectral] = None,
+                 coulomb: Optional[Spectral] = None, default_r_on: float = 0.0, mode: str = "none") -> None:
+        if spectral is None and coulomb is not None:
+            warnings.warn("The 'coulomb' parameter is deprecated; use 'spectral' instead.", DeprecationWarning,
+                          stacklevel=2)
+            spectral = coulomb
+        if spectral is None:
+            raise ValueError("'spectral' (or deprecated 'coulomb') must be provided.")
+        if not isinstance(spectral, Spectral):
+            raise TypeError(f"ESP: 'spectral' must be an esp.Spectral instance, got {type(spectral).__name__!r}.")
+        if mode not in self._accepted_modes:
+            raise ValueError("ESP: Pair mode must be 'none' for ESP (L(r) already vanishes at r_c).")
+        _check_positive_float(default_r_cut, "default_r_cut")
+        _check_nonneg_float(default_r_on, "default_r_on")
+        super().__init__()
+        self._nlist = nlist
+        self._default_r_cut = float(default_r_cut)
+        self._default_r_on = float(default_r_on)
+        self.mode = mode
+        self.params: _PairParams = _PairParams()
+        self.r_cut: Dict[Tuple[str, str], float] = {}
+        self._spectral = spectral
+        spectral._pair = self
+
+    @staticmethod
+    def _validate_params(params: dict) -> dict:
+        """Pair parameters carry no user-settable fields (src/esp.py:547-563)."""
+        if params and set(params.keys()) - {"_reserved"}:
+            warnings.warn("ESP: Local.params accepts an empty dict {}; all ESP parameters are read from the "
+                          f"associated Spectral object. Ignoring keys: {set(params.keys())!r}.", stacklevel=3)
+        return {}
+
+    def _sync_params_from_spectral(self) -> None:
+        """Copy (kappa, rcut, alpha, V_cut = 0) into every registered type pair
+        (src/esp.py:569-617)."""
+        if not self._attached:
+            return
+        if not self._spectral._attached:
+            raise RuntimeError("ESP: the associated Spectral object is not attached. Attach Spectral before Local.")
+        kappa = self._spectral.kappa
+        for key in list(self.params.keys()):
+            dict.__setitem__(self.params, key, dict(kappa=kappa, rcut=self._spectral.r_cut,
+                                                    alpha=self._spectral.alpha, V_cut=0.0))
+
+    def _check_cutoffs(self) -> None:
+        rc = self._spectral.r_cut
+        for key, v in self.r_cut.items():
+            if abs(float(v) - rc) > 1e-12 * rc:
+                raise ValueError(f"ESP: r_cut{key!r} = {v} differs from the Spectral cutoff {rc}; "
+                                 "the split requires one cutoff.")
+        if abs(self._default_r_cut - rc) > 1e-12 * rc:
+            raise ValueError(f"ESP: default_r_cut {self._default_r_cut} differs from the Spectral cutoff {rc}.")
+
+    def _attach_hook(self) -> None:
+        if not self._spectral._attached or self._spectral._simulation is not self._simulation:
+            raise RuntimeError("ESP: attach the associated Spectral object to the same simulation before Local.")
+        self._check_cutoffs()
+        st = self._simulation.state
+        self._alloc(st.N, st.pos4.device)
+        self._sync_params_from_spectral()
+
+    def _detach_hook(self) -> None:
+        self._spectral._pair = None
+
+    def _batch_handle(self):
+        return self._spectral._batch_handle()
+
+    def _compute(self) -> None:
+        from ._lib import ESP_SHORT_RANGE
+        self._check_cutoffs()
+        b = self._spectral._batch_handle()
+        st = self._simulation.state
+        lists = self._nlist.lists(self._simulation, b)
+        b.compute(st.pos4, st.charge, self._force, self._energy, self._virial, nlist=lists, flags=ESP_SHORT_RANGE)
+
+    def __repr__(self) -> str:
+        s = self._spectral
+        k = "auto" if s._kappa is None else "%.4g" % s._kappa
+        return f"esp.Local(r_cut={s._r_cut}, kappa={k}, alpha={s._alpha})"
+
+
+class _PairParams(dict):
+    """Type-pair parameter dictionary: keys are (type_a, type_b) tuples,
+    values pass through Local._validate_params."""
+
+    def __setitem__(self, key, value) -> None:
+        if not (isinstance(key, tuple) and len(key) == 2):
+            raise TypeError("ESP: Local.params keys are (type_a, type_b) tuples.")
+        if not isinstance(value, dict):
+            raise TypeError("ESP: Local.params values must be dicts.")
+        super().__setitem__(key, Local._validate_params(value))
+
+
+# ----------------------------------------------------------------------------- factory
+def make_esp_forces(nlist: NeighborList, r_cut: float, resolution: Sequence[int] = (32, 32, 32), order: int = 6,
+                    kappa: Optional[float] = None, alpha: float = 0.0,
+                    n_table: int = DEFAULT_TABLE_SEGMENTS) -> Tuple[Spectral, Local]:
+    """Coupled (Spectral, Local) pair sharing one cutoff (src/esp.py:632-693)."""
+    spectral = Spectral(nlist=nlist, default_r_cut=r_cut, resolution=resolution, order=order, kappa=kappa,
+                        alpha=alpha, n_table=n_table)
+    local = Local(nlist=nlist, default_r_cut=r_cut, spectral=spectral)
+    return spectral, local
+
+
+Coulomb = Spectral
+Pair = Local
+
+__all__ = ["Spectral", "Local", "make_esp_forces", "Coulomb", "Pair", "MAX_ORDER", "DEFAULT_TABLE_SEGMENTS",
+           "MIN_TABLE_SEGMENTS", "NeighborList", "State", "Simulation"]
