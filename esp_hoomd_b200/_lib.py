@@ -26,6 +26,8 @@ EXPORTS = [
     "esp_batch_total_particles", "esp_batch_destroy", "esp_pswf_eval_pairs", "esp_batch_build_nlist",
     "esp_batch_nve_step1", "esp_batch_nve_step2", "esp_spread", "esp_get_sort", "esp_get_potential",
     "esp_batch_md_run", "esp_batch_set_timing", "esp_batch_stage_times", "esp_spread_noalloc",
+    "esp_server_create", "esp_server_submit", "esp_server_start", "esp_server_status", "esp_server_wait_all",
+    "esp_server_get_stats", "esp_server_destroy",
 ]
 
 STAGES = ["bin", "sort", "spread", "fft", "interp", "pair", "nlist", "nve"]
@@ -44,6 +46,33 @@ class EspInfo(ctypes.Structure):
                 ("c_window", ctypes.c_double), ("rcut", ctypes.c_double), ("lambda0", ctypes.c_double),
                 ("m2", ctypes.c_double), ("split_fit_err", ctypes.c_double), ("window_fit_err", ctypes.c_double),
                 ("device_bytes", ctypes.c_longlong)]
+
+
+class EspServerConfig(ctypes.Structure):
+    _fields_ = [("params", EspParams), ("hbm_budget", ctypes.c_longlong), ("max_systems", ctypes.c_int),
+                ("max_particles", ctypes.c_int)]
+
+
+class EspRequest(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int), ("Lx", ctypes.c_double), ("Ly", ctypes.c_double), ("Lz", ctypes.c_double),
+                ("rcut", ctypes.c_double), ("skin", ctypes.c_double), ("nlist_cap", ctypes.c_int),
+                ("nsteps", ctypes.c_int), ("dt", ctypes.c_double), ("arrival", ctypes.c_double),
+                ("pos4", ctypes.c_void_p), ("vel4", ctypes.c_void_p), ("charge", ctypes.c_void_p),
+                ("out_pos4", ctypes.c_void_p), ("out_vel4", ctypes.c_void_p), ("out_force4", ctypes.c_void_p),
+                ("out_energy", ctypes.c_void_p)]
+
+
+class EspRequestStatus(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int), ("t_arrival", ctypes.c_double), ("t_admit", ctypes.c_double),
+                ("t_done", ctypes.c_double), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("footprint", ctypes.c_longlong)]
+
+
+class EspServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong), ("failed", ctypes.c_longlong),
+                ("rounds", ctypes.c_longlong), ("particle_steps", ctypes.c_longlong),
+                ("influence_builds", ctypes.c_longlong), ("influence_hits", ctypes.c_longlong),
+                ("max_active", ctypes.c_int), ("peak_bytes", ctypes.c_longlong), ("arena_bytes", ctypes.c_longlong)]
 
 
 _lib = None
@@ -91,6 +120,13 @@ def get_lib() -> ctypes.CDLL:
         lib.esp_batch_md_run.argtypes = [P, P, P, P, P, P, P, P, P, P, P, I, D, I]
         lib.esp_batch_set_timing.argtypes = [P, I]
         lib.esp_batch_stage_times.argtypes = [P, P, P]
+        lib.esp_server_create.argtypes = [ctypes.POINTER(EspServerConfig), ctypes.POINTER(P)]
+        lib.esp_server_submit.argtypes = [P, ctypes.POINTER(EspRequest), ctypes.POINTER(ctypes.c_longlong)]
+        lib.esp_server_start.argtypes = [P]
+        lib.esp_server_status.argtypes = [P, ctypes.c_longlong, ctypes.POINTER(EspRequestStatus)]
+        lib.esp_server_wait_all.argtypes = [P, D]
+        lib.esp_server_get_stats.argtypes = [P, ctypes.POINTER(EspServerStats)]
+        lib.esp_server_destroy.argtypes = [P]
         lib.esp_spread_noalloc.argtypes = [P, ctypes.POINTER(EspParams), D, D, D, P, P, I, P]
         for name in EXPORTS:
             if name != "esp_last_error":

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "esp_b200.h"
+#include "esp_host_util.h"
 #include "esp_kernels.h"
 #include "esp_md.h"
 #include "esp_tables.h"
@@ -23,22 +24,16 @@
 using namespace espb;
 
 namespace {
-
 thread_local std::string g_err;
+}  // namespace
+
+namespace espb {
 
 int fail(int code, const std::string& msg) {
     g_err = msg;
     return code;
 }
 
-#define ESPB_CK(x)                                                                                  \
-    do {                                                                                            \
-        cudaError_t e_ = (x);                                                                       \
-        if (e_ != cudaSuccess) return fail(ESP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
-
-// Required k-space resolution kappa_N = pi r_c / h for a relative RMS force
-// target (measured against FP64 Ewald on rock-salt lattices, P = 8..12).
 double kappa_required(double target) {
     const double lt[] = {-3, -4, -5, -6, -7, -8};
     const double kv[] = {11.5, 14.0, 18.5, 22.0, 26.0, 30.0};
@@ -50,6 +45,13 @@ double kappa_required(double target) {
             return kv[i] + f * (kv[i + 1] - kv[i]);
         }
     return kv[5];
+}
+
+double split_c_for_spacing(double rcut, double h) {
+    // 0.93 kappa_N, rounded to 0.5: the measured optimum against FP64 Ewald
+    // at P = 8, h = r_c / 6
+    const double c = std::round(2.0 * 0.93 * M_PI * rcut / h) * 0.5;
+    return std::max(2.0, std::min(60.0, c));
 }
 
 uint32_t radix_plan(int n) {
@@ -98,36 +100,56 @@ void choose_pitch(int P, int E, int& PX, int& PP) {
     }
 }
 
-struct DevAlloc {
-    std::vector<void*> ptrs;
-    long long bytes = 0;
-    template <class T>
-    int get(T*& p, size_t n) {
-        p = nullptr;
-        if (n == 0) n = 1;
-        cudaError_t e = cudaMalloc((void**)&p, n * sizeof(T));
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return fail(ESP_ERR_ALLOC, std::string("cudaMalloc of ") + std::to_string(n * sizeof(T)) +
-                                           " bytes failed: " + cudaGetErrorString(e));
-        }
-        ptrs.push_back(p);
-        bytes += (long long)(n * sizeof(T));
-        return 0;
+int build_param_set(double c, double cw, int P, int D, double rcut, PsetHost& h, ParamSet& d) {
+    try {
+        h.split.build(c);
+        h.win.build(P, cw, D);
+    } catch (const std::exception& ex) {
+        return fail(ESP_ERR_INVALID, ex.what());
     }
-    void release() {
-        for (void* p : ptrs) cudaFree(p);
-        ptrs.clear();
-        bytes = 0;
-    }
-    ~DevAlloc() { release(); }
-};
+    h.rcut = rcut;
+    if (h.split.qv.size() > (size_t)MAX_QC)
+        return fail(ESP_ERR_UNSUPPORTED, "split polynomial needs more than 32 coefficients");
+    d = ParamSet{};
+    for (int a = 0; a < P; ++a)
+        for (int j = 0; j <= D; ++j) d.wcoef[a * (MAX_D + 1) + j] = (float)h.win.coef[(size_t)a * (D + 1) + j];
+    d.nq = (int)h.split.qv.size();
+    for (int j = 0; j < d.nq; ++j) d.qv[j] = (float)h.split.qv[j];
+    for (int j = 1; j < d.nq; ++j) d.dqv[j - 1] = (float)(2.0 * j * h.split.qv[j]);
+    d.rcut = (float)rcut;
+    d.rcut2 = (float)(rcut * rcut);
+    d.inv_rcut = (float)(1.0 / rcut);
+    d.two_inv_rcut3 = (float)(2.0 / (rcut * rcut * rcut));
+    d.self_coef = -0.5 * h.split.lambda0 * INV_4PI_D / rcut;
+    d.bg_coef = -0.25 * rcut * rcut * h.split.m2;
+    return 0;
+}
 
-struct PsetHost {
-    Split split;
-    Window win;
-    double rcut = 0;
-};
+void influence_inputs(const SysDev& S, const PsetHost& h, double Lx, double Ly, double Lz, double rcut,
+                      std::vector<double>& w1d, std::vector<double>& tq, std::vector<double>& wq) {
+    w1d.assign(S.nx + S.ny + S.nz, 0.0);
+    const int nn[3] = {S.nx, S.ny, S.nz};
+    const double L[3] = {Lx, Ly, Lz};
+    int o = 0;
+    for (int d = 0; d < 3; ++d)
+        for (int i = 0; i < nn[d]; ++i) {
+            const int f = (i < (nn[d] + 1) / 2) ? i : nn[d] - i;
+            w1d[o++] = h.win.fourier(2.0 * M_PI * f / nn[d]);
+        }
+    double kmax2 = 0;
+    for (int d = 0; d < 3; ++d) {
+        const double k = M_PI * nn[d] / L[d];
+        kmax2 += k * k;
+    }
+    const double kap_max = std::sqrt(kmax2) * rcut;
+    const int nq = std::max(48, std::min(320, (int)(0.6 * kap_max) + 40));
+    gauss_legendre01(nq, tq, wq);
+    for (int j = 0; j < nq; ++j) wq[j] *= h.split.pro.psi(tq[j]) / h.split.pro.int01;
+}
+
+}  // namespace espb
+
+namespace {
 
 // Per-stage CUDA-event timing on the launching stream. Records are queued
 // without synchronising; read() synchronises once and sums the elapsed
@@ -317,15 +339,8 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
     for (int s = 0; s < ns; ++s)
         for (int d = 0; d < 3; ++d) hmax_all = std::max(hmax_all, box[3 * s + d] / mesh[3 * s + d]);
     for (int s = 0; s < ns; ++s) {
-        double c;
-        if (p.kappa > 0) {
-            c = p.kappa * p.rcut;
-        } else {
-            // 0.93 kappa_N (kappa_N = pi r_c / h), rounded to 0.5: the
-            // measured optimum against FP64 Ewald at P = 8, h = r_c / 6
-            c = std::round(2.0 * 0.93 * M_PI * p.rcut / hmax_all) * 0.5;
-        }
-        c = std::max(2.0, std::min(60.0, c));
+        const double c = p.kappa > 0 ? std::max(2.0, std::min(60.0, p.kappa * p.rcut))
+                                     : split_c_for_spacing(p.rcut, hmax_all);
         const double cw = p.window_c > 0 ? p.window_c : 2.2 * P;
         c_split[s] = c;
         c_win[s] = cw;
@@ -333,27 +348,9 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         auto it = pmap.find(key);
         if (it == pmap.end()) {
             PsetHost h;
-            try {
-                h.split.build(c);
-                h.win.build(P, cw, D);
-            } catch (const std::exception& ex) {
-                return fail(ESP_ERR_INVALID, ex.what());
-            }
-            h.rcut = p.rcut;
-            if (h.split.qv.size() > (size_t)MAX_QC)
-                return fail(ESP_ERR_UNSUPPORTED, "split polynomial needs more than 32 coefficients");
-            ParamSet d{};
-            for (int a = 0; a < P; ++a)
-                for (int j = 0; j <= D; ++j) d.wcoef[a * (MAX_D + 1) + j] = (float)h.win.coef[(size_t)a * (D + 1) + j];
-            d.nq = (int)h.split.qv.size();
-            for (int j = 0; j < d.nq; ++j) d.qv[j] = (float)h.split.qv[j];
-            for (int j = 1; j < d.nq; ++j) d.dqv[j - 1] = (float)(2.0 * j * h.split.qv[j]);
-            d.rcut = (float)p.rcut;
-            d.rcut2 = (float)(p.rcut * p.rcut);
-            d.inv_rcut = (float)(1.0 / p.rcut);
-            d.two_inv_rcut3 = (float)(2.0 / (p.rcut * p.rcut * p.rcut));
-            d.self_coef = -0.5 * h.split.lambda0 * INV_4PI_D / p.rcut;
-            d.bg_coef = -0.25 * p.rcut * p.rcut * h.split.m2;
+            ParamSet d;
+            const int rc = build_param_set(c, cw, P, D, p.rcut, h, d);
+            if (rc) return rc;
             it = pmap.emplace(key, (int)psh.size()).first;
             psh.push_back(std::move(h));
             psd.push_back(d);
@@ -508,24 +505,9 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
     for (int s : g_first) {
         const SysDev& S = sd[s];
         const PsetHost& h = psh[S.pset];
-        std::vector<double> w1d(S.nx + S.ny + S.nz);
-        const int nn[3] = {S.nx, S.ny, S.nz};
-        int o = 0;
-        for (int d = 0; d < 3; ++d)
-            for (int i = 0; i < nn[d]; ++i) {
-                const int f = (i < (nn[d] + 1) / 2) ? i : nn[d] - i;
-                w1d[o++] = h.win.fourier(2.0 * M_PI * f / nn[d]);
-            }
-        double kmax2 = 0;
-        for (int d = 0; d < 3; ++d) {
-            const double k = M_PI * nn[d] / box[3 * s + d];
-            kmax2 += k * k;
-        }
-        const double kap_max = std::sqrt(kmax2) * p.rcut;
-        const int nq = std::max(48, std::min(320, (int)(0.6 * kap_max) + 40));
-        std::vector<double> tq, wq;
-        gauss_legendre01(nq, tq, wq);
-        for (int j = 0; j < nq; ++j) wq[j] *= h.split.pro.psi(tq[j]) / h.split.pro.int01;
+        std::vector<double> w1d, tq, wq;
+        influence_inputs(S, h, box[3 * s], box[3 * s + 1], box[3 * s + 2], p.rcut, w1d, tq, wq);
+        const int nq = (int)tq.size();
         double *d_w1d = nullptr, *d_tq = nullptr, *d_wq = nullptr;
         ESPB_CK(cudaMalloc(&d_w1d, w1d.size() * sizeof(double)));
         ESPB_CK(cudaMalloc(&d_tq, nq * sizeof(double)));

@@ -197,6 +197,89 @@ class Batch:
             pass
 
 
+def _host_ptr(a, dtype, count: int, name: str):
+    """Address of a contiguous host array (numpy, or a CPU torch tensor such
+    as a pinned one) holding at least `count` elements of `dtype`."""
+    if a is None:
+        return None
+    if isinstance(a, torch.Tensor):
+        if a.is_cuda or not a.is_contiguous() or a.numel() < count:
+            raise ValueError("%s: contiguous host tensor of %d elements expected" % (name, count))
+        return ctypes.c_void_p(a.data_ptr())
+    if not (isinstance(a, np.ndarray) and a.dtype == dtype and a.flags["C_CONTIGUOUS"] and a.size >= count):
+        raise ValueError("%s: contiguous %s array of %d elements expected" % (name, np.dtype(dtype).name, count))
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Server:
+    """Continuous-batching request server over the C ABI (esp_server_*).
+
+    Host buffers passed to ``submit`` are referenced until ``close`` (the
+    server reads and writes them asynchronously)."""
+
+    def __init__(self, params: EspParams, hbm_budget: int = 4 << 30, max_systems: int = 512,
+                 max_particles: int = 262144):
+        self._lib = get_lib()
+        self._h = ctypes.c_void_p()
+        cfg = _lib.EspServerConfig(params=params, hbm_budget=int(hbm_budget), max_systems=int(max_systems),
+                                   max_particles=int(max_particles))
+        check(self._lib.esp_server_create(ctypes.byref(cfg), ctypes.byref(self._h)), "esp_server_create")
+        self._keep = []
+
+    def submit(self, pos4, charge, box: Sequence[float], rcut: float, vel4=None, nsteps: int = 10,
+               dt: float = 0.002, skin: float = 0.4, arrival: float = 0.0, nlist_cap: int = 0, out_pos4=None,
+               out_vel4=None, out_force4=None, out_energy=None) -> int:
+        N = int(len(charge))
+        r = _lib.EspRequest()
+        r.N = N
+        r.Lx, r.Ly, r.Lz = (float(b) for b in box)
+        r.rcut = float(rcut)
+        r.skin = float(skin)
+        r.nlist_cap = int(nlist_cap)
+        r.nsteps = int(nsteps)
+        r.dt = float(dt)
+        r.arrival = float(arrival)
+        r.pos4 = _host_ptr(pos4, np.float32, 4 * N, "pos4")
+        r.vel4 = _host_ptr(vel4, np.float32, 4 * N, "vel4")
+        r.charge = _host_ptr(charge, np.float32, N, "charge")
+        r.out_pos4 = _host_ptr(out_pos4, np.float32, 4 * N, "out_pos4")
+        r.out_vel4 = _host_ptr(out_vel4, np.float32, 4 * N, "out_vel4")
+        r.out_force4 = _host_ptr(out_force4, np.float32, 4 * N, "out_force4")
+        r.out_energy = _host_ptr(out_energy, np.float64, 1, "out_energy")
+        rid = ctypes.c_longlong()
+        check(self._lib.esp_server_submit(self._h, ctypes.byref(r), ctypes.byref(rid)), "esp_server_submit")
+        self._keep.append((pos4, vel4, charge, out_pos4, out_vel4, out_force4, out_energy))
+        return int(rid.value)
+
+    def start(self) -> None:
+        check(self._lib.esp_server_start(self._h), "esp_server_start")
+
+    def status(self, rid: int) -> dict:
+        s = _lib.EspRequestStatus()
+        check(self._lib.esp_server_status(self._h, int(rid), ctypes.byref(s)), "esp_server_status")
+        return {f[0]: getattr(s, f[0]) for f in _lib.EspRequestStatus._fields_}
+
+    def wait_all(self, timeout: float = 600.0) -> None:
+        check(self._lib.esp_server_wait_all(self._h, float(timeout)), "esp_server_wait_all")
+
+    def stats(self) -> dict:
+        s = _lib.EspServerStats()
+        check(self._lib.esp_server_get_stats(self._h, ctypes.byref(s)), "esp_server_get_stats")
+        return {f[0]: getattr(s, f[0]) for f in _lib.EspServerStats._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.esp_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+        self._keep = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def pswf_eval_pairs(rsq: torch.Tensor, qiqj: torch.Tensor, rcut: float, table, stream=None):
     """Reference-format evaluator over n pairs on the GPU (FP64).
 

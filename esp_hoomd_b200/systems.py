@@ -52,17 +52,20 @@ def rocksalt(n: int, spacing: float = 1.0, jitter: float = 0.1, seed: int = 0, T
 def water(n_mol: int, density: float = 33.4, seed: int = 0, q_o: float = -0.8476, r_oh: float = 0.1,
           angle_deg: float = 109.47) -> System:
     """Rigid three-site water molecules (O, H, H) at a number density of
-    molecules per nm^3, centres on a jittered cubic lattice, uniformly
-    random orientations (unit quaternions). Velocities zero; masses
-    16/1/1."""
+    molecules per nm^3, centres on a jittered cubic lattice (m^3 sites,
+    m = ceil(n_mol^(1/3)); when n_mol is not a cube a seeded random subset
+    of the sites is occupied), uniformly random orientations (unit
+    quaternions). Velocities zero; masses 16/1/1."""
     rng = np.random.default_rng(seed)
     m = int(round(n_mol ** (1.0 / 3.0)))
-    if m ** 3 != n_mol:
-        raise ValueError("n_mol must be a perfect cube")
+    if m ** 3 < n_mol:
+        m += 1
     L = (n_mol / density) ** (1.0 / 3.0)
     a = L / m
     ix, iy, iz = np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij")
     centres = (np.stack([ix.ravel(), iy.ravel(), iz.ravel()], -1) + 0.5) * a
+    if m ** 3 != n_mol:
+        centres = centres[np.sort(rng.choice(m ** 3, size=n_mol, replace=False))]
     centres += rng.uniform(-0.05 * a, 0.05 * a, centres.shape)
     half = math.radians(angle_deg) / 2.0
     body = np.array([[0.0, 0.0, 0.0],

@@ -206,6 +206,81 @@ int esp_batch_md_run(esp_batch* b, void* stream, float* pos4, float* vel4, const
                      const unsigned* n_neigh, const unsigned* nlist, float* force4, double* energy, double* virial6,
                      int nsteps, double dt, int use_graph);
 
+/* ---------------------------------------------------------------- serving
+ * Continuous-batching request server (no counterpart in the reference, whose
+ * ForceCompute serves one HOOMD simulation). A request is one system: a
+ * neighbour-list build, one evaluation (ESP_ALL) and `nsteps` velocity-Verlet
+ * steps, each with a full evaluation. A worker thread admits arrived requests
+ * in arrival order while their device footprint fits the budget (particle,
+ * mesh, neighbour-list and tile ranges of arenas allocated once at create),
+ * keeps each admitted system's particles, sorted records, meshes and
+ * influence table resident across its steps, and advances every admitted
+ * system by one evaluation per round: one launch per stage over all of them
+ * (the batched kernels), so requests that arrive while others run join the
+ * next round and share its launches. Influence tables are cached by (cutoff,
+ * box, mesh) across requests. All systems of a server share one split
+ * bandwidth c (chosen from the target error); the mesh of each request
+ * follows its box and cutoff. Host input and output buffers stay owned by the
+ * caller and must stay valid until the request is done (page-locked memory
+ * lets the copies run asynchronously). */
+typedef struct esp_server esp_server;
+
+typedef struct esp_server_config {
+    esp_params params;        /* order, target_error, window, tile; rcut is per request */
+    long long hbm_budget;     /* device bytes for all request state (arenas), >= 256 MB */
+    int max_systems;          /* systems admitted at once (slots), 1..4096 */
+    int max_particles;        /* largest single request */
+} esp_server_config;
+
+typedef struct esp_request {
+    int N;                    /* particles */
+    double Lx, Ly, Lz;        /* orthorhombic box */
+    double rcut;              /* real-space cutoff of this system */
+    double skin;              /* neighbour-list buffer: list radius rcut + skin */
+    int nlist_cap;            /* neighbour-list row capacity; 0 = from the mean density */
+    int nsteps;               /* NVE steps after the first evaluation */
+    double dt;
+    double arrival;           /* seconds after esp_server_start at which the request arrives */
+    const float* pos4;        /* host, 4N floats (x, y, z, unused) */
+    const float* vel4;        /* host, 4N floats (vx, vy, vz, mass); NULL when nsteps == 0 */
+    const float* charge;      /* host, N floats */
+    float* out_pos4;          /* host outputs after the last step, each may be NULL */
+    float* out_vel4;
+    float* out_force4;        /* forces and per-particle energies of the last evaluation */
+    double* out_energy;       /* total energy of the last evaluation */
+} esp_request;
+
+typedef struct esp_request_status {
+    int state;                /* 0 waiting, 1 running, 2 done, < 0 failed (ESP_ERR_*) */
+    double t_arrival, t_admit, t_done;  /* seconds after esp_server_start */
+    int nx, ny, nz;           /* mesh chosen for the request */
+    long long footprint;      /* device bytes held while admitted */
+} esp_request_status;
+
+typedef struct esp_server_stats {
+    long long submitted, completed, failed;
+    long long rounds;         /* evaluation rounds launched */
+    long long particle_steps; /* particle evaluations completed (N per evaluation) */
+    long long influence_builds, influence_hits;
+    int max_active;           /* largest number of systems admitted at once */
+    long long peak_bytes;     /* largest footprint admitted at once */
+    long long arena_bytes;    /* device bytes of the arenas */
+} esp_server_stats;
+
+int esp_server_create(const esp_server_config* cfg, esp_server** out);
+/* Queues a request (arrival times must not decrease from one submit to the
+ * next); `id` receives its index (0, 1, 2, ...). */
+int esp_server_submit(esp_server* s, const esp_request* r, long long* id);
+/* Starts the clock that arrival times count from (requests submitted before
+ * start wait for it). */
+int esp_server_start(esp_server* s);
+int esp_server_status(esp_server* s, long long id, esp_request_status* st);
+/* Blocks until every submitted request is done or failed, or timeout_s
+ * passes (ESP_ERR_INVALID then). */
+int esp_server_wait_all(esp_server* s, double timeout_s);
+int esp_server_get_stats(esp_server* s, esp_server_stats* st);
+int esp_server_destroy(esp_server* s);
+
 /* ---------------------------------------------------------------- timing
  * Per-stage CUDA-event timing on the launching stream (no counterpart in
  * the reference, whose Autotuner times kernels for block-size selection,
