@@ -9,10 +9,14 @@ advances sum(N) particles by 10 MD steps (particle-steps = 10 sum N).
 Reported beside the batched number: the plain path (the same systems, one
 system per launch sequence), the end-to-end number through the C ABI with
 pinned host buffers copied in and results copied out every step, the
-roofline of the dominant kernel (CUDA events on the launching stream), and
-the CPU baseline (the FP64 oracle port on the host cores).
+roofline of the dominant kernel (CUDA events on the launching stream), the
+CPU baseline (the FP64 oracle port on the host cores), and the served
+stream: Poisson arrivals of mixed rock-salt / water requests through the
+continuous-batching server at several rates, with p50/p99 latency and
+throughput per rate.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                       [--no-serve] [--serve-requests R] [--serve-rates a,b,c]
 """
 from __future__ import annotations
 
@@ -199,6 +203,91 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- serving
+SERVE_BUDGET = 64 << 30
+SERVE_STEPS = 10
+
+
+def _serve_pool(seed: int):
+    """Request templates: every rock-salt size n = 8, 10, ..., 64 (r_c 3.0,
+    skin 0.4) and 16 water boxes of 1,000-32,768 molecules (r_c 0.9 nm, skin
+    0.1), as page-locked host inputs."""
+    import torch
+    from esp_hoomd_b200 import systems
+    rng = np.random.default_rng(seed)
+    pool = {"rocksalt": [], "water": []}
+
+    def pinned(s):
+        p4 = np.zeros((s.N, 4), np.float32)
+        p4[:, :3] = s.pos
+        v4 = np.zeros((s.N, 4), np.float32)
+        v4[:, :3] = s.vel
+        v4[:, 3] = s.mass
+        t = [torch.from_numpy(a).pin_memory() for a in (p4, v4, s.q.astype(np.float32))]
+        out = torch.empty((s.N, 4), dtype=torch.float32).pin_memory()
+        return {"N": s.N, "box": s.box, "pos4": t[0], "vel4": t[1], "q": t[2], "out_pos4": out}
+
+    for n in range(8, 65, 2):
+        d = pinned(systems.rocksalt(n, seed=int(rng.integers(1 << 30))))
+        d.update(rcut=3.0, skin=0.4)
+        pool["rocksalt"].append(d)
+    for m in np.sort(rng.integers(1000, 32769, size=16)):
+        d = pinned(systems.water(int(m), seed=int(rng.integers(1 << 30))))
+        d.update(rcut=0.9, skin=0.1)
+        pool["water"].append(d)
+    return pool
+
+
+def run_serving(args, pool):
+    """Poisson streams of requests (50/50 rock-salt / water, each one
+    neighbour list + 1 evaluation + 10 NVE steps) through the server at
+    several arrival rates; latency = completion - arrival per request."""
+    import torch
+    from esp_hoomd_b200 import native
+    srv = native.Server(native.make_params(order=8, target_error=1e-5), hbm_budget=SERVE_BUDGET,
+                        max_systems=1024, max_particles=262144)
+    rng = np.random.default_rng(SEED + 5)
+    n_warm = len(pool["rocksalt"]) + len(pool["water"])
+    energies = torch.zeros(n_warm + args.serve_requests * len(args.serve_rates), dtype=torch.float64).pin_memory()
+    slot = [0]
+
+    def submit(d, arrival):
+        i = slot[0]
+        slot[0] += 1
+        return srv.submit(d["pos4"], d["q"], d["box"], d["rcut"], vel4=d["vel4"], nsteps=SERVE_STEPS, dt=DT,
+                          skin=d["skin"], arrival=arrival, out_pos4=d["out_pos4"], out_energy=energies[i:i + 1])
+
+    # warm-up: every template once (kernels, parameter sets, influence tables)
+    warm = [submit(d, 0.0) for kind in ("rocksalt", "water") for d in pool[kind]]
+    srv.start()
+    srv.wait_all(600)
+    base = max(srv.status(i)["t_done"] for i in warm) + 0.05
+    out = []
+    for rate in args.serve_rates:
+        gaps = rng.exponential(1.0 / rate, size=args.serve_requests)
+        arr = base + np.cumsum(gaps)
+        kinds = rng.random(args.serve_requests) < 0.5
+        ids, nsum = [], 0
+        for a, is_rs in zip(arr, kinds):
+            tmpl = pool["rocksalt" if is_rs else "water"]
+            d = tmpl[int(rng.integers(len(tmpl)))]
+            nsum += d["N"]
+            ids.append(submit(d, float(a)))
+        srv.wait_all(1800)
+        st = [srv.status(i) for i in ids]
+        ok = [s for s in st if s["state"] == 2]
+        lat = np.array([s["t_done"] - s["t_arrival"] for s in ok]) * 1e3
+        span = max(s["t_done"] for s in ok) - arr[0]
+        out.append({"rate_per_s": rate, "requests": len(ids), "completed": len(ok),
+                    "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                    "mean_ms": float(lat.mean()), "throughput": nsum * SERVE_STEPS / span,
+                    "requests_per_s": len(ok) / span})
+        base = max(s["t_done"] for s in ok) + 0.05
+    stats = srv.stats()
+    srv.close()
+    return out, stats
+
+
 # ----------------------------------------------------------------------------- GPU arm
 def run_ours(args):
     import torch
@@ -382,6 +471,19 @@ def run_ours(args):
             line["cpu_baseline"] = {"value": n_tot / wall, "unit": UNIT, "cores": 1, "kind": "port",
                                     "sample": "FP64 oracle evaluation + NVE update of rock-salt n=%s (%d particles)"
                                               % (ns, n_tot)}
+        if not args.no_serve:
+            b.close()
+            torch.cuda.empty_cache()
+            rates, sst = run_serving(args, _serve_pool(SEED + 6))
+            mid = rates[len(rates) // 2]
+            line["serving"] = {
+                "workload": "Poisson arrivals, 50/50 rock-salt n even ~U{8..64} (r_c 3.0) / water 1,000-32,768 "
+                            "molecules (r_c 0.9 nm); each request = nlist + 1 evaluation + 10 NVE steps; "
+                            "64 GB HBM budget; latency = completion - arrival (host clock)",
+                "unit": UNIT, "rates": rates, "p50_ms": mid["p50_ms"], "p99_ms": mid["p99_ms"],
+                "at_rate_per_s": mid["rate_per_s"],
+                "server": {k: sst[k] for k in ("rounds", "max_active", "peak_bytes", "arena_bytes",
+                                               "influence_builds", "influence_hits", "failed")}}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -399,6 +501,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--systems", type=int, default=N_SYS,
                     help="evaluate only the first S systems of the batch (small cases for profiling)")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=1000, help="requests per arrival rate")
+    ap.add_argument("--serve-rates", type=lambda v: [float(x) for x in v.split(",")], default=[100.0, 200.0, 400.0],
+                    help="comma-separated arrival rates (requests/s)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
