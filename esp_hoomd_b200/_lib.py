@@ -27,7 +27,7 @@ EXPORTS = [
     "esp_batch_nve_step1", "esp_batch_nve_step2", "esp_spread", "esp_get_sort", "esp_get_potential",
     "esp_batch_md_run", "esp_batch_set_timing", "esp_batch_stage_times", "esp_spread_noalloc",
     "esp_server_create", "esp_server_submit", "esp_server_start", "esp_server_status", "esp_server_wait_all",
-    "esp_server_get_stats", "esp_server_destroy",
+    "esp_server_get_stats", "esp_server_destroy", "esp_set_exclusions", "esp_batch_set_exclusions",
 ]
 
 STAGES = ["bin", "sort", "spread", "fft", "interp", "pair", "nlist", "nve"]
@@ -127,6 +127,8 @@ def get_lib() -> ctypes.CDLL:
         lib.esp_server_wait_all.argtypes = [P, D]
         lib.esp_server_get_stats.argtypes = [P, ctypes.POINTER(EspServerStats)]
         lib.esp_server_destroy.argtypes = [P]
+        lib.esp_set_exclusions.argtypes = [P, P, P, I]
+        lib.esp_batch_set_exclusions.argtypes = [P, P, P, I]
         lib.esp_spread_noalloc.argtypes = [P, ctypes.POINTER(EspParams), D, D, D, P, P, I, P]
         for name in EXPORTS:
             if name != "esp_last_error":

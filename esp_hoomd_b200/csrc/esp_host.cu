@@ -248,6 +248,11 @@ struct esp_batch {
     uint32_t *d_ckey = nullptr, *d_ccount = nullptr, *d_cstart = nullptr, *d_cperm = nullptr, *d_slot_cell = nullptr;
     float4 *d_wpos = nullptr, *d_cpos = nullptr;
     int* d_overflow = nullptr;
+    // excluded pairs (caller-owned device arrays), applied by every
+    // long-range evaluation
+    const uint32_t* ex_n = nullptr;
+    const uint32_t* ex_list = nullptr;
+    int ex_pitch = 0;
 
     StageTimer timer;
     struct GraphKey {
@@ -623,6 +628,12 @@ int esp_batch::compute(cudaStream_t st, const float* pos4, const float* q, const
         timer.begin(ESP_STAGE_INTERP, st);
         ESPB_CK(launch_interp(a, st));
         timer.end(st);
+        if (ex_n) {
+            a.ex_n = ex_n;
+            a.ex_list = ex_list;
+            a.ex_pitch = ex_pitch;
+            ESPB_CK(launch_exclusions(a, st));
+        }
     } else {
         // bin counted particles per tile; clear the histogram for the next call
         ESPB_CK(cudaMemsetAsync(d_tcount, 0, (size_t)n_tiles * sizeof(uint32_t), st));
@@ -958,6 +969,24 @@ int esp_batch_total_particles(const esp_batch* b) { return b ? b->totN : -1; }
 int esp_batch_destroy(esp_batch* b) {
     delete b;
     return 0;
+}
+
+int esp_batch_set_exclusions(esp_batch* b, const unsigned* n_ex, const unsigned* ex_list, int ex_pitch) {
+    if (!b) return fail(ESP_ERR_INVALID, "null batch");
+    if (n_ex && (!ex_list || ex_pitch <= 0)) return fail(ESP_ERR_INVALID, "exclusion list needs ex_list and ex_pitch > 0");
+    b->ex_n = n_ex;
+    b->ex_list = n_ex ? ex_list : nullptr;
+    b->ex_pitch = n_ex ? ex_pitch : 0;
+    if (b->graph_exec) {  // captured steps hold the previous pointers
+        cudaGraphExecDestroy(b->graph_exec);
+        b->graph_exec = nullptr;
+    }
+    return 0;
+}
+
+int esp_set_exclusions(esp_ctx* c, const unsigned* n_ex, const unsigned* ex_list, int ex_pitch) {
+    if (!c) return fail(ESP_ERR_INVALID, "null context");
+    return esp_batch_set_exclusions(&c->b, n_ex, ex_list, ex_pitch);
 }
 
 int esp_batch_md_run(esp_batch* b, void* stream, float* pos4, float* vel4, const float* charge, const unsigned* head,

@@ -1571,6 +1571,90 @@ cudaError_t launch_pair(const LaunchArgs& a, cudaStream_t st) {
     }
 }
 
+// ============================================================================
+// a9 (K7): exclusion correction, src/ESPForceComputeGPU.cu:391-471. The mesh
+// sums q_i q_j Phi(r) over every pair, Phi = 1/(4 pi r) - L(r): that is
+// Q(r^2/r_c^2) / (4 pi r_c) inside r_c and the bare 1/(4 pi r) beyond. For
+// each excluded pair this kernel subtracts it: force, half the pair energy
+// per side (exclusions are listed from both sides) and the virial. Unlike
+// the reference, which skips excluded pairs beyond r_c, pairs at any
+// distance are corrected. One thread per particle, after the interpolation
+// has written the mesh forces.
+// ============================================================================
+__global__ void k_exclusions(const int2* __restrict__ chunks, const SysDev* __restrict__ sys,
+                             const ParamSet* __restrict__ psets, const float4* __restrict__ posq,
+                             const uint32_t* __restrict__ n_ex, const uint32_t* __restrict__ ex_list, int ex_pitch,
+                             float4* __restrict__ force, double* __restrict__ acc) {
+    __shared__ double red[32 * 7];
+    const int2 ch = chunks[blockIdx.x];
+    const SysDev S = sys[ch.x];
+    const ParamSet& ps = psets[S.pset];
+    const int i = ch.y + threadIdx.x;
+    const bool valid = i < S.p_off + S.N;
+    const uint32_t n = valid ? n_ex[i] : 0u;
+    float fx = 0.f, fy = 0.f, fz = 0.f, en = 0.f, v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (n > 0) {
+        const float4 pi = posq[i];
+        const float irc2 = ps.inv_rcut * ps.inv_rcut;
+        for (uint32_t k = 0; k < n; ++k) {
+            const uint32_t jl = ex_list[(size_t)i * ex_pitch + k];
+            if (jl >= (uint32_t)S.N) continue;
+            const float4 pj = posq[S.p_off + (int)jl];
+            float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            dx -= S.Lx * rintf(dx * S.inv_Lx);
+            dy -= S.Ly * rintf(dy * S.inv_Ly);
+            dz -= S.Lz * rintf(dz * S.inv_Lz);
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            float phi, dphi_r;  // Phi and (dPhi/dr) / r
+            if (r2 < ps.rcut2) {
+                const float vv = fmaf(2.f * irc2, r2, -1.f);
+                float qv = ps.qv[ps.nq - 1], dq = ps.nq >= 2 ? ps.dqv[ps.nq - 2] : 0.f;
+                for (int c = ps.nq - 2; c >= 0; --c) qv = fmaf(qv, vv, ps.qv[c]);
+                for (int c = ps.nq - 3; c >= 0; --c) dq = fmaf(dq, vv, ps.dqv[c]);
+                phi = INV_4PI_F * qv * ps.inv_rcut;
+                dphi_r = INV_4PI_F * ps.two_inv_rcut3 * dq;
+            } else {
+                float ri = rsqrtf(r2);
+                ri = ri * fmaf(-0.5f * r2 * ri, ri, 1.5f);
+                phi = INV_4PI_F * ri;
+                dphi_r = -INV_4PI_F * ri * ri * ri;
+            }
+            const float qq = pi.w * pj.w;
+            const float f = qq * dphi_r;
+            fx = fmaf(f, dx, fx);
+            fy = fmaf(f, dy, fy);
+            fz = fmaf(f, dz, fz);
+            en = fmaf(-0.5f * qq, phi, en);
+            v[0] = fmaf(f * dx, dx, v[0]);
+            v[1] = fmaf(f * dx, dy, v[1]);
+            v[2] = fmaf(f * dx, dz, v[2]);
+            v[3] = fmaf(f * dy, dy, v[3]);
+            v[4] = fmaf(f * dy, dz, v[4]);
+            v[5] = fmaf(f * dz, dz, v[5]);
+        }
+        float4 fo = force[i];
+        fo.x += fx;
+        fo.y += fy;
+        fo.z += fz;
+        fo.w += en;
+        force[i] = fo;
+    }
+    double e[7] = {(double)en, 0.5 * v[0], 0.5 * v[1], 0.5 * v[2], 0.5 * v[3], 0.5 * v[4], 0.5 * v[5]};
+    block_sum_f64<7>(e, red);
+    if (threadIdx.x == 0) {
+        atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_E], e[0]);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_WK + k], e[1 + k]);
+    }
+}
+
+cudaError_t launch_exclusions(const LaunchArgs& a, cudaStream_t st) {
+    if (a.n_chunks == 0 || !a.ex_n) return cudaSuccess;
+    k_exclusions<<<a.n_chunks, 256, 0, st>>>(a.chunks, a.sys, a.psets, a.posq, a.ex_n, a.ex_list, a.ex_pitch,
+                                             a.force, a.acc);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_finalize(const LaunchArgs& a, cudaStream_t st) {
     k_finalize<<<(a.nsys + 127) / 128, 128, 0, st>>>(a.sys, a.psets, a.nsys, a.acc, a.energy, a.virial, a.add_bg);
     return cudaGetLastError();

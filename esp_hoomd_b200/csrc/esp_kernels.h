@@ -81,6 +81,9 @@ struct LaunchArgs {
     const uint32_t* nl_head = nullptr;
     const uint32_t* nl_n = nullptr;
     const uint32_t* nl_list = nullptr;
+    const uint32_t* ex_n = nullptr;     // exclusions: row i holds ex_list[i * ex_pitch + k], k < ex_n[i]
+    const uint32_t* ex_list = nullptr;
+    int ex_pitch = 0;
 };
 
 cudaError_t launch_scan(const uint32_t* cnt, uint32_t* start, int n, cudaStream_t st);
@@ -92,6 +95,7 @@ cudaError_t launch_spread(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_fft(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_interp(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_pair(const LaunchArgs& a, cudaStream_t st);
+cudaError_t launch_exclusions(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_finalize(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_influence(const SysDev& S, const double* w1d, const double* tq, const double* wq, int nq,
                              double rcut, double psi_floor, float2* gtab, cudaStream_t st);

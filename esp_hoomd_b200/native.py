@@ -100,6 +100,12 @@ class Context:
     def invalidate(self) -> None:
         check(self._lib.esp_invalidate(self._h), "esp_invalidate")
 
+    def set_exclusions(self, n_ex: Optional[torch.Tensor], ex_list: Optional[torch.Tensor] = None,
+                       ex_pitch: int = 0) -> None:
+        """Excluded pairs (device uint32 arrays, row i = ex_list[i * ex_pitch:]); None clears."""
+        self._ex = (n_ex, ex_list)
+        check(self._lib.esp_set_exclusions(self._h, _ptr(n_ex), _ptr(ex_list), int(ex_pitch)), "esp_set_exclusions")
+
     def info(self) -> dict:
         inf = EspInfo()
         check(self._lib.esp_get_info(self._h, ctypes.byref(inf)), "esp_get_info")
@@ -168,6 +174,14 @@ class Batch:
         check(self._lib.esp_batch_md_run(self._h, _stream(stream), _ptr(pos4), _ptr(vel4), _ptr(q), _ptr(head),
                                          _ptr(nn), _ptr(nl), _ptr(force4), _ptr(energy), _ptr(virial), int(nsteps),
                                          float(dt), int(bool(use_graph))), "esp_batch_md_run")
+
+    def set_exclusions(self, n_ex: Optional[torch.Tensor], ex_list: Optional[torch.Tensor] = None,
+                       ex_pitch: int = 0) -> None:
+        """Excluded pairs of all systems (rows by concatenated index, local
+        excluded indices); None clears."""
+        self._ex = (n_ex, ex_list)
+        check(self._lib.esp_batch_set_exclusions(self._h, _ptr(n_ex), _ptr(ex_list), int(ex_pitch)),
+              "esp_batch_set_exclusions")
 
     def set_timing(self, on: bool) -> None:
         check(self._lib.esp_batch_set_timing(self._h, int(bool(on))), "esp_batch_set_timing")

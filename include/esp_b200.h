@@ -108,6 +108,17 @@ int esp_compute(esp_ctx* ctx, void* stream, const float* pos4, const float* char
 int esp_get_info(const esp_ctx* ctx, esp_info* info);
 int esp_destroy(esp_ctx* ctx);
 
+/* Excluded pairs: the input of ESPForceComputeGPU::fixExclusionsGPU
+ * (src/ESPForceComputeGPU.cc:390-420) and its kernel
+ * (src/ESPForceComputeGPU.cu:391-471), HOOMD's NeighborList exclusion arrays.
+ * Particle i excludes ex_list[i * ex_pitch + k], k < n_ex[i] (device arrays,
+ * indices local to the system, every pair listed from both sides). Every
+ * later long-range evaluation removes the mesh's interaction of these pairs
+ * (force, energy, virial) at any distance; the neighbour list given to the
+ * short-range term must leave them out, as HOOMD's does. The arrays stay
+ * owned by the caller and must stay valid while set; n_ex = NULL clears. */
+int esp_set_exclusions(esp_ctx* ctx, const unsigned* n_ex, const unsigned* ex_list, int ex_pitch);
+
 /* Stage outputs, for validation of single stages (no reference
  * counterpart: the reference exposes only the final forces).
  * esp_spread: bin + sort + spreading of (pos4, charge) into the caller's
@@ -168,6 +179,9 @@ int esp_batch_compute(esp_batch* b, void* stream, const float* pos4, const float
 int esp_batch_get_info(const esp_batch* b, int sys, esp_info* info);
 int esp_batch_total_particles(const esp_batch* b);
 int esp_batch_destroy(esp_batch* b);
+/* Exclusions of a batch, as esp_set_exclusions: rows by the particle's index
+ * in the concatenated arrays, excluded indices local to its system. */
+int esp_batch_set_exclusions(esp_batch* b, const unsigned* n_ex, const unsigned* ex_list, int ex_pitch);
 
 /* ---------------------------------------------------------------- evaluator
  * EvaluatorPairPSWF::evalForceAndEnergy (src/EvaluatorPairPSWF.h:274-295)

@@ -248,6 +248,75 @@ def pair_forces(pos, q, box, split, rcut, nl_head, nl_count, nl_list):
     return F, en, vir
 
 
+def exclusion_correction(pos, q, box, split, rcut, n_ex, ex_list, ex_pitch):
+    """Removes the mesh's long-range interaction of excluded pairs
+    (``gpu_esp_fix_exclusions_kernel``, ``src/ESPForceComputeGPU.cu:391-471``).
+
+    The mesh sums ``q_i q_j Phi(r)`` over every pair, with
+    ``Phi = 1/(4 pi r) - L(r)``: ``Q(r^2/r_c^2) / (4 pi r_c)`` inside the
+    cutoff, the bare ``1/(4 pi r)`` beyond it (the reference skips excluded
+    pairs beyond r_c). Exclusions of particle i are
+    ``ex_list[i * ex_pitch + k], k < n_ex[i]``, listed from both sides; each
+    side takes half of the pair energy. Returns (F[N,3], e[N], virial[6]).
+    """
+    pos = np.asarray(pos, dtype=np.float64)
+    L = np.asarray(box, dtype=np.float64)
+    N = pos.shape[0]
+    cnt = np.asarray(n_ex, dtype=np.int64)
+    i_idx = np.repeat(np.arange(N), cnt)
+    k_idx = np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+    j_idx = np.asarray(ex_list, dtype=np.int64)[i_idx * ex_pitch + k_idx]
+    d = pos[i_idx] - pos[j_idx]
+    d -= L * np.round(d / L)
+    r2 = np.sum(d * d, -1)
+    inside = r2 < rcut * rcut
+    u = np.where(inside, r2 / (rcut * rcut), 0.0)
+    r = np.sqrt(np.where(inside, 1.0, r2))
+    phi = np.where(inside, INV_4PI * split.Q(u) / rcut, INV_4PI / r)
+    # dPhi/dr / r
+    dphi_r = np.where(inside, INV_4PI * 2.0 * split.dQ(u) / rcut ** 3, -INV_4PI / (r * r * r))
+    qq = q[i_idx] * q[j_idx]
+    f = qq * dphi_r  # correction force on i is +f d (minus the mesh's -dE/dr)
+    F = np.zeros((N, 3))
+    np.add.at(F, i_idx, f[:, None] * d)
+    en = np.zeros(N)
+    np.add.at(en, i_idx, -0.5 * qq * phi)
+    W = 0.5 * np.einsum("p,pa,pb->ab", f, d, d)
+    vir = np.array([W[0, 0], W[0, 1], W[0, 2], W[1, 1], W[1, 2], W[2, 2]])
+    return F, en, vir
+
+
+def molecule_exclusions(n_mol: int, per_mol: int):
+    """Exclusions of rigid molecules of `per_mol` consecutive particles:
+    every particle excludes the others of its molecule. Returns
+    (n_ex[N], ex_list[N * (per_mol - 1)], ex_pitch)."""
+    N = n_mol * per_mol
+    pitch = per_mol - 1
+    n_ex = np.full(N, pitch, dtype=np.uint32)
+    ex = np.zeros(N * pitch, dtype=np.uint32)
+    for i in range(N):
+        m0 = (i // per_mol) * per_mol
+        ex[i * pitch:(i + 1) * pitch] = [j for j in range(m0, m0 + per_mol) if j != i]
+    return n_ex, ex, pitch
+
+
+def remove_pairs(nlist, n_ex, ex_list, ex_pitch):
+    """A CSR neighbour list without the excluded pairs (HOOMD's neighbour
+    list leaves them out)."""
+    head, cnt, lst = nlist
+    excl = set()
+    for i in range(len(n_ex)):
+        for k in range(int(n_ex[i])):
+            excl.add((i, int(ex_list[i * ex_pitch + k])))
+    nh, nc, nl = [], [], []
+    for i in range(len(head)):
+        nh.append(len(nl))
+        row = [int(j) for j in lst[head[i]:head[i] + cnt[i]] if (i, int(j)) not in excl]
+        nl.extend(row)
+        nc.append(len(row))
+    return (np.array(nh, dtype=np.uint32), np.array(nc, dtype=np.uint32), np.array(nl, dtype=np.uint32))
+
+
 def neighbor_list(pos, box, rlist):
     """Full CSR neighbour list of all pairs with r < rlist (minimum image).
     Rows are sorted by neighbour index. Returns (head, count, list)."""
@@ -283,9 +352,11 @@ def background_energy(q, params):
     return -(Q * Q) / (2.0 * V) * (params.rcut ** 2 * params.split.m2 * 0.5)
 
 
-def esp(pos, q, params, nlist=None, return_parts: bool = False):
+def esp(pos, q, params, nlist=None, return_parts: bool = False, exclusions=None):
     """Full ESP evaluation in FP64: returns (E, F[N,3], virial[6]) and,
-    with return_parts, a dict of the stage outputs."""
+    with return_parts, a dict of the stage outputs. `exclusions` =
+    (n_ex, ex_list, ex_pitch) applies the exclusion correction (the
+    neighbour list must then leave the excluded pairs out)."""
     pos = np.asarray(pos, dtype=np.float64)
     q = np.asarray(q, dtype=np.float64)
     G = influence(params)
@@ -294,6 +365,8 @@ def esp(pos, q, params, nlist=None, return_parts: bool = False):
     pot, Fm = interpolate(pos, q, phi, params)
     if nlist is None:
         nlist = neighbor_list(pos, params.box, params.rcut)
+        if exclusions is not None:
+            nlist = remove_pairs(nlist, *exclusions)
     Fp, ep, Wp = pair_forces(pos, q, params.box, params.split, params.rcut, *nlist)
     E_rec = 0.5 * float(np.sum(q * pot))
     E_self = self_energy(q, params)
@@ -303,6 +376,12 @@ def esp(pos, q, params, nlist=None, return_parts: bool = False):
     E = E_rec + float(np.sum(ep)) + E_self + E_bg
     F = Fm + Fp
     vir = Wk + Wp
+    if exclusions is not None:
+        Fx, ex_e, Wx = exclusion_correction(pos, q, params.box, params.split, params.rcut, *exclusions)
+        F = F + Fx
+        E += float(np.sum(ex_e))
+        vir = vir + Wx
+        ep = ep + ex_e
     if return_parts:
         return E, F, vir, dict(rho=rho, phi=phi, pot=pot, F_mesh=Fm, F_pair=Fp, e_pair=ep, E_rec=E_rec,
                                E_self=E_self, E_bg=E_bg, W_k=Wk, W_pair=Wp, G=G)

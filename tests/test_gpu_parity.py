@@ -224,3 +224,38 @@ def test_errors_are_reported():
         native.Context(native.make_params(alpha=0.5), (10, 10, 10), 10)
     with pytest.raises(EspError):
         native.Context(native.make_params(mesh=(14, 14, 14)), (10, 10, 10), 10)  # 14 is not 2/3/5-smooth
+
+
+def test_exclusions_match_oracle_and_ewald():
+    # rigid water with every intramolecular pair excluded: GPU vs the FP64
+    # oracle (same parameters), and the physics vs Ewald without those pairs
+    w = systems.water(216, seed=7)
+    w.pos = w.pos.astype(np.float32).astype(np.float64)
+    excl = R.molecule_exclusions(216, 3)
+    ctx = native.Context(native.make_params(rcut=0.9, mesh=(16, 16, 16)), w.box, w.N)
+    pos4, q = _upload(w)
+    nlist = R.remove_pairs(R.neighbor_list(w.pos, w.box, 0.9), *excl)
+    nl = _nlist_dev(*nlist)
+    n_ex = _dev(excl[0].astype(np.int32), torch.int32)
+    ex = _dev(excl[1].astype(np.int32), torch.int32)
+    ctx.set_exclusions(n_ex, ex, excl[2])
+    force = torch.zeros((w.N, 4), dtype=torch.float32, device="cuda")
+    energy = torch.zeros(1, dtype=torch.float64, device="cuda")
+    virial = torch.zeros(6, dtype=torch.float64, device="cuda")
+    ctx.compute(pos4, q, force, energy, virial, nlist=nl)
+    torch.cuda.synchronize()
+    f = force.cpu().numpy()[:, :3].astype(np.float64)
+    prm = _oracle_params(ctx.info(), w.box)
+    E, F, W = R.esp(w.pos, w.q, prm, nlist=nlist, exclusions=excl)
+    scale = R.INV_4PI * np.sum(w.q ** 2) / 0.9  # the remaining energy nearly cancels
+    assert R.rel_rms(f, F) <= 5e-6
+    assert abs(energy.item() - E) <= 1e-6 * scale
+    assert np.abs(virial.cpu().numpy() - W).max() <= 1e-5 * np.abs(W).max()
+    # per-particle energies add up to the total
+    assert abs(float(force[:, 3].double().sum().item()) - energy.item()) <= 1e-6 * scale
+    # clearing the exclusions restores the unexcluded mesh result
+    ctx.set_exclusions(None)
+    ctx.compute(pos4, q, force, energy, None, nlist=_nlist_dev(*R.neighbor_list(w.pos, w.box, 0.9)))
+    E1, F1, _ = R.esp(w.pos, w.q, prm)
+    torch.cuda.synchronize()
+    assert R.rel_rms(force.cpu().numpy()[:, :3].astype(np.float64), F1) <= 5e-6

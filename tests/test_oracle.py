@@ -179,3 +179,32 @@ def test_water_system():
     assert abs(w.q.sum()) < 1e-12
     L = w.box[0]
     assert abs(L - (27 / 33.4) ** (1 / 3)) < 1e-12
+
+
+def test_exclusion_correction_matches_ewald_without_excluded_pairs():
+    # rigid water: every atom excludes the other two of its molecule; the
+    # physical answer is Ewald minus the bare Coulomb of the excluded pairs
+    w = systems.water(216, seed=7)
+    L = np.asarray(w.box)
+    excl = R.molecule_exclusions(216, 3)
+    prm = tables.ESPParams(mesh=(16, 16, 16), box=w.box, rcut=0.9, split=tables.split_cached(22.5),
+                           window=tables.window_cached(8, 17.6, 10))
+    E, F, W = R.esp(w.pos, w.q, prm, exclusions=excl)
+    E0, F0, W0 = ewald(w.pos, w.q, w.box)
+    n_ex, ex, pitch = excl
+    for i in range(w.N):
+        for k in range(int(n_ex[i])):
+            j = int(ex[i * pitch + k])
+            d = w.pos[i] - w.pos[j]
+            d -= L * np.round(d / L)
+            r = np.sqrt(d @ d)
+            qq = w.q[i] * w.q[j]
+            E0 -= 0.5 * qq * R.INV_4PI / r
+            F0[i] -= qq * R.INV_4PI * d / r ** 3
+            W0 -= 0.5 * qq * R.INV_4PI / r ** 3 * np.array([d[0] * d[0], d[0] * d[1], d[0] * d[2],
+                                                             d[1] * d[1], d[1] * d[2], d[2] * d[2]])
+    assert R.rel_rms(F, F0) < 1e-5
+    # the remaining (intermolecular) energy nearly cancels: measure its error
+    # against the system's energy scale sum q^2 / (4 pi r_c)
+    assert abs(E - E0) < 1e-7 * R.INV_4PI * np.sum(w.q ** 2) / 0.9
+    assert np.abs(W - W0).max() < 1e-5 * np.abs(W0).max()
