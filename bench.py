@@ -138,67 +138,54 @@ def _traffic_from_profiles(kernel: str):
 
 
 # ----------------------------------------------------------------------------- CPU baseline
-def _cpu_eval(args):
-    """One FP64 oracle evaluation + NVE update of one system (worker)."""
-    n, seed = args
-    sys.path.insert(0, ROOT)
-    from esp_hoomd_b200 import systems, tables
-    from oracle import esp_ref as R
-    s = systems.rocksalt(n, seed=seed)
-    mesh = tables.smooth235(int(math.ceil(s.box[0] / (math.pi * RCUT / 18.5))))
-    c = round(2 * 0.93 * math.pi * RCUT / (s.box[0] / mesh)) * 0.5
-    prm = tables.ESPParams(mesh=(mesh,) * 3, box=s.box, rcut=RCUT, split=tables.split_cached(c),
-                           window=tables.window_cached(8, 17.6, 10))
-    G = R.influence(prm)  # per-box table, built outside the timed part
-    t0 = time.perf_counter()
-    nl = R.neighbor_list(s.pos, s.box, RCUT + SKIN)
-    rho = R.spread(s.pos, s.q, prm)
-    phi, _ = R.mesh_potential(rho, G)
-    _, fm = R.interpolate(s.pos, s.q, phi, prm)
-    fp, _, _ = R.pair_forces(s.pos, s.q, s.box, prm.split, RCUT, *nl)
-    v = s.vel + DT * (fm + fp)
-    _ = s.pos + DT * v
-    return s.N, time.perf_counter() - t0
+def cpu_sample(count: int, rank: int = 0):
+    """The first `count` systems of the rank's batch (the same systems the
+    GPU step runs), with the C oracle's parameters (same mesh rule)."""
+    from oracle import esp_port as EP
+    sl = _systems(rank, min(count, N_SYS))
+    return sl, EP.plan(sl, RCUT)
 
 
-def cpu_baseline(sample_ns, seeds, procs: int):
-    import multiprocessing as mp
-    work = list(zip(sample_ns, seeds))
+def cpu_baseline(sl, prm, threads: int, cache=None):
+    """One GPU-step's work on the CPU: for every system of the sample a
+    neighbour list, one evaluation and 10 NVE steps, FP64, in the compiled
+    restatement of the pipeline (oracle/esp_oracle.c), one system per
+    OpenMP thread. Returns (particle-steps, seconds)."""
+    from oracle import esp_port as EP
     t0 = time.perf_counter()
-    if procs > 1:
-        with mp.get_context("spawn").Pool(procs) as pool:
-            res = pool.map(_cpu_eval, work)
-    else:
-        res = [_cpu_eval(w) for w in work]
-    wall = time.perf_counter() - t0
-    n_tot = sum(r[0] for r in res)
-    return n_tot, wall, sum(r[1] for r in res)
+    EP.run_batch(sl, prm, RCUT + SKIN, MD_STEPS, DT, threads=threads, influence_cache=cache)
+    return MD_STEPS * sum(s.N for s in sl), time.perf_counter() - t0
 
 
 def run_reference(args):
+    """The reference's CPU path is stubs (src/ESPForceCompute.cc:236-248) and
+    the plugin cannot be built without HOOMD; this arm times the FP64 C
+    restatement of the same path on all host threads, each step one bounded
+    sample of the batched workload."""
+    from oracle import esp_port as EP
     rank, world, _ = _env_rank()
     if rank != 0:
         return
-    cores = os.cpu_count() or 1
-    ns = [8, 16, 24, 32]
-    seeds = [SEED * 100000 + i for i in range(len(ns))]
+    threads = EP.max_threads()
+    sl, prm = cpu_sample(max(4, 2 * threads))
+    cache = EP.influence_tables(prm)  # built outside the timed steps
     for _ in range(args.warmup):
-        cpu_baseline(ns, seeds, min(cores, len(ns)))
-    times = []
-    n_tot = 0
+        cpu_baseline(sl[:1], prm[:1], threads, cache)
+    times, n_ps = [], 0
     for _ in range(args.steps):
-        n_tot, wall, _ = cpu_baseline(ns, seeds, min(cores, len(ns)))
+        n_ps, wall = cpu_baseline(sl, prm, threads, cache)
         times.append(wall)
     t = sum(times) / len(times)
-    value = n_tot / t
-    sample = "oracle FP64 evaluation + NVE update of rock-salt n=%s (%d particles) per step, %d processes" % (
-        ns, n_tot, min(cores, len(ns)))
+    value = n_ps / t
+    sample = ("FP64 C restatement (oracle/esp_oracle.c): nlist + 1 evaluation + 10 NVE steps of the first %d "
+              "systems of the batched256 workload (%d particles) per step, %d OpenMP threads"
+              % (len(sl), sum(s.N for s in sl), threads))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "batched256 rock-salt (CPU sample)", "rcut": RCUT, "order": 8},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": min(cores, len(ns)), "kind": "port",
-                             "sample": sample},
+            "config": {"workload": "batched256 rock-salt (CPU sample of %d systems)" % len(sl), "rcut": RCUT,
+                       "order": 8},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -465,12 +452,16 @@ def run_ours(args):
                 "gpu_launches": int(args.steps * (K_NLIST + K_EVAL + MD_STEPS * (K_EVAL + K_NVE))),
                 "clocks": clk.summary()}
         if not args.no_cpu:
-            ns = [int(N[i]) for i in np.argsort(N)[::64]]
-            ns = [round(x ** (1 / 3)) for x in ns]
-            n_tot, wall, _ = cpu_baseline(ns, [SEED * 100000 + i for i in range(len(ns))], 1)
-            line["cpu_baseline"] = {"value": n_tot / wall, "unit": UNIT, "cores": 1, "kind": "port",
-                                    "sample": "FP64 oracle evaluation + NVE update of rock-salt n=%s (%d particles)"
-                                              % (ns, n_tot)}
+            from oracle import esp_port as EP
+            threads = EP.max_threads()
+            csl, cprm = cpu_sample(max(4, 2 * threads), rank)
+            cache = EP.influence_tables(cprm)
+            n_ps, wall = cpu_baseline(csl, cprm, threads, cache)
+            line["cpu_baseline"] = {
+                "value": n_ps / wall, "unit": UNIT, "cores": threads, "kind": "port",
+                "sample": "FP64 C restatement (oracle/esp_oracle.c): nlist + 1 evaluation + 10 NVE steps of the "
+                          "first %d systems of this batch (%d particles), %d OpenMP threads"
+                          % (len(csl), sum(s.N for s in csl), threads)}
         if not args.no_serve:
             b.close()
             torch.cuda.empty_cache()

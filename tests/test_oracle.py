@@ -208,3 +208,37 @@ def test_exclusion_correction_matches_ewald_without_excluded_pairs():
     # against the system's energy scale sum q^2 / (4 pi r_c)
     assert abs(E - E0) < 1e-7 * R.INV_4PI * np.sum(w.q ** 2) / 0.9
     assert np.abs(W - W0).max() < 1e-5 * np.abs(W0).max()
+
+
+def test_c_port_matches_numpy_oracle():
+    # the compiled FP64 restatement (the timed CPU baseline) against the numpy
+    # oracle on float32-representable positions (the mesh stage's input)
+    from oracle import esp_port as EP
+    s = systems.rocksalt(10, seed=21)
+    s.pos = s.pos.astype(np.float32).astype(np.float64)
+    prm = EP.plan([s], 3.0)
+    _, _, F, E = EP.run_batch([s], prm, 3.4, 0, 0.002, threads=1)
+    E0, F0, _ = R.esp(s.pos, s.q, prm[0], nlist=R.neighbor_list(s.pos, s.box, 3.4))
+    assert R.rel_rms(F[0], F0) < 1e-12
+    assert abs(E[0] - E0) < 1e-12 * abs(E0)
+
+
+def test_c_port_batch_is_independent_of_threads_and_conserves_energy():
+    from oracle import esp_port as EP
+    sl = [systems.rocksalt(n, seed=30 + n) for n in (8, 10, 8)] + [systems.water(216, seed=5)]
+    rs, wa = sl[:3], sl[3:]
+    prm_rs = EP.plan(rs, 3.0)
+    p1, v1, F1, E1 = EP.run_batch(rs, prm_rs, 3.4, 20, 0.002, threads=1)
+    p2, v2, F2, E2 = EP.run_batch(rs, prm_rs, 3.4, 20, 0.002, threads=3)
+    assert np.array_equal(E1, E2) and all(np.array_equal(a, b) for a, b in zip(p1, p2))
+    # kinetic + potential energy of the rock-salt systems over 20 NVE steps
+    _, _, _, E0 = EP.run_batch(rs, prm_rs, 3.4, 0, 0.002, threads=1)
+    for s, v, e0, e1 in zip(rs, v1, E0, E1):
+        k0 = 0.5 * np.sum(s.mass[:, None] * s.vel ** 2)
+        k1 = 0.5 * np.sum(s.mass[:, None] * v ** 2)
+        assert abs((k1 + e1) - (k0 + e0)) < 1e-4 * abs(k0 + e0)
+    # water (r_c 0.9 nm) against Ewald
+    prm_w = EP.plan(wa, 0.9)
+    _, _, Fw, Ew = EP.run_batch(wa, prm_w, 1.0, 0, 0.002, threads=1)
+    E_e, F_e, _ = ewald(wa[0].pos, wa[0].q, wa[0].box)
+    assert R.rel_rms(Fw[0], F_e) < 1e-5
