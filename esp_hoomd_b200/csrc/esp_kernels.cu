@@ -430,7 +430,7 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1
 constexpr int SPREAD_CHM = 64;  // particles staged per round (multiple of 8)
 
 template <int P>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
     k_spread_mma(const int* __restrict__ tile_sys, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
                  int T, int D, const uint32_t* __restrict__ start, const float4* __restrict__ srec,
                  const uint32_t* __restrict__ srel, double* __restrict__ rho) {
@@ -1264,7 +1264,7 @@ struct PairEval {
 };
 
 template <int TPP, int NQ, bool VIR>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 5)
     k_pair(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
            const float4* __restrict__ posq, const uint32_t* __restrict__ head, const uint32_t* __restrict__ nn,
            const uint32_t* __restrict__ nlist, float4* __restrict__ force, double* __restrict__ acc, int accumulate,

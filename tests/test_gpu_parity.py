@@ -259,3 +259,21 @@ def test_exclusions_match_oracle_and_ewald():
     E1, F1, _ = R.esp(w.pos, w.q, prm)
     torch.cuda.synchronize()
     assert R.rel_rms(force.cpu().numpy()[:, :3].astype(np.float64), F1) <= 5e-6
+
+
+@pytest.mark.parametrize("order,target", [(6, 1e-3), (8, 1e-5), (10, 1e-5)])
+def test_water_accuracy_sweep(order, target):
+    # the water-like accuracy sweep (three-site molecules, r_c 0.9 nm, no
+    # exclusions) at the planner's mesh for each target, FP32 path vs Ewald
+    w = systems.water(512, seed=9)
+    w.pos = w.pos.astype(np.float32).astype(np.float64)
+    ctx = native.Context(native.make_params(order=order, rcut=0.9, target_error=target), w.box, w.N)
+    pos4, q = _upload(w)
+    nl = _nlist_dev(*R.neighbor_list(w.pos, w.box, 0.9))
+    force = torch.zeros((w.N, 4), dtype=torch.float32, device="cuda")
+    energy = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ctx.compute(pos4, q, force, energy, None, nlist=nl)
+    torch.cuda.synchronize()
+    E0, F0, _ = ewald(w.pos, w.q, w.box)
+    assert R.rel_rms(force.cpu().numpy()[:, :3].astype(np.float64), F0) <= target
+    assert abs(energy.item() - E0) <= target * abs(E0)
