@@ -28,7 +28,11 @@ EXPORTS = [
     "esp_batch_md_run", "esp_batch_set_timing", "esp_batch_stage_times", "esp_spread_noalloc",
     "esp_server_create", "esp_server_submit", "esp_server_start", "esp_server_status", "esp_server_wait_all",
     "esp_server_get_stats", "esp_server_destroy", "esp_set_exclusions", "esp_batch_set_exclusions",
+    "esp_compute_f64", "esp_batch_compute_f64",
 ]
+
+ESP_FP32 = 0
+ESP_FP64 = 1
 
 STAGES = ["bin", "sort", "spread", "fft", "interp", "pair", "nlist", "nve"]
 
@@ -37,7 +41,8 @@ class EspParams(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("order", ctypes.c_int),
                 ("kappa", ctypes.c_double), ("rcut", ctypes.c_double), ("alpha", ctypes.c_double),
                 ("n_table", ctypes.c_int), ("target_error", ctypes.c_double), ("window_c", ctypes.c_double),
-                ("window_degree", ctypes.c_int), ("tile", ctypes.c_int), ("threads_per_particle", ctypes.c_int)]
+                ("window_degree", ctypes.c_int), ("tile", ctypes.c_int), ("threads_per_particle", ctypes.c_int),
+                ("precision", ctypes.c_int)]
 
 
 class EspInfo(ctypes.Structure):
@@ -129,6 +134,8 @@ def get_lib() -> ctypes.CDLL:
         lib.esp_server_destroy.argtypes = [P]
         lib.esp_set_exclusions.argtypes = [P, P, P, I]
         lib.esp_batch_set_exclusions.argtypes = [P, P, P, I]
+        lib.esp_compute_f64.argtypes = [P, P, P, P, I, P, P, P, P, P, P, I]
+        lib.esp_batch_compute_f64.argtypes = [P, P, P, P, P, P, P, P, P, P, I]
         lib.esp_spread_noalloc.argtypes = [P, ctypes.POINTER(EspParams), D, D, D, P, P, I, P]
         for name in EXPORTS:
             if name != "esp_last_error":

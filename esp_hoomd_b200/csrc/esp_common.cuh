@@ -43,6 +43,7 @@ struct SysDev {
     float Lx, Ly, Lz;
     float inv_Lx, inv_Ly, inv_Lz;
     double gxd, gyd, gzd;  // n / L in FP64
+    double Lxd, Lyd, Lzd;  // box lengths in FP64 (FP64 mode)
     double V;
     int pset;          // parameter-set index
     int twx, twy, twz; // twiddle-table offsets per axis
@@ -57,6 +58,7 @@ struct ParamSet {
     float rcut, rcut2, inv_rcut, two_inv_rcut3;
     double self_coef;    // per-particle self energy = self_coef * q^2
     double bg_coef;      // E_bg = bg_coef * Q^2 / V
+    double rcut_d;       // r_c in FP64 (FP64 mode)
 };
 
 // ----------------------------------------------------------------------------

@@ -100,9 +100,9 @@ void choose_pitch(int P, int E, int& PX, int& PP) {
     }
 }
 
-int build_param_set(double c, double cw, int P, int D, double rcut, PsetHost& h, ParamSet& d) {
+int build_param_set(double c, double cw, int P, int D, double rcut, PsetHost& h, ParamSet& d, double tol) {
     try {
-        h.split.build(c);
+        h.split.build(c, tol);
         h.win.build(P, cw, D);
     } catch (const std::exception& ex) {
         return fail(ESP_ERR_INVALID, ex.what());
@@ -122,6 +122,7 @@ int build_param_set(double c, double cw, int P, int D, double rcut, PsetHost& h,
     d.two_inv_rcut3 = (float)(2.0 / (rcut * rcut * rcut));
     d.self_coef = -0.5 * h.split.lambda0 * INV_4PI_D / rcut;
     d.bg_coef = -0.25 * rcut * rcut * h.split.m2;
+    d.rcut_d = rcut;
     return 0;
 }
 
@@ -248,6 +249,17 @@ struct esp_batch {
     uint32_t *d_ckey = nullptr, *d_ccount = nullptr, *d_cstart = nullptr, *d_cperm = nullptr, *d_slot_cell = nullptr;
     float4 *d_wpos = nullptr, *d_cpos = nullptr;
     int* d_overflow = nullptr;
+    // FP64 mode: tables, records, spectrum and work lists
+    bool f64 = false;
+    DevAlloc mem64;
+    double4 *d_posq64 = nullptr, *d_trec64 = nullptr, *d_srec64 = nullptr;
+    double *d_w64 = nullptr, *d_q64 = nullptr, *d_phi64 = nullptr;
+    double2 *d_tw64 = nullptr, *d_cbuf = nullptr, *d_gtab64 = nullptr;
+    int2 *d_pch64 = nullptr, *d_xl = nullptr, *d_yl = nullptr, *d_zl = nullptr;
+    int n_pch64 = 0, n_xl = 0, n_yl = 0, n_zl = 0, nq64 = 0;
+    int plan64(const std::vector<float2>& tw, long long g_total);
+    int compute_f64(cudaStream_t st, const double* pos4, const double* q, const unsigned* head, const unsigned* nn,
+                    const unsigned* nl, double* force4, double* energy, double* virial, int flags);
     // excluded pairs (caller-owned device arrays), applied by every
     // long-range evaluation
     const uint32_t* ex_n = nullptr;
@@ -283,6 +295,9 @@ struct esp_batch {
 
 int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* boxes, const int* mesh_) {
     mem.release();
+    mem64.release();
+    f64 = false;
+    if (p.precision != ESP_FP32 && p.precision != ESP_FP64) return fail(ESP_ERR_INVALID, "precision must be ESP_FP32 or ESP_FP64");
     nlmem.release();
     nl_rlist = -1;
     prm = p;
@@ -354,7 +369,8 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         if (it == pmap.end()) {
             PsetHost h;
             ParamSet d;
-            const int rc = build_param_set(c, cw, P, D, p.rcut, h, d);
+            // the FP64 mode fits the split polynomial to 1e-12 (FP32 needs 1e-8)
+            const int rc = build_param_set(c, cw, P, D, p.rcut, h, d, p.precision == ESP_FP64 ? 1e-12 : 1e-8);
             if (rc) return rc;
             it = pmap.emplace(key, (int)psh.size()).first;
             psh.push_back(std::move(h));
@@ -405,6 +421,9 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         S.gxd = S.nx / box[3 * s];
         S.gyd = S.ny / box[3 * s + 1];
         S.gzd = S.nz / box[3 * s + 2];
+        S.Lxd = box[3 * s];
+        S.Lyd = box[3 * s + 1];
+        S.Lzd = box[3 * s + 2];
         S.V = box[3 * s] * box[3 * s + 1] * box[3 * s + 2];
         S.pset = sys_pset[s];
         S.twx = twid(S.nx);
@@ -506,6 +525,10 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         ESPB_CK(launch_interp(a, 0));
         ESPB_CK(launch_fft(a, 0));
     }
+    f64 = p.precision == ESP_FP64;
+    if (f64) {
+        if ((rc = plan64(tw, g_off))) return rc;
+    }
     // influence tables (FP64 on the GPU)
     for (int s : g_first) {
         const SysDev& S = sd[s];
@@ -521,12 +544,116 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         ESPB_CK(cudaMemcpy(d_tq, tq.data(), nq * sizeof(double), cudaMemcpyHostToDevice));
         ESPB_CK(cudaMemcpy(d_wq, wq.data(), nq * sizeof(double), cudaMemcpyHostToDevice));
         cudaError_t e = launch_influence(S, d_w1d, d_tq, d_wq, nq, p.rcut, 1e-14, d_gtab, 0);
+        if (e == cudaSuccess && f64) e = launch_influence64(S, d_w1d, d_tq, d_wq, nq, p.rcut, 1e-14, d_gtab64, 0);
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
         cudaFree(d_w1d);
         cudaFree(d_tq);
         cudaFree(d_wq);
         if (e != cudaSuccess) return fail(ESP_ERR_CUDA, std::string("influence build: ") + cudaGetErrorString(e));
     }
+    return 0;
+}
+
+// FP64 tables (window and split coefficients in double, twiddles from FP64
+// angles), FP64 records and spectrum, and the FP64 work lists: 32 particles
+// per pair chunk, four mesh lines per FFT item.
+int esp_batch::plan64(const std::vector<float2>& tw, long long g_total) {
+    const PsetHost& h = psh[0];
+    std::vector<double> w64(h.win.coef.begin(), h.win.coef.end());
+    std::vector<double> q64(h.split.qv.begin(), h.split.qv.end());
+    nq64 = (int)q64.size();
+    std::vector<double2> tw64(tw.size());
+    for (const SysDev& S : sd)
+        for (int d = 0; d < 3; ++d) {
+            const int n = d == 0 ? S.nx : (d == 1 ? S.ny : S.nz);
+            const int off = d == 0 ? S.twx : (d == 1 ? S.twy : S.twz);
+            for (int t = 0; t < n; ++t) {
+                const double a = -2.0 * M_PI * t / n;
+                tw64[off + t] = make_double2(std::cos(a), std::sin(a));
+            }
+        }
+    std::vector<int2> pch, xl, yl, zl;
+    long long M = 0;
+    for (int s = 0; s < nsys; ++s) {
+        const SysDev& S = sd[s];
+        for (int i = 0; i < S.N; i += 32) pch.push_back(make_int2(s, S.p_off + i));
+        const long long lx = (long long)S.ny * S.nz, ly = (long long)S.nx * S.nz, lz = (long long)S.nx * S.ny;
+        for (long long l = 0; l < lx; l += 4) xl.push_back(make_int2(s, (int)l));
+        for (long long l = 0; l < ly; l += 4) yl.push_back(make_int2(s, (int)l));
+        for (long long l = 0; l < lz; l += 4) zl.push_back(make_int2(s, (int)l));
+        M += (long long)S.nx * S.ny * S.nz;
+    }
+    n_pch64 = (int)pch.size();
+    n_xl = (int)xl.size();
+    n_yl = (int)yl.size();
+    n_zl = (int)zl.size();
+    int rc = 0;
+    if ((rc = mem64.get(d_posq64, totN)) || (rc = mem64.get(d_trec64, totN)) || (rc = mem64.get(d_srec64, totN)) ||
+        (rc = mem64.get(d_w64, w64.size())) || (rc = mem64.get(d_q64, q64.size())) || (rc = mem64.get(d_phi64, M)) ||
+        (rc = mem64.get(d_tw64, tw64.size())) || (rc = mem64.get(d_cbuf, M)) || (rc = mem64.get(d_gtab64, g_total)) ||
+        (rc = mem64.get(d_pch64, pch.size())) || (rc = mem64.get(d_xl, xl.size())) || (rc = mem64.get(d_yl, yl.size())) ||
+        (rc = mem64.get(d_zl, zl.size())))
+        return rc;
+    ESPB_CK(cudaMemcpy(d_w64, w64.data(), w64.size() * sizeof(double), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(d_q64, q64.data(), q64.size() * sizeof(double), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(d_tw64, tw64.data(), tw64.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(d_pch64, pch.data(), pch.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(d_xl, xl.data(), xl.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(d_yl, yl.data(), yl.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(d_zl, zl.data(), zl.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    ESPB_CK(launch64_configure(P, T));
+    return 0;
+}
+
+int esp_batch::compute_f64(cudaStream_t st, const double* pos4, const double* q, const unsigned* head,
+                           const unsigned* nn, const unsigned* nl, double* force4, double* energy, double* virial,
+                           int flags) {
+    if (!f64) return fail(ESP_ERR_UNSUPPORTED, "context planned for FP32: create it with precision ESP_FP64");
+    if (!pos4 || !q || !force4) return fail(ESP_ERR_INVALID, "null position, charge or force pointer");
+    if (!(flags & ESP_ALL)) return fail(ESP_ERR_INVALID, "flags select no term");
+    if ((flags & ESP_SHORT_RANGE) && (!head || !nn || !nl))
+        return fail(ESP_ERR_INVALID, "short-range term needs the neighbour list");
+    Launch64 b;
+    b.a = args();
+    LaunchArgs& a = b.a;
+    if (energy) a.energy = energy;
+    if (virial) a.virial = virial;
+    a.want_virial = virial != nullptr;
+    a.nl_head = head;
+    a.nl_n = nn;
+    a.nl_list = nl;
+    a.ex_n = ex_n;
+    a.ex_list = ex_list;
+    a.ex_pitch = ex_pitch;
+    b.long_range = flags & ESP_LONG_RANGE;
+    b.short_range = flags & ESP_SHORT_RANGE;
+    a.add_bg = b.long_range ? 1 : 0;
+    b.pos_in = reinterpret_cast<const double4*>(pos4);
+    b.q_in = q;
+    b.posq = d_posq64;
+    b.trec = d_trec64;
+    b.srec = d_srec64;
+    b.force = reinterpret_cast<double4*>(force4);
+    b.wcoef = d_w64;
+    b.qv = d_q64;
+    b.nq = nq64;
+    b.tw = d_tw64;
+    b.cbuf = d_cbuf;
+    b.phi = d_phi64;
+    b.gtab = d_gtab64;
+    b.pchunks = d_pch64;
+    b.n_pchunks = n_pch64;
+    b.xl = d_xl;
+    b.yl = d_yl;
+    b.zl = d_zl;
+    b.n_xl = n_xl;
+    b.n_yl = n_yl;
+    b.n_zl = n_zl;
+    ESPB_CK(cudaMemsetAsync(d_acc, 0, (size_t)nsys * ACC_STRIDE * sizeof(double), st));
+    ESPB_CK(launch64_eval(b, st));
+    if (!b.long_range)  // the bin stage counted particles per tile; clear for the next call
+        ESPB_CK(cudaMemsetAsync(d_tcount, 0, (size_t)n_tiles * sizeof(uint32_t), st));
+    ESPB_CK(launch_finalize(a, st));
     return 0;
 }
 
@@ -594,6 +721,7 @@ LaunchArgs esp_batch::args() const {
 
 int esp_batch::compute(cudaStream_t st, const float* pos4, const float* q, const unsigned* head, const unsigned* nn,
                        const unsigned* nl, float* force4, double* energy, double* virial, int flags) {
+    if (f64) return fail(ESP_ERR_UNSUPPORTED, "context planned for FP64: use esp_compute_f64");
     if (!pos4 || !q || !force4) return fail(ESP_ERR_INVALID, "null position, charge or force pointer");
     if (!(flags & ESP_ALL)) return fail(ESP_ERR_INVALID, "flags select no term");
     if ((flags & ESP_SHORT_RANGE) && (!head || !nn || !nl))
@@ -899,6 +1027,26 @@ int esp_compute(esp_ctx* c, void* stream, const float* pos4, const float* charge
     return c->b.compute((cudaStream_t)stream, pos4, charge, head, n_neigh, nlist, force4, energy, virial6, flags);
 }
 
+int esp_compute_f64(esp_ctx* c, void* stream, const double* pos4, const double* charge, int N, const unsigned* head,
+                    const unsigned* n_neigh, const unsigned* nlist, double* force4, double* energy, double* virial6,
+                    int flags) {
+    if (!c) return fail(ESP_ERR_INVALID, "null context");
+    if (N < 0) return fail(ESP_ERR_INVALID, "negative particle count");
+    if (N != c->N || c->dirty) {
+        c->N = N;
+        int rc = c->b.plan(c->prm, 1, &c->N, c->L, nullptr);
+        if (rc) return rc;
+        c->dirty = false;
+    }
+    if (N == 0) {
+        cudaStream_t st = (cudaStream_t)stream;
+        if (energy) ESPB_CK(cudaMemsetAsync(energy, 0, sizeof(double), st));
+        if (virial6) ESPB_CK(cudaMemsetAsync(virial6, 0, 6 * sizeof(double), st));
+        return 0;
+    }
+    return c->b.compute_f64((cudaStream_t)stream, pos4, charge, head, n_neigh, nlist, force4, energy, virial6, flags);
+}
+
 int esp_get_info(const esp_ctx* c, esp_info* info) {
     if (!c) return fail(ESP_ERR_INVALID, "null context");
     return c->b.info(0, info);
@@ -957,6 +1105,13 @@ int esp_batch_compute(esp_batch* b, void* stream, const float* pos4, const float
                       int flags) {
     if (!b) return fail(ESP_ERR_INVALID, "null batch");
     return b->compute((cudaStream_t)stream, pos4, charge, head, n_neigh, nlist, force4, energy, virial6, flags);
+}
+
+int esp_batch_compute_f64(esp_batch* b, void* stream, const double* pos4, const double* charge, const unsigned* head,
+                          const unsigned* n_neigh, const unsigned* nlist, double* force4, double* energy,
+                          double* virial6, int flags) {
+    if (!b) return fail(ESP_ERR_INVALID, "null batch");
+    return b->compute_f64((cudaStream_t)stream, pos4, charge, head, n_neigh, nlist, force4, energy, virial6, flags);
 }
 
 int esp_batch_get_info(const esp_batch* b, int sys, esp_info* info) {
@@ -1218,6 +1373,9 @@ extern "C" int esp_spread_noalloc(void* stream, const esp_params* p, double Lx, 
     S.gxd = n[0] / Lx;
     S.gyd = n[1] / Ly;
     S.gzd = n[2] / Lz;
+    S.Lxd = Lx;
+    S.Lyd = Ly;
+    S.Lzd = Lz;
     S.V = Lx * Ly * Lz;
 
     unsigned char* base = nullptr;

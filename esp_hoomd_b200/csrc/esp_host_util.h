@@ -74,7 +74,7 @@ struct PsetHost {
 
 // Builds the split (bandwidth c) and window (P, c_w, degree D) tables and
 // the device parameter block for cutoff rcut. Returns 0 or an ESP_ERR_* code.
-int build_param_set(double c, double cw, int P, int D, double rcut, PsetHost& h, ParamSet& d);
+int build_param_set(double c, double cw, int P, int D, double rcut, PsetHost& h, ParamSet& d, double tol = 1e-8);
 
 // Inputs of the influence kernel for system S: the window's Fourier
 // transform per axis (w1d, nx + ny + nz values) and the quadrature nodes and

@@ -1006,9 +1006,10 @@ __global__ void __launch_bounds__(512)
 //   GB = (-2 Psi / k^2 + r_c Psi'(|k| r_c) / |k|) / (k^2 V w^2)
 // Psi by Gauss-Legendre quadrature of the prolate (weights pre-scaled).
 // ============================================================================
+template <typename T2>
 __global__ void k_influence(SysDev S, const double* __restrict__ w1d, const double* __restrict__ tq,
                             const double* __restrict__ wq, int nq, double rcut, double psi_floor,
-                            float2* __restrict__ gtab) {
+                            T2* __restrict__ gtab) {
     const long long total = (long long)S.nz * S.ny * S.nxh;
     const double twopi = 6.283185307179586;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
@@ -1021,7 +1022,7 @@ __global__ void k_influence(SysDev S, const double* __restrict__ w1d, const doub
         const double kxv = twopi * kx / (double)S.Lx, kyv = twopi * fy / (double)S.Ly,
                      kzv = twopi * fz / (double)S.Lz;
         const double k2 = kxv * kxv + kyv * kyv + kzv * kzv;
-        float2 out = make_float2(0.f, 0.f);
+        double gx = 0.0, gy = 0.0;
         // Nyquist planes of even meshes are dropped: there Psi(kappa_N) is
         // at the split's truncation level while 1/w^2 amplifies aliasing
         // and round-off the most
@@ -1038,10 +1039,13 @@ __global__ void k_influence(SysDev S, const double* __restrict__ w1d, const doub
             if (psi > psi_floor) {
                 const double w = w1d[kx] * w1d[S.nx + y] * w1d[S.nx + S.ny + z];
                 const double den = k2 * S.V * w * w;
-                out.x = (float)(psi / den);
-                out.y = (float)((-2.0 * psi / k2 + rcut * dpsi / kk) / den);
+                gx = psi / den;
+                gy = (-2.0 * psi / k2 + rcut * dpsi / kk) / den;
             }
         }
+        T2 out;
+        out.x = gx;
+        out.y = gy;
         gtab[S.g_off + idx] = out;
     }
 }
@@ -1664,7 +1668,15 @@ cudaError_t launch_influence(const SysDev& S, const double* w1d, const double* t
                              double rcut, double psi_floor, float2* gtab, cudaStream_t st) {
     const long long total = (long long)S.nz * S.ny * S.nxh;
     const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
-    k_influence<<<blocks, 256, 0, st>>>(S, w1d, tq, wq, nq, rcut, psi_floor, gtab);
+    k_influence<float2><<<blocks, 256, 0, st>>>(S, w1d, tq, wq, nq, rcut, psi_floor, gtab);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_influence64(const SysDev& S, const double* w1d, const double* tq, const double* wq, int nq,
+                               double rcut, double psi_floor, double2* gtab, cudaStream_t st) {
+    const long long total = (long long)S.nz * S.ny * S.nxh;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+    k_influence<double2><<<blocks, 256, 0, st>>>(S, w1d, tq, wq, nq, rcut, psi_floor, gtab);
     return cudaGetLastError();
 }
 

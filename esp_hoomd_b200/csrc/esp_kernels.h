@@ -96,6 +96,33 @@ cudaError_t launch_fft(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_interp(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_pair(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_exclusions(const LaunchArgs& a, cudaStream_t st);
+
+// FP64 mode (esp_f64.cu): the shared fields of `a` (descriptors, chunks,
+// tiles, keys, permutation, charge mesh, accumulators, neighbour list,
+// exclusions) plus the FP64 arrays.
+struct Launch64 {
+    LaunchArgs a;
+    bool long_range = true, short_range = true;
+    const double4* pos_in = nullptr;
+    const double* q_in = nullptr;
+    double4 *posq = nullptr, *trec = nullptr, *srec = nullptr, *force = nullptr;
+    const double* wcoef = nullptr;  // window [P][D+1]
+    const double* qv = nullptr;     // split Q(v) coefficients
+    int nq = 0;
+    const double2* tw = nullptr;    // exp(-2 pi i t / n) per axis length
+    double2* cbuf = nullptr;        // full complex spectrum
+    double* phi = nullptr;          // potential mesh
+    const double2* gtab = nullptr;  // {G, G B} half spectrum
+    const int2* pchunks = nullptr;  // 32 particles per chunk (8 lanes per particle)
+    int n_pchunks = 0;
+    const int2 *xl = nullptr, *yl = nullptr, *zl = nullptr;  // {sys, first line}, 4 lines per item
+    int n_xl = 0, n_yl = 0, n_zl = 0;
+};
+size_t spread64_smem(int P, int T);
+cudaError_t launch64_configure(int P, int T);
+cudaError_t launch64_eval(const Launch64& b, cudaStream_t st);
+cudaError_t launch_influence64(const SysDev& S, const double* w1d, const double* tq, const double* wq, int nq,
+                               double rcut, double psi_floor, double2* gtab, cudaStream_t st);
 cudaError_t launch_finalize(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_influence(const SysDev& S, const double* w1d, const double* tq, const double* wq, int nq,
                              double rcut, double psi_floor, float2* gtab, cudaStream_t st);

@@ -518,6 +518,9 @@ int esp_server::admit(Request* q, Staging& sg) {
     S.gxd = S.nx / r.Lx;
     S.gyd = S.ny / r.Ly;
     S.gzd = S.nz / r.Lz;
+    S.Lxd = r.Lx;
+    S.Lyd = r.Ly;
+    S.Lzd = r.Lz;
     S.V = r.Lx * r.Ly * r.Lz;
     S.pset = ps;
     S.twx = tw_off[S.nx];

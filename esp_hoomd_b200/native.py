@@ -14,7 +14,8 @@ from ._lib import EspInfo, EspParams, check, get_lib
 
 def make_params(order: int = 8, rcut: float = 3.0, kappa: float = 0.0, mesh: Optional[Sequence[int]] = None,
                 target_error: float = 1e-5, window_c: float = 0.0, window_degree: int = 0, tile: int = 0,
-                threads_per_particle: int = 0, alpha: float = 0.0, n_table: int = 512) -> EspParams:
+                threads_per_particle: int = 0, alpha: float = 0.0, n_table: int = 512,
+                precision: int = 0) -> EspParams:
     p = EspParams()
     check(get_lib().esp_params_default(ctypes.byref(p)), "esp_params_default")
     p.order = int(order)
@@ -29,6 +30,7 @@ def make_params(order: int = 8, rcut: float = 3.0, kappa: float = 0.0, mesh: Opt
     p.window_degree = int(window_degree)
     p.tile = int(tile)
     p.threads_per_particle = int(threads_per_particle)
+    p.precision = int(precision)
     return p
 
 
@@ -67,6 +69,15 @@ class Context:
         check(self._lib.esp_compute(self._h, _stream(stream), _ptr(pos4), _ptr(q), int(pos4.shape[0]), _ptr(head),
                                     _ptr(nn), _ptr(nl), _ptr(force4), _ptr(energy), _ptr(virial), int(flags)),
               "esp_compute")
+
+    def compute_f64(self, pos4: torch.Tensor, q: torch.Tensor, force4: torch.Tensor,
+                    energy: Optional[torch.Tensor] = None, virial: Optional[torch.Tensor] = None, nlist=None,
+                    flags: int = _lib.ESP_ALL, stream=None) -> None:
+        """FP64 evaluation (float64 tensors; context created with precision=1)."""
+        head, nn, nl = nlist if nlist is not None else (None, None, None)
+        check(self._lib.esp_compute_f64(self._h, _stream(stream), _ptr(pos4), _ptr(q), int(pos4.shape[0]),
+                                        _ptr(head), _ptr(nn), _ptr(nl), _ptr(force4), _ptr(energy), _ptr(virial),
+                                        int(flags)), "esp_compute_f64")
 
     def spread(self, pos4: torch.Tensor, q: torch.Tensor, stream=None) -> torch.Tensor:
         """Charge mesh rho[nz, ny, nx] (float64) of the bin+sort+spread stages."""

@@ -37,6 +37,10 @@ extern "C" {
 #define ESP_ERR_UNSUPPORTED (-4) /* parameter outside the supported set */
 #define ESP_ERR_OVERFLOW (-5)    /* neighbour list capacity exceeded */
 
+/* precision of a context (esp_params.precision) */
+#define ESP_FP32 0 /* FP32 bulk arithmetic, FP64 reductions (esp_compute) */
+#define ESP_FP64 1 /* every stage in FP64 (esp_compute_f64) */
+
 /* compute flags */
 #define ESP_LONG_RANGE 1  /* mesh part + self + background (esp.Spectral) */
 #define ESP_SHORT_RANGE 2 /* pair part over the neighbour list (esp.Local) */
@@ -60,6 +64,7 @@ typedef struct esp_params {
     int window_degree;   /* window polynomial degree; 0 = auto */
     int tile;            /* tile edge in mesh cells; 0 = auto */
     int threads_per_particle; /* pair kernel lanes per particle: 4, 8, 16, 32; 0 = auto */
+    int precision;       /* ESP_FP32 (default) or ESP_FP64 */
 } esp_params;
 
 /* Resolved configuration of a context or of one system of a batch. */
@@ -104,6 +109,15 @@ int esp_invalidate(esp_ctx* ctx);
 int esp_compute(esp_ctx* ctx, void* stream, const float* pos4, const float* charge, int N,
                 const unsigned* head, const unsigned* n_neigh, const unsigned* nlist,
                 float* force4, double* energy, double* virial6, int flags);
+
+/* FP64 evaluation (contexts created with precision ESP_FP64), for HOOMD
+ * double builds: positions and forces are 4 doubles per particle (Scalar4 =
+ * double4), charges doubles; otherwise as esp_compute. Every stage runs in
+ * FP64 (split polynomial fitted to 1e-12), the path for accuracy targets
+ * below the FP32 floor (~1e-7 relative RMS force error). */
+int esp_compute_f64(esp_ctx* ctx, void* stream, const double* pos4, const double* charge, int N,
+                    const unsigned* head, const unsigned* n_neigh, const unsigned* nlist,
+                    double* force4, double* energy, double* virial6, int flags);
 
 int esp_get_info(const esp_ctx* ctx, esp_info* info);
 int esp_destroy(esp_ctx* ctx);
@@ -176,6 +190,9 @@ int esp_batch_create(const esp_params* p, int nsys, const int* N, const double* 
 int esp_batch_compute(esp_batch* b, void* stream, const float* pos4, const float* charge, const unsigned* head,
                       const unsigned* n_neigh, const unsigned* nlist, float* force4, double* energy,
                       double* virial6, int flags);
+int esp_batch_compute_f64(esp_batch* b, void* stream, const double* pos4, const double* charge, const unsigned* head,
+                          const unsigned* n_neigh, const unsigned* nlist, double* force4, double* energy,
+                          double* virial6, int flags);
 int esp_batch_get_info(const esp_batch* b, int sys, esp_info* info);
 int esp_batch_total_particles(const esp_batch* b);
 int esp_batch_destroy(esp_batch* b);
