@@ -28,7 +28,7 @@ EXPORTS = [
     "esp_batch_md_run", "esp_batch_set_timing", "esp_batch_stage_times", "esp_spread_noalloc",
     "esp_server_create", "esp_server_submit", "esp_server_start", "esp_server_status", "esp_server_wait_all",
     "esp_server_get_stats", "esp_server_destroy", "esp_set_exclusions", "esp_batch_set_exclusions",
-    "esp_compute_f64", "esp_batch_compute_f64",
+    "esp_compute_f64", "esp_batch_compute_f64", "esp_batch_autotune",
 ]
 
 ESP_FP32 = 0
@@ -42,7 +42,7 @@ class EspParams(ctypes.Structure):
                 ("kappa", ctypes.c_double), ("rcut", ctypes.c_double), ("alpha", ctypes.c_double),
                 ("n_table", ctypes.c_int), ("target_error", ctypes.c_double), ("window_c", ctypes.c_double),
                 ("window_degree", ctypes.c_int), ("tile", ctypes.c_int), ("threads_per_particle", ctypes.c_int),
-                ("precision", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("fft_mode", ctypes.c_int)]
 
 
 class EspInfo(ctypes.Structure):
@@ -136,6 +136,7 @@ def get_lib() -> ctypes.CDLL:
         lib.esp_batch_set_exclusions.argtypes = [P, P, P, I]
         lib.esp_compute_f64.argtypes = [P, P, P, P, I, P, P, P, P, P, P, I]
         lib.esp_batch_compute_f64.argtypes = [P, P, P, P, P, P, P, P, P, P, I]
+        lib.esp_batch_autotune.argtypes = [P, P, P, P, P, P, P, I, I, ctypes.POINTER(EspParams), P, I]
         lib.esp_spread_noalloc.argtypes = [P, ctypes.POINTER(EspParams), D, D, D, P, P, I, P]
         for name in EXPORTS:
             if name != "esp_last_error":

@@ -291,6 +291,8 @@ struct esp_batch {
     int build_nlist(cudaStream_t st, const float* pos4, double rlist, int cap, unsigned* head, unsigned* nn,
                     unsigned* nl);
     int info(int s, esp_info* out) const;
+    int autotune(cudaStream_t st, const float* pos4, const float* q, const unsigned* head, const unsigned* nn,
+                 const unsigned* nl, int flags, int reps, esp_params* chosen, double* trial_ms, int max_trials);
 };
 
 int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* boxes, const int* mesh_) {
@@ -461,7 +463,7 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         for (int t = 0; t < S.ntx * S.nty * S.ntz; ++t) tile_sys[S.t_off + t] = s;
         // whole planes / slabs in shared memory when they fit, else per-line passes
         const int sp = fft_plane_smem(S.nx, S.ny), ss = fft_slab_smem(S.nx, S.nz);
-        if (sp <= FFT_SMEM_MAX) {
+        if (sp <= FFT_SMEM_MAX && p.fft_mode == 0) {
             smem_plane = std::max(smem_plane, sp);
             for (int z = 0; z < S.nz; ++z) pi.push_back(make_int2(s, z));
         } else {
@@ -470,7 +472,7 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
             for (int z = 0; z < S.nz; ++z)
                 for (int k0 = 0; k0 < S.nxh; k0 += FFT_B_YZ) yi.push_back(make_int4(s, z, k0, 0));
         }
-        if (ss <= FFT_SMEM_MAX) {
+        if (ss <= FFT_SMEM_MAX && p.fft_mode == 0) {
             smem_slab = std::max(smem_slab, ss);
             for (int y = 0; y < S.ny; ++y) si.push_back(make_int2(s, y));
         } else {
@@ -923,6 +925,93 @@ int esp_batch::build_nlist(cudaStream_t st, const float* pos4, double rlist, int
     return 0;
 }
 
+int esp_batch::autotune(cudaStream_t st, const float* pos4, const float* q, const unsigned* head,
+                        const unsigned* nn, const unsigned* nl, int flags, int reps, esp_params* chosen,
+                        double* trial_ms, int max_trials) {
+    if (f64) return fail(ESP_ERR_UNSUPPORTED, "the autotuner times the FP32 path");
+    if (reps < 1) return fail(ESP_ERR_INVALID, "reps must be positive");
+    const std::vector<int> Nv = N;
+    const std::vector<double> boxv = box;
+    const std::vector<int> meshv = mesh;  // candidates keep the meshes (and so the accuracy)
+    esp_params cur = prm;
+    cur.tile = T;
+    cur.threads_per_particle = tpp;
+    float* d_force = nullptr;
+    double* d_e = nullptr;
+    ESPB_CK(cudaMalloc(&d_force, (size_t)std::max(totN, 1) * 16));
+    ESPB_CK(cudaMalloc(&d_e, (size_t)nsys * sizeof(double)));
+    cudaEvent_t e0, e1;
+    ESPB_CK(cudaEventCreate(&e0));
+    ESPB_CK(cudaEventCreate(&e1));
+    int ntrial = 0;
+    auto run = [&](const esp_params& c, double& ms) -> int {
+        int rc = plan(c, (int)Nv.size(), Nv.data(), boxv.data(), meshv.data());
+        if (rc) return rc;
+        if ((rc = compute(st, pos4, q, head, nn, nl, d_force, d_e, nullptr, flags))) return rc;  // warm-up
+        ESPB_CK(cudaEventRecord(e0, st));
+        for (int k = 0; k < reps; ++k)
+            if ((rc = compute(st, pos4, q, head, nn, nl, d_force, d_e, nullptr, flags))) return rc;
+        ESPB_CK(cudaEventRecord(e1, st));
+        ESPB_CK(cudaEventSynchronize(e1));
+        float t = 0.f;
+        ESPB_CK(cudaEventElapsedTime(&t, e0, e1));
+        ms = t / reps;
+        if (trial_ms && ntrial < max_trials) trial_ms[ntrial] = ms;
+        ++ntrial;
+        return 0;
+    };
+    int rc = 0;
+    double best_ms = 0;
+    esp_params best = cur;
+    if ((rc = run(cur, best_ms))) goto done;
+    {
+        // pair lanes per particle
+        for (int t : {4, 16}) {
+            esp_params c = best;
+            c.threads_per_particle = t;
+            double ms = 0;
+            if ((rc = run(c, ms))) goto done;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = c;
+            }
+        }
+        // tile edge: the 16^3 tensor-core tile and two smaller dense tiles
+        const int Tdef = std::max(1, 17 - P);
+        for (int t : {Tdef - 1, Tdef - 2}) {
+            if (t < 2 || t == best.tile) continue;
+            esp_params c = best;
+            c.tile = t;
+            double ms = 0;
+            if ((rc = run(c, ms))) goto done;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = c;
+            }
+        }
+        // FFT pass form
+        {
+            esp_params c = best;
+            c.fft_mode = best.fft_mode ? 0 : 1;
+            double ms = 0;
+            if ((rc = run(c, ms))) goto done;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = c;
+            }
+        }
+    }
+done:
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d_force);
+    cudaFree(d_e);
+    if (rc) return rc;
+    if ((rc = plan(best, (int)Nv.size(), Nv.data(), boxv.data(), meshv.data()))) return rc;
+    if (chosen) *chosen = best;
+    return 0;
+}
+
 int esp_batch::info(int s, esp_info* out) const {
     if (!out || s < 0 || s >= nsys) return fail(ESP_ERR_INVALID, "bad system index or null info");
     const SysDev& S = sd[s];
@@ -1112,6 +1201,14 @@ int esp_batch_compute_f64(esp_batch* b, void* stream, const double* pos4, const 
                           double* virial6, int flags) {
     if (!b) return fail(ESP_ERR_INVALID, "null batch");
     return b->compute_f64((cudaStream_t)stream, pos4, charge, head, n_neigh, nlist, force4, energy, virial6, flags);
+}
+
+int esp_batch_autotune(esp_batch* b, void* stream, const float* pos4, const float* charge, const unsigned* head,
+                       const unsigned* n_neigh, const unsigned* nlist, int flags, int reps, esp_params* chosen,
+                       double* trial_ms, int max_trials) {
+    if (!b) return fail(ESP_ERR_INVALID, "null batch");
+    return b->autotune((cudaStream_t)stream, pos4, charge, head, n_neigh, nlist, flags, reps, chosen, trial_ms,
+                       max_trials);
 }
 
 int esp_batch_get_info(const esp_batch* b, int sys, esp_info* info) {

@@ -15,7 +15,7 @@ from ._lib import EspInfo, EspParams, check, get_lib
 def make_params(order: int = 8, rcut: float = 3.0, kappa: float = 0.0, mesh: Optional[Sequence[int]] = None,
                 target_error: float = 1e-5, window_c: float = 0.0, window_degree: int = 0, tile: int = 0,
                 threads_per_particle: int = 0, alpha: float = 0.0, n_table: int = 512,
-                precision: int = 0) -> EspParams:
+                precision: int = 0, fft_mode: int = 0) -> EspParams:
     p = EspParams()
     check(get_lib().esp_params_default(ctypes.byref(p)), "esp_params_default")
     p.order = int(order)
@@ -31,6 +31,7 @@ def make_params(order: int = 8, rcut: float = 3.0, kappa: float = 0.0, mesh: Opt
     p.tile = int(tile)
     p.threads_per_particle = int(threads_per_particle)
     p.precision = int(precision)
+    p.fft_mode = int(fft_mode)
     return p
 
 
@@ -193,6 +194,19 @@ class Batch:
         self._ex = (n_ex, ex_list)
         check(self._lib.esp_batch_set_exclusions(self._h, _ptr(n_ex), _ptr(ex_list), int(ex_pitch)),
               "esp_batch_set_exclusions")
+
+    def autotune(self, pos4, q, nlist=None, flags: int = _lib.ESP_ALL, reps: int = 3, stream=None) -> dict:
+        """Times candidate plans on these inputs and keeps the fastest; returns
+        the chosen knobs and the per-candidate milliseconds per evaluation."""
+        head, nn, nl = nlist if nlist is not None else (None, None, None)
+        chosen = EspParams()
+        trials = np.zeros(16, dtype=np.float64)
+        check(self._lib.esp_batch_autotune(self._h, _stream(stream), _ptr(pos4), _ptr(q), _ptr(head), _ptr(nn),
+                                           _ptr(nl), int(flags), int(reps), ctypes.byref(chosen),
+                                           trials.ctypes.data_as(ctypes.c_void_p), int(trials.size)),
+              "esp_batch_autotune")
+        return {"tile": chosen.tile, "threads_per_particle": chosen.threads_per_particle,
+                "fft_mode": chosen.fft_mode, "trial_ms": [float(t) for t in trials if t > 0]}
 
     def set_timing(self, on: bool) -> None:
         check(self._lib.esp_batch_set_timing(self._h, int(bool(on))), "esp_batch_set_timing")

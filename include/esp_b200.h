@@ -65,6 +65,7 @@ typedef struct esp_params {
     int tile;            /* tile edge in mesh cells; 0 = auto */
     int threads_per_particle; /* pair kernel lanes per particle: 4, 8, 16, 32; 0 = auto */
     int precision;       /* ESP_FP32 (default) or ESP_FP64 */
+    int fft_mode;        /* 0: whole planes/slabs in shared memory where they fit; 1: per-line passes */
 } esp_params;
 
 /* Resolved configuration of a context or of one system of a batch. */
@@ -193,6 +194,19 @@ int esp_batch_compute(esp_batch* b, void* stream, const float* pos4, const float
 int esp_batch_compute_f64(esp_batch* b, void* stream, const double* pos4, const double* charge, const unsigned* head,
                           const unsigned* n_neigh, const unsigned* nlist, double* force4, double* energy,
                           double* virial6, int flags);
+/* Autotuner (no reference counterpart; the reference's Autotuner<1> only
+ * picks block sizes, src/ESPForceComputeGPU.cc:52-61): times `reps`
+ * evaluations (flags as esp_batch_compute) of candidate plans on the given
+ * inputs with CUDA events on `stream` -- pair lanes per particle (4, 8, 16),
+ * tile edge (the 16^3 tensor-core tile and smaller dense tiles), FFT pass form
+ * (whole planes/slabs in shared memory or per-line passes) -- by coordinate
+ * descent, keeps the fastest plan (same meshes and accuracy) and writes its
+ * parameters to `chosen` (may be NULL) and the per-candidate times (ms per
+ * evaluation, up to `max_trials`) to `trial_ms` (may be NULL). Synchronises
+ * `stream`; allocates like esp_batch_create. */
+int esp_batch_autotune(esp_batch* b, void* stream, const float* pos4, const float* charge, const unsigned* head,
+                       const unsigned* n_neigh, const unsigned* nlist, int flags, int reps, esp_params* chosen,
+                       double* trial_ms, int max_trials);
 int esp_batch_get_info(const esp_batch* b, int sys, esp_info* info);
 int esp_batch_total_particles(const esp_batch* b);
 int esp_batch_destroy(esp_batch* b);

@@ -277,3 +277,33 @@ def test_water_accuracy_sweep(order, target):
     E0, F0, _ = ewald(w.pos, w.q, w.box)
     assert R.rel_rms(force.cpu().numpy()[:, :3].astype(np.float64), F0) <= target
     assert abs(energy.item() - E0) <= target * abs(E0)
+
+
+def test_autotune_keeps_results():
+    # the autotuner re-plans with the fastest candidate on the same meshes:
+    # forces and energies are the same as before tuning, within the parity
+    # tolerance, and every candidate was timed
+    sl = [systems.rocksalt(n, seed=7100 + n) for n in (10, 12, 14)]
+    N = [s.N for s in sl]
+    b = native.Batch(native.make_params(), N, [s.box for s in sl])
+    pos4 = np.zeros((sum(N), 4), np.float32)
+    pos4[:, :3] = np.concatenate([s.pos for s in sl])
+    pos = torch.tensor(pos4, device="cuda")
+    q = torch.tensor(np.concatenate([s.q for s in sl]).astype(np.float32), device="cuda")
+    tot = sum(N)
+    head = torch.zeros(tot, dtype=torch.int32, device="cuda")
+    nn = torch.zeros_like(head)
+    nl = torch.zeros(tot * 256, dtype=torch.int32, device="cuda")
+    b.build_nlist(pos, 3.4, 256, head, nn, nl)
+    f0 = torch.zeros((tot, 4), device="cuda")
+    e0 = torch.zeros(3, dtype=torch.float64, device="cuda")
+    b.compute(pos, q, f0, e0, nlist=(head, nn, nl))
+    res = b.autotune(pos, q, nlist=(head, nn, nl), reps=2)
+    assert res["threads_per_particle"] in (4, 8, 16) and 5 <= res["tile"] <= 9 and res["fft_mode"] in (0, 1)
+    assert len(res["trial_ms"]) >= 5 and min(res["trial_ms"]) > 0
+    f1 = torch.zeros_like(f0)
+    e1 = torch.zeros_like(e0)
+    b.compute(pos, q, f1, e1, nlist=(head, nn, nl))
+    torch.cuda.synchronize()
+    assert R.rel_rms(f1.cpu().numpy()[:, :3].astype(np.float64), f0.cpu().numpy()[:, :3].astype(np.float64)) <= 5e-6
+    assert np.allclose(e1.cpu().numpy(), e0.cpu().numpy(), rtol=2e-6, atol=0)
