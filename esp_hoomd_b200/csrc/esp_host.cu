@@ -313,7 +313,7 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
     N.assign(N_, N_ + ns);
     box.assign(boxes, boxes + 3 * ns);
     mesh.assign(3 * ns, 0);
-    tpp = p.threads_per_particle ? p.threads_per_particle : 8;
+    tpp = p.threads_per_particle ? p.threads_per_particle : 4;  // the tuned choice on the mixed batch
     if (tpp != 4 && tpp != 8 && tpp != 16 && tpp != 32)
         return fail(ESP_ERR_UNSUPPORTED, "threads_per_particle must be 4, 8, 16 or 32");
     const double target = p.target_error > 0 ? p.target_error : 1e-5;
@@ -966,7 +966,8 @@ int esp_batch::autotune(cudaStream_t st, const float* pos4, const float* q, cons
     if ((rc = run(cur, best_ms))) goto done;
     {
         // pair lanes per particle
-        for (int t : {4, 16}) {
+        for (int t : {4, 8, 16}) {
+            if (t == best.threads_per_particle) continue;
             esp_params c = best;
             c.threads_per_particle = t;
             double ms = 0;

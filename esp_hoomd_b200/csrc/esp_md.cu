@@ -88,8 +88,12 @@ __global__ void k_nlist(const int* __restrict__ cell_sys, int n_cells_total, con
                 const int xx = (cx + dx + C.ncx) % C.ncx;
                 const uint32_t c = (uint32_t)(C.c_off + (zz * C.ncy + yy) * C.ncx + xx);
                 const uint32_t b = cstart[c], e = cstart[c + 1];
+                // the next candidate is loaded before the current one is
+                // tested, so each load's latency overlaps one test
+                float4 nxt = b < e ? cpos[b] : make_float4(0.f, 0.f, 0.f, 0.f);
                 for (uint32_t s = b; s < e; ++s) {
-                    const float4 pj = cpos[s];
+                    const float4 pj = nxt;
+                    if (s + 1 < e) nxt = cpos[s + 1];
                     const int j = __float_as_int(pj.w);
                     if (j == i) continue;
                     float ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;

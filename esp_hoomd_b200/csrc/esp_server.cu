@@ -241,7 +241,7 @@ int esp_server::init(const esp_server_config& cfg) {
     if (cfg.hbm_budget < (256LL << 20)) return fail(ESP_ERR_INVALID, "hbm_budget must be at least 256 MB");
     max_slots = cfg.max_systems;
     max_particles = cfg.max_particles;
-    tpp = prm.threads_per_particle ? prm.threads_per_particle : 8;
+    tpp = prm.threads_per_particle ? prm.threads_per_particle : 4;
     if (tpp != 4 && tpp != 8 && tpp != 16 && tpp != 32)
         return fail(ESP_ERR_UNSUPPORTED, "threads_per_particle must be 4, 8, 16 or 32");
     T = prm.tile > 0 ? prm.tile : std::max(1, 17 - P);

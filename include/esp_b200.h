@@ -63,7 +63,7 @@ typedef struct esp_params {
     double window_c;     /* window bandwidth c_w; 0 = auto */
     int window_degree;   /* window polynomial degree; 0 = auto */
     int tile;            /* tile edge in mesh cells; 0 = auto */
-    int threads_per_particle; /* pair kernel lanes per particle: 4, 8, 16, 32; 0 = auto */
+    int threads_per_particle; /* pair kernel lanes per particle: 4, 8, 16, 32; 0 = 4 */
     int precision;       /* ESP_FP32 (default) or ESP_FP64 */
     int fft_mode;        /* 0: whole planes/slabs in shared memory where they fit; 1: per-line passes */
 } esp_params;

@@ -193,9 +193,10 @@ def test_batch_alone_equals_in_mix():
         a, z = b.offsets[i], b.offsets[i + 1]
         fa = f.cpu().numpy()
         assert np.abs(fa - fb[a:z]).max() <= 1e-6 * np.abs(fa).max()
-        assert abs(e.item() - eb[i].item()) <= 1e-9 * abs(e.item())
         # the FP64 charge-mesh flush is atomic, so mesh sums may round in a
-        # different order: agreement to 1e-6 of the largest component
+        # different order before the FP32 potential: energies agree to 1e-8
+        # relative, virials to 1e-6 of the largest component
+        assert abs(e.item() - eb[i].item()) <= 1e-8 * abs(e.item())
         va, vbi = v.cpu().numpy(), vb[6 * i:6 * i + 6].cpu().numpy()
         assert np.abs(va - vbi).max() <= 1e-6 * np.abs(va).max()
 
