@@ -54,6 +54,19 @@ def _env_rank():
         int(os.environ.get("LOCAL_RANK", "0"))
 
 
+def max_over_ranks(ms: float, world: int, device=None) -> float:
+    """The slowest rank's time: every rank calls this with its own device-timed
+    milliseconds (an all-reduce MAX; ranks run independent replicas, so this is
+    the only collective of the data path)."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _systems(rank: int, count: int = N_SYS):
     """The first `count` systems of the rank's 256-system batch."""
     from esp_hoomd_b200 import systems
@@ -341,10 +354,7 @@ def run_ours(args):
         en.record(stream)
         barrier()
     ms = st.elapsed_time(en) / args.steps
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, world, dev)
     value = world * tot * MD_STEPS / (ms_max * 1e-3)
 
     # -- stage timing (live CUDA events on the launching stream, same workload, no graph)
@@ -431,11 +441,8 @@ def run_ours(args):
         e2e_step()
     en.record(stream)
     barrier()
-    e2e_ms = st.elapsed_time(en) / args.steps
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * tot * MD_STEPS / (float(t.item()) * 1e-3)
+    e2e_ms = max_over_ranks(st.elapsed_time(en) / args.steps, world, dev)
+    e2e_value = world * tot * MD_STEPS / (e2e_ms * 1e-3)
 
     if rank == 0:
         cores = os.cpu_count() or 1
