@@ -81,23 +81,18 @@ uint32_t radix_plan(int n) {
     return code;
 }
 
-// (PX, PP) pitches of the interpolation tile: the lanes of one particle
-// group read the stencil planes oz + c (c < P) at a common (x, y), so the
-// plane pitch spreads c * PP over distinct banks.
+// (PX, PP) pitches of the interpolation tile. A group of G lanes serves one
+// particle (lane c reads stencil plane oz + c) and K = 32 / G groups share a
+// warp. With the plane pitch PP = K (mod 32) a group's lanes fall in the bank
+// class of its row start, and with the row pitch PX a multiple of K that
+// class is the particle's x origin mod K; the kernel orders particles so the
+// K groups of a warp have distinct classes (conflict-free reads).
 void choose_pitch(int P, int E, int& PX, int& PP) {
-    PX = E;
-    PP = E * E;
-    int best = 1 << 30;
-    for (int pp = E * E; pp <= E * E + 32; ++pp) {
-        int cnt[32] = {0};
-        int worst = 0;
-        for (int c = 0; c < P; ++c) worst = std::max(worst, ++cnt[(c * pp) & 31]);
-        const int score = worst * 1000 + (pp - E * E);
-        if (score < best) {
-            best = score;
-            PP = pp;
-        }
-    }
+    const int G = P <= 4 ? 4 : (P <= 8 ? 8 : 16);
+    const int K = 32 / G;
+    PX = (E + K - 1) / K * K;
+    PP = E * PX;
+    while (PP % 32 != K) ++PP;
 }
 
 int build_param_set(double c, double cw, int P, int D, double rcut, PsetHost& h, ParamSet& d, double tol) {

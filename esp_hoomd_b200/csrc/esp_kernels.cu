@@ -1061,7 +1061,7 @@ __global__ void k_influence(SysDev S, const double* __restrict__ w1d, const doub
 // words of the interpolation staging area: the per-chunk weights, or (before
 // the first chunk) the wrapped row offsets and x indices of the region
 __host__ __device__ inline int interp_stage_words(int P, int CH, int E) {
-    return CH * 6 * P > E * E + E ? CH * 6 * P : E * E + E;
+    return CH * (6 * P + 1) > E * E + E ? CH * (6 * P + 1) : E * E + E;
 }
 
 template <int P>
@@ -1093,7 +1093,10 @@ __global__ void __launch_bounds__(128)
     float* wts = sm + E * PP;                      // [CH][6P] wx dwx wy dwy wz dwz (index tables first)
     float* qv = wts + interp_stage_words(P, C::CH, E);  // [CH] charges
     int* org = reinterpret_cast<int*>(qv + C::CH); // [CH] packed origins
-    float* wc = reinterpret_cast<float*>(org + C::CH);  // [P][D+1]
+    int* order = org + C::CH;                      // [CH] processing order of the chunk
+    float* wc = reinterpret_cast<float*>(order + C::CH);  // [P][D+1]
+    constexpr int WS = 6 * P + 1;                  // weight row stride (odd: conflict-free broadcasts)
+    constexpr int K = 32 / C::G;                   // particle groups per warp
     const int lt = t - S.t_off;
     const int X0 = (lt % S.ntx) * T, Y0 = ((lt / S.ntx) % S.nty) * T, Z0 = (lt / (S.ntx * S.nty)) * T;
     // stage the extended region with asynchronous 4-byte copies (every
@@ -1153,8 +1156,8 @@ __global__ void __launch_bounds__(128)
                         w = horner_w(&wc[a2 * (D + 1)], D, tt);
                         dw = horner_dw(&wc[a2 * (D + 1)], D, tt);
                     }
-                    wts[p * 6 * P + ax * 2 * P + a2] = w;
-                    wts[p * 6 * P + ax * 2 * P + P + a2] = dw;
+                    wts[p * WS + ax * 2 * P + a2] = w;
+                    wts[p * WS + ax * 2 * P + P + a2] = dw;
                 }
             }
             for (int p = threadIdx.x; p < nc; p += blockDim.x) {
@@ -1163,12 +1166,41 @@ __global__ void __launch_bounds__(128)
             }
         }
         __syncthreads();
+        if (C::CH <= 32 && threadIdx.x < 32) {
+            // processing order: queue position q prefers a particle whose x
+            // origin is congruent to q mod K, so the K groups of a warp read
+            // potential rows in disjoint bank classes (plane pitch = K mod 32,
+            // row pitch a multiple of K); particles left over fill the free
+            // positions in order
+            const int j = threadIdx.x;
+            const unsigned full = 0xffffffffu, lt = (1u << j) - 1u;
+            const bool valid = j < nc;
+            const int cls = valid ? ((org[j] & 255) & (K - 1)) : -1;
+            int rank = 0, cpos = 0;
+            const int pk = j & (K - 1);
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const unsigned m = __ballot_sync(full, cls == k);
+                if (cls == k) rank = __popc(m & lt);
+                if (pk == k) cpos = __popc(m);
+            }
+            const int slots = valid ? (nc - cls + K - 1) / K : 0;
+            const bool placed = valid && rank < slots;
+            const unsigned fm = __ballot_sync(full, j < nc && j / K >= cpos);
+            const unsigned lm = __ballot_sync(full, valid && !placed);
+            if (placed) order[cls + K * rank] = j;
+            else if (valid) order[__fns(fm, 0, __popc(lm & lt) + 1)] = j;
+        } else if (C::CH > 32) {
+            for (int p = threadIdx.x; p < nc; p += blockDim.x) order[p] = p;
+        }
+        __syncthreads();
         for (int pp = 0; pp < nc; pp += C::NG) {
-            const int p = pp + grp;
-            const bool act = p < nc && gl < P;
+            const int qq = pp + grp;
+            const int p = qq < nc ? order[qq] : qq;
+            const bool act = qq < nc && gl < P;
             float pot = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
             if (act) {
-                const float* W = wts + p * 6 * P;
+                const float* W = wts + p * WS;
                 float wx[P], dwx[P];
 #pragma unroll
                 for (int a2 = 0; a2 < P; ++a2) {
@@ -1207,7 +1239,7 @@ __global__ void __launch_bounds__(128)
                 gy += __shfl_xor_sync(0xffffffffu, gy, o, C::G);
                 gz += __shfl_xor_sync(0xffffffffu, gz, o, C::G);
             }
-            if (p < nc && gl == 0) {
+            if (qq < nc && gl == 0) {
                 const float q = qv[p];
                 const double e_i = 0.5 * (double)q * pot + self_coef * (double)q * q;
                 force[perm[s0 + base + p]] = make_float4(q * gxs * gx, q * gys * gy, q * gzs * gz, (float)e_i);
@@ -1453,7 +1485,7 @@ template <int P>
 static cudaError_t launch_interp_p(const LaunchArgs& a, cudaStream_t st) {
     using C = InterpCfg<P>;
     const int E = a.T + P - 1;
-    const size_t smem = ((size_t)E * a.PP + interp_stage_words(P, C::CH, E) + 2 * C::CH + P * (MAX_D + 1)) * 4;
+    const size_t smem = ((size_t)E * a.PP + interp_stage_words(P, C::CH, E) + 3 * C::CH + P * (MAX_D + 1)) * 4;
     if (a.configure_only)
         return cudaFuncSetAttribute(k_interp<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (a.n_tiles == 0) return cudaSuccess;
