@@ -28,7 +28,8 @@ EXPORTS = [
     "esp_batch_md_run", "esp_batch_set_timing", "esp_batch_stage_times", "esp_spread_noalloc",
     "esp_server_create", "esp_server_submit", "esp_server_start", "esp_server_status", "esp_server_wait_all",
     "esp_server_get_stats", "esp_server_destroy", "esp_set_exclusions", "esp_batch_set_exclusions",
-    "esp_compute_f64", "esp_batch_compute_f64", "esp_batch_autotune",
+    "esp_compute_f64", "esp_batch_compute_f64", "esp_batch_autotune", "esp_batch_lj", "esp_batch_lj_f64",
+    "esp_batch_nve_step1_f64", "esp_batch_nve_step2_f64",
 ]
 
 ESP_FP32 = 0
@@ -136,6 +137,10 @@ def get_lib() -> ctypes.CDLL:
         lib.esp_batch_set_exclusions.argtypes = [P, P, P, I]
         lib.esp_compute_f64.argtypes = [P, P, P, P, I, P, P, P, P, P, P, I]
         lib.esp_batch_compute_f64.argtypes = [P, P, P, P, P, P, P, P, P, P, I]
+        lib.esp_batch_lj.argtypes = [P, P, P, P, P, P, D, D, D, P, P]
+        lib.esp_batch_lj_f64.argtypes = [P, P, P, P, P, P, D, D, D, P, P]
+        lib.esp_batch_nve_step1_f64.argtypes = [P, P, P, P, P, D]
+        lib.esp_batch_nve_step2_f64.argtypes = [P, P, P, P, D]
         lib.esp_batch_autotune.argtypes = [P, P, P, P, P, P, P, I, I, ctypes.POINTER(EspParams), P, I]
         lib.esp_spread_noalloc.argtypes = [P, ctypes.POINTER(EspParams), D, D, D, P, P, I, P]
         for name in EXPORTS:

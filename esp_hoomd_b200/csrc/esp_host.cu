@@ -1289,6 +1289,40 @@ int esp_batch_nve_step1(esp_batch* b, void* stream, float* pos4, float* vel4, co
     return 0;
 }
 
+int esp_batch_lj(esp_batch* b, void* stream, const float* pos4, const unsigned* head, const unsigned* n_neigh,
+                 const unsigned* nlist, double epsilon, double sigma, double r_cut, float* force4, double* energy) {
+    if (!b || !pos4 || !head || !n_neigh || !nlist || !force4) return fail(ESP_ERR_INVALID, "null argument");
+    if (!(sigma > 0) || !(r_cut > 0)) return fail(ESP_ERR_INVALID, "sigma and r_cut must be positive");
+    ESPB_CK(launch_lj(b->d_chunks, b->n_chunks, b->d_sys, pos4, head, n_neigh, nlist, epsilon, sigma, r_cut, force4,
+                      energy, false, (cudaStream_t)stream));
+    return 0;
+}
+
+int esp_batch_lj_f64(esp_batch* b, void* stream, const double* pos4, const unsigned* head, const unsigned* n_neigh,
+                     const unsigned* nlist, double epsilon, double sigma, double r_cut, double* force4,
+                     double* energy) {
+    if (!b || !pos4 || !head || !n_neigh || !nlist || !force4) return fail(ESP_ERR_INVALID, "null argument");
+    if (!(sigma > 0) || !(r_cut > 0)) return fail(ESP_ERR_INVALID, "sigma and r_cut must be positive");
+    ESPB_CK(launch_lj(b->d_chunks, b->n_chunks, b->d_sys, pos4, head, n_neigh, nlist, epsilon, sigma, r_cut, force4,
+                      energy, true, (cudaStream_t)stream));
+    return 0;
+}
+
+int esp_batch_nve_step1_f64(esp_batch* b, void* stream, double* pos4, double* vel4, const double* force4, double dt) {
+    if (!b || !pos4 || !vel4 || !force4) return fail(ESP_ERR_INVALID, "null argument");
+    ESPB_CK(launch_nve64(1, b->d_chunks, b->n_chunks, b->d_sys, reinterpret_cast<double4*>(pos4),
+                         reinterpret_cast<double4*>(vel4), reinterpret_cast<const double4*>(force4), dt,
+                         (cudaStream_t)stream));
+    return 0;
+}
+
+int esp_batch_nve_step2_f64(esp_batch* b, void* stream, double* vel4, const double* force4, double dt) {
+    if (!b || !vel4 || !force4) return fail(ESP_ERR_INVALID, "null argument");
+    ESPB_CK(launch_nve64(2, b->d_chunks, b->n_chunks, b->d_sys, nullptr, reinterpret_cast<double4*>(vel4),
+                         reinterpret_cast<const double4*>(force4), dt, (cudaStream_t)stream));
+    return 0;
+}
+
 int esp_batch_nve_step2(esp_batch* b, void* stream, float* vel4, const float* force4, double dt) {
     if (!b || !vel4 || !force4) return fail(ESP_ERR_INVALID, "null argument");
     ESPB_CK(launch_nve2(b->d_chunks, b->n_chunks, b->d_sys, reinterpret_cast<float4*>(vel4),

@@ -161,6 +161,111 @@ __global__ void k_nve2(const int2* __restrict__ chunks, const SysDev* __restrict
     vel[i] = v;
 }
 
+// Lennard-Jones core repulsion of the MD harness (the C1 workload's
+// LJ eps, sigma, r_cut), over the same full neighbour list: adds forces and
+// half the pair energy per particle to force, the system total to energy[s].
+template <typename T4, typename T>
+__global__ void k_lj(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, const T4* __restrict__ pos,
+                     const uint32_t* __restrict__ head, const uint32_t* __restrict__ nn,
+                     const uint32_t* __restrict__ nl, T eps, T sig2, T rc2, T4* __restrict__ force,
+                     double* __restrict__ energy) {
+    __shared__ double red[32];
+    const int2 ch = chunks[blockIdx.x];
+    const SysDev S = sys[ch.x];
+    const int i = ch.y + threadIdx.x;
+    const T L[3] = {(T)S.Lxd, (T)S.Lyd, (T)S.Lzd};
+    double e1[1] = {0.0};
+    if (i < S.p_off + S.N) {
+        const T4 pi = pos[i];
+        T fx = 0, fy = 0, fz = 0, en = 0;
+        const uint32_t h = head[i], n = nn[i];
+        for (uint32_t k = 0; k < n; ++k) {
+            const T4 pj = pos[S.p_off + (int)nl[h + k]];
+            T d[3] = {pi.x - pj.x, pi.y - pj.y, pi.z - pj.z};
+            for (int a = 0; a < 3; ++a) d[a] -= L[a] * rint(d[a] / L[a]);
+            const T r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            if (r2 < rc2 && r2 > 0) {
+                const T s2 = sig2 / r2, s6 = s2 * s2 * s2;
+                const T fdr = (T)24 * eps * ((T)2 * s6 * s6 - s6) / r2;
+                en += (T)4 * eps * (s6 * s6 - s6);
+                fx += fdr * d[0];
+                fy += fdr * d[1];
+                fz += fdr * d[2];
+            }
+        }
+        T4 f = force[i];
+        f.x += fx;
+        f.y += fy;
+        f.z += fz;
+        f.w += (T)0.5 * en;
+        force[i] = f;
+        e1[0] = 0.5 * (double)en;
+    }
+    block_sum_f64<1>(e1, red);
+    if (threadIdx.x == 0 && energy) atomicAdd(&energy[ch.x], e1[0]);
+}
+
+__global__ void k64_nve1(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, double4* __restrict__ pos,
+                         double4* __restrict__ vel, const double4* __restrict__ force, double dt) {
+    const int2 ch = chunks[blockIdx.x];
+    const SysDev& S = sys[ch.x];
+    const int i = ch.y + threadIdx.x;
+    if (i >= S.p_off + S.N) return;
+    double4 v = vel[i];
+    const double4 f = force[i];
+    const double h = 0.5 * dt / v.w;
+    v.x += h * f.x;
+    v.y += h * f.y;
+    v.z += h * f.z;
+    double4 p = pos[i];
+    const double L[3] = {S.Lxd, S.Lyd, S.Lzd};
+    double x[3] = {p.x + dt * v.x, p.y + dt * v.y, p.z + dt * v.z};
+    for (int a = 0; a < 3; ++a) {
+        x[a] -= L[a] * floor(x[a] / L[a]);
+        if (x[a] >= L[a]) x[a] -= L[a];
+        if (x[a] < 0.0) x[a] += L[a];
+    }
+    pos[i] = make_double4(x[0], x[1], x[2], p.w);
+    vel[i] = v;
+}
+
+__global__ void k64_nve2(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, double4* __restrict__ vel,
+                         const double4* __restrict__ force, double dt) {
+    const int2 ch = chunks[blockIdx.x];
+    const SysDev& S = sys[ch.x];
+    const int i = ch.y + threadIdx.x;
+    if (i >= S.p_off + S.N) return;
+    double4 v = vel[i];
+    const double4 f = force[i];
+    const double h = 0.5 * dt / v.w;
+    v.x += h * f.x;
+    v.y += h * f.y;
+    v.z += h * f.z;
+    vel[i] = v;
+}
+
+cudaError_t launch_lj(const int2* chunks, int n_chunks, const SysDev* sys, const void* pos, const uint32_t* head,
+                      const uint32_t* nn, const uint32_t* nl, double eps, double sigma, double rcut, void* force,
+                      double* energy, bool f64, cudaStream_t st) {
+    if (n_chunks == 0) return cudaSuccess;
+    if (f64)
+        k_lj<double4, double><<<n_chunks, 256, 0, st>>>(chunks, sys, (const double4*)pos, head, nn, nl, eps,
+                                                        sigma * sigma, rcut * rcut, (double4*)force, energy);
+    else
+        k_lj<float4, float><<<n_chunks, 256, 0, st>>>(chunks, sys, (const float4*)pos, head, nn, nl, (float)eps,
+                                                      (float)(sigma * sigma), (float)(rcut * rcut), (float4*)force,
+                                                      energy);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_nve64(int half, const int2* chunks, int n_chunks, const SysDev* sys, double4* pos, double4* vel,
+                         const double4* force, double dt, cudaStream_t st) {
+    if (n_chunks == 0) return cudaSuccess;
+    if (half == 1) k64_nve1<<<n_chunks, 256, 0, st>>>(chunks, sys, pos, vel, force, dt);
+    else k64_nve2<<<n_chunks, 256, 0, st>>>(chunks, sys, vel, force, dt);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_nlist(const NlistArgs& a, cudaStream_t st) {
     if (a.n_chunks == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(a.overflow, 0, sizeof(int), st);

@@ -43,5 +43,10 @@ cudaError_t launch_nve1(const int2* chunks, int n_chunks, const SysDev* sys, flo
                         const float4* force, float dt, cudaStream_t st);
 cudaError_t launch_nve2(const int2* chunks, int n_chunks, const SysDev* sys, float4* vel, const float4* force,
                         float dt, cudaStream_t st);
+cudaError_t launch_lj(const int2* chunks, int n_chunks, const SysDev* sys, const void* pos, const uint32_t* head,
+                      const uint32_t* nn, const uint32_t* nl, double eps, double sigma, double rcut, void* force,
+                      double* energy, bool f64, cudaStream_t st);
+cudaError_t launch_nve64(int half, const int2* chunks, int n_chunks, const SysDev* sys, double4* pos, double4* vel,
+                         const double4* force, double dt, cudaStream_t st);
 
 }  // namespace espb

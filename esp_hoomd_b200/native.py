@@ -208,6 +208,29 @@ class Batch:
         return {"tile": chosen.tile, "threads_per_particle": chosen.threads_per_particle,
                 "fft_mode": chosen.fft_mode, "trial_ms": [float(t) for t in trials if t > 0]}
 
+    def compute_f64(self, pos4, q, force4, energy=None, virial=None, nlist=None, flags: int = _lib.ESP_ALL,
+                    stream=None) -> None:
+        """FP64 evaluation (float64 tensors; batch created with precision=1)."""
+        head, nn, nl = nlist if nlist is not None else (None, None, None)
+        check(self._lib.esp_batch_compute_f64(self._h, _stream(stream), _ptr(pos4), _ptr(q), _ptr(head), _ptr(nn),
+                                              _ptr(nl), _ptr(force4), _ptr(energy), _ptr(virial), int(flags)),
+              "esp_batch_compute_f64")
+
+    def lj(self, pos4, nlist, epsilon: float, sigma: float, r_cut: float, force4, energy=None, stream=None) -> None:
+        """Adds Lennard-Jones forces/energies (float32 or float64 tensors)."""
+        head, nn, nl = nlist
+        fn = self._lib.esp_batch_lj_f64 if pos4.dtype == torch.float64 else self._lib.esp_batch_lj
+        check(fn(self._h, _stream(stream), _ptr(pos4), _ptr(head), _ptr(nn), _ptr(nl), float(epsilon), float(sigma),
+                 float(r_cut), _ptr(force4), _ptr(energy)), "esp_batch_lj")
+
+    def nve_step1_f64(self, pos4, vel4, force4, dt: float, stream=None) -> None:
+        check(self._lib.esp_batch_nve_step1_f64(self._h, _stream(stream), _ptr(pos4), _ptr(vel4), _ptr(force4),
+                                                float(dt)), "esp_batch_nve_step1_f64")
+
+    def nve_step2_f64(self, vel4, force4, dt: float, stream=None) -> None:
+        check(self._lib.esp_batch_nve_step2_f64(self._h, _stream(stream), _ptr(vel4), _ptr(force4), float(dt)),
+              "esp_batch_nve_step2_f64")
+
     def set_timing(self, on: bool) -> None:
         check(self._lib.esp_batch_set_timing(self._h, int(bool(on))), "esp_batch_set_timing")
 

@@ -241,6 +241,21 @@ int esp_batch_build_nlist(esp_batch* b, void* stream, const float* pos4, double 
 int esp_batch_nve_step1(esp_batch* b, void* stream, float* pos4, float* vel4, const float* force4, double dt);
 int esp_batch_nve_step2(esp_batch* b, void* stream, float* vel4, const float* force4, double dt);
 
+/* FP64 velocity-Verlet halves (double4 positions, velocities with mass in
+ * w, forces), as esp_batch_nve_step1/2. */
+int esp_batch_nve_step1_f64(esp_batch* b, void* stream, double* pos4, double* vel4, const double* force4, double dt);
+int esp_batch_nve_step2_f64(esp_batch* b, void* stream, double* vel4, const double* force4, double dt);
+
+/* Lennard-Jones core repulsion of the harness, 4 eps ((sigma/r)^12 -
+ * (sigma/r)^6) for r < r_cut (no shift), over the full neighbour list:
+ * ADDS the forces and half the pair energy per particle to force4 and each
+ * system's LJ energy to energy[s] (device doubles, may be NULL). */
+int esp_batch_lj(esp_batch* b, void* stream, const float* pos4, const unsigned* head, const unsigned* n_neigh,
+                 const unsigned* nlist, double epsilon, double sigma, double r_cut, float* force4, double* energy);
+int esp_batch_lj_f64(esp_batch* b, void* stream, const double* pos4, const unsigned* head, const unsigned* n_neigh,
+                     const unsigned* nlist, double epsilon, double sigma, double r_cut, double* force4,
+                     double* energy);
+
 /* nsteps velocity-Verlet steps of every system of the batch: per step
  * step1, a full evaluation (ESP_ALL) at the new positions into force4 /
  * energy / virial, step2. force4 must hold the forces of the current

@@ -317,6 +317,31 @@ def remove_pairs(nlist, n_ex, ex_list, ex_pitch):
     return (np.array(nh, dtype=np.uint32), np.array(nc, dtype=np.uint32), np.array(nl, dtype=np.uint32))
 
 
+def lj_forces(pos, box, nlist, eps, sigma, rcut):
+    """Lennard-Jones 4 eps ((sigma/r)^12 - (sigma/r)^6), r < rcut, unshifted,
+    over a full CSR neighbour list (the MD harness's core repulsion).
+    Returns (F[N,3], e[N]) with half the pair energy per particle."""
+    pos = np.asarray(pos, dtype=np.float64)
+    L = np.asarray(box, dtype=np.float64)
+    head, cnt, lst = nlist
+    N = pos.shape[0]
+    cnt = np.asarray(cnt, dtype=np.int64)
+    i_idx = np.repeat(np.arange(N), cnt)
+    offs = np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+    j_idx = np.asarray(lst, dtype=np.int64)[np.repeat(np.asarray(head, dtype=np.int64), cnt) + offs]
+    d = pos[i_idx] - pos[j_idx]
+    d -= L * np.round(d / L)
+    r2 = np.sum(d * d, -1)
+    m = (r2 < rcut * rcut) & (r2 > 0)
+    s6 = np.where(m, (sigma * sigma / np.where(m, r2, 1.0)) ** 3, 0.0)
+    fdr = np.where(m, 24.0 * eps * (2.0 * s6 * s6 - s6) / np.where(m, r2, 1.0), 0.0)
+    F = np.zeros((N, 3))
+    np.add.at(F, i_idx, fdr[:, None] * d)
+    en = np.zeros(N)
+    np.add.at(en, i_idx, 0.5 * 4.0 * eps * (s6 * s6 - s6))
+    return F, en
+
+
 def neighbor_list(pos, box, rlist):
     """Full CSR neighbour list of all pairs with r < rlist (minimum image).
     Rows are sorted by neighbour index. Returns (head, count, list)."""
