@@ -288,6 +288,81 @@ def run_serving(args, pool):
     return out, stats
 
 
+# ----------------------------------------------------------------------------- scale-up
+def run_scaleup(args):
+    """The plain one-system path at the scale-up size: 10^6 rock-salt ions
+    (100^3 lattice, L = 100, mesh 200^3, support 8, r_c 3.0, 1e-5 target).
+    A step = neighbour list + one evaluation + 10 NVE steps (CUDA graph), as
+    in the batched workload. Reports every stage's live CUDA-event time and
+    its fraction of the measured HBM peak for its algorithmic bytes."""
+    import torch
+    from esp_hoomd_b200 import native, systems
+    from esp_hoomd_b200._lib import ESP_ALL
+    dev = torch.device("cuda", 0)
+    s = systems.rocksalt(100, seed=1001)
+    N = s.N
+    b = native.Batch(native.make_params(order=8, rcut=RCUT, target_error=1e-5), [N], [s.box])
+    p4 = np.zeros((N, 4), np.float32)
+    p4[:, :3] = s.pos
+    v4 = np.zeros((N, 4), np.float32)
+    v4[:, :3] = s.vel
+    v4[:, 3] = 1.0
+    pos = torch.tensor(p4, device=dev)
+    vel = torch.tensor(v4, device=dev)
+    q = torch.tensor(s.q.astype(np.float32), device=dev)
+    head = torch.zeros(N, dtype=torch.int32, device=dev)
+    nn = torch.zeros_like(head)
+    nl = torch.zeros(N * CAP, dtype=torch.int32, device=dev)
+    force = torch.zeros((N, 4), device=dev)
+    energy = torch.zeros(1, dtype=torch.float64, device=dev)
+    virial = torch.zeros(6, dtype=torch.float64, device=dev)
+
+    def request(use_graph=True):
+        b.build_nlist(pos, RCUT + SKIN, CAP, head, nn, nl)
+        b.compute(pos, q, force, energy, virial, nlist=(head, nn, nl), flags=ESP_ALL)
+        b.md_run(pos, vel, q, force, energy, None, (head, nn, nl), MD_STEPS, DT, use_graph=use_graph)
+
+    for _ in range(max(3, args.warmup)):
+        request()
+    torch.cuda.synchronize()
+    st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(0) as clk:
+        st.record()
+        for _ in range(args.steps):
+            request()
+        en.record()
+        torch.cuda.synchronize()
+    ms = st.elapsed_time(en) / args.steps
+    b.set_timing(True)
+    for _ in range(2):
+        request(use_graph=False)
+    stt = b.stage_times()
+    b.set_timing(False)
+    inf = b.info(0)
+    M = inf["nx"] * inf["ny"] * inf["nz"]
+    mean_nn = float(nn.double().mean().item())
+    alg = {"pair": 4.0 * N * mean_nn + 32.0 * N, "spread": 20.0 * N + 4.0 * M, "interp": 36.0 * N + 4.0 * M,
+           "fft": 5 * 2 * 8.0 * M / 2, "sort": 40.0 * N, "bin": 40.0 * N, "nlist": 16.0 * N + 4.0 * N * mean_nn,
+           "nve": 48.0 * N}
+    peak, peak_kind = _peak_gbs()
+    stages = {}
+    for k, (tot_ms, cnt) in stt.items():
+        if cnt == 0:
+            continue
+        t = tot_ms / cnt
+        gbs = alg[k] / (t * 1e-3) / 1e9
+        stages[k] = {"ms_per_launch": t, "algorithmic_bytes": alg[k], "achieved_gbs": gbs, "frac_hbm": gbs / peak}
+    line = {"metric": "particle-steps/s (plain path, one 10^6-particle system)", "value": N * MD_STEPS / (ms * 1e-3),
+            "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "scaleup: rock-salt 100^3 (N = 1,000,000), L = 100, seed 1001, "
+                                   "1 nlist + 1 eval + 10 NVE steps per step",
+                       "mesh": [inf["nx"], inf["ny"], inf["nz"]], "order": 8, "rcut": RCUT,
+                       "mean_neighbours": mean_nn},
+            "peak_gbs": peak, "peak_kind": peak_kind, "stages": stages, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 # ----------------------------------------------------------------------------- GPU arm
 def run_ours(args):
     import torch
@@ -506,6 +581,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--systems", type=int, default=N_SYS,
                     help="evaluate only the first S systems of the batch (small cases for profiling)")
+    ap.add_argument("--workload", default="batched256", choices=["batched256", "scaleup"],
+                    help="scaleup: the plain path on one 10^6-particle system (a second measurement)")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default plan)")
     ap.add_argument("--serve-requests", type=int, default=1000, help="requests per arrival rate")
@@ -514,6 +591,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "scaleup":
+        run_scaleup(args)
     else:
         run_ours(args)
 
