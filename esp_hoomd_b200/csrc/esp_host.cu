@@ -244,6 +244,11 @@ struct esp_batch {
     uint32_t *d_ckey = nullptr, *d_ccount = nullptr, *d_cstart = nullptr, *d_cperm = nullptr, *d_slot_cell = nullptr;
     float4 *d_wpos = nullptr, *d_cpos = nullptr;
     int* d_overflow = nullptr;
+    // second stream for the concurrent pair term, its force array and the
+    // fork/join events (created at plan time, kept across re-plans)
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    float4* d_fsr = nullptr;
     // FP64 mode: tables, records, spectrum and work lists
     bool f64 = false;
     DevAlloc mem64;
@@ -273,6 +278,12 @@ struct esp_batch {
     cudaGraphExec_t graph_exec = nullptr;
     ~esp_batch() {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (st2) {
+            cudaStreamSynchronize(st2);
+            cudaStreamDestroy(st2);
+        }
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
     }
 
     LaunchArgs args() const;
@@ -495,8 +506,13 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         (rc = mem.get(d_x, xi.size())) || (rc = mem.get(d_y, yi.size())) || (rc = mem.get(d_z, zi.size())) ||
         (rc = mem.get(d_p, pi.size())) || (rc = mem.get(d_s, si.size())) ||
         (rc = mem.get(d_acc, (size_t)ns * ACC_STRIDE)) || (rc = mem.get(d_energy, ns)) ||
-        (rc = mem.get(d_virial, (size_t)ns * 6)))
+        (rc = mem.get(d_virial, (size_t)ns * 6)) || (rc = mem.get(d_fsr, totN)))
         return rc;
+    if (!st2) {
+        ESPB_CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+        ESPB_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        ESPB_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    }
     ESPB_CK(cudaMemcpy(d_sys, sd.data(), ns * sizeof(SysDev), cudaMemcpyHostToDevice));
     ESPB_CK(cudaMemcpy(d_pset, psd.data(), psd.size() * sizeof(ParamSet), cudaMemcpyHostToDevice));
     ESPB_CK(cudaMemcpy(d_chunks, chunks.data(), chunks.size() * sizeof(int2), cudaMemcpyHostToDevice));
@@ -740,6 +756,21 @@ int esp_batch::compute(cudaStream_t st, const float* pos4, const float* q, const
     timer.begin(ESP_STAGE_BIN, st);
     ESPB_CK(launch_bin(a, st));
     timer.end(st);
+    // The pair term needs only the wrapped positions of the bin stage: with
+    // both terms requested it runs on a second stream, into its own force
+    // array, concurrently with spread -> FFT -> interpolation (whose kernels
+    // leave issue slots idle), and is added before the totals. Stage timing
+    // keeps the sequential order so that per-stage times stay separable.
+    const bool fork = lr && sr && !timer.on && d_fsr;
+    if (fork) {
+        ESPB_CK(cudaEventRecord(ev_fork, st));
+        ESPB_CK(cudaStreamWaitEvent(st2, ev_fork, 0));
+        LaunchArgs ap = a;
+        ap.force = d_fsr;
+        ap.accumulate = 0;
+        ESPB_CK(launch_pair(ap, st2));
+        ESPB_CK(cudaEventRecord(ev_join, st2));
+    }
     if (lr) {
         timer.begin(ESP_STAGE_SORT, st);
         ESPB_CK(launch_sort(a, st));
@@ -763,7 +794,10 @@ int esp_batch::compute(cudaStream_t st, const float* pos4, const float* q, const
         // bin counted particles per tile; clear the histogram for the next call
         ESPB_CK(cudaMemsetAsync(d_tcount, 0, (size_t)n_tiles * sizeof(uint32_t), st));
     }
-    if (sr) {
+    if (fork) {
+        ESPB_CK(cudaStreamWaitEvent(st, ev_join, 0));
+        ESPB_CK(launch_add_forces(a.chunks, a.n_chunks, a.sys, d_fsr, a.force, st));
+    } else if (sr) {
         timer.begin(ESP_STAGE_PAIR, st);
         ESPB_CK(launch_pair(a, st));
         timer.end(st);

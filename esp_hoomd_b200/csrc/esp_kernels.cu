@@ -1684,6 +1684,27 @@ __global__ void k_exclusions(const int2* __restrict__ chunks, const SysDev* __re
     }
 }
 
+// force += add (the concurrently computed pair forces and energies).
+__global__ void k_add_forces(const int2* __restrict__ chunks, const SysDev* __restrict__ sys,
+                             const float4* __restrict__ add, float4* __restrict__ force) {
+    const int2 ch = chunks[blockIdx.x];
+    const int i = ch.y + threadIdx.x;
+    if (i >= sys[ch.x].p_off + sys[ch.x].N) return;
+    const float4 b = add[i];
+    float4 f = force[i];
+    f.x += b.x;
+    f.y += b.y;
+    f.z += b.z;
+    f.w += b.w;
+    force[i] = f;
+}
+
+cudaError_t launch_add_forces(const int2* chunks, int n_chunks, const SysDev* sys, const float4* add, float4* force,
+                              cudaStream_t st) {
+    if (n_chunks) k_add_forces<<<n_chunks, 256, 0, st>>>(chunks, sys, add, force);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_exclusions(const LaunchArgs& a, cudaStream_t st) {
     if (a.n_chunks == 0 || !a.ex_n) return cudaSuccess;
     k_exclusions<<<a.n_chunks, 256, 0, st>>>(a.chunks, a.sys, a.psets, a.posq, a.ex_n, a.ex_list, a.ex_pitch,

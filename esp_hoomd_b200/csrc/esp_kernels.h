@@ -96,6 +96,8 @@ cudaError_t launch_fft(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_interp(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_pair(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_exclusions(const LaunchArgs& a, cudaStream_t st);
+cudaError_t launch_add_forces(const int2* chunks, int n_chunks, const SysDev* sys, const float4* add, float4* force,
+                              cudaStream_t st);
 
 // FP64 mode (esp_f64.cu): the shared fields of `a` (descriptors, chunks,
 // tiles, keys, permutation, charge mesh, accumulators, neighbour list,
