@@ -1577,7 +1577,9 @@ static cudaError_t launch_pair_t(const LaunchArgs& a, cudaStream_t st) {
                                                       a.nl_list, a.force, a.acc, a.accumulate, a.pc)
     if (a.nq <= 8) ESPB_PAIR(8);
     else if (a.nq <= 10) ESPB_PAIR(10);
+    else if (a.nq <= 11) ESPB_PAIR(11);
     else if (a.nq <= 12) ESPB_PAIR(12);
+    else if (a.nq <= 13) ESPB_PAIR(13);
     else if (a.nq <= 14) ESPB_PAIR(14);
     else if (a.nq <= 16) ESPB_PAIR(16);
     else if (a.nq <= 20) ESPB_PAIR(20);

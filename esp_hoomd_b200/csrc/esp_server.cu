@@ -406,7 +406,7 @@ int esp_server::admit(Request* q, Staging& sg) {
         if ((int)pset_rcut.size() >= MAX_PSETS) return fail(ESP_ERR_UNSUPPORTED, "more than 16 distinct cutoffs");
         PsetHost h;
         ParamSet d;
-        int rc = build_param_set(c_split, c_win, P, D, r.rcut, h, d);
+        int rc = build_param_set(c_split, c_win, P, D, r.rcut, h, d, 3e-8);
         if (rc) return rc;
         ps = (int)pset_rcut.size();
         pset_rcut.push_back(r.rcut);
