@@ -121,11 +121,14 @@ __device__ __forceinline__ float horner_dw(const float* c, int D, float t) {
     return v;
 }
 
-// Default window degree for support P (what the planner picks when the
-// degree is not set): the staging kernels unroll this case fully.
+// Default window degree of the FP32 path for support P (what the planner
+// picks when the degree is not set; the staging kernels unroll this case
+// fully): P for P >= 8 (fit error 4.7e-9 at P = 8, below the FP32
+// evaluation's rounding), 9 below that. The FP64 mode uses max(P + 2, 9).
+__host__ __device__ constexpr int default_window_degree(int P) { return P >= 8 ? P : 9; }
 template <int P>
 constexpr int default_window_degree() {
-    return P + 2 > 9 ? P + 2 : 9;
+    return default_window_degree(P);
 }
 
 // One window segment held in registers by the thread that evaluates it

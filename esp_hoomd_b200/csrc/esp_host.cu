@@ -351,7 +351,8 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         }
         totN += N[s];
     }
-    D = p.window_degree > 0 ? p.window_degree : std::max(P + 2, 9);
+    D = p.window_degree > 0 ? p.window_degree
+                            : (p.precision == ESP_FP64 ? std::max(P + 2, 9) : default_window_degree(P));
     if (D > MAX_D) return fail(ESP_ERR_UNSUPPORTED, "window degree must be <= 15");
     // parameter sets
     std::map<std::tuple<double, double>, int> pmap;
@@ -1510,7 +1511,7 @@ extern "C" int esp_spread_noalloc(void* stream, const esp_params* p, double Lx, 
         return fail(ESP_ERR_UNSUPPORTED, "esp_spread_noalloc: " + std::to_string(n_tiles) +
                                              " tiles exceed its fixed scratch limit of " +
                                              std::to_string(NA_MAX_TILES));
-    const int D = p->window_degree > 0 ? p->window_degree : std::max(P + 2, 9);
+    const int D = p->window_degree > 0 ? p->window_degree : default_window_degree(P);
     if (D > MAX_D) return fail(ESP_ERR_UNSUPPORTED, "window degree must be <= 15");
     if (p->window_c < 0) return fail(ESP_ERR_INVALID, "window_c must be >= 0");
     const double cw = p->window_c > 0 ? p->window_c : 2.2 * P;

@@ -246,7 +246,7 @@ int esp_server::init(const esp_server_config& cfg) {
         return fail(ESP_ERR_UNSUPPORTED, "threads_per_particle must be 4, 8, 16 or 32");
     T = prm.tile > 0 ? prm.tile : std::max(1, 17 - P);
     if (T > 64) return fail(ESP_ERR_UNSUPPORTED, "tile edge must be <= 64");
-    D = prm.window_degree > 0 ? prm.window_degree : std::max(P + 2, 9);
+    D = prm.window_degree > 0 ? prm.window_degree : default_window_degree(P);
     if (D > MAX_D) return fail(ESP_ERR_UNSUPPORTED, "window degree must be <= 15");
     kreq = kappa_required(prm.target_error > 0 ? prm.target_error : 1e-5);
     // the split bandwidth of a system meshed at exactly h = pi r_c / kappa_N;
