@@ -274,10 +274,27 @@ struct esp_batch {
             return pos == o.pos && vel == o.vel && q == o.q && head == o.head && nn == o.nn && nl == o.nl &&
                    force == o.force && energy == o.energy && virial == o.virial && dt == o.dt;
         }
-    } graph_key{};
-    cudaGraphExec_t graph_exec = nullptr;
+    };
+    // captured MD steps, one per distinct set of caller pointers; a few
+    // entries so that a caller alternating between buffer sets (uploads of
+    // the next batch overlapping this one) does not recapture every call.
+    // The least recently used entry is replaced.
+    static constexpr int N_GRAPHS = 4;
+    struct GraphEntry {
+        GraphKey key{};
+        cudaGraphExec_t exec = nullptr;
+        unsigned long long used = 0;
+    } graphs[N_GRAPHS];
+    unsigned long long graph_tick = 0;
+    void drop_graphs() {
+        for (GraphEntry& g : graphs)
+            if (g.exec) {
+                cudaGraphExecDestroy(g.exec);
+                g.exec = nullptr;
+            }
+    }
     ~esp_batch() {
-        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        drop_graphs();
         if (st2) {
             cudaStreamSynchronize(st2);
             cudaStreamDestroy(st2);
@@ -529,10 +546,7 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
     if (!si.empty()) ESPB_CK(cudaMemcpy(d_s, si.data(), si.size() * sizeof(int2), cudaMemcpyHostToDevice));
     ESPB_CK(cudaMemset(d_tcount, 0, n_tiles * sizeof(uint32_t)));
     ESPB_CK(cudaMemset(d_rho, 0, (size_t)std::max<long long>(m_off, 1) * sizeof(double)));
-    if (graph_exec) {
-        cudaGraphExecDestroy(graph_exec);
-        graph_exec = nullptr;
-    }
+    drop_graphs();
     {
         // kernel attributes are set here, outside any stream capture
         LaunchArgs a = args();
@@ -835,10 +849,19 @@ int esp_batch::md_run(cudaStream_t st, float* pos4, float* vel4, const float* q,
         return 0;
     }
     const GraphKey key{pos4, vel4, q, head, nn, nl, force4, energy, virial, dt};
-    if (!graph_exec || !(key == graph_key)) {
-        if (graph_exec) {
-            cudaGraphExecDestroy(graph_exec);
-            graph_exec = nullptr;
+    GraphEntry* ge = nullptr;
+    for (GraphEntry& g : graphs)
+        if (g.exec && g.key == key) ge = &g;
+    if (!ge) {
+        ge = &graphs[0];
+        for (GraphEntry& g : graphs)
+            if (!g.exec || g.used < ge->used) {
+                ge = &g;
+                if (!g.exec) break;
+            }
+        if (ge->exec) {
+            cudaGraphExecDestroy(ge->exec);
+            ge->exec = nullptr;
         }
         cudaStream_t cs = nullptr;
         ESPB_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
@@ -858,12 +881,16 @@ int esp_batch::md_run(cudaStream_t st, float* pos4, float* vel4, const float* q,
             if (g) cudaGraphDestroy(g);
             return rc;
         }
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&graph_exec, g, 0);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&ge->exec, g, 0);
         if (g) cudaGraphDestroy(g);
-        if (e != cudaSuccess) return fail(ESP_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-        graph_key = key;
+        if (e != cudaSuccess) {
+            ge->exec = nullptr;
+            return fail(ESP_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        }
+        ge->key = key;
     }
-    for (int k = 0; k < nsteps; ++k) ESPB_CK(cudaGraphLaunch(graph_exec, st));
+    ge->used = ++graph_tick;
+    for (int k = 0; k < nsteps; ++k) ESPB_CK(cudaGraphLaunch(ge->exec, st));
     return 0;
 }
 
@@ -1262,10 +1289,7 @@ int esp_batch_set_exclusions(esp_batch* b, const unsigned* n_ex, const unsigned*
     b->ex_n = n_ex;
     b->ex_list = n_ex ? ex_list : nullptr;
     b->ex_pitch = n_ex ? ex_pitch : 0;
-    if (b->graph_exec) {  // captured steps hold the previous pointers
-        cudaGraphExecDestroy(b->graph_exec);
-        b->graph_exec = nullptr;
-    }
+    b->drop_graphs();  // captured steps hold the previous pointers
     return 0;
 }
 

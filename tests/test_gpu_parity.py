@@ -308,3 +308,44 @@ def test_autotune_keeps_results():
     torch.cuda.synchronize()
     assert R.rel_rms(f1.cpu().numpy()[:, :3].astype(np.float64), f0.cpu().numpy()[:, :3].astype(np.float64)) <= 5e-6
     assert np.allclose(e1.cpu().numpy(), e0.cpu().numpy(), rtol=2e-6, atol=0)
+
+
+def test_md_graphs_follow_buffer_sets():
+    """Captured MD steps are cached per set of caller pointers: alternating
+    between two buffer sets replays the graph of each set, and the result
+    matches the same steps run without a graph."""
+    sys_list = [systems.rocksalt(n, seed=900 + n) for n in (8, 10)]
+    N = [s.N for s in sys_list]
+    b = native.Batch(native.make_params(), N, [s.box for s in sys_list])
+    tot = sum(N)
+    p4 = np.zeros((tot, 4), np.float32)
+    p4[:, :3] = np.concatenate([s.pos for s in sys_list])
+    v4 = np.zeros((tot, 4), np.float32)
+    v4[:, :3] = np.concatenate([s.vel for s in sys_list])
+    v4[:, 3] = 1.0
+    q = torch.tensor(np.concatenate([s.q for s in sys_list]).astype(np.float32), device="cuda")
+    head = torch.zeros(tot, dtype=torch.int32, device="cuda")
+    nn = torch.zeros_like(head)
+    nl = torch.zeros(tot * 256, dtype=torch.int32, device="cuda")
+
+    def fresh():
+        return (torch.tensor(p4, device="cuda"), torch.tensor(v4, device="cuda"),
+                torch.zeros((tot, 4), device="cuda"), torch.zeros(len(N), dtype=torch.float64, device="cuda"))
+
+    def run(bufs, use_graph):
+        p, v, f, e = bufs
+        b.build_nlist(p, 3.4, 256, head, nn, nl)
+        b.compute(p, q, f, e, None, nlist=(head, nn, nl), flags=ESP_ALL)
+        b.md_run(p, v, q, f, e, None, (head, nn, nl), 5, 0.002, use_graph=use_graph)
+
+    ref, a, c = fresh(), fresh(), fresh()
+    for _ in range(3):
+        run(ref, False)
+    for _ in range(3):  # A, C, A, C, A, C: two cached graphs, each replayed
+        run(a, True)
+        run(c, True)
+    torch.cuda.synchronize()
+    for got in (a, c):
+        for x, y in zip(got, ref):
+            xa, ya = x.double().cpu().numpy(), y.double().cpu().numpy()
+            assert np.abs(xa - ya).max() <= 1e-5 * max(np.abs(ya).max(), 1.0)
