@@ -241,7 +241,7 @@ struct esp_batch {
     int n_cells = 0;
     CellDev* d_cells = nullptr;
     int* d_cell_sys = nullptr;
-    uint32_t *d_ckey = nullptr, *d_ccount = nullptr, *d_cstart = nullptr, *d_cperm = nullptr, *d_slot_cell = nullptr;
+    uint32_t *d_ckey = nullptr, *d_ccount = nullptr, *d_cstart = nullptr, *d_cperm = nullptr;
     float4 *d_wpos = nullptr, *d_cpos = nullptr;
     int* d_overflow = nullptr;
     // second stream for the concurrent pair term, its force array and the
@@ -944,7 +944,7 @@ int esp_batch::build_nlist(cudaStream_t st, const float* pos4, double rlist, int
         if ((rc = nlmem.get(d_cells, nsys)) || (rc = nlmem.get(d_cell_sys, n_cells)) ||
             (rc = nlmem.get(d_ckey, totN)) || (rc = nlmem.get(d_ccount, n_cells)) ||
             (rc = nlmem.get(d_cstart, n_cells + 1)) || (rc = nlmem.get(d_cperm, totN)) ||
-            (rc = nlmem.get(d_slot_cell, totN)) || (rc = nlmem.get(d_wpos, totN)) || (rc = nlmem.get(d_cpos, totN)) ||
+            (rc = nlmem.get(d_wpos, totN)) || (rc = nlmem.get(d_cpos, totN)) ||
             (rc = nlmem.get(d_overflow, 1)))
             return rc;
         ESPB_CK(cudaMemcpy(d_cells, cells.data(), nsys * sizeof(CellDev), cudaMemcpyHostToDevice));
@@ -967,7 +967,6 @@ int esp_batch::build_nlist(cudaStream_t st, const float* pos4, double rlist, int
     a.perm_u = d_cperm;
     a.wpos = d_wpos;
     a.cpos = d_cpos;
-    a.slot_cell = d_slot_cell;
     a.rlist2 = (float)(rlist * rlist);
     a.cap = cap;
     a.head = head;

@@ -56,68 +56,139 @@ __global__ void k_cell_sort(const uint32_t* __restrict__ start, const uint32_t* 
     }
 }
 
-// One thread per particle, visited in cell order; scans the 27 surrounding
-// cells in a fixed order, so every row is deterministic.
-__global__ void k_nlist(const int* __restrict__ cell_sys, int n_cells_total, const SysDev* __restrict__ sys,
-                        const CellDev* __restrict__ cells, const uint32_t* __restrict__ cstart,
-                        const float4* __restrict__ cpos, float rlist2, int cap, uint32_t* __restrict__ head,
-                        uint32_t* __restrict__ nn, uint32_t* __restrict__ nl, int* __restrict__ overflow,
-                        const uint32_t* __restrict__ slot_cell, int total) {
-    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= total) return;
-    const uint32_t cidx = slot_cell[slot];
+// One CTA per cell, one thread per particle of the cell (passes of
+// NL_THREADS). The particles of the 27 surrounding cells are staged in
+// shared memory, in the fixed (dz, dy, dx) order and ascending slot inside
+// each cell, so every row is deterministic; each thread scans them with
+// broadcast shared loads. With at least 3 cells on every axis each
+// surrounding cell is a distinct periodic image and its particles are
+// staged already shifted by that image, so the test needs no wrap; smaller
+// cell grids take the minimum-image test.
+constexpr int NL_THREADS = 64;
+constexpr int NL_STAGE = 1024;
+
+template <bool MINIMG>
+__device__ __forceinline__ uint32_t nl_scan(const float4* __restrict__ cand, int n, float4 pi, int i, const SysDev& S,
+                                            float rlist2, uint32_t cap, uint32_t* __restrict__ row, uint32_t cnt,
+                                            bool active) {
+#pragma unroll 4
+    for (int k = 0; k < n; ++k) {
+        const float4 pj = cand[k];
+        float ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
+        if (MINIMG) {
+            ddx -= S.Lx * rintf(ddx * S.inv_Lx);
+            ddy -= S.Ly * rintf(ddy * S.inv_Ly);
+            ddz -= S.Lz * rintf(ddz * S.inv_Lz);
+        }
+        const int j = __float_as_int(pj.w);
+        if (active && ddx * ddx + ddy * ddy + ddz * ddz < rlist2 && j != i) {
+            if (cnt < cap) row[cnt] = (uint32_t)(j - S.p_off);
+            ++cnt;
+        }
+    }
+    return cnt;
+}
+
+__global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ cell_sys, const SysDev* __restrict__ sys,
+                                                      const CellDev* __restrict__ cells,
+                                                      const uint32_t* __restrict__ cstart,
+                                                      const float4* __restrict__ cpos, float rlist2, int cap,
+                                                      uint32_t* __restrict__ head, uint32_t* __restrict__ nn,
+                                                      uint32_t* __restrict__ nl, int* __restrict__ overflow) {
+    __shared__ float4 cand[NL_STAGE];
+    __shared__ uint32_t seg_src[27];   // first slot of each surrounding cell
+    __shared__ uint32_t seg_off[28];   // exclusive prefix of their counts
+    __shared__ float seg_shift[27][3];
+    const uint32_t cidx = blockIdx.x;
+    const uint32_t c0 = cstart[cidx], c1 = cstart[cidx + 1];
+    if (c0 == c1) return;
     const int si = cell_sys[cidx];
     const SysDev& S = sys[si];
     const CellDev& C = cells[si];
-    const float4 pi = cpos[slot];
-    const int i = __float_as_int(pi.w);
     const int lc = (int)cidx - C.c_off;
     const int cx = lc % C.ncx, cy = (lc / C.ncx) % C.ncy, cz = lc / (C.ncx * C.ncy);
-    const long long hrow = (long long)C.nl_off + (long long)(i - S.p_off) * cap;
-    uint32_t cnt = 0;
-    // with fewer than 3 cells on an axis the -1/+1 neighbours coincide:
-    // visit each distinct cell once (offsets {0,1} for 2 cells, {0} for 1)
-    const int z0 = C.ncz >= 3 ? -1 : 0, z1 = C.ncz >= 3 ? 1 : C.ncz - 1;
-    const int y0 = C.ncy >= 3 ? -1 : 0, y1 = C.ncy >= 3 ? 1 : C.ncy - 1;
-    const int x0 = C.ncx >= 3 ? -1 : 0, x1 = C.ncx >= 3 ? 1 : C.ncx - 1;
-    for (int dz = z0; dz <= z1; ++dz) {
-        const int zz = (cz + dz + C.ncz) % C.ncz;
-        for (int dy = y0; dy <= y1; ++dy) {
-            const int yy = (cy + dy + C.ncy) % C.ncy;
-            for (int dx = x0; dx <= x1; ++dx) {
-                const int xx = (cx + dx + C.ncx) % C.ncx;
+    const bool minimg = C.ncx < 3 || C.ncy < 3 || C.ncz < 3;
+    const int tid = threadIdx.x;
+    if (tid < 32) {
+        // surrounding cell t = (iz * 3 + iy) * 3 + ix; with fewer than 3
+        // cells on an axis the -1/+1 neighbours coincide, so only the
+        // distinct ones ({0, 1} for 2 cells, {0} for 1) are visited
+        uint32_t n = 0;
+        if (tid < 27) {
+            const int ix = tid % 3, iy = (tid / 3) % 3, iz = tid / 9;
+            const int dx = (C.ncx >= 3 ? -1 : 0) + ix, dy = (C.ncy >= 3 ? -1 : 0) + iy,
+                      dz = (C.ncz >= 3 ? -1 : 0) + iz;
+            const bool ok = dx <= (C.ncx >= 3 ? 1 : C.ncx - 1) && dy <= (C.ncy >= 3 ? 1 : C.ncy - 1) &&
+                            dz <= (C.ncz >= 3 ? 1 : C.ncz - 1);
+            int xx = cx + dx, yy = cy + dy, zz = cz + dz;
+            float sx = 0.f, sy = 0.f, sz = 0.f;
+            if (xx < 0) { xx += C.ncx; sx = -S.Lx; } else if (xx >= C.ncx) { xx -= C.ncx; sx = S.Lx; }
+            if (yy < 0) { yy += C.ncy; sy = -S.Ly; } else if (yy >= C.ncy) { yy -= C.ncy; sy = S.Ly; }
+            if (zz < 0) { zz += C.ncz; sz = -S.Lz; } else if (zz >= C.ncz) { zz -= C.ncz; sz = S.Lz; }
+            uint32_t b = 0;
+            if (ok) {
                 const uint32_t c = (uint32_t)(C.c_off + (zz * C.ncy + yy) * C.ncx + xx);
-                const uint32_t b = cstart[c], e = cstart[c + 1];
-                // the next candidate is loaded before the current one is
-                // tested, so each load's latency overlaps one test
-                float4 nxt = b < e ? cpos[b] : make_float4(0.f, 0.f, 0.f, 0.f);
-                for (uint32_t s = b; s < e; ++s) {
-                    const float4 pj = nxt;
-                    if (s + 1 < e) nxt = cpos[s + 1];
-                    const int j = __float_as_int(pj.w);
-                    if (j == i) continue;
-                    float ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
-                    ddx -= S.Lx * rintf(ddx * S.inv_Lx);
-                    ddy -= S.Ly * rintf(ddy * S.inv_Ly);
-                    ddz -= S.Lz * rintf(ddz * S.inv_Lz);
-                    if (ddx * ddx + ddy * ddy + ddz * ddz < rlist2) {
-                        if (cnt < (uint32_t)cap) nl[hrow + cnt] = (uint32_t)(j - S.p_off);
-                        ++cnt;
-                    }
-                }
+                b = cstart[c];
+                n = cstart[c + 1] - b;
+            }
+            seg_src[tid] = b;
+            seg_shift[tid][0] = minimg ? 0.f : sx;
+            seg_shift[tid][1] = minimg ? 0.f : sy;
+            seg_shift[tid][2] = minimg ? 0.f : sz;
+        }
+        uint32_t inc = n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (tid >= o) inc += v;
+        }
+        if (tid < 27) seg_off[tid] = inc - n;
+        if (tid == 26) seg_off[27] = inc;
+    }
+    __syncthreads();
+    const uint32_t total = seg_off[27];
+    auto stage = [&](uint32_t base) {
+        const uint32_t top = min(total, base + (uint32_t)NL_STAGE);
+        for (int s = 0; s < 27; ++s) {
+            const uint32_t lo = max(seg_off[s], base), hi = min(seg_off[s + 1], top);
+            for (uint32_t g = lo + tid; g < hi; g += NL_THREADS) {
+                float4 p = cpos[seg_src[s] + (g - seg_off[s])];
+                p.x += seg_shift[s][0];
+                p.y += seg_shift[s][1];
+                p.z += seg_shift[s][2];
+                cand[g - base] = p;
             }
         }
+    };
+    const bool one_stage = total <= (uint32_t)NL_STAGE;
+    if (one_stage) {
+        stage(0);
+        __syncthreads();
     }
-    head[i] = (uint32_t)hrow;
-    nn[i] = cnt;
-    if (cnt > (uint32_t)cap) atomicOr(overflow, 1);
-}
-
-__global__ void k_fill_slot_cell(const uint32_t* __restrict__ cstart, int n_cells, uint32_t* __restrict__ slot_cell) {
-    const int c = blockIdx.x;
-    if (c >= n_cells) return;
-    const uint32_t b = cstart[c], e = cstart[c + 1];
-    for (uint32_t s = b + threadIdx.x; s < e; s += blockDim.x) slot_cell[s] = (uint32_t)c;
+    for (uint32_t p0 = c0; p0 < c1; p0 += NL_THREADS) {
+        const uint32_t slot = p0 + tid;
+        const bool active = slot < c1;
+        const float4 pi = active ? cpos[slot] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+        const int i = __float_as_int(pi.w);
+        const long long hrow = (long long)C.nl_off + (long long)(i - S.p_off) * cap;
+        uint32_t* row = nl + (active ? hrow : 0);
+        uint32_t cnt = 0;
+        for (uint32_t base = 0; base < total; base += NL_STAGE) {
+            if (!one_stage) {
+                __syncthreads();
+                stage(base);
+                __syncthreads();
+            }
+            const int n = (int)min((uint32_t)NL_STAGE, total - base);
+            cnt = minimg ? nl_scan<true>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row, cnt, active)
+                         : nl_scan<false>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row, cnt, active);
+        }
+        if (active) {
+            head[i] = (uint32_t)hrow;
+            nn[i] = cnt;
+            if (cnt > (uint32_t)cap) atomicOr(overflow, 1);
+        }
+    }
 }
 
 __global__ void k_nve1(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, float4* __restrict__ pos,
@@ -275,10 +346,8 @@ cudaError_t launch_nlist(const NlistArgs& a, cudaStream_t st) {
     if ((e = launch_scatter(a.chunks, a.n_chunks, a.sys, a.ckey, a.cstart, a.ccount, a.perm_u, st)) != cudaSuccess)
         return e;
     k_cell_sort<<<a.n_cells, 256, 0, st>>>(a.cstart, a.perm_u, a.wpos, a.cpos);
-    k_fill_slot_cell<<<a.n_cells, 64, 0, st>>>(a.cstart, a.n_cells, a.slot_cell);
-    k_nlist<<<(a.total + 127) / 128, 128, 0, st>>>(a.cell_sys, a.n_cells, a.sys, a.cells, a.cstart, a.cpos,
-                                                   a.rlist2, a.cap, a.head, a.nn, a.nl, a.overflow, a.slot_cell,
-                                                   a.total);
+    k_nlist<<<a.n_cells, NL_THREADS, 0, st>>>(a.cell_sys, a.sys, a.cells, a.cstart, a.cpos, a.rlist2, a.cap,
+                                              a.head, a.nn, a.nl, a.overflow);
     return cudaGetLastError();
 }
 

@@ -29,7 +29,6 @@ struct NlistArgs {
     uint32_t* perm_u = nullptr;
     float4* wpos = nullptr;
     float4* cpos = nullptr;
-    uint32_t* slot_cell = nullptr;
     float rlist2 = 0.f;
     int cap = 0;
     uint32_t* head = nullptr;

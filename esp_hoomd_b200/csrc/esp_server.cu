@@ -174,7 +174,7 @@ struct esp_server {
            *d_srec = nullptr, *d_wpos = nullptr, *d_cpos = nullptr;
     float* d_q = nullptr;
     uint32_t *d_rel = nullptr, *d_key = nullptr, *d_perm_u = nullptr, *d_perm = nullptr, *d_srel = nullptr,
-             *d_head = nullptr, *d_nn = nullptr, *d_ckey = nullptr, *d_cperm = nullptr, *d_slot_cell = nullptr,
+             *d_head = nullptr, *d_nn = nullptr, *d_ckey = nullptr, *d_cperm = nullptr,
              *d_ccount = nullptr, *d_cstart = nullptr, *d_nl = nullptr;
     int* d_tile_sys = nullptr;
     uint32_t *d_tcount = nullptr, *d_tstart = nullptr;
@@ -295,7 +295,7 @@ int esp_server::init(const esp_server_config& cfg) {
         (rc = mem.get(d_rel, P_cap)) || (rc = mem.get(d_key, P_cap)) || (rc = mem.get(d_perm_u, P_cap)) ||
         (rc = mem.get(d_perm, P_cap)) || (rc = mem.get(d_srel, P_cap)) || (rc = mem.get(d_head, P_cap)) ||
         (rc = mem.get(d_nn, P_cap)) || (rc = mem.get(d_ckey, P_cap)) || (rc = mem.get(d_cperm, max_particles)) ||
-        (rc = mem.get(d_cpos, max_particles)) || (rc = mem.get(d_slot_cell, max_particles)) ||
+        (rc = mem.get(d_cpos, max_particles)) ||
         (rc = mem.get(d_ccount, C_cap)) || (rc = mem.get(d_cstart, C_cap + 1)) || (rc = mem.get(d_nl, NL_cap)) ||
         (rc = mem.get(d_tile_sys, T_cap)) || (rc = mem.get(d_tcount, T_cap)) || (rc = mem.get(d_tstart, T_cap + 1)) ||
         (rc = mem.get(d_rho, M_cap)) || (rc = mem.get(d_phi, M_cap)) || (rc = mem.get(d_spec, M_cap)) ||
@@ -581,7 +581,6 @@ int esp_server::admit(Request* q, Staging& sg) {
     na.perm_u = d_cperm;
     na.wpos = d_wpos;
     na.cpos = d_cpos;
-    na.slot_cell = d_slot_cell;
     na.rlist2 = (float)(rlist * rlist);
     na.cap = cap;
     na.head = d_head;

@@ -201,18 +201,23 @@ def test_batch_alone_equals_in_mix():
         assert np.abs(va - vbi).max() <= 1e-6 * np.abs(va).max()
 
 
-def test_gpu_nlist_matches_oracle():
-    s = systems.rocksalt(10, seed=77)
+@pytest.mark.parametrize("n,rlist,cap", [
+    (10, 3.4, 256),   # 2 cells per axis: minimum-image test
+    (12, 3.4, 256),   # 3 cells per axis: shifted images
+    (20, 3.4, 256),   # 5 cells per axis
+    (16, 5.29, 768),  # 152 particles per cell: several passes and staging rounds
+])
+def test_gpu_nlist_matches_oracle(n, rlist, cap):
+    s = systems.rocksalt(n, seed=77)
     b = native.Batch(native.make_params(), [s.N], [s.box])
     pos4 = np.zeros((s.N, 4), dtype=np.float32)
     pos4[:, :3] = s.pos
-    cap = 256
     head = torch.zeros(s.N, dtype=torch.int32, device="cuda")
     nn = torch.zeros(s.N, dtype=torch.int32, device="cuda")
     nl = torch.zeros(s.N * cap, dtype=torch.int32, device="cuda")
-    b.build_nlist(_dev(pos4, torch.float32), 3.4, cap, head, nn, nl)
+    b.build_nlist(_dev(pos4, torch.float32), rlist, cap, head, nn, nl)
     h, c, l = head.cpu().numpy(), nn.cpu().numpy(), nl.cpu().numpy()
-    rh, rc, rl = R.neighbor_list(s.pos.astype(np.float32).astype(np.float64), s.box, 3.4)
+    rh, rc, rl = R.neighbor_list(s.pos.astype(np.float32).astype(np.float64), s.box, rlist)
     assert np.array_equal(c, rc.astype(np.int32))
     for i in range(s.N):
         assert set(l[h[i]:h[i] + c[i]].tolist()) == set(rl[rh[i]:rh[i] + rc[i]].tolist())
