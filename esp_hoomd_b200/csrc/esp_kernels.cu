@@ -401,9 +401,12 @@ __global__ void __launch_bounds__(256)
 // outside each stencil). Warp w owns rows Y = 2w, 2w+1 (two m16 tiles, X =
 // 0..15) and both n8 tiles of Z; each k-step of 8 particles issues
 // mma.sync m16n8k8 TF32 with 3xTF32 operand splitting (hi*hi + hi*lo +
-// lo*hi: FP32-level products). Per k-step the A fragments are built from
-// the staged 1D weights, B fragments are the particles' shifted z weights.
-// Every four k-steps (32 particles) the FP32 block accumulators are
+// lo*hi: FP32-level products). Each staged particle has three 16-point
+// rows, zero outside its stencil and already shifted to its origin (x
+// weights times charge, y weights, z weights pre-split into TF32 parts), so
+// a k-step's A fragments are one product and split per element and its B
+// fragments are plain shared loads.
+// Every eight k-steps (64 particles) the FP32 block accumulators are
 // Kahan-merged into (sum, comp) registers; the tile is flushed with one
 // FP64 atomic per point.
 // ----------------------------------------------------------------------------
@@ -413,9 +416,12 @@ __device__ __forceinline__ uint32_t f2tf32(float x) {
     return r;
 }
 
+// x = hi + lo exactly in FP32; hi is x rounded to TF32, lo is passed as raw
+// FP32 bits: the MMA reads its TF32 part (the dropped bits of lo are below
+// 2^-21 |x|, the level of the omitted lo*lo term)
 __device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
     hi = f2tf32(x);
-    lo = f2tf32(x - __uint_as_float(hi));
+    lo = __float_as_uint(x - __uint_as_float(hi));
 }
 
 __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
@@ -428,6 +434,7 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1
 }
 
 constexpr int SPREAD_CHM = 64;  // particles staged per round (multiple of 8)
+constexpr int SPREAD_MS = 24;   // staged row stride: rows of 4 consecutive particles hit disjoint banks
 
 template <int P>
 __global__ void __launch_bounds__(256, 3)
@@ -442,11 +449,14 @@ __global__ void __launch_bounds__(256, 3)
     const int si = tile_sys[t];
     const SysDev S = sys[si];
     const ParamSet& ps = psets[S.pset];
-    float* wzs = reinterpret_cast<float*>(smm4);   // [CH][16] shifted z weights
-    float* pwx = wzs + SPREAD_CHM * 16;            // [CH][P] x weights * q
-    float* pwy = pwx + SPREAD_CHM * P;             // [CH][P]
-    int* pxy = reinterpret_cast<int*>(pwy + SPREAD_CHM * P);  // [CH] origins
-    float* wc = reinterpret_cast<float*>(pxy + SPREAD_CHM);   // [P][D+1]
+    // per staged particle, rows of 16 region points (stride SPREAD_MS), zero
+    // outside the particle's stencil: x weights * q, y weights, and the z
+    // weights already split into TF32 high and low parts
+    float* wxs = reinterpret_cast<float*>(smm4);
+    float* wys = wxs + SPREAD_CHM * SPREAD_MS;
+    uint32_t* wzh = reinterpret_cast<uint32_t*>(wys + SPREAD_CHM * SPREAD_MS);
+    uint32_t* wzl = wzh + SPREAD_CHM * SPREAD_MS;
+    float* wc = reinterpret_cast<float*>(wzl + SPREAD_CHM * SPREAD_MS);  // [P][D+1]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, tg = lane & 3;
     for (int i = tid; i < P * (D + 1); i += blockDim.x) wc[i] = ps.wcoef[(i / (D + 1)) * (MAX_D + 1) + (i % (D + 1))];
     float acc[2][2][4], sum[2][2][4], cmp[2][2][4];
@@ -465,12 +475,13 @@ __global__ void __launch_bounds__(256, 3)
         const int nc = min(SPREAD_CHM, np - base);
         const int ncp = (nc + 7) & ~7;  // padded to whole k-steps (zero weights)
         __syncthreads();
-        for (int k = tid; k < ncp * 16; k += blockDim.x) wzs[k] = 0.f;
-        for (int k = tid; k < ncp * P; k += blockDim.x) {
-            pwx[k] = 0.f;
-            pwy[k] = 0.f;
+        for (int k = tid; k < ncp * SPREAD_MS / 4; k += blockDim.x) {
+            const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+            reinterpret_cast<float4*>(wxs)[k] = z;
+            reinterpret_cast<float4*>(wys)[k] = z;
+            reinterpret_cast<float4*>(wzh)[k] = z;
+            reinterpret_cast<float4*>(wzl)[k] = z;
         }
-        if (tid < ncp) pxy[tid] = 0;
         __syncthreads();
         {
             // thread (a, j0) evaluates window segment a for items j0, j0 + nla, ...
@@ -482,41 +493,40 @@ __global__ void __launch_bounds__(256, 3)
                 for (int j = j0; j < nc * 3; j += nla) {
                     const int p = j / 3, ax = j - 3 * p;
                     const float4 rec = srec[s0 + base + p];
+                    const int o = (int)((srel[s0 + base + p] >> (8 * ax)) & 255u);
                     const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
                     const float w = D == DD ? sp.w(tt) : horner_w(&wc[a * (D + 1)], D, tt);
-                    if (ax == 0)
-                        pwx[p * P + a] = w * rec.w;
-                    else if (ax == 1)
-                        pwy[p * P + a] = w;
-                    else
-                        wzs[p * 16 + (int)((srel[s0 + base + p] >> 16) & 255u) + a] = w;
+                    const int k = p * SPREAD_MS + o + a;
+                    if (ax == 0) {
+                        wxs[k] = w * rec.w;
+                    } else if (ax == 1) {
+                        wys[k] = w;
+                    } else {
+                        uint32_t h, l;
+                        split_tf32(w, h, l);
+                        wzh[k] = h;
+                        wzl[k] = l;
+                    }
                 }
             }
-            for (int p = tid; p < nc; p += blockDim.x) pxy[p] = (int)(srel[s0 + base + p] & 0xffffu);
         }
         __syncthreads();
         for (int k0 = 0; k0 < ncp; k0 += 8) {
-            const int p1 = k0 + tg, p2 = k0 + tg + 4;
+            const int r1 = (k0 + tg) * SPREAD_MS, r2 = r1 + 4 * SPREAD_MS;  // particles k0 + tg, k0 + tg + 4
             // B fragments: b0 = wz_{p1}[Z], b1 = wz_{p2}[Z], Z = 8 nt + g
             uint32_t bh[2][2], bl[2][2];
 #pragma unroll
             for (int nt = 0; nt < 2; ++nt) {
-                split_tf32(wzs[p1 * 16 + 8 * nt + g], bh[nt][0], bl[nt][0]);
-                split_tf32(wzs[p2 * 16 + 8 * nt + g], bh[nt][1], bl[nt][1]);
+                bh[nt][0] = wzh[r1 + 8 * nt + g];
+                bl[nt][0] = wzl[r1 + 8 * nt + g];
+                bh[nt][1] = wzh[r2 + 8 * nt + g];
+                bl[nt][1] = wzl[r2 + 8 * nt + g];
             }
-            const int o1 = pxy[p1], o2 = pxy[p2];
-            const int ox1 = o1 & 255, oy1 = (o1 >> 8) & 255, ox2 = o2 & 255, oy2 = (o2 >> 8) & 255;
-            const int ax1 = g - ox1, ax1b = g + 8 - ox1, ax2 = g - ox2, ax2b = g + 8 - ox2;
-            const float wx1 = (unsigned)ax1 < (unsigned)P ? pwx[p1 * P + ax1] : 0.f;
-            const float wx1b = (unsigned)ax1b < (unsigned)P ? pwx[p1 * P + ax1b] : 0.f;
-            const float wx2 = (unsigned)ax2 < (unsigned)P ? pwx[p2 * P + ax2] : 0.f;
-            const float wx2b = (unsigned)ax2b < (unsigned)P ? pwx[p2 * P + ax2b] : 0.f;
+            const float wx1 = wxs[r1 + g], wx1b = wxs[r1 + g + 8], wx2 = wxs[r2 + g], wx2b = wxs[r2 + g + 8];
 #pragma unroll
             for (int mt = 0; mt < 2; ++mt) {
                 const int Y = 2 * warp + mt;
-                const int ay1 = Y - oy1, ay2 = Y - oy2;
-                const float wy1 = (unsigned)ay1 < (unsigned)P ? pwy[p1 * P + ay1] : 0.f;
-                const float wy2 = (unsigned)ay2 < (unsigned)P ? pwy[p2 * P + ay2] : 0.f;
+                const float wy1 = wys[r1 + Y], wy2 = wys[r2 + Y];
                 uint32_t ah0, al0, ah1, al1, ah2, al2, ah3, al3;
                 split_tf32(wx1 * wy1, ah0, al0);   // row X = g,     particle p1
                 split_tf32(wx1b * wy1, ah1, al1);  // row X = g + 8, particle p1
@@ -529,7 +539,7 @@ __global__ void __launch_bounds__(256, 3)
                     mma_tf32(acc[mt][nt], ah0, ah1, ah2, ah3, bh[nt][0], bh[nt][1]);
                 }
             }
-            if (++ksteps == 4) {
+            if (++ksteps == 8) {
                 ksteps = 0;
 #pragma unroll
                 for (int m = 0; m < 2; ++m)
@@ -1059,9 +1069,10 @@ __global__ void k_influence(SysDev S, const double* __restrict__ w1d, const doub
 // the group sums its four partials (potential, gradient) with shuffles.
 // ============================================================================
 // words of the interpolation staging area: the per-chunk weights, or (before
-// the first chunk) the wrapped row offsets and x indices of the region
+// the first chunk) the wrapped row offsets, shared row offsets and x
+// indices of the region
 __host__ __device__ inline int interp_stage_words(int P, int CH, int E) {
-    return CH * (6 * P + 1) > E * E + E ? CH * (6 * P + 1) : E * E + E;
+    return CH * (6 * P + 1) > 2 * E * E + E ? CH * (6 * P + 1) : 2 * E * E + E;
 }
 
 template <int P>
@@ -1102,15 +1113,19 @@ __global__ void __launch_bounds__(128)
     // stage the extended region with asynchronous 4-byte copies (every
     // thread keeps all its loads in flight; periodic wrap per axis)
     {
-        // wrapped row offsets per (Y, Z) and x indices, then one 4-byte
-        // asynchronous copy per point (all of a thread's copies in flight)
+        // wrapped global row offsets and shared row offsets per (Y, Z) row,
+        // wrapped x indices, then one 4-byte asynchronous copy per point
+        // (all of a thread's copies in flight)
         int* rowo = reinterpret_cast<int*>(wts);  // the staging area holds the index tables first
-        int* xs = rowo + E * E;
+        int* srow = rowo + E * E;
+        int* xs = srow + E * E;
         for (int i = threadIdx.x; i < E * E; i += blockDim.x) {
-            int gy = Y0 + i % E, gz = Z0 + i / E;
+            const int Y = i % E, Z = i / E;
+            int gy = Y0 + Y, gz = Z0 + Z;
             while (gy >= S.ny) gy -= S.ny;
             while (gz >= S.nz) gz -= S.nz;
             rowo[i] = (gz * S.ny + gy) * S.nx;
+            srow[i] = Z * PP + Y * PX;
         }
         for (int i = threadIdx.x; i < E; i += blockDim.x) {
             int gx = X0 + i;
@@ -1119,11 +1134,15 @@ __global__ void __launch_bounds__(128)
         }
         __syncthreads();
         const float* base = phi + S.m_off;
-        for (int idx = threadIdx.x; idx < E * E * E; idx += blockDim.x) {
-            const int X = idx % E, r = idx / E;
-            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sm[(r / E) * PP + (r % E) * PX + X]);
-            const float* src = base + rowo[r] + xs[X];
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src));
+        const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+        // rows padded to a power of two wide, so the point index splits by shifts
+        int sh = 4;
+        while ((1 << sh) < E) ++sh;
+        for (int idx = threadIdx.x; idx < (E * E) << sh; idx += blockDim.x) {
+            const int r = idx >> sh, X = idx & ((1 << sh) - 1);
+            if (X < E)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sbase + 4u * (uint32_t)(srow[r] + X)),
+                             "l"(base + rowo[r] + xs[X]));
         }
         asm volatile("cp.async.commit_group;\n" ::);
         asm volatile("cp.async.wait_group 0;\n" ::);
@@ -1271,8 +1290,10 @@ struct PairEval {
         dx -= Lx * rintf(dx * iLx);
         dy -= Ly * rintf(dy * iLy);
         dz -= Lz * rintf(dz * iLz);
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 < rc2 && r2 > 0.f) {
+        const float r2x = dx * dx + dy * dy + dz * dz;
+        const bool in = r2x < rc2 && r2x > 0.f;
+        const float r2 = in ? r2x : rc2;
+        {
             float ri = rsqrtf(r2);
             ri = ri * fmaf(-0.5f * r2 * ri, ri, 1.5f);  // one Newton step: ~1 ulp
             const float v = fmaf(2.f * irc2, r2, -1.f);
@@ -1281,7 +1302,7 @@ struct PairEval {
             for (int c = NQ - 2; c >= 0; --c) qv = fmaf(qv, v, pc.q[c]);
 #pragma unroll
             for (int c = NQ - 3; c >= 0; --c) dq = fmaf(dq, v, pc.d[c]);
-            const float qq = pi.w * pj.w * INV_4PI_F;
+            const float qq = in ? pi.w * pj.w * INV_4PI_F : 0.f;
             const float fdr = qq * fmaf(tirc3, dq, ri * ri * ri);
             en = fmaf(qq, ri - qv * irc, en);
             fx = fmaf(fdr, dx, fx);
@@ -1460,7 +1481,7 @@ static cudaError_t launch_spread_p(const LaunchArgs& a, cudaStream_t st) {
     const size_t NL = (size_t)nb * nb * nb * C::P3;
     const size_t smem = NL * sizeof(float2) + (size_t)C::CH * P * 4 * 4 + C::CH * 4 + P * (MAX_D + 1) * 4;
     const size_t smem_d = (size_t)SPREAD_CHD * 16 * 4 + (size_t)SPREAD_CHD * (2 * P + 1) * 4 + P * (MAX_D + 1) * 4;
-    const size_t smem_m = (size_t)SPREAD_CHM * 16 * 4 + (size_t)SPREAD_CHM * (2 * P + 1) * 4 + P * (MAX_D + 1) * 4;
+    const size_t smem_m = (size_t)SPREAD_CHM * SPREAD_MS * 4 * 4 + P * (MAX_D + 1) * 4;
     if (a.configure_only) {
         cudaError_t e = cudaFuncSetAttribute(k_spread_mma<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m);
         if (e != cudaSuccess) return e;
