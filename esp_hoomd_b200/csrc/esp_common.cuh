@@ -27,7 +27,7 @@ enum AccSlot {
     ACC_QSUM = 0,   // sum q
     ACC_Q2SUM = 1,  // sum q^2
     ACC_E = 2,      // sum of per-particle energies (mesh + self + pair)
-    ACC_EK = 3,     // k-space energy (diagnostic; equals the mesh energy)
+    ACC_EK = 3,     // k-space energy (diagnostic, with the virial; equals the mesh energy)
     ACC_WK = 4,     // k-space virial xx,xy,xz,yy,yz,zz (4..9)
     ACC_WP = 10,    // pair virial (10..15)
 };

@@ -643,13 +643,24 @@ __device__ __forceinline__ void dft_small(float2 (&v)[R]) {
     }
 }
 
+// Quotient by a divisor fixed for a loop: n / d = umulhi(n, ceil(2^32 / d)),
+// exact when n and d are below 2^16 (division by invariant integers,
+// Granlund and Montgomery 1994). Every FFT index is below 2^16: lines are at
+// most FFT_MAX_N = 256 points and a CTA holds at most 256 x 129 of them.
+struct Div16 {
+    uint32_t d, m;
+    __device__ __forceinline__ explicit Div16(int dd) : d((uint32_t)dd), m(dd > 1 ? 0xffffffffu / (uint32_t)dd + 1u : 0u) {}
+    __device__ __forceinline__ int div(int n) const { return d > 1 ? (int)__umulhi((uint32_t)n, m) : n; }
+};
+
 template <int R, bool INV>
 __device__ __forceinline__ void fft_stage(const float2* __restrict__ src, float2* __restrict__ dst, int n, int B,
                                           int SB, int Ns, const float2* __restrict__ tw) {
     const int m = n / R;
     const int stride = n / (Ns * R);
+    const Div16 dB(B), dNs(Ns);
     for (int idx = threadIdx.x; idx < m * B; idx += blockDim.x) {
-        const int b = idx % B, j = idx / B, k = j % Ns;
+        const int j = dB.div(idx), b = idx - j * B, jq = dNs.div(j), k = j - jq * Ns;
         float2 v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = src[(j + r * m) * SB + b];
@@ -663,7 +674,7 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ src, float2
             }
         }
         dft_small<R, INV>(v);
-        const int o = (j / Ns) * Ns * R + k;
+        const int o = jq * Ns * R + k;
 #pragma unroll
         for (int r = 0; r < R; ++r) dst[(o + r * Ns) * SB + b] = v[r];
     }
@@ -704,8 +715,9 @@ __global__ void k_fftx_fwd(const int4* __restrict__ items, const SysDev* __restr
     constexpr int B = FFT_B_X, SB = FFT_SB_X;  // padded line stride: conflict-free row access
     float2* s0 = sb;
     float2* s1 = sb + n * SB;
+    const Div16 dn(n), dh(S.nxh);
     for (int idx = threadIdx.x; idx < B * n; idx += blockDim.x) {
-        const int b = idx / n, i = idx - b * n, y = y0 + 2 * b;
+        const int b = dn.div(idx), i = idx - b * n, y = y0 + 2 * b;
         float2 v = make_float2(0.f, 0.f);
         if (y < S.ny) {
             const long long g = S.m_off + ((long long)z * S.ny + y) * n + i;
@@ -717,8 +729,8 @@ __global__ void k_fftx_fwd(const int4* __restrict__ items, const SysDev* __restr
     __syncthreads();
     const float2* r = fft_lines<false>(s0, s1, n, B, SB, tw + S.twx, S.radx);
     for (int idx = threadIdx.x; idx < B * S.nxh; idx += blockDim.x) {
-        const int b = idx / S.nxh, k = idx - b * S.nxh;
-        const float2 zk = r[k * SB + b], zn = r[((n - k) % n) * SB + b];
+        const int b = dh.div(idx), k = idx - b * S.nxh;
+        const float2 zk = r[k * SB + b], zn = r[(k ? n - k : 0) * SB + b];
         const int y = y0 + 2 * b;
         if (y < S.ny)
             spec[S.s_off + ((long long)z * S.ny + y) * S.nxh + k] =
@@ -754,6 +766,7 @@ __global__ void k_ffty(const int4* __restrict__ items, const SysDev* __restrict_
 
 // z pass: forward transform, k-space energy and virial (FP64), influence
 // multiply, inverse transform -- the only pass that holds whole k-columns.
+template <bool VIR>
 __global__ void k_fftz_conv(const int4* __restrict__ items, const SysDev* __restrict__ sys,
                             const float2* __restrict__ tw, const float2* __restrict__ gtab,
                             float2* __restrict__ spec, double* __restrict__ acc) {
@@ -776,6 +789,7 @@ __global__ void k_fftz_conv(const int4* __restrict__ items, const SysDev* __rest
     const double twopi = 6.283185307179586;
     const int fy = (y < (S.ny + 1) / 2) ? y : y - S.ny;
     const double kyv = twopi * fy / (double)S.Ly;
+    const double ckx = twopi / (double)S.Lx, ckz = twopi / (double)S.Lz;  // 2 pi / L
     double e[7] = {0, 0, 0, 0, 0, 0, 0};
     for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
         const int z = idx / B, b = idx - z * B, kx = kx0 + b;
@@ -785,18 +799,20 @@ __global__ void k_fftz_conv(const int4* __restrict__ items, const SysDev* __rest
         }
         const float2 gb = gtab[S.g_off + z * rowstride + (long long)y * S.nxh + kx];
         const float2 d = r[idx];
-        const double p2 = (double)d.x * d.x + (double)d.y * d.y;
-        const double mult = (kx == 0 || 2 * kx == S.nx) ? 0.5 : 1.0;
-        const double ek = mult * (double)gb.x * p2, eb = mult * (double)gb.y * p2;
-        const int fz = (z < (n + 1) / 2) ? z : z - n;
-        const double kxv = twopi * kx / (double)S.Lx, kzv = twopi * fz / (double)S.Lz;
-        e[0] += ek;
-        e[1] += ek + eb * kxv * kxv;
-        e[2] += eb * kxv * kyv;
-        e[3] += eb * kxv * kzv;
-        e[4] += ek + eb * kyv * kyv;
-        e[5] += eb * kyv * kzv;
-        e[6] += ek + eb * kzv * kzv;
+        if (VIR) {
+            const double p2 = (double)d.x * d.x + (double)d.y * d.y;
+            const double mult = (kx == 0 || 2 * kx == S.nx) ? 0.5 : 1.0;
+            const double ek = mult * (double)gb.x * p2, eb = mult * (double)gb.y * p2;
+            const int fz = (z < (n + 1) / 2) ? z : z - n;
+            const double kxv = ckx * kx, kzv = ckz * fz;
+            e[0] += ek;
+            e[1] += ek + eb * kxv * kxv;
+            e[2] += eb * kxv * kyv;
+            e[3] += eb * kxv * kzv;
+            e[4] += ek + eb * kyv * kyv;
+            e[5] += eb * kyv * kzv;
+            e[6] += ek + eb * kzv * kzv;
+        }
         r[idx] = make_float2(d.x * gb.x, d.y * gb.x);
     }
     __syncthreads();
@@ -805,10 +821,12 @@ __global__ void k_fftz_conv(const int4* __restrict__ items, const SysDev* __rest
         const int z = idx / B, b = idx - z * B, kx = kx0 + b;
         if (kx < S.nxh) spec[S.s_off + z * rowstride + (long long)y * S.nxh + kx] = o[idx];
     }
-    block_sum_f64<7>(e, red);
-    if (threadIdx.x == 0)
+    if (VIR) {
+        block_sum_f64<7>(e, red);
+        if (threadIdx.x == 0)
 #pragma unroll
-        for (int k = 0; k < 7; ++k) atomicAdd(&acc[it.x * ACC_STRIDE + ACC_EK + k], e[k]);
+            for (int k = 0; k < 7; ++k) atomicAdd(&acc[it.x * ACC_STRIDE + ACC_EK + k], e[k]);
+    }
 }
 
 // Inverse x pass (C2R): two Hermitian half-spectrum rows A, B are extended
@@ -824,8 +842,9 @@ __global__ void k_fftx_inv(const int4* __restrict__ items, const SysDev* __restr
     constexpr int B = FFT_B_X, SB = FFT_SB_X;
     float2* s0 = sb;
     float2* s1 = sb + n * SB;
+    const Div16 dn(n);
     for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
-        const int b = idx / n, k = idx - b * n, ya = y0 + 2 * b, yb = ya + 1;
+        const int b = dn.div(idx), k = idx - b * n, ya = y0 + 2 * b, yb = ya + 1;
         const bool up = k >= S.nxh;
         const int kk = up ? n - k : k;
         float2 A = ya < S.ny ? spec[S.s_off + ((long long)z * S.ny + ya) * S.nxh + kk] : make_float2(0.f, 0.f);
@@ -843,7 +862,7 @@ __global__ void k_fftx_inv(const int4* __restrict__ items, const SysDev* __restr
     __syncthreads();
     const float2* r = fft_lines<true>(s0, s1, n, B, SB, tw + S.twx, S.radx);
     for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
-        const int b = idx / n, i = idx - b * n, y = y0 + 2 * b;
+        const int b = dn.div(idx), i = idx - b * n, y = y0 + 2 * b;
         if (y < S.ny) {
             const float2 v = r[i * SB + b];
             const long long g = S.m_off + ((long long)z * S.ny + y) * n + i;
@@ -878,8 +897,9 @@ __global__ void __launch_bounds__(512)
     float2* s0 = sb;
     float2* s1 = sb + cap;
     const double* src = rho + S.m_off + (long long)z * ny * nx;
+    const Div16 dnx(nx), dnh(nxh);
     for (int idx = threadIdx.x; idx < np * nx; idx += blockDim.x) {
-        const int b = idx / nx, i = idx - b * nx, y = 2 * b;
+        const int b = dnx.div(idx), i = idx - b * nx, y = 2 * b;
         float2 v;
         v.x = (float)src[y * nx + i];
         v.y = (y + 1 < ny) ? (float)src[(y + 1) * nx + i] : 0.f;
@@ -889,8 +909,8 @@ __global__ void __launch_bounds__(512)
     float2* r = fft_lines<false>(s0, s1, nx, np, SBx, tw + S.twx, S.radx);
     float2* o = (r == s0) ? s1 : s0;
     for (int idx = threadIdx.x; idx < np * nxh; idx += blockDim.x) {
-        const int b = idx / nxh, k = idx - b * nxh;
-        const float2 zk = r[k * SBx + b], zn = r[((nx - k) % nx) * SBx + b];
+        const int b = dnh.div(idx), k = idx - b * nxh;
+        const float2 zk = r[k * SBx + b], zn = r[(k ? nx - k : 0) * SBx + b];
         o[(2 * b) * SBy + k] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
         if (2 * b + 1 < ny) o[(2 * b + 1) * SBy + k] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
     }
@@ -898,7 +918,7 @@ __global__ void __launch_bounds__(512)
     const float2* r2 = fft_lines<false>(o, r, ny, nxh, SBy, tw + S.twy, S.rady);
     float2* dst = spec + S.s_off + (long long)z * ny * nxh;
     for (int idx = threadIdx.x; idx < ny * nxh; idx += blockDim.x) {
-        const int y = idx / nxh, k = idx - y * nxh;
+        const int y = dnh.div(idx), k = idx - y * nxh;
         dst[idx] = r2[y * SBy + k];
     }
 }
@@ -915,15 +935,16 @@ __global__ void __launch_bounds__(512)
     float2* s0 = sb;
     float2* s1 = sb + cap;
     const float2* src = spec + S.s_off + (long long)z * ny * nxh;
+    const Div16 dnx(nx), dnh(nxh);
     for (int idx = threadIdx.x; idx < ny * nxh; idx += blockDim.x) {
-        const int y = idx / nxh, k = idx - y * nxh;
+        const int y = dnh.div(idx), k = idx - y * nxh;
         s0[y * SBy + k] = src[idx];
     }
     __syncthreads();
     float2* r = fft_lines<true>(s0, s1, ny, nxh, SBy, tw + S.twy, S.rady);
     float2* o = (r == s0) ? s1 : s0;
     for (int idx = threadIdx.x; idx < np * nx; idx += blockDim.x) {
-        const int b = idx / nx, k = idx - b * nx;
+        const int b = dnx.div(idx), k = idx - b * nx;
         const bool up = k >= nxh;
         const int kk = up ? nx - k : k;
         float2 A = r[(2 * b) * SBy + kk];
@@ -943,7 +964,7 @@ __global__ void __launch_bounds__(512)
     float* dst = phi + S.m_off + (long long)z * ny * nx;
     double* rz = rho + S.m_off + (long long)z * ny * nx;
     for (int idx = threadIdx.x; idx < np * nx; idx += blockDim.x) {
-        const int b = idx / nx, i = idx - b * nx;
+        const int b = dnx.div(idx), i = idx - b * nx;
         const float2 v = r2[i * SBx + b];
         dst[(2 * b) * nx + i] = v.x;
         rz[(2 * b) * nx + i] = 0.0;  // clear the charge mesh for the next spread
@@ -954,8 +975,9 @@ __global__ void __launch_bounds__(512)
     }
 }
 
-// z pass over a whole xz-slab (fixed y): forward, energy/virial, influence
-// multiply, inverse.
+// z pass over a whole xz-slab (fixed y): forward, energy/virial (VIR: when
+// the virial is requested), influence multiply, inverse.
+template <bool VIR>
 __global__ void __launch_bounds__(512)
     k_fft_slab_z(const int2* __restrict__ items, const SysDev* __restrict__ sys, const float2* __restrict__ tw,
                  const float2* __restrict__ gtab, float2* __restrict__ spec, double* __restrict__ acc) {
@@ -969,8 +991,9 @@ __global__ void __launch_bounds__(512)
     const long long rowstride = (long long)S.ny * nxh;
     float2* base = spec + S.s_off + (long long)y * nxh;
     const float2* gbase = gtab + S.g_off + (long long)y * nxh;
+    const Div16 dnh(nxh);
     for (int idx = threadIdx.x; idx < nz * nxh; idx += blockDim.x) {
-        const int z = idx / nxh, k = idx - z * nxh;
+        const int z = dnh.div(idx), k = idx - z * nxh;
         s0[z * SBz + k] = base[z * rowstride + k];
     }
     __syncthreads();
@@ -979,35 +1002,40 @@ __global__ void __launch_bounds__(512)
     const double twopi = 6.283185307179586;
     const int fy = (y < (S.ny + 1) / 2) ? y : y - S.ny;
     const double kyv = twopi * fy / (double)S.Ly;
+    const double ckx = twopi / (double)S.Lx, ckz = twopi / (double)S.Lz;  // 2 pi / L
     double e[7] = {0, 0, 0, 0, 0, 0, 0};
     for (int idx = threadIdx.x; idx < nz * nxh; idx += blockDim.x) {
-        const int z = idx / nxh, kx = idx - z * nxh;
+        const int z = dnh.div(idx), kx = idx - z * nxh;
         const float2 gb = gbase[z * rowstride + kx];
         float2& d = r[z * SBz + kx];
-        const double p2 = (double)d.x * d.x + (double)d.y * d.y;
-        const double mult = (kx == 0 || 2 * kx == S.nx) ? 0.5 : 1.0;
-        const double ek = mult * (double)gb.x * p2, eb = mult * (double)gb.y * p2;
-        const int fz = (z < (nz + 1) / 2) ? z : z - nz;
-        const double kxv = twopi * kx / (double)S.Lx, kzv = twopi * fz / (double)S.Lz;
-        e[0] += ek;
-        e[1] += ek + eb * kxv * kxv;
-        e[2] += eb * kxv * kyv;
-        e[3] += eb * kxv * kzv;
-        e[4] += ek + eb * kyv * kyv;
-        e[5] += eb * kyv * kzv;
-        e[6] += ek + eb * kzv * kzv;
+        if (VIR) {
+            const double p2 = (double)d.x * d.x + (double)d.y * d.y;
+            const double mult = (kx == 0 || 2 * kx == S.nx) ? 0.5 : 1.0;
+            const double ek = mult * (double)gb.x * p2, eb = mult * (double)gb.y * p2;
+            const int fz = (z < (nz + 1) / 2) ? z : z - nz;
+            const double kxv = ckx * kx, kzv = ckz * fz;
+            e[0] += ek;
+            e[1] += ek + eb * kxv * kxv;
+            e[2] += eb * kxv * kyv;
+            e[3] += eb * kxv * kzv;
+            e[4] += ek + eb * kyv * kyv;
+            e[5] += eb * kyv * kzv;
+            e[6] += ek + eb * kzv * kzv;
+        }
         d = make_float2(d.x * gb.x, d.y * gb.x);
     }
     __syncthreads();
     const float2* o = fft_lines<true>(r, other, nz, nxh, SBz, tw + S.twz, S.radz);
     for (int idx = threadIdx.x; idx < nz * nxh; idx += blockDim.x) {
-        const int z = idx / nxh, k = idx - z * nxh;
+        const int z = dnh.div(idx), k = idx - z * nxh;
         base[z * rowstride + k] = o[z * SBz + k];
     }
-    block_sum_f64<7>(e, red);
-    if (threadIdx.x == 0)
+    if (VIR) {
+        block_sum_f64<7>(e, red);
+        if (threadIdx.x == 0)
 #pragma unroll
-        for (int k = 0; k < 7; ++k) atomicAdd(&acc[it.x * ACC_STRIDE + ACC_EK + k], e[k]);
+            for (int k = 0; k < 7; ++k) atomicAdd(&acc[it.x * ACC_STRIDE + ACC_EK + k], e[k]);
+    }
 }
 
 // ============================================================================
@@ -1573,18 +1601,32 @@ cudaError_t launch_fft(const LaunchArgs& a, cudaStream_t st) {
         if ((e = cudaFuncSetAttribute(k_fftx_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx))) return e;
         if ((e = cudaFuncSetAttribute(k_ffty<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz))) return e;
         if ((e = cudaFuncSetAttribute(k_ffty<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz))) return e;
-        if ((e = cudaFuncSetAttribute(k_fftz_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz))) return e;
+        if ((e = cudaFuncSetAttribute(k_fftz_conv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz))) return e;
+        if ((e = cudaFuncSetAttribute(k_fftz_conv<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz)))
+            return e;
         if ((e = cudaFuncSetAttribute(k_fft_plane_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_MAX)))
             return e;
         if ((e = cudaFuncSetAttribute(k_fft_plane_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_MAX)))
             return e;
-        return cudaFuncSetAttribute(k_fft_slab_z, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_MAX);
+        if ((e = cudaFuncSetAttribute(k_fft_slab_z<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_MAX)))
+            return e;
+        return cudaFuncSetAttribute(k_fft_slab_z<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_MAX);
     }
     if (a.n_pitems) k_fft_plane_fwd<<<a.n_pitems, 512, a.smem_plane, st>>>(a.pitems, a.sys, a.tw, a.rho, a.spec);
     if (a.n_xitems) k_fftx_fwd<<<a.n_xitems, 256, smx, st>>>(a.xitems, a.sys, a.tw, a.rho, a.spec);
     if (a.n_yitems) k_ffty<false><<<a.n_yitems, 256, smy, st>>>(a.yitems, a.sys, a.tw, a.spec);
-    if (a.n_sitems) k_fft_slab_z<<<a.n_sitems, 512, a.smem_slab, st>>>(a.sitems, a.sys, a.tw, a.gtab, a.spec, a.acc);
-    if (a.n_zitems) k_fftz_conv<<<a.n_zitems, 256, smz, st>>>(a.zitems, a.sys, a.tw, a.gtab, a.spec, a.acc);
+    if (a.n_sitems) {
+        if (a.want_virial)
+            k_fft_slab_z<true><<<a.n_sitems, 512, a.smem_slab, st>>>(a.sitems, a.sys, a.tw, a.gtab, a.spec, a.acc);
+        else
+            k_fft_slab_z<false><<<a.n_sitems, 512, a.smem_slab, st>>>(a.sitems, a.sys, a.tw, a.gtab, a.spec, a.acc);
+    }
+    if (a.n_zitems) {
+        if (a.want_virial)
+            k_fftz_conv<true><<<a.n_zitems, 256, smz, st>>>(a.zitems, a.sys, a.tw, a.gtab, a.spec, a.acc);
+        else
+            k_fftz_conv<false><<<a.n_zitems, 256, smz, st>>>(a.zitems, a.sys, a.tw, a.gtab, a.spec, a.acc);
+    }
     if (a.n_yitems) k_ffty<true><<<a.n_yitems, 256, smy, st>>>(a.yitems, a.sys, a.tw, a.spec);
     if (a.n_xitems) k_fftx_inv<<<a.n_xitems, 256, smx, st>>>(a.xitems, a.sys, a.tw, a.spec, a.phi, a.rho);
     if (a.n_pitems) k_fft_plane_inv<<<a.n_pitems, 512, a.smem_plane, st>>>(a.pitems, a.sys, a.tw, a.spec, a.phi, a.rho);
