@@ -33,6 +33,7 @@ __global__ void k_bin(const int2* __restrict__ chunks, const SysDev* __restrict_
     const SysDev S = sys[ch.x];
     const int i = ch.y + threadIdx.x;
     double qs[2] = {0.0, 0.0};
+    uint32_t kk = 0xffffffffu;  // tile of this lane (none for lanes past the system)
     if (i < S.p_off + S.N) {
         const float4 p = pos_in[i];
         const float q = q_in[i];
@@ -62,13 +63,18 @@ __global__ void k_bin(const int2* __restrict__ chunks, const SysDev* __restrict_
         const int tx = i0m[0] / T, ty = i0m[1] / T, tz = i0m[2] / T;
         const uint32_t k = (uint32_t)(S.t_off + (tz * S.nty + ty) * S.ntx + tx);
         key[i] = k;
-        atomicAdd(&tile_count[k], 1u);
+        kk = k;
         posq[i] = make_float4(x, y, z, q);
         trec[i] = make_float4(tt[0], tt[1], tt[2], q);
         rel[i] = (uint32_t)(i0m[0] - tx * T) | ((uint32_t)(i0m[1] - ty * T) << 8) |
                  ((uint32_t)(i0m[2] - tz * T) << 16);
         qs[0] = q;
         qs[1] = (double)q * q;
+    }
+    {
+        // one atomic per distinct tile of the warp
+        const unsigned grp = __match_any_sync(0xffffffffu, kk);
+        if (kk != 0xffffffffu && (threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&tile_count[kk], (uint32_t)__popc(grp));
     }
     block_sum_f64<2>(qs, red);
     if (threadIdx.x == 0) {
@@ -78,14 +84,36 @@ __global__ void k_bin(const int2* __restrict__ chunks, const SysDev* __restrict_
 }
 
 // Exclusive scan of n counts (single CTA of 1024 threads); start[n] = total.
-__global__ void k_scan(const uint32_t* __restrict__ cnt, uint32_t* __restrict__ start, int n) {
+// Each round covers 1024 x SCAN_PER consecutive counts, SCAN_PER per thread
+// (16-byte loads and stores when both arrays are 16-byte aligned).
+constexpr int SCAN_PER = 16;
+
+__global__ void __launch_bounds__(1024) k_scan(const uint32_t* __restrict__ cnt, uint32_t* __restrict__ start, int n) {
     __shared__ uint32_t wsum[32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const bool vec = ((reinterpret_cast<uintptr_t>(cnt) | reinterpret_cast<uintptr_t>(start)) & 15u) == 0;
     uint32_t carry = 0;
-    for (int base = 0; base < n; base += 1024) {
-        const int i = base + threadIdx.x;
-        const uint32_t v = i < n ? cnt[i] : 0u;
-        uint32_t x = v;
+    for (int base = 0; base < n; base += 1024 * SCAN_PER) {
+        const int i0 = base + threadIdx.x * SCAN_PER;
+        const bool full = vec && i0 + SCAN_PER <= n;
+        uint32_t v[SCAN_PER];
+        if (full) {
+#pragma unroll
+            for (int k = 0; k < SCAN_PER / 4; ++k) {
+                const uint4 u = reinterpret_cast<const uint4*>(cnt + i0)[k];
+                v[4 * k] = u.x;
+                v[4 * k + 1] = u.y;
+                v[4 * k + 2] = u.z;
+                v[4 * k + 3] = u.w;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < SCAN_PER; ++k) v[k] = i0 + k < n ? cnt[i0 + k] : 0u;
+        }
+        uint32_t tsum = 0;
+#pragma unroll
+        for (int k = 0; k < SCAN_PER; ++k) tsum += v[k];
+        uint32_t x = tsum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -103,8 +131,22 @@ __global__ void k_scan(const uint32_t* __restrict__ cnt, uint32_t* __restrict__ 
             wsum[lane] = w;
         }
         __syncthreads();
-        const uint32_t pre = wid > 0 ? wsum[wid - 1] : 0u;
-        if (i < n) start[i] = carry + pre + x - v;
+        uint32_t run = carry + (wid > 0 ? wsum[wid - 1] : 0u) + x - tsum;
+#pragma unroll
+        for (int k = 0; k < SCAN_PER; ++k) {
+            const uint32_t c = v[k];
+            v[k] = run;
+            run += c;
+        }
+        if (full) {
+#pragma unroll
+            for (int k = 0; k < SCAN_PER / 4; ++k)
+                reinterpret_cast<uint4*>(start + i0)[k] = make_uint4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < SCAN_PER; ++k)
+                if (i0 + k < n) start[i0 + k] = v[k];
+        }
         const uint32_t total = wsum[31];
         __syncthreads();
         carry += total;
@@ -120,10 +162,15 @@ __global__ void k_scatter(const int2* __restrict__ chunks, const SysDev* __restr
     const int2 ch = chunks[blockIdx.x];
     const SysDev S = sys[ch.x];
     const int i = ch.y + threadIdx.x;
-    if (i >= S.p_off + S.N) return;
-    const uint32_t k = key[i];
-    const uint32_t slot = start[k] + atomicSub(&cnt[k], 1u) - 1u;
-    perm_u[slot] = (uint32_t)i;
+    const bool valid = i < S.p_off + S.N;
+    const uint32_t k = valid ? key[i] : 0xffffffffu;
+    // lanes with the same tile take consecutive slots with one atomic
+    const unsigned grp = __match_any_sync(0xffffffffu, k);
+    const int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
+    uint32_t top = 0;
+    if (valid && lane == leader) top = atomicSub(&cnt[k], (uint32_t)__popc(grp));
+    top = __shfl_sync(0xffffffffu, top, leader);
+    if (valid) perm_u[start[k] + top - 1u - (uint32_t)__popc(grp & ((1u << lane) - 1u))] = (uint32_t)i;
 }
 
 // Deterministic per-tile order: particles of one tile sorted by index, so
@@ -1580,7 +1627,7 @@ cudaError_t launch_bin(const LaunchArgs& a, cudaStream_t st) {
 cudaError_t launch_sort(const LaunchArgs& a, cudaStream_t st) {
     k_scan<<<1, 1024, 0, st>>>(a.tile_count, a.tile_start, a.n_tiles);
     if (a.n_chunks) k_scatter<<<a.n_chunks, 256, 0, st>>>(a.chunks, a.sys, a.key, a.tile_start, a.tile_count, a.perm_u);
-    if (a.n_tiles) k_tile_sort<<<a.n_tiles, 256, 0, st>>>(a.tile_start, a.perm_u, a.perm, a.trec, a.rel, a.srec, a.srel);
+    if (a.n_tiles) k_tile_sort<<<a.n_tiles, 128, 0, st>>>(a.tile_start, a.perm_u, a.perm, a.trec, a.rel, a.srec, a.srel);
     return cudaGetLastError();
 }
 

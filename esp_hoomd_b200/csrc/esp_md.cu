@@ -16,8 +16,8 @@ __global__ void k_cell_bin(const int2* __restrict__ chunks, const SysDev* __rest
     const SysDev& S = sys[ch.x];
     const CellDev& C = cells[ch.x];
     const int i = ch.y + threadIdx.x;
-    if (i >= S.p_off + S.N) return;
-    const float4 p = pos[i];
+    const bool valid = i < S.p_off + S.N;
+    const float4 p = valid ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
     float x = p.x - S.Lx * floorf(p.x * S.inv_Lx);
     float y = p.y - S.Ly * floorf(p.y * S.inv_Ly);
     float z = p.z - S.Lz * floorf(p.z * S.inv_Lz);
@@ -29,9 +29,12 @@ __global__ void k_cell_bin(const int2* __restrict__ chunks, const SysDev* __rest
     cx = max(cx, 0);
     cy = max(cy, 0);
     cz = max(cz, 0);
-    const uint32_t k = (uint32_t)(C.c_off + (cz * C.ncy + cy) * C.ncx + cx);
+    const uint32_t k = valid ? (uint32_t)(C.c_off + (cz * C.ncy + cy) * C.ncx + cx) : 0xffffffffu;
+    // one atomic per distinct cell of the warp
+    const unsigned grp = __match_any_sync(0xffffffffu, k);
+    if (!valid) return;
+    if ((threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&ccount[k], (uint32_t)__popc(grp));
     ckey[i] = k;
-    atomicAdd(&ccount[k], 1u);
     wpos[i] = make_float4(x, y, z, __int_as_float(i));
 }
 
