@@ -88,9 +88,13 @@ uint32_t radix_plan(int n) {
 // class is the particle's x origin mod K; the kernel orders particles so the
 // K groups of a warp have distinct classes (conflict-free reads).
 void choose_pitch(int P, int E, int& PX, int& PP) {
+    // interpolation region pitches: plane pitch = K (mod 32), so the G lanes
+    // of a particle read G banks K apart; row pitch = 1 (mod K), so the bank
+    // class of a particle is (ox + oy) mod K, close to uniform over a tile
     const int G = P <= 4 ? 4 : (P <= 8 ? 8 : 16);
     const int K = 32 / G;
-    PX = (E + K - 1) / K * K;
+    PX = E;
+    while (PX % K != 1) ++PX;
     PP = E * PX;
     while (PP % 32 != K) ++PP;
 }

@@ -1261,15 +1261,15 @@ __global__ void __launch_bounds__(128)
         }
         __syncthreads();
         if (C::CH <= 32 && threadIdx.x < 32) {
-            // processing order: queue position q prefers a particle whose x
-            // origin is congruent to q mod K, so the K groups of a warp read
-            // potential rows in disjoint bank classes (plane pitch = K mod 32,
-            // row pitch a multiple of K); particles left over fill the free
+            // processing order: queue position q prefers a particle whose
+            // bank class (ox + oy) mod K is q mod K, so the K groups of a warp
+            // read potential rows in disjoint bank classes (plane pitch = K
+            // mod 32, row pitch = 1 mod K); particles left over fill the free
             // positions in order
             const int j = threadIdx.x;
             const unsigned full = 0xffffffffu, lt = (1u << j) - 1u;
             const bool valid = j < nc;
-            const int cls = valid ? ((org[j] & 255) & (K - 1)) : -1;
+            const int cls = valid ? (((org[j] & 255) + ((org[j] >> 8) & 255)) & (K - 1)) : -1;
             int rank = 0, cpos = 0;
             const int pk = j & (K - 1);
 #pragma unroll
@@ -1360,17 +1360,19 @@ struct PairEval {
     float rc2, irc2, irc, tirc3, Lx, Ly, Lz, iLx, iLy, iLz;
     float fx = 0.f, fy = 0.f, fz = 0.f, en = 0.f;
     float vxx = 0.f, vxy = 0.f, vxz = 0.f, vyy = 0.f, vyz = 0.f, vzz = 0.f;
+    template <bool WRAP = true>
     __device__ __forceinline__ void pair(const float4& pi, const float4& pj) {
         float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-        dx -= Lx * rintf(dx * iLx);
-        dy -= Ly * rintf(dy * iLy);
-        dz -= Lz * rintf(dz * iLz);
+        if (WRAP) {
+            dx -= Lx * rintf(dx * iLx);
+            dy -= Ly * rintf(dy * iLy);
+            dz -= Lz * rintf(dz * iLz);
+        }
         const float r2x = dx * dx + dy * dy + dz * dz;
         const bool in = r2x < rc2 && r2x > 0.f;
         const float r2 = in ? r2x : rc2;
         {
-            float ri = rsqrtf(r2);
-            ri = ri * fmaf(-0.5f * r2 * ri, ri, 1.5f);  // one Newton step: ~1 ulp
+            const float ri = rsqrtf(r2);  // hardware estimate, a few ulp
             const float v = fmaf(2.f * irc2, r2, -1.f);
             float qv = pc.q[NQ - 1], dq = pc.d[NQ - 2];
 #pragma unroll
@@ -1419,6 +1421,17 @@ __global__ void __launch_bounds__(256, 5)
     const int i = ch.y + threadIdx.x / TPP;
     const int sub = threadIdx.x % TPP;
     const bool valid = i < S.p_off + S.N;
+    // particles at least r_c from every face (positions are wrapped into
+    // the box) see every in-cutoff neighbour in the same image; a warp whose
+    // particles all are skips the minimum-image wrap (out-of-cutoff pairs
+    // are masked whatever their displacement)
+    bool inner = true;
+    if (valid) {
+        const float4 p = posq[i];
+        const float rc = ps.rcut;
+        inner = p.x >= rc && p.x <= S.Lx - rc && p.y >= rc && p.y <= S.Ly - rc && p.z >= rc && p.z <= S.Lz - rc;
+    }
+    const bool interior = __all_sync(0xffffffffu, inner);
     if (valid) {
         const float4 pi = posq[i];
         const uint32_t n = nn[i], h = head[i];
@@ -1428,16 +1441,30 @@ __global__ void __launch_bounds__(256, 5)
             // 16-byte row segments: each lane streams 4 neighbour indices
             const uint4* row = reinterpret_cast<const uint4*>(nlist + h);
             const uint32_t n4 = n >> 2;
-            for (uint32_t k4 = sub; k4 < n4; k4 += TPP) {
-                const uint4 jj = __ldg(&row[k4]);
-                const float4 p0 = __ldg(&posq[po + (int)jj.x]);
-                const float4 p1 = __ldg(&posq[po + (int)jj.y]);
-                const float4 p2 = __ldg(&posq[po + (int)jj.z]);
-                const float4 p3 = __ldg(&posq[po + (int)jj.w]);
-                ev.pair(pi, p0);
-                ev.pair(pi, p1);
-                ev.pair(pi, p2);
-                ev.pair(pi, p3);
+            if (interior) {
+                for (uint32_t k4 = sub; k4 < n4; k4 += TPP) {
+                    const uint4 jj = __ldg(&row[k4]);
+                    const float4 p0 = __ldg(&posq[po + (int)jj.x]);
+                    const float4 p1 = __ldg(&posq[po + (int)jj.y]);
+                    const float4 p2 = __ldg(&posq[po + (int)jj.z]);
+                    const float4 p3 = __ldg(&posq[po + (int)jj.w]);
+                    ev.template pair<false>(pi, p0);
+                    ev.template pair<false>(pi, p1);
+                    ev.template pair<false>(pi, p2);
+                    ev.template pair<false>(pi, p3);
+                }
+            } else {
+                for (uint32_t k4 = sub; k4 < n4; k4 += TPP) {
+                    const uint4 jj = __ldg(&row[k4]);
+                    const float4 p0 = __ldg(&posq[po + (int)jj.x]);
+                    const float4 p1 = __ldg(&posq[po + (int)jj.y]);
+                    const float4 p2 = __ldg(&posq[po + (int)jj.z]);
+                    const float4 p3 = __ldg(&posq[po + (int)jj.w]);
+                    ev.pair(pi, p0);
+                    ev.pair(pi, p1);
+                    ev.pair(pi, p2);
+                    ev.pair(pi, p3);
+                }
             }
             k0 = n4 << 2;
         }
