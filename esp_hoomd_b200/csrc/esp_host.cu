@@ -274,16 +274,18 @@ struct esp_batch {
     struct GraphKey {
         const void *pos, *vel, *q, *head, *nn, *nl, *force, *energy, *virial;
         double dt;
+        bool with_energy;
         bool operator==(const GraphKey& o) const {
             return pos == o.pos && vel == o.vel && q == o.q && head == o.head && nn == o.nn && nl == o.nl &&
-                   force == o.force && energy == o.energy && virial == o.virial && dt == o.dt;
+                   force == o.force && energy == o.energy && virial == o.virial && dt == o.dt &&
+                   with_energy == o.with_energy;
         }
     };
     // captured MD steps, one per distinct set of caller pointers; a few
     // entries so that a caller alternating between buffer sets (uploads of
     // the next batch overlapping this one) does not recapture every call.
     // The least recently used entry is replaced.
-    static constexpr int N_GRAPHS = 4;
+    static constexpr int N_GRAPHS = 8;
     struct GraphEntry {
         GraphKey key{};
         cudaGraphExec_t exec = nullptr;
@@ -312,8 +314,11 @@ struct esp_batch {
     int md_run(cudaStream_t st, float* pos4, float* vel4, const float* q, const unsigned* head, const unsigned* nn,
                const unsigned* nl, float* force4, double* energy, double* virial, int nsteps, double dt,
                int use_graph);
+    // want_energy = false (MD steps whose energies are overwritten by the
+    // next step) leaves the pair energies out of force.w and energy
     int compute(cudaStream_t st, const float* pos4, const float* q, const unsigned* head, const unsigned* nn,
-                const unsigned* nl, float* force4, double* energy, double* virial, int flags);
+                const unsigned* nl, float* force4, double* energy, double* virial, int flags,
+                bool want_energy = true);
     int spread_only(cudaStream_t st, const float* pos4, const float* q, double* rho_out);
     int build_nlist(cudaStream_t st, const float* pos4, double rlist, int cap, unsigned* head, unsigned* nn,
                     unsigned* nl);
@@ -754,7 +759,8 @@ LaunchArgs esp_batch::args() const {
 }
 
 int esp_batch::compute(cudaStream_t st, const float* pos4, const float* q, const unsigned* head, const unsigned* nn,
-                       const unsigned* nl, float* force4, double* energy, double* virial, int flags) {
+                       const unsigned* nl, float* force4, double* energy, double* virial, int flags,
+                       bool want_energy) {
     if (f64) return fail(ESP_ERR_UNSUPPORTED, "context planned for FP64: use esp_compute_f64");
     if (!pos4 || !q || !force4) return fail(ESP_ERR_INVALID, "null position, charge or force pointer");
     if (!(flags & ESP_ALL)) return fail(ESP_ERR_INVALID, "flags select no term");
@@ -767,6 +773,7 @@ int esp_batch::compute(cudaStream_t st, const float* pos4, const float* q, const
     if (energy) a.energy = energy;
     if (virial) a.virial = virial;
     a.want_virial = virial != nullptr;
+    a.want_energy = (want_energy || a.want_virial) ? 1 : 0;
     a.nl_head = head;
     a.nl_n = nn;
     a.nl_list = nl;
@@ -832,12 +839,14 @@ int esp_batch::md_run(cudaStream_t st, float* pos4, float* vel4, const float* q,
                       double dt, int use_graph) {
     if (nsteps < 0) return fail(ESP_ERR_INVALID, "negative step count");
     if (!pos4 || !vel4 || !q || !force4 || !head || !nn || !nl) return fail(ESP_ERR_INVALID, "null pointer");
-    auto step = [&]() -> int {
+    // Every step overwrites the energies (force.w, energy) of the previous
+    // one, so only the last step evaluates the pair energies.
+    auto step = [&](bool with_energy) -> int {
         timer.begin(ESP_STAGE_NVE, st);
         ESPB_CK(launch_nve1(d_chunks, n_chunks, d_sys, reinterpret_cast<float4*>(pos4),
                             reinterpret_cast<float4*>(vel4), reinterpret_cast<const float4*>(force4), (float)dt, st));
         timer.end(st);
-        int rc = compute(st, pos4, q, head, nn, nl, force4, energy, virial, ESP_ALL);
+        int rc = compute(st, pos4, q, head, nn, nl, force4, energy, virial, ESP_ALL, with_energy);
         if (rc) return rc;
         timer.begin(ESP_STAGE_NVE, st);
         ESPB_CK(launch_nve2(d_chunks, n_chunks, d_sys, reinterpret_cast<float4*>(vel4),
@@ -847,54 +856,65 @@ int esp_batch::md_run(cudaStream_t st, float* pos4, float* vel4, const float* q,
     };
     if (!use_graph || timer.on) {
         for (int k = 0; k < nsteps; ++k) {
-            int rc = step();
+            int rc = step(k == nsteps - 1);
             if (rc) return rc;
         }
         return 0;
     }
-    const GraphKey key{pos4, vel4, q, head, nn, nl, force4, energy, virial, dt};
-    GraphEntry* ge = nullptr;
-    for (GraphEntry& g : graphs)
-        if (g.exec && g.key == key) ge = &g;
-    if (!ge) {
-        ge = &graphs[0];
+    // one captured step per (caller pointers, energy or not)
+    auto graph_for = [&](bool with_energy, cudaGraphExec_t& out) -> int {
+        const GraphKey key{pos4, vel4, q, head, nn, nl, force4, energy, virial, dt, with_energy};
+        GraphEntry* ge = nullptr;
         for (GraphEntry& g : graphs)
-            if (!g.exec || g.used < ge->used) {
-                ge = &g;
-                if (!g.exec) break;
+            if (g.exec && g.key == key) ge = &g;
+        if (!ge) {
+            ge = &graphs[0];
+            for (GraphEntry& g : graphs)
+                if (!g.exec || g.used < ge->used) {
+                    ge = &g;
+                    if (!g.exec) break;
+                }
+            if (ge->exec) {
+                cudaGraphExecDestroy(ge->exec);
+                ge->exec = nullptr;
             }
-        if (ge->exec) {
-            cudaGraphExecDestroy(ge->exec);
-            ge->exec = nullptr;
-        }
-        cudaStream_t cs = nullptr;
-        ESPB_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-        cudaGraph_t g = nullptr;
-        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-        int rc = 0;
-        if (e == cudaSuccess) {
-            cudaStream_t saved = st;
-            st = cs;
-            rc = step();
-            st = saved;
-            cudaError_t e2 = cudaStreamEndCapture(cs, &g);
-            if (e == cudaSuccess) e = e2;
-        }
-        cudaStreamDestroy(cs);
-        if (rc) {
+            cudaStream_t cs = nullptr;
+            ESPB_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+            int rc = 0;
+            if (e == cudaSuccess) {
+                cudaStream_t saved = st;
+                st = cs;
+                rc = step(with_energy);
+                st = saved;
+                cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+                if (e == cudaSuccess) e = e2;
+            }
+            cudaStreamDestroy(cs);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&ge->exec, g, 0);
             if (g) cudaGraphDestroy(g);
-            return rc;
+            if (e != cudaSuccess) {
+                ge->exec = nullptr;
+                return fail(ESP_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            }
+            ge->key = key;
         }
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&ge->exec, g, 0);
-        if (g) cudaGraphDestroy(g);
-        if (e != cudaSuccess) {
-            ge->exec = nullptr;
-            return fail(ESP_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-        }
-        ge->key = key;
-    }
-    ge->used = ++graph_tick;
-    for (int k = 0; k < nsteps; ++k) ESPB_CK(cudaGraphLaunch(ge->exec, st));
+        ge->used = ++graph_tick;
+        out = ge->exec;
+        return 0;
+    };
+    if (nsteps == 0) return 0;
+    cudaGraphExec_t g_last = nullptr, g_mid = nullptr;
+    int rc = 0;
+    if (nsteps > 1 && (rc = graph_for(false, g_mid))) return rc;
+    if ((rc = graph_for(true, g_last))) return rc;
+    for (int k = 0; k + 1 < nsteps; ++k) ESPB_CK(cudaGraphLaunch(g_mid, st));
+    ESPB_CK(cudaGraphLaunch(g_last, st));
     return 0;
 }
 

@@ -1354,7 +1354,7 @@ __global__ void __launch_bounds__(128)
 //   force_divr = qiqj/(4 pi) (1/r^3 + 2 Q'(u)/r_c^3)
 // (the split form of EvaluatorPairPSWF::evalForceAndEnergy).
 // ============================================================================
-template <int NQ, bool VIR>
+template <int NQ, bool VIR, bool EN>
 struct PairEval {
     const PairCoef& pc;  // the kernel parameter: constant-bank operands
     float rc2, irc2, irc, tirc3, Lx, Ly, Lz, iLx, iLy, iLz;
@@ -1374,14 +1374,17 @@ struct PairEval {
         {
             const float ri = rsqrtf(r2);  // hardware estimate, a few ulp
             const float v = fmaf(2.f * irc2, r2, -1.f);
-            float qv = pc.q[NQ - 1], dq = pc.d[NQ - 2];
-#pragma unroll
-            for (int c = NQ - 2; c >= 0; --c) qv = fmaf(qv, v, pc.q[c]);
+            float dq = pc.d[NQ - 2];
 #pragma unroll
             for (int c = NQ - 3; c >= 0; --c) dq = fmaf(dq, v, pc.d[c]);
             const float qq = in ? pi.w * pj.w * INV_4PI_F : 0.f;
             const float fdr = qq * fmaf(tirc3, dq, ri * ri * ri);
-            en = fmaf(qq, ri - qv * irc, en);
+            if (EN) {
+                float qv = pc.q[NQ - 1];
+#pragma unroll
+                for (int c = NQ - 2; c >= 0; --c) qv = fmaf(qv, v, pc.q[c]);
+                en = fmaf(qq, ri - qv * irc, en);
+            }
             fx = fmaf(fdr, dx, fx);
             fy = fmaf(fdr, dy, fy);
             fz = fmaf(fdr, dz, fz);
@@ -1397,7 +1400,9 @@ struct PairEval {
     }
 };
 
-template <int TPP, int NQ, bool VIR>
+// EN: pair energies (per particle and per system); without them the split
+// polynomial Q itself is not needed, only Q'.
+template <int TPP, int NQ, bool VIR, bool EN>
 __global__ void __launch_bounds__(256, 5)
     k_pair(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
            const float4* __restrict__ posq, const uint32_t* __restrict__ head, const uint32_t* __restrict__ nn,
@@ -1407,7 +1412,7 @@ __global__ void __launch_bounds__(256, 5)
     const int2 ch = chunks[blockIdx.x];
     const SysDev S = sys[ch.x];
     const ParamSet& ps = psets[S.pset];
-    PairEval<NQ, VIR> ev{pc};
+    PairEval<NQ, VIR, EN> ev{pc};
     ev.rc2 = ps.rcut2;
     ev.irc = ps.inv_rcut;
     ev.irc2 = ps.inv_rcut * ps.inv_rcut;
@@ -1495,7 +1500,7 @@ __global__ void __launch_bounds__(256, 5)
 #pragma unroll
             for (int k = 0; k < 6; ++k) atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_WP + k], e[1 + k]);
         }
-    } else {
+    } else if (EN) {
         double e[1] = {sub == 0 ? 0.5 * (double)en : 0.0};
         block_sum_f64<1>(e, red);
         if (threadIdx.x == 0) atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_E], e[0]);
@@ -1707,11 +1712,11 @@ cudaError_t launch_fft(const LaunchArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-template <int TPP, bool VIR>
+template <int TPP, bool VIR, bool EN>
 static cudaError_t launch_pair_t(const LaunchArgs& a, cudaStream_t st) {
-#define ESPB_PAIR(NQ)                                                                                    \
-    k_pair<TPP, NQ, VIR><<<a.n_pchunks, 256, 0, st>>>(a.pchunks, a.sys, a.psets, a.posq, a.nl_head, a.nl_n, \
-                                                      a.nl_list, a.force, a.acc, a.accumulate, a.pc)
+#define ESPB_PAIR(NQ)                                                                                        \
+    k_pair<TPP, NQ, VIR, EN><<<a.n_pchunks, 256, 0, st>>>(a.pchunks, a.sys, a.psets, a.posq, a.nl_head, a.nl_n, \
+                                                          a.nl_list, a.force, a.acc, a.accumulate, a.pc)
     if (a.nq <= 8) ESPB_PAIR(8);
     else if (a.nq <= 10) ESPB_PAIR(10);
     else if (a.nq <= 11) ESPB_PAIR(11);
@@ -1730,18 +1735,27 @@ cudaError_t launch_pair(const LaunchArgs& a, cudaStream_t st) {
     if (a.n_pchunks == 0) return cudaSuccess;
     if (a.want_virial) {
         switch (a.tpp) {
-            case 4: return launch_pair_t<4, true>(a, st);
-            case 8: return launch_pair_t<8, true>(a, st);
-            case 16: return launch_pair_t<16, true>(a, st);
-            case 32: return launch_pair_t<32, true>(a, st);
+            case 4: return launch_pair_t<4, true, true>(a, st);
+            case 8: return launch_pair_t<8, true, true>(a, st);
+            case 16: return launch_pair_t<16, true, true>(a, st);
+            case 32: return launch_pair_t<32, true, true>(a, st);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    if (a.want_energy) {
+        switch (a.tpp) {
+            case 4: return launch_pair_t<4, false, true>(a, st);
+            case 8: return launch_pair_t<8, false, true>(a, st);
+            case 16: return launch_pair_t<16, false, true>(a, st);
+            case 32: return launch_pair_t<32, false, true>(a, st);
             default: return cudaErrorInvalidValue;
         }
     }
     switch (a.tpp) {
-        case 4: return launch_pair_t<4, false>(a, st);
-        case 8: return launch_pair_t<8, false>(a, st);
-        case 16: return launch_pair_t<16, false>(a, st);
-        case 32: return launch_pair_t<32, false>(a, st);
+        case 4: return launch_pair_t<4, false, false>(a, st);
+        case 8: return launch_pair_t<8, false, false>(a, st);
+        case 16: return launch_pair_t<16, false, false>(a, st);
+        case 32: return launch_pair_t<32, false, false>(a, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -75,6 +75,7 @@ struct LaunchArgs {
     double* virial = nullptr;
     int add_bg = 1;
     int want_virial = 1;
+    int want_energy = 1;  // pair energies; 0 only inside MD steps whose energies are overwritten
     int spread_mode = 0;  // 0: tensor-core spreading when E == 16; 1: CUDA-core kernels  // accumulate the pair virial (skipped when no virial is requested)
     int configure_only = 0;
     int nmax_x = FFT_MAX_N, nmax_y = FFT_MAX_N, nmax_z = FFT_MAX_N;  // longest line per axis  // set kernel attributes (plan time) instead of launching

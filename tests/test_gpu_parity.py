@@ -354,3 +354,37 @@ def test_md_graphs_follow_buffer_sets():
         for x, y in zip(got, ref):
             xa, ya = x.double().cpu().numpy(), y.double().cpu().numpy()
             assert np.abs(xa - ya).max() <= 1e-5 * max(np.abs(ya).max(), 1.0)
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_md_run_final_energy_is_full(use_graph):
+    """MD steps before the last skip the pair energies (the next step
+    overwrites them): the energy and per-particle energies that md_run leaves
+    equal a full evaluation at its final positions."""
+    sys_list = [systems.rocksalt(n, seed=950 + n) for n in (8, 12)]
+    N = [s.N for s in sys_list]
+    b = native.Batch(native.make_params(), N, [s.box for s in sys_list])
+    tot = sum(N)
+    p4 = np.zeros((tot, 4), np.float32)
+    p4[:, :3] = np.concatenate([s.pos for s in sys_list])
+    v4 = np.zeros((tot, 4), np.float32)
+    v4[:, :3] = np.concatenate([s.vel for s in sys_list])
+    v4[:, 3] = 1.0
+    pos, vel = torch.tensor(p4, device="cuda"), torch.tensor(v4, device="cuda")
+    q = torch.tensor(np.concatenate([s.q for s in sys_list]).astype(np.float32), device="cuda")
+    head = torch.zeros(tot, dtype=torch.int32, device="cuda")
+    nn = torch.zeros_like(head)
+    nl = torch.zeros(tot * 256, dtype=torch.int32, device="cuda")
+    f = torch.zeros((tot, 4), device="cuda")
+    e = torch.zeros(len(N), dtype=torch.float64, device="cuda")
+    b.build_nlist(pos, 3.4, 256, head, nn, nl)
+    b.compute(pos, q, f, e, None, nlist=(head, nn, nl), flags=ESP_ALL)
+    b.md_run(pos, vel, q, f, e, None, (head, nn, nl), 6, 0.002, use_graph=use_graph)
+    f2 = torch.zeros_like(f)
+    e2 = torch.zeros_like(e)
+    b.compute(pos, q, f2, e2, None, nlist=(head, nn, nl), flags=ESP_ALL)
+    torch.cuda.synchronize()
+    assert np.abs(e.cpu().numpy() - e2.cpu().numpy()).max() <= 1e-8 * np.abs(e2.cpu().numpy()).max()
+    a, c = f.cpu().numpy(), f2.cpu().numpy()
+    assert np.abs(a[:, 3] - c[:, 3]).max() <= 1e-5 * np.abs(c[:, 3]).max()
+    assert R.rel_rms(a[:, :3].astype(np.float64), c[:, :3].astype(np.float64)) <= 1e-6
