@@ -932,7 +932,7 @@ __global__ void k_fftx_inv(const int4* __restrict__ items, const SysDev* __restr
 // ----------------------------------------------------------------------------
 __device__ __forceinline__ int odd_up(int v) { return v | 1; }
 
-__global__ void __launch_bounds__(512)
+__global__ void __launch_bounds__(256)
     k_fft_plane_fwd(const int2* __restrict__ items, const SysDev* __restrict__ sys, const float2* __restrict__ tw,
                     const double* __restrict__ rho, float2* __restrict__ spec) {
     extern __shared__ float2 sb[];
@@ -970,7 +970,7 @@ __global__ void __launch_bounds__(512)
     }
 }
 
-__global__ void __launch_bounds__(512)
+__global__ void __launch_bounds__(256)
     k_fft_plane_inv(const int2* __restrict__ items, const SysDev* __restrict__ sys, const float2* __restrict__ tw,
                     const float2* __restrict__ spec, float* __restrict__ phi, double* __restrict__ rho) {
     extern __shared__ float2 sb[];
@@ -1025,7 +1025,7 @@ __global__ void __launch_bounds__(512)
 // z pass over a whole xz-slab (fixed y): forward, energy/virial (VIR: when
 // the virial is requested), influence multiply, inverse.
 template <bool VIR>
-__global__ void __launch_bounds__(512)
+__global__ void __launch_bounds__(256)
     k_fft_slab_z(const int2* __restrict__ items, const SysDev* __restrict__ sys, const float2* __restrict__ tw,
                  const float2* __restrict__ gtab, float2* __restrict__ spec, double* __restrict__ acc) {
     extern __shared__ float2 sb[];
@@ -1691,14 +1691,14 @@ cudaError_t launch_fft(const LaunchArgs& a, cudaStream_t st) {
             return e;
         return cudaFuncSetAttribute(k_fft_slab_z<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_MAX);
     }
-    if (a.n_pitems) k_fft_plane_fwd<<<a.n_pitems, 512, a.smem_plane, st>>>(a.pitems, a.sys, a.tw, a.rho, a.spec);
+    if (a.n_pitems) k_fft_plane_fwd<<<a.n_pitems, 256, a.smem_plane, st>>>(a.pitems, a.sys, a.tw, a.rho, a.spec);
     if (a.n_xitems) k_fftx_fwd<<<a.n_xitems, 256, smx, st>>>(a.xitems, a.sys, a.tw, a.rho, a.spec);
     if (a.n_yitems) k_ffty<false><<<a.n_yitems, 256, smy, st>>>(a.yitems, a.sys, a.tw, a.spec);
     if (a.n_sitems) {
         if (a.want_virial)
-            k_fft_slab_z<true><<<a.n_sitems, 512, a.smem_slab, st>>>(a.sitems, a.sys, a.tw, a.gtab, a.spec, a.acc);
+            k_fft_slab_z<true><<<a.n_sitems, 256, a.smem_slab, st>>>(a.sitems, a.sys, a.tw, a.gtab, a.spec, a.acc);
         else
-            k_fft_slab_z<false><<<a.n_sitems, 512, a.smem_slab, st>>>(a.sitems, a.sys, a.tw, a.gtab, a.spec, a.acc);
+            k_fft_slab_z<false><<<a.n_sitems, 256, a.smem_slab, st>>>(a.sitems, a.sys, a.tw, a.gtab, a.spec, a.acc);
     }
     if (a.n_zitems) {
         if (a.want_virial)
@@ -1708,7 +1708,7 @@ cudaError_t launch_fft(const LaunchArgs& a, cudaStream_t st) {
     }
     if (a.n_yitems) k_ffty<true><<<a.n_yitems, 256, smy, st>>>(a.yitems, a.sys, a.tw, a.spec);
     if (a.n_xitems) k_fftx_inv<<<a.n_xitems, 256, smx, st>>>(a.xitems, a.sys, a.tw, a.spec, a.phi, a.rho);
-    if (a.n_pitems) k_fft_plane_inv<<<a.n_pitems, 512, a.smem_plane, st>>>(a.pitems, a.sys, a.tw, a.spec, a.phi, a.rho);
+    if (a.n_pitems) k_fft_plane_inv<<<a.n_pitems, 256, a.smem_plane, st>>>(a.pitems, a.sys, a.tw, a.spec, a.phi, a.rho);
     return cudaGetLastError();
 }
 
