@@ -453,9 +453,10 @@ __global__ void __launch_bounds__(256)
 // weights times charge, y weights, z weights pre-split into TF32 parts), so
 // a k-step's A fragments are one product and split per element and its B
 // fragments are plain shared loads.
-// Every eight k-steps (64 particles) the FP32 block accumulators are
-// Kahan-merged into (sum, comp) registers; the tile is flushed with one
-// FP64 atomic per point.
+// Every eight k-steps (64 particles) the FP32 block accumulators are added
+// to FP64 sums in shared memory, 16 per lane and private to it (no barrier,
+// no atomic, no registers held); the tile is flushed with one FP64 atomic
+// per point.
 // ----------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t f2tf32(float x) {
     uint32_t r;
@@ -503,10 +504,13 @@ __global__ void __launch_bounds__(256, 3)
     float* wys = wxs + SPREAD_CHM * SPREAD_MS;
     uint32_t* wzh = reinterpret_cast<uint32_t*>(wys + SPREAD_CHM * SPREAD_MS);
     uint32_t* wzl = wzh + SPREAD_CHM * SPREAD_MS;
-    float* wc = reinterpret_cast<float*>(wzl + SPREAD_CHM * SPREAD_MS);  // [P][D+1]
+    // FP64 block sums, private to each lane: [warp][mt][nt][i][lane]
+    double* bsum = reinterpret_cast<double*>(wzl + SPREAD_CHM * SPREAD_MS);
+    float* wc = reinterpret_cast<float*>(bsum + 8 * 16 * 32);  // [P][D+1]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, tg = lane & 3;
     for (int i = tid; i < P * (D + 1); i += blockDim.x) wc[i] = ps.wcoef[(i / (D + 1)) * (MAX_D + 1) + (i % (D + 1))];
-    float acc[2][2][4], sum[2][2][4], cmp[2][2][4];
+    float acc[2][2][4];
+    double* mysum = bsum + warp * 16 * 32 + lane;  // element e at mysum[32 e]
 #pragma unroll
     for (int m = 0; m < 2; ++m)
 #pragma unroll
@@ -514,8 +518,7 @@ __global__ void __launch_bounds__(256, 3)
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 acc[m][n][i] = 0.f;
-                sum[m][n][i] = 0.f;
-                cmp[m][n][i] = 0.f;
+                mysum[32 * ((m * 2 + n) * 4 + i)] = 0.0;
             }
     int ksteps = 0;
     for (int base = 0; base < np; base += SPREAD_CHM) {
@@ -594,10 +597,7 @@ __global__ void __launch_bounds__(256, 3)
                     for (int n = 0; n < 2; ++n)
 #pragma unroll
                         for (int i = 0; i < 4; ++i) {
-                            const float y = __fsub_rn(acc[m][n][i], cmp[m][n][i]);
-                            const float ts = __fadd_rn(sum[m][n][i], y);
-                            cmp[m][n][i] = __fsub_rn(__fsub_rn(ts, sum[m][n][i]), y);
-                            sum[m][n][i] = ts;
+                            mysum[32 * ((m * 2 + n) * 4 + i)] += (double)acc[m][n][i];
                             acc[m][n][i] = 0.f;
                         }
             }
@@ -633,8 +633,7 @@ __global__ void __launch_bounds__(256, 3)
         for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                const float rest = acc[mt][nt][i] - cmp[mt][nt][i];
-                const double v = (double)sum[mt][nt][i] + (double)rest;
+                const double v = mysum[32 * ((mt * 2 + nt) * 4 + i)] + (double)acc[mt][nt][i];
                 if (v != 0.0) atomicAdd(rb + zo[nt][i & 1] + yo + xo[i >> 1], v);
             }
     }
@@ -1588,7 +1587,7 @@ static cudaError_t launch_spread_p(const LaunchArgs& a, cudaStream_t st) {
     const size_t NL = (size_t)nb * nb * nb * C::P3;
     const size_t smem = NL * sizeof(float2) + (size_t)C::CH * P * 4 * 4 + C::CH * 4 + P * (MAX_D + 1) * 4;
     const size_t smem_d = (size_t)SPREAD_CHD * 16 * 4 + (size_t)SPREAD_CHD * (2 * P + 1) * 4 + P * (MAX_D + 1) * 4;
-    const size_t smem_m = (size_t)SPREAD_CHM * SPREAD_MS * 4 * 4 + P * (MAX_D + 1) * 4;
+    const size_t smem_m = (size_t)SPREAD_CHM * SPREAD_MS * 4 * 4 + 8 * 16 * 32 * 8 + P * (MAX_D + 1) * 4;
     if (a.configure_only) {
         cudaError_t e = cudaFuncSetAttribute(k_spread_mma<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m);
         if (e != cudaSuccess) return e;
