@@ -70,10 +70,20 @@ __global__ void k_cell_sort(const uint32_t* __restrict__ start, const uint32_t* 
 constexpr int NL_THREADS = 64;
 constexpr int NL_STAGE = 1024;
 
+// store v at p when ok, as one predicated store (the candidate loop has no
+// per-candidate branch)
+__device__ __forceinline__ void store_if(bool ok, uint32_t* p, uint32_t v) {
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q st.global.u32 [%0], %1;\n\t}" ::"l"(p), "r"(v),
+        "r"((uint32_t)ok)
+        : "memory");
+}
+
+// Appends the staged candidates within rlist of pi to row (threads without a
+// particle carry a NaN position, which tests false against everything).
 template <bool MINIMG>
 __device__ __forceinline__ uint32_t nl_scan(const float4* __restrict__ cand, int n, float4 pi, int i, const SysDev& S,
-                                            float rlist2, uint32_t cap, uint32_t* __restrict__ row, uint32_t cnt,
-                                            bool active) {
+                                            float rlist2, uint32_t cap, uint32_t* __restrict__ row, uint32_t cnt) {
 #pragma unroll 4
     for (int k = 0; k < n; ++k) {
         const float4 pj = cand[k];
@@ -84,10 +94,9 @@ __device__ __forceinline__ uint32_t nl_scan(const float4* __restrict__ cand, int
             ddz -= S.Lz * rintf(ddz * S.inv_Lz);
         }
         const int j = __float_as_int(pj.w);
-        if (active && ddx * ddx + ddy * ddy + ddz * ddz < rlist2 && j != i) {
-            if (cnt < cap) row[cnt] = (uint32_t)(j - S.p_off);
-            ++cnt;
-        }
+        const bool hit = ddx * ddx + ddy * ddy + ddz * ddz < rlist2 && j != i;
+        store_if(hit && cnt < cap, row + cnt, (uint32_t)(j - S.p_off));
+        cnt += hit ? 1u : 0u;
     }
     return cnt;
 }
@@ -171,7 +180,7 @@ __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ ce
     for (uint32_t p0 = c0; p0 < c1; p0 += NL_THREADS) {
         const uint32_t slot = p0 + tid;
         const bool active = slot < c1;
-        const float4 pi = active ? cpos[slot] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+        const float4 pi = active ? cpos[slot] : make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, __int_as_float(-1));
         const int i = __float_as_int(pi.w);
         const long long hrow = (long long)C.nl_off + (long long)(i - S.p_off) * cap;
         uint32_t* row = nl + (active ? hrow : 0);
@@ -183,8 +192,8 @@ __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ ce
                 __syncthreads();
             }
             const int n = (int)min((uint32_t)NL_STAGE, total - base);
-            cnt = minimg ? nl_scan<true>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row, cnt, active)
-                         : nl_scan<false>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row, cnt, active);
+            cnt = minimg ? nl_scan<true>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row, cnt)
+                         : nl_scan<false>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row, cnt);
         }
         if (active) {
             head[i] = (uint32_t)hrow;
