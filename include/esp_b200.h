@@ -259,9 +259,13 @@ int esp_batch_lj_f64(esp_batch* b, void* stream, const double* pos4, const unsig
 /* nsteps velocity-Verlet steps of every system of the batch: per step
  * step1, a full evaluation (ESP_ALL) at the new positions into force4 /
  * energy / virial, step2. force4 must hold the forces of the current
- * positions on entry. With use_graph != 0 one step is captured in a CUDA
- * graph on first use (and whenever a pointer or dt changes) and replayed.
- * The neighbour list is used as given (no rebuild). */
+ * positions on entry. On return force4 (with per-particle energies in w),
+ * energy and virial are those of the final positions; the steps before the
+ * last, whose energies the next step overwrites, skip the pair energies.
+ * With use_graph != 0 one step is captured in a CUDA graph on first use
+ * (and whenever a pointer or dt changes; one graph per pointer set, a few
+ * sets kept) and replayed. The neighbour list is used as given (no
+ * rebuild). */
 int esp_batch_md_run(esp_batch* b, void* stream, float* pos4, float* vel4, const float* charge, const unsigned* head,
                      const unsigned* n_neigh, const unsigned* nlist, float* force4, double* energy, double* virial6,
                      int nsteps, double dt, int use_graph);
