@@ -714,7 +714,7 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ src, float2
             const int ts = k * stride;
 #pragma unroll
             for (int r = 1; r < R; ++r) {
-                float2 w = __ldg(&tw[ts * r]);
+                float2 w = tw[ts * r];
                 if (INV) w.y = -w.y;
                 v[r] = cmul(v[r], w);
             }
@@ -942,6 +942,10 @@ __global__ void __launch_bounds__(256)
     const int cap = max(nx * SBx, ny * SBy);
     float2* s0 = sb;
     float2* s1 = sb + cap;
+    float2* twx = sb + 2 * cap;  // twiddles of both axes, staged once
+    float2* twy = twx + nx;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) twx[i] = tw[S.twx + i];
+    for (int i = threadIdx.x; i < ny; i += blockDim.x) twy[i] = tw[S.twy + i];
     const double* src = rho + S.m_off + (long long)z * ny * nx;
     const Div16 dnx(nx), dnh(nxh);
     for (int idx = threadIdx.x; idx < np * nx; idx += blockDim.x) {
@@ -952,7 +956,7 @@ __global__ void __launch_bounds__(256)
         s0[i * SBx + b] = v;
     }
     __syncthreads();
-    float2* r = fft_lines<false>(s0, s1, nx, np, SBx, tw + S.twx, S.radx);
+    float2* r = fft_lines<false>(s0, s1, nx, np, SBx, twx, S.radx);
     float2* o = (r == s0) ? s1 : s0;
     for (int idx = threadIdx.x; idx < np * nxh; idx += blockDim.x) {
         const int b = dnh.div(idx), k = idx - b * nxh;
@@ -961,7 +965,7 @@ __global__ void __launch_bounds__(256)
         if (2 * b + 1 < ny) o[(2 * b + 1) * SBy + k] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
     }
     __syncthreads();
-    const float2* r2 = fft_lines<false>(o, r, ny, nxh, SBy, tw + S.twy, S.rady);
+    const float2* r2 = fft_lines<false>(o, r, ny, nxh, SBy, twy, S.rady);
     float2* dst = spec + S.s_off + (long long)z * ny * nxh;
     for (int idx = threadIdx.x; idx < ny * nxh; idx += blockDim.x) {
         const int y = dnh.div(idx), k = idx - y * nxh;
@@ -980,6 +984,10 @@ __global__ void __launch_bounds__(256)
     const int cap = max(nx * SBx, ny * SBy);
     float2* s0 = sb;
     float2* s1 = sb + cap;
+    float2* twx = sb + 2 * cap;  // twiddles of both axes, staged once
+    float2* twy = twx + nx;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) twx[i] = tw[S.twx + i];
+    for (int i = threadIdx.x; i < ny; i += blockDim.x) twy[i] = tw[S.twy + i];
     const float2* src = spec + S.s_off + (long long)z * ny * nxh;
     const Div16 dnx(nx), dnh(nxh);
     for (int idx = threadIdx.x; idx < ny * nxh; idx += blockDim.x) {
@@ -987,7 +995,7 @@ __global__ void __launch_bounds__(256)
         s0[y * SBy + k] = src[idx];
     }
     __syncthreads();
-    float2* r = fft_lines<true>(s0, s1, ny, nxh, SBy, tw + S.twy, S.rady);
+    float2* r = fft_lines<true>(s0, s1, ny, nxh, SBy, twy, S.rady);
     float2* o = (r == s0) ? s1 : s0;
     for (int idx = threadIdx.x; idx < np * nx; idx += blockDim.x) {
         const int b = dnx.div(idx), k = idx - b * nx;
@@ -1006,7 +1014,7 @@ __global__ void __launch_bounds__(256)
         o[k * SBx + b] = make_float2(A.x - Bv.y, A.y + Bv.x);
     }
     __syncthreads();
-    const float2* r2 = fft_lines<true>(o, r, nx, np, SBx, tw + S.twx, S.radx);
+    const float2* r2 = fft_lines<true>(o, r, nx, np, SBx, twx, S.radx);
     float* dst = phi + S.m_off + (long long)z * ny * nx;
     double* rz = rho + S.m_off + (long long)z * ny * nx;
     for (int idx = threadIdx.x; idx < np * nx; idx += blockDim.x) {
@@ -1034,6 +1042,8 @@ __global__ void __launch_bounds__(256)
     const int y = it.y, nz = S.nz, nxh = S.nxh, SBz = odd_up(nxh);
     float2* s0 = sb;
     float2* s1 = sb + nz * SBz;
+    float2* twz = sb + 2 * nz * SBz;  // twiddles, staged once
+    for (int i = threadIdx.x; i < nz; i += blockDim.x) twz[i] = tw[S.twz + i];
     const long long rowstride = (long long)S.ny * nxh;
     float2* base = spec + S.s_off + (long long)y * nxh;
     const float2* gbase = gtab + S.g_off + (long long)y * nxh;
@@ -1043,7 +1053,7 @@ __global__ void __launch_bounds__(256)
         s0[z * SBz + k] = base[z * rowstride + k];
     }
     __syncthreads();
-    float2* r = fft_lines<false>(s0, s1, nz, nxh, SBz, tw + S.twz, S.radz);
+    float2* r = fft_lines<false>(s0, s1, nz, nxh, SBz, twz, S.radz);
     float2* other = (r == s0) ? s1 : s0;
     const double twopi = 6.283185307179586;
     const int fy = (y < (S.ny + 1) / 2) ? y : y - S.ny;
@@ -1071,7 +1081,7 @@ __global__ void __launch_bounds__(256)
         d = make_float2(d.x * gb.x, d.y * gb.x);
     }
     __syncthreads();
-    const float2* o = fft_lines<true>(r, other, nz, nxh, SBz, tw + S.twz, S.radz);
+    const float2* o = fft_lines<true>(r, other, nz, nxh, SBz, twz, S.radz);
     for (int idx = threadIdx.x; idx < nz * nxh; idx += blockDim.x) {
         const int z = dnh.div(idx), k = idx - z * nxh;
         base[z * rowstride + k] = o[z * SBz + k];

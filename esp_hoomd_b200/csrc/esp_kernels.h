@@ -16,12 +16,13 @@ constexpr int FFT_SMEM_MAX = 220 * 1024;  // shared memory of the plane / slab F
 
 // shared memory (bytes) of the plane pass of an nx x ny plane and of the z
 // pass of an nz x nxh slab; line strides are rounded up to odd numbers
+// (two line buffers plus the twiddles of the transformed axes)
 inline int fft_plane_smem(int nx, int ny) {
     const int np = (ny + 1) / 2, nxh = nx / 2 + 1;
     const int c = std::max(nx * (np | 1), ny * (nxh | 1));
-    return 2 * c * 8;
+    return (2 * c + nx + ny) * 8;
 }
-inline int fft_slab_smem(int nx, int nz) { return 2 * nz * ((nx / 2 + 1) | 1) * 8; }
+inline int fft_slab_smem(int nx, int nz) { return (2 * nz * ((nx / 2 + 1) | 1) + nz) * 8; }
 
 // Split-polynomial coefficients of a batch, passed by value so the pair
 // kernel's FMAs read them from the kernel-parameter constant bank.
