@@ -1410,9 +1410,10 @@ struct PairEval {
 };
 
 // EN: pair energies (per particle and per system); without them the split
-// polynomial Q itself is not needed, only Q'.
+// polynomial Q itself is not needed, only Q', and the kernel (32 registers)
+// keeps 8 CTAs per SM resident so that more position gathers are in flight.
 template <int TPP, int NQ, bool VIR, bool EN>
-__global__ void __launch_bounds__(256, 5)
+__global__ void __launch_bounds__(256, EN ? 5 : 8)
     k_pair(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
            const float4* __restrict__ posq, const uint32_t* __restrict__ head, const uint32_t* __restrict__ nn,
            const uint32_t* __restrict__ nlist, float4* __restrict__ force, double* __restrict__ acc, int accumulate,
