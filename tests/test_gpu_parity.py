@@ -388,3 +388,66 @@ def test_md_run_final_energy_is_full(use_graph):
     a, c = f.cpu().numpy(), f2.cpu().numpy()
     assert np.abs(a[:, 3] - c[:, 3]).max() <= 1e-5 * np.abs(c[:, 3]).max()
     assert R.rel_rms(a[:, :3].astype(np.float64), c[:, :3].astype(np.float64)) <= 1e-6
+
+
+def test_empty_system_in_batch():
+    """A system with no particles in the middle of a batch: zero energy and
+    virial, and its neighbours in the batch get the same results as alone."""
+    a, c = systems.rocksalt(8, seed=971), systems.rocksalt(10, seed=972)
+    N = [a.N, 0, c.N]
+    boxes = [a.box, (10.0, 10.0, 10.0), c.box]
+    b = native.Batch(native.make_params(), N, boxes)
+    tot = a.N + c.N
+    p4 = np.zeros((tot, 4), np.float32)
+    p4[:, :3] = np.concatenate([a.pos, c.pos])
+    pos = torch.tensor(p4, device="cuda")
+    q = torch.tensor(np.concatenate([a.q, c.q]).astype(np.float32), device="cuda")
+    head = torch.zeros(tot, dtype=torch.int32, device="cuda")
+    nn = torch.zeros_like(head)
+    nl = torch.zeros(tot * 256, dtype=torch.int32, device="cuda")
+    b.build_nlist(pos, 3.4, 256, head, nn, nl)
+    f = torch.zeros((tot, 4), device="cuda")
+    e = torch.zeros(3, dtype=torch.float64, device="cuda")
+    w = torch.zeros(18, dtype=torch.float64, device="cuda")
+    b.compute(pos, q, f, e, w, nlist=(head, nn, nl), flags=ESP_ALL)
+    torch.cuda.synchronize()
+    assert e[1].item() == 0.0 and np.all(w[6:12].cpu().numpy() == 0.0)
+    fb = f.cpu().numpy()
+    for k, (s, lo) in enumerate(((a, 0), (c, a.N))):
+        b1 = native.Batch(native.make_params(), [s.N], [s.box])
+        p1 = pos[lo:lo + s.N].contiguous()
+        h1 = torch.zeros(s.N, dtype=torch.int32, device="cuda")
+        n1 = torch.zeros_like(h1)
+        l1 = torch.zeros(s.N * 256, dtype=torch.int32, device="cuda")
+        b1.build_nlist(p1, 3.4, 256, h1, n1, l1)
+        f1 = torch.zeros((s.N, 4), device="cuda")
+        e1 = torch.zeros(1, dtype=torch.float64, device="cuda")
+        b1.compute(p1, q[lo:lo + s.N].contiguous(), f1, e1, None, nlist=(h1, n1, l1), flags=ESP_ALL)
+        torch.cuda.synchronize()
+        fa = f1.cpu().numpy()
+        assert np.abs(fa - fb[lo:lo + s.N]).max() <= 1e-6 * np.abs(fa).max()
+        assert abs(e1.item() - e[2 * k].item()) <= 1e-8 * abs(e1.item())
+
+
+def test_nlist_row_overflow_is_reported():
+    """Rows longer than the capacity fail with ESP_ERR_OVERFLOW; n_neigh then
+    holds the counts the caller needs, and rows keep their first cap entries."""
+    s = systems.rocksalt(12, seed=973)
+    b = native.Batch(native.make_params(), [s.N], [s.box])
+    p4 = np.zeros((s.N, 4), np.float32)
+    p4[:, :3] = s.pos
+    pos = torch.tensor(p4, device="cuda")
+    cap = 64
+    head = torch.zeros(s.N, dtype=torch.int32, device="cuda")
+    nn = torch.zeros_like(head)
+    nl = torch.zeros(s.N * cap, dtype=torch.int32, device="cuda")
+    with pytest.raises(EspError) as ei:
+        b.build_nlist(pos, 3.4, cap, head, nn, nl)
+    assert ei.value.code == -5
+    rh, rc, rl = R.neighbor_list(s.pos.astype(np.float32).astype(np.float64), s.box, 3.4)
+    c = nn.cpu().numpy()
+    assert np.array_equal(c, rc.astype(np.int32))
+    h, l = head.cpu().numpy(), nl.cpu().numpy()
+    for i in range(0, s.N, 97):
+        row = set(l[h[i]:h[i] + cap].tolist())
+        assert row <= set(rl[rh[i]:rh[i] + rc[i]].tolist())
