@@ -452,7 +452,8 @@ __global__ void __launch_bounds__(256)
 // rows, zero outside its stencil and already shifted to its origin (x
 // weights times charge, y weights, z weights pre-split into TF32 parts), so
 // a k-step's A fragments are one product and split per element and its B
-// fragments are plain shared loads.
+// fragments are plain shared loads. The next chunk's particle records are
+// prefetched into shared memory (cp.async) while the current chunk runs.
 // Every eight k-steps (64 particles) the FP32 block accumulators are added
 // to FP64 sums in shared memory, 16 per lane and private to it (no barrier,
 // no atomic, no registers held); the tile is flushed with one FP64 atomic
@@ -506,7 +507,10 @@ __global__ void __launch_bounds__(256, 3)
     uint32_t* wzl = wzh + SPREAD_CHM * SPREAD_MS;
     // FP64 block sums, private to each lane: [warp][mt][nt][i][lane]
     double* bsum = reinterpret_cast<double*>(wzl + SPREAD_CHM * SPREAD_MS);
-    float* wc = reinterpret_cast<float*>(bsum + 8 * 16 * 32);  // [P][D+1]
+    // particle records of the current and the next chunk (prefetched)
+    float4* crec = reinterpret_cast<float4*>(bsum + 8 * 16 * 32);  // [2][CHM]
+    uint32_t* crel = reinterpret_cast<uint32_t*>(crec + 2 * SPREAD_CHM);  // [2][CHM]
+    float* wc = reinterpret_cast<float*>(crel + 2 * SPREAD_CHM);  // [P][D+1]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, tg = lane & 3;
     for (int i = tid; i < P * (D + 1); i += blockDim.x) wc[i] = ps.wcoef[(i / (D + 1)) * (MAX_D + 1) + (i % (D + 1))];
     float acc[2][2][4];
@@ -521,10 +525,24 @@ __global__ void __launch_bounds__(256, 3)
                 mysum[32 * ((m * 2 + n) * 4 + i)] = 0.0;
             }
     int ksteps = 0;
-    for (int base = 0; base < np; base += SPREAD_CHM) {
+    auto prefetch = [&](int base, int buf) {
+        const int n = min(SPREAD_CHM, np - base);
+        if (tid < n) {
+            const uint32_t d1 = (uint32_t)__cvta_generic_to_shared(&crec[buf * SPREAD_CHM + tid]);
+            const uint32_t d2 = (uint32_t)__cvta_generic_to_shared(&crel[buf * SPREAD_CHM + tid]);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d1), "l"(srec + s0 + base + tid));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d2), "l"(srel + s0 + base + tid));
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+    prefetch(0, 0);
+    for (int base = 0, cb = 0; base < np; base += SPREAD_CHM, cb ^= 1) {
         const int nc = min(SPREAD_CHM, np - base);
         const int ncp = (nc + 7) & ~7;  // padded to whole k-steps (zero weights)
-        __syncthreads();
+        __syncthreads();  // previous chunk consumed (weights and records)
+        if (base + SPREAD_CHM < np) prefetch(base + SPREAD_CHM, cb ^ 1);
+        else asm volatile("cp.async.commit_group;\n" ::);
+        asm volatile("cp.async.wait_group 1;\n" ::);  // this chunk's records have landed
         for (int k = tid; k < ncp * SPREAD_MS / 4; k += blockDim.x) {
             const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
             reinterpret_cast<float4*>(wxs)[k] = z;
@@ -542,8 +560,8 @@ __global__ void __launch_bounds__(256, 3)
                 if (D == DD) sp.load(&wc[a * (D + 1)]);
                 for (int j = j0; j < nc * 3; j += nla) {
                     const int p = j / 3, ax = j - 3 * p;
-                    const float4 rec = srec[s0 + base + p];
-                    const int o = (int)((srel[s0 + base + p] >> (8 * ax)) & 255u);
+                    const float4 rec = crec[cb * SPREAD_CHM + p];
+                    const int o = (int)((crel[cb * SPREAD_CHM + p] >> (8 * ax)) & 255u);
                     const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
                     const float w = D == DD ? sp.w(tt) : horner_w(&wc[a * (D + 1)], D, tt);
                     const int k = p * SPREAD_MS + o + a;
@@ -1598,7 +1616,8 @@ static cudaError_t launch_spread_p(const LaunchArgs& a, cudaStream_t st) {
     const size_t NL = (size_t)nb * nb * nb * C::P3;
     const size_t smem = NL * sizeof(float2) + (size_t)C::CH * P * 4 * 4 + C::CH * 4 + P * (MAX_D + 1) * 4;
     const size_t smem_d = (size_t)SPREAD_CHD * 16 * 4 + (size_t)SPREAD_CHD * (2 * P + 1) * 4 + P * (MAX_D + 1) * 4;
-    const size_t smem_m = (size_t)SPREAD_CHM * SPREAD_MS * 4 * 4 + 8 * 16 * 32 * 8 + P * (MAX_D + 1) * 4;
+    const size_t smem_m =
+        (size_t)SPREAD_CHM * SPREAD_MS * 4 * 4 + 8 * 16 * 32 * 8 + 2 * SPREAD_CHM * 20 + P * (MAX_D + 1) * 4;
     if (a.configure_only) {
         cudaError_t e = cudaFuncSetAttribute(k_spread_mma<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m);
         if (e != cudaSuccess) return e;
