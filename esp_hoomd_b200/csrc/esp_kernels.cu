@@ -1169,6 +1169,8 @@ __global__ void k_influence(SysDev S, const double* __restrict__ w1d, const doub
 // threads). A group of G lanes serves one particle: lane c owns stencil
 // plane z = oz + c and contracts it separably (x, then y) in registers;
 // the group sums its four partials (potential, gradient) with shuffles.
+// Each chunk's particle records and output slots are prefetched into shared
+// memory (cp.async) while the previous chunk is interpolated.
 // ============================================================================
 // words of the interpolation staging area: the per-chunk weights, or (before
 // the first chunk) the wrapped row offsets, shared row offsets and x
@@ -1202,7 +1204,12 @@ __global__ void __launch_bounds__(128)
     const SysDev S = sys[si];
     const ParamSet& ps = psets[S.pset];
     const int E = T + P - 1;
-    float* sm = reinterpret_cast<float*>(sm4);     // [E*PP] potential
+    // particle records (position/t, origin, output slot) of the current and
+    // the next chunk: the next chunk's are prefetched while this one runs
+    float4* crec = sm4;                                                     // [2][CH]
+    uint32_t* crel = reinterpret_cast<uint32_t*>(crec + 2 * C::CH);         // [2][CH]
+    uint32_t* cprm = crel + 2 * C::CH;                                      // [2][CH]
+    float* sm = reinterpret_cast<float*>(cprm + 2 * C::CH);  // [E*PP] potential
     float* wts = sm + E * PP;                      // [CH][6P] wx dwx wy dwy wz dwz (index tables first)
     float* qv = wts + interp_stage_words(P, C::CH, E);  // [CH] charges
     int* org = reinterpret_cast<int*>(qv + C::CH); // [CH] packed origins
@@ -1247,17 +1254,31 @@ __global__ void __launch_bounds__(128)
                              "l"(base + rowo[r] + xs[X]));
         }
         asm volatile("cp.async.commit_group;\n" ::);
-        asm volatile("cp.async.wait_group 0;\n" ::);
     }
+    auto prefetch = [&](int base, int buf) {
+        const int n = min(C::CH, np - base);
+        for (int p = threadIdx.x; p < n; p += blockDim.x) {
+            const uint32_t d1 = (uint32_t)__cvta_generic_to_shared(&crec[buf * C::CH + p]);
+            const uint32_t d2 = (uint32_t)__cvta_generic_to_shared(&crel[buf * C::CH + p]);
+            const uint32_t d3 = (uint32_t)__cvta_generic_to_shared(&cprm[buf * C::CH + p]);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d1), "l"(srec + s0 + base + p));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d2), "l"(srel + s0 + base + p));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d3), "l"(perm + s0 + base + p));
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+    prefetch(0, 0);
+    asm volatile("cp.async.wait_group 0;\n" ::);  // region and first chunk
     for (int i = threadIdx.x; i < P * (D + 1); i += blockDim.x)
         wc[i] = ps.wcoef[(i / (D + 1)) * (MAX_D + 1) + (i % (D + 1))];
     const int grp = threadIdx.x / C::G, gl = threadIdx.x % C::G;
     const float gxs = (float)S.gxd, gys = (float)S.gyd, gzs = (float)S.gzd;
     const double self_coef = ps.self_coef;
     double esum = 0.0;
-    for (int base = 0; base < np; base += C::CH) {
+    for (int base = 0, cb = 0; base < np; base += C::CH, cb ^= 1) {
         const int nc = min(C::CH, np - base);
-        __syncthreads();  // region / coefficients staged; previous chunk consumed
+        __syncthreads();  // region / coefficients / records staged; previous chunk consumed
+        if (base + C::CH < np) prefetch(base + C::CH, cb ^ 1);
         {
             // thread (a, j0) evaluates window segment a (value and derivative)
             constexpr int DD = default_window_degree<P>();
@@ -1267,7 +1288,7 @@ __global__ void __launch_bounds__(128)
                 if (D == DD) sp.load(&wc[a2 * (D + 1)]);
                 for (int j = j0; j < nc * 3; j += nla) {
                     const int p = j / 3, ax = j - 3 * p;
-                    const float4 rec = srec[s0 + base + p];
+                    const float4 rec = crec[cb * C::CH + p];
                     const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
                     float w, dw;
                     if (D == DD) {
@@ -1282,8 +1303,8 @@ __global__ void __launch_bounds__(128)
                 }
             }
             for (int p = threadIdx.x; p < nc; p += blockDim.x) {
-                qv[p] = srec[s0 + base + p].w;
-                org[p] = (int)srel[s0 + base + p];
+                qv[p] = crec[cb * C::CH + p].w;
+                org[p] = (int)crel[cb * C::CH + p];
             }
         }
         __syncthreads();
@@ -1363,10 +1384,11 @@ __global__ void __launch_bounds__(128)
             if (qq < nc && gl == 0) {
                 const float q = qv[p];
                 const double e_i = 0.5 * (double)q * pot + self_coef * (double)q * q;
-                force[perm[s0 + base + p]] = make_float4(q * gxs * gx, q * gys * gy, q * gzs * gz, (float)e_i);
+                force[cprm[cb * C::CH + p]] = make_float4(q * gxs * gx, q * gys * gy, q * gzs * gz, (float)e_i);
                 esum += e_i;
             }
         }
+        asm volatile("cp.async.wait_group 0;\n" ::);  // next chunk's records (made visible by the top barrier)
     }
     double ev[1] = {esum};
     block_sum_f64<1>(ev, red);
@@ -1642,7 +1664,8 @@ template <int P>
 static cudaError_t launch_interp_p(const LaunchArgs& a, cudaStream_t st) {
     using C = InterpCfg<P>;
     const int E = a.T + P - 1;
-    const size_t smem = ((size_t)E * a.PP + interp_stage_words(P, C::CH, E) + 3 * C::CH + P * (MAX_D + 1)) * 4;
+    const size_t smem =
+        ((size_t)E * a.PP + interp_stage_words(P, C::CH, E) + 3 * C::CH + P * (MAX_D + 1)) * 4 + 2 * C::CH * 24;
     if (a.configure_only)
         return cudaFuncSetAttribute(k_interp<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (a.n_tiles == 0) return cudaSuccess;
