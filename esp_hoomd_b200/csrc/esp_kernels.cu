@@ -1450,10 +1450,12 @@ struct PairEval {
 };
 
 // EN: pair energies (per particle and per system); without them the split
-// polynomial Q itself is not needed, only Q', and the kernel (32 registers)
-// keeps 8 CTAs per SM resident so that more position gathers are in flight.
+// polynomial Q itself is not needed, only Q', and the kernel (40 registers)
+// keeps 6 CTAs per SM resident so that more position gathers are in flight.
+// Each lane loads its next 16-byte row segment of neighbour indices one
+// iteration ahead of the gathers that use it.
 template <int TPP, int NQ, bool VIR, bool EN>
-__global__ void __launch_bounds__(256, EN ? 5 : 8)
+__global__ void __launch_bounds__(256, EN ? 5 : 6)
     k_pair(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
            const float4* __restrict__ posq, const uint32_t* __restrict__ head, const uint32_t* __restrict__ nn,
            const uint32_t* __restrict__ nlist, float4* __restrict__ force, double* __restrict__ acc, int accumulate,
@@ -1497,8 +1499,10 @@ __global__ void __launch_bounds__(256, EN ? 5 : 8)
             const uint4* row = reinterpret_cast<const uint4*>(nlist + h);
             const uint32_t n4 = n >> 2;
             if (interior) {
+                uint4 jn = sub < n4 ? __ldg(&row[sub]) : make_uint4(0u, 0u, 0u, 0u);
                 for (uint32_t k4 = sub; k4 < n4; k4 += TPP) {
-                    const uint4 jj = __ldg(&row[k4]);
+                    const uint4 jj = jn;  // this row segment; the next one is loaded ahead
+                    if (k4 + TPP < n4) jn = __ldg(&row[k4 + TPP]);
                     const float4 p0 = __ldg(&posq[po + (int)jj.x]);
                     const float4 p1 = __ldg(&posq[po + (int)jj.y]);
                     const float4 p2 = __ldg(&posq[po + (int)jj.z]);
@@ -1509,8 +1513,10 @@ __global__ void __launch_bounds__(256, EN ? 5 : 8)
                     ev.template pair<false>(pi, p3);
                 }
             } else {
+                uint4 jn = sub < n4 ? __ldg(&row[sub]) : make_uint4(0u, 0u, 0u, 0u);
                 for (uint32_t k4 = sub; k4 < n4; k4 += TPP) {
-                    const uint4 jj = __ldg(&row[k4]);
+                    const uint4 jj = jn;
+                    if (k4 + TPP < n4) jn = __ldg(&row[k4 + TPP]);
                     const float4 p0 = __ldg(&posq[po + (int)jj.x]);
                     const float4 p1 = __ldg(&posq[po + (int)jj.y]);
                     const float4 p2 = __ldg(&posq[po + (int)jj.z]);
