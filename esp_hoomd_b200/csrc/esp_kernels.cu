@@ -180,19 +180,31 @@ __global__ void k_tile_sort(const uint32_t* __restrict__ start, const uint32_t* 
                             uint32_t* __restrict__ perm, const float4* __restrict__ trec,
                             const uint32_t* __restrict__ rel, float4* __restrict__ srec,
                             uint32_t* __restrict__ srel) {
-    __shared__ uint32_t sm[SORT_CAP];
+    __shared__ __align__(16) uint32_t sm[SORT_CAP];
     const uint32_t s0 = start[blockIdx.x];
     const uint32_t n = start[blockIdx.x + 1] - s0;
     if (n == 0) return;
     const bool cached = n <= (uint32_t)SORT_CAP;
-    if (cached)
+    const uint32_t n4 = (n + 3u) >> 2;
+    if (cached) {
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sm[i] = perm_u[s0 + i];
+        // pad to whole 16-byte groups with a value no index is above
+        if (threadIdx.x < 4u * n4 - n) sm[n + threadIdx.x] = 0xffffffffu;
+    }
     __syncthreads();
     const uint32_t* src = cached ? sm : perm_u + s0;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         const uint32_t v = src[i];
         uint32_t r = 0;
-        for (uint32_t j = 0; j < n; ++j) r += (src[j] < v) ? 1u : 0u;
+        if (cached) {
+            // rank = number of smaller indices, four per shared load
+            for (uint32_t j = 0; j < n4; ++j) {
+                const uint4 u = reinterpret_cast<const uint4*>(sm)[j];
+                r += (u.x < v ? 1u : 0u) + (u.y < v ? 1u : 0u) + (u.z < v ? 1u : 0u) + (u.w < v ? 1u : 0u);
+            }
+        } else {
+            for (uint32_t j = 0; j < n; ++j) r += (src[j] < v) ? 1u : 0u;
+        }
         perm[s0 + r] = v;
         srec[s0 + r] = trec[v];
         srel[s0 + r] = rel[v];
