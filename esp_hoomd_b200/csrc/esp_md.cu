@@ -42,19 +42,31 @@ __global__ void k_cell_bin(const int2* __restrict__ chunks, const SysDev* __rest
 // cell-sorted positions.
 __global__ void k_cell_sort(const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm_u,
                             const float4* __restrict__ wpos, float4* __restrict__ cpos) {
-    __shared__ uint32_t sm[1024];
+    __shared__ __align__(16) uint32_t sm[1024];
     const uint32_t s0 = start[blockIdx.x];
     const uint32_t n = start[blockIdx.x + 1] - s0;
     if (n == 0) return;
     const bool cached = n <= 1024u;
-    if (cached)
+    const uint32_t n4 = (n + 3u) >> 2;
+    if (cached) {
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sm[i] = perm_u[s0 + i];
+        // pad to whole 16-byte groups with a value no index is above
+        if (threadIdx.x < 4u * n4 - n) sm[n + threadIdx.x] = 0xffffffffu;
+    }
     __syncthreads();
     const uint32_t* src = cached ? sm : perm_u + s0;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         const uint32_t v = src[i];
         uint32_t r = 0;
-        for (uint32_t j = 0; j < n; ++j) r += (src[j] < v) ? 1u : 0u;
+        if (cached) {
+            // rank = number of smaller indices, four per shared load
+            for (uint32_t j = 0; j < n4; ++j) {
+                const uint4 u = reinterpret_cast<const uint4*>(sm)[j];
+                r += (u.x < v ? 1u : 0u) + (u.y < v ? 1u : 0u) + (u.z < v ? 1u : 0u) + (u.w < v ? 1u : 0u);
+            }
+        } else {
+            for (uint32_t j = 0; j < n; ++j) r += (src[j] < v) ? 1u : 0u;
+        }
         cpos[s0 + r] = wpos[v];
     }
 }
