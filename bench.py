@@ -208,6 +208,74 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- checker and comparison legs
+def accuracy_leg(b, sl, pos_h, q, nlist, dev):
+    """The metric's accuracy bar, measured on the timed workload: one
+    evaluation of the timed plan (same Batch, same shared split) at the
+    batch's initial positions, and the forces and energies of its smallest,
+    a middle (n = 24) and its largest member against FP64 Ewald (the
+    oracle's workload-size sum, run as the checker after the timed regions)."""
+    import torch
+    from oracle.ewald_torch import ewald_torch
+    head, nn, nl = nlist
+    tot = pos_h.shape[0]
+    pos = torch.tensor(pos_h, device=dev)
+    b.build_nlist(pos, RCUT + SKIN, CAP, head, nn, nl)
+    force = torch.zeros((tot, 4), device=dev)
+    energy = torch.zeros(len(sl), dtype=torch.float64, device=dev)
+    b.compute(pos, q, force, energy, None, nlist=(head, nn, nl))
+    torch.cuda.synchronize(dev)
+    f = force.double().cpu().numpy()
+    e = energy.cpu().numpy()
+    ns = [round(s.N ** (1.0 / 3.0)) for s in sl]
+    off = np.concatenate([[0], np.cumsum([s.N for s in sl])])
+    picks = sorted({ns.index(min(ns)), ns.index(max(ns))} | ({ns.index(24)} if 24 in ns else set()))
+    rows = []
+    for i in picks:
+        p = pos_h[off[i]:off[i + 1], :3].astype(np.float64)
+        E0, F0, _ = ewald_torch(p, sl[i].q, sl[i].box, device=dev)
+        fi = f[off[i]:off[i + 1], :3]
+        rows.append({"system": int(i), "n": int(ns[i]), "N": int(sl[i].N),
+                     "mesh": b.info(i)["nx"], "force_rel_rms": float(np.sqrt(((fi - F0) ** 2).sum() / (F0 ** 2).sum())),
+                     "energy_rel": float(abs(e[i] - E0) / abs(E0))})
+    return {"reference": "FP64 Ewald (oracle/ewald_torch.py, truncation ~1e-11), same positions",
+            "split_c": b.info(0)["c_split"], "systems": rows,
+            "force_rel_rms": max(r["force_rel_rms"] for r in rows),
+            "energy_rel": max(r["energy_rel"] for r in rows)}
+
+
+def cufft_leg(b, nsys, dev, reps=5):
+    """cuFFT (through torch.fft) on the batch's meshes, timed only as a
+    comparison with the hand-written passes: per mesh size class one batched
+    R2C, the influence multiply, one batched C2R -- the FFT stage's work."""
+    import torch
+    from collections import Counter
+    sizes = Counter((b.info(i)["nx"], b.info(i)["ny"], b.info(i)["nz"]) for i in range(nsys))
+    bufs = []
+    for (nx, ny, nz), c in sorted(sizes.items()):
+        x = torch.randn((c, nz, ny, nx), device=dev)
+        g = torch.rand((nz, ny, nx // 2 + 1), device=dev)
+        bufs.append((x, g, (nz, ny, nx)))
+
+    def run():
+        for x, g, s in bufs:
+            y = torch.fft.rfftn(x, dim=(1, 2, 3))
+            y *= g
+            torch.fft.irfftn(y, s=s, dim=(1, 2, 3), out=x)
+
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize(dev)
+    st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st.record()
+    for _ in range(reps):
+        run()
+    en.record()
+    torch.cuda.synchronize(dev)
+    return {"cufft_ms": st.elapsed_time(en) / reps, "size_classes": len(bufs),
+            "desc": "torch.fft (cuFFT) batched rfftn + multiply + irfftn per mesh size class, FP32"}
+
+
 # ----------------------------------------------------------------------------- serving
 SERVE_BUDGET = 64 << 30
 SERVE_STEPS = 10
@@ -573,6 +641,10 @@ def run_ours(args):
                 "autotune": tuned,
                 "gpu_launches": int(args.steps * (K_NLIST + k_eval + MD_STEPS * (k_eval + K_NVE))),
                 "clocks": clk.summary()}
+        line["fft"] = {"ours_ms": stage_ms.get("fft")}
+        line["fft"].update(cufft_leg(b, N.size, dev))
+        if not args.no_accuracy:
+            line["accuracy"] = accuracy_leg(b, sl, pos_h, q, (head, nn, nl), dev)
         if not args.no_cpu:
             from oracle import esp_port as EP
             threads = EP.max_threads()
@@ -612,6 +684,7 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the FP64 Ewald check of the timed plan")
     ap.add_argument("--systems", type=int, default=N_SYS,
                     help="evaluate only the first S systems of the batch (small cases for profiling)")
     ap.add_argument("--workload", default="batched256", choices=["batched256", "scaleup"],

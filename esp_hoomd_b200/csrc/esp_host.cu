@@ -1461,15 +1461,39 @@ static __device__ __align__(256) unsigned char g_na_scratch[NA_BYTES];
 constexpr int NA_MAX_DEVICES = 64;
 std::mutex g_na_mutex;
 unsigned char* g_na_base[NA_MAX_DEVICES] = {};
+void* g_na_ctx[NA_MAX_DEVICES] = {};
 
-// One-time set-up per device, with that device current: the scratch
-// array's device address and the spreading kernels' shared-memory limits.
+// The driver context current on this thread (cuCtxGetCurrent through the
+// runtime's driver entry point, so the library needs no link to libcuda).
+void* na_current_context() {
+    typedef int (*GetCurrent)(void**);
+    static GetCurrent fn = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<GetCurrent>(f);
+        looked_up = true;
+    }
+    void* ctx = nullptr;
+    if (fn) fn(&ctx);
+    return ctx;
+}
+
+// Set-up per device, with that device current: the scratch array's device
+// address and the spreading kernels' shared-memory limits. Done on the first
+// call on a device, and again when the device's context has changed since
+// (after cudaDeviceReset the old address is no longer valid).
 int na_setup(unsigned char** base) {
     int dev = 0;
     ESPB_CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= NA_MAX_DEVICES) return fail(ESP_ERR_UNSUPPORTED, "device index above 63");
+    ESPB_CK(cudaSetDevice(dev));  // makes the device's primary context current
+    void* ctx = na_current_context();
     std::lock_guard<std::mutex> lock(g_na_mutex);
-    if (!g_na_base[dev]) {
+    if (!g_na_base[dev] || g_na_ctx[dev] != ctx) {
         void* ptr = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&ptr, g_na_scratch);
         if (e != cudaSuccess || !ptr)
@@ -1483,6 +1507,7 @@ int na_setup(unsigned char** base) {
             ESPB_CK(launch_spread(a, 0));
         }
         g_na_base[dev] = static_cast<unsigned char*>(ptr);
+        g_na_ctx[dev] = ctx;
     }
     *base = g_na_base[dev];
     return 0;
@@ -1541,6 +1566,8 @@ extern "C" int esp_spread_noalloc(void* stream, const esp_params* p, double Lx, 
                                              " particles (esp_spread has no such limit)");
     const int P = p->order;
     if (P < 2 || P > MAX_P) return fail(ESP_ERR_UNSUPPORTED, "order must be in [2, 12]");
+    if (p->precision != ESP_FP32 && p->precision != ESP_FP64)
+        return fail(ESP_ERR_INVALID, "precision must be ESP_FP32 or ESP_FP64");
     const double L[3] = {Lx, Ly, Lz};
     const int n[3] = {p->nx, p->ny, p->nz};
     int T = p->tile > 0 ? p->tile : 17 - P;
@@ -1558,7 +1585,10 @@ extern "C" int esp_spread_noalloc(void* stream, const esp_params* p, double Lx, 
         return fail(ESP_ERR_UNSUPPORTED, "esp_spread_noalloc: " + std::to_string(n_tiles) +
                                              " tiles exceed its fixed scratch limit of " +
                                              std::to_string(NA_MAX_TILES));
-    const int D = p->window_degree > 0 ? p->window_degree : default_window_degree(P);
+    // the window of esp_create for the same parameters (FP64 contexts fit it
+    // to a higher degree); the spreading itself runs the FP32 kernels
+    const int D = p->window_degree > 0 ? p->window_degree
+                                       : (p->precision == ESP_FP64 ? std::max(P + 2, 9) : default_window_degree(P));
     if (D > MAX_D) return fail(ESP_ERR_UNSUPPORTED, "window degree must be <= 15");
     if (p->window_c < 0) return fail(ESP_ERR_INVALID, "window_c must be >= 0");
     const double cw = p->window_c > 0 ? p->window_c : 2.2 * P;

@@ -161,12 +161,16 @@ int esp_get_potential(const esp_ctx* ctx, void* stream, float* phi);
  *  - Limits: 1 <= N <= ESP_SPREAD_NOALLOC_MAX_N particles and at most
  *    ESP_SPREAD_NOALLOC_MAX_TILES tiles; larger inputs are rejected with
  *    ESP_ERR_UNSUPPORTED (use esp_spread for them).
- *  - Parameters: p->order, p->window_c, p->window_degree and p->tile as in
- *    esp_create; the mesh p->nx, p->ny, p->nz must be given (no automatic
- *    choice), each in [max(order, 4), 256]; tile + order - 1 <= 16.
+ *  - Parameters: p->order, p->window_c, p->window_degree, p->tile and
+ *    p->precision (ESP_FP32 or ESP_FP64; it selects the default window
+ *    degree, as in esp_create) as in esp_create; the mesh p->nx, p->ny, p->nz
+ *    must be given (no automatic choice), each in [max(order, 4), 256];
+ *    tile + order - 1 <= 16.
  *  - The first call on a device (per device, with that device current) looks
  *    up the scratch array's device address and sets the spreading kernels'
  *    shared-memory limits; make that first call before any stream capture.
+ *    The set-up is redone when the device's context changes (for example
+ *    after cudaDeviceReset), on the next call.
  *  - Every call on a device shares the one scratch array: calls whose work
  *    overlaps on the GPU (different streams, or different host threads,
  *    without ordering between them) race and give wrong meshes. Calls

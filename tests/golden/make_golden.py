@@ -1,7 +1,8 @@
 """Regenerate the committed golden fixtures from the reference.
 
 Run from the repository root in a checkout that has the reference sources
-(default /root/reference, override with ESP_REF):
+(the directory ``reference`` beside the repository root by default,
+override with ESP_REF):
 
     make -C oracle ref          # builds oracle/_ref/libpswf_ref.so
     python tests/golden/make_golden.py
@@ -28,7 +29,7 @@ sys.path.insert(0, ROOT)
 
 from esp_hoomd_b200.tables import parse_pswf_coeffs_header  # noqa: E402
 
-REF = os.environ.get("ESP_REF", "/root/reference")
+REF = os.environ.get("ESP_REF", os.path.join(os.path.dirname(ROOT), "reference"))
 
 
 def main() -> None:
