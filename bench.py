@@ -50,7 +50,7 @@ MD_STEPS = 10
 # passes: 3 whole-plane/slab kernels (fft_mode 0) or 5 per-line kernels
 K_EVAL_BASE = 9
 K_FFT = {0: 3, 1: 5}
-K_NLIST = 5      # cell_bin, scan, scatter, cell_sort, nlist
+K_NLIST = 6      # cell_bin, scan, scatter, cell_sort, nlist, pack (cell-staged pair list; 5 for HOOMD rows)
 K_NVE = 2
 
 
@@ -217,13 +217,15 @@ def accuracy_leg(b, sl, pos_h, q, nlist, dev):
     oracle's workload-size sum, run as the checker after the timed regions)."""
     import torch
     from oracle.ewald_torch import ewald_torch
-    head, nn, nl = nlist
     tot = pos_h.shape[0]
     pos = torch.tensor(pos_h, device=dev)
-    b.build_nlist(pos, RCUT + SKIN, CAP, head, nn, nl)
+    if nlist is not None:
+        b.build_nlist(pos, RCUT + SKIN, CAP, *nlist)
+    else:
+        b.build_pairlist(pos, RCUT + SKIN, CAP)
     force = torch.zeros((tot, 4), device=dev)
     energy = torch.zeros(len(sl), dtype=torch.float64, device=dev)
-    b.compute(pos, q, force, energy, None, nlist=(head, nn, nl))
+    b.compute(pos, q, force, energy, None, nlist=nlist)
     torch.cuda.synchronize(dev)
     f = force.double().cpu().numpy()
     e = energy.cpu().numpy()
@@ -391,9 +393,14 @@ def run_scaleup(args):
     virial = torch.zeros(6, dtype=torch.float64, device=dev)
 
     def request(use_graph=True):
-        b.build_nlist(pos, RCUT + SKIN, CAP, head, nn, nl)
-        b.compute(pos, q, force, energy, virial, nlist=(head, nn, nl), flags=ESP_ALL)
-        b.md_run(pos, vel, q, force, energy, None, (head, nn, nl), MD_STEPS, DT, use_graph=use_graph)
+        if args.hoomd_list:
+            b.build_nlist(pos, RCUT + SKIN, CAP, head, nn, nl)
+            nlist = (head, nn, nl)
+        else:
+            b.build_pairlist(pos, RCUT + SKIN, CAP)
+            nlist = None
+        b.compute(pos, q, force, energy, virial, nlist=nlist, flags=ESP_ALL)
+        b.md_run(pos, vel, q, force, energy, None, nlist, MD_STEPS, DT, use_graph=use_graph)
 
     for _ in range(max(3, args.warmup)):
         request()
@@ -413,8 +420,11 @@ def run_scaleup(args):
     b.set_timing(False)
     inf = b.info(0)
     M = inf["nx"] * inf["ny"] * inf["nz"]
+    if not args.hoomd_list:
+        b.pairlist_check()
+        b.build_nlist(pos, RCUT + SKIN, CAP, head, nn, nl)  # neighbour counts for the byte model
     mean_nn = float(nn.double().mean().item())
-    alg = {"pair": 4.0 * N * mean_nn + 32.0 * N, "spread": 20.0 * N + 4.0 * M, "interp": 36.0 * N + 4.0 * M,
+    alg = {"pair": (4.0 if args.hoomd_list else 2.0) * N * mean_nn + 32.0 * N, "spread": 20.0 * N + 4.0 * M, "interp": 36.0 * N + 4.0 * M,
            "fft": 5 * 2 * 8.0 * M / 2, "sort": 40.0 * N, "bin": 40.0 * N, "nlist": 16.0 * N + 4.0 * N * mean_nn,
            "nve": 48.0 * N}
     peak, peak_kind = _peak_gbs()
@@ -475,10 +485,16 @@ def run_ours(args):
 
     def request(bb, p, v, use_graph=True, qq=q, e=energy):
         # the first evaluation reports energy and virial; the NVE steps need
-        # forces and energies only
-        bb.build_nlist(p, RCUT + SKIN, CAP, head, nn, nl)
-        bb.compute(p, qq, force, e, virial, nlist=(head, nn, nl), flags=ESP_ALL)
-        bb.md_run(p, v, qq, force, e, None, (head, nn, nl), MD_STEPS, DT, use_graph=use_graph)
+        # forces and energies only. Default: the library's cell-staged pair
+        # list; --hoomd-list: HOOMD-layout rows built by the harness
+        if args.hoomd_list:
+            bb.build_nlist(p, RCUT + SKIN, CAP, head, nn, nl)
+            nlist = (head, nn, nl)
+        else:
+            bb.build_pairlist(p, RCUT + SKIN, CAP)
+            nlist = None
+        bb.compute(p, qq, force, e, virial, nlist=nlist, flags=ESP_ALL)
+        bb.md_run(p, v, qq, force, e, None, nlist, MD_STEPS, DT, use_graph=use_graph)
 
     def barrier():
         if world > 1:
@@ -487,9 +503,13 @@ def run_ours(args):
 
     tuned = None
     if not args.no_tune:
-        # the autotuner picks pair lanes, tile edge and FFT pass form on this batch
-        b.build_nlist(pos, RCUT + SKIN, CAP, head, nn, nl)
-        tuned = b.autotune(pos, q, nlist=(head, nn, nl), reps=2)
+        # the autotuner picks pair lanes (HOOMD-list kernel), tile edge and FFT pass form on this batch
+        if args.hoomd_list:
+            b.build_nlist(pos, RCUT + SKIN, CAP, head, nn, nl)
+            tuned = b.autotune(pos, q, nlist=(head, nn, nl), reps=2)
+        else:
+            b.build_pairlist(pos, RCUT + SKIN, CAP)
+            tuned = b.autotune(pos, q, nlist=None, reps=2)
         pos.copy_(pos0)
     for _ in range(max(3, args.warmup)):
         request(b, pos, vel)
@@ -514,10 +534,15 @@ def run_ours(args):
     stage_ms = {k: v[0] / max(v[1], 1) for k, v in stt.items() if v[1] > 0}
     stage_total = {k: v[0] for k, v in stt.items() if v[1] > 0}
     dom = max(stage_total, key=stage_total.get)
+    if not args.hoomd_list:
+        b.pairlist_check()  # no row of the timed steps overflowed
+        b.build_nlist(pos, RCUT + SKIN, CAP, head, nn, nl)  # neighbour counts for the byte model
     mean_nn = float(nn.double().mean().item())
     M = sum(b.info(i)["nx"] * b.info(i)["ny"] * b.info(i)["nz"] for i in range(N.size))
     # algorithmic bytes per launch of each stage (FP32 storage)
-    alg = {"pair": 4.0 * tot * mean_nn + 16.0 * tot + 16.0 * tot,
+    # pair: index stream (4 B per entry for HOOMD rows, 2 B for the
+    # cell-staged list) + positions in + forces out
+    alg = {"pair": (4.0 if args.hoomd_list else 2.0) * tot * mean_nn + 16.0 * tot + 16.0 * tot,
            "spread": 20.0 * tot + 4.0 * M,
            "interp": 20.0 * tot + 4.0 * M + 16.0 * tot,
            "fft": 5 * 2 * 8.0 * M / 2,
@@ -525,7 +550,7 @@ def run_ours(args):
            "bin": 40.0 * tot,
            "nlist": 16.0 * tot + 4.0 * tot * mean_nn,
            "nve": 48.0 * tot}
-    kname = {"pair": "k_pair", "spread": "k_spread", "interp": "k_interp", "fft": "k_fft", "nlist": "k_nlist",
+    kname = {"pair": "k_pair" if args.hoomd_list else "k_pair_cells", "spread": "k_spread", "interp": "k_interp", "fft": "k_fft", "nlist": "k_nlist",
              "sort": "k_tile_sort", "bin": "k_bin", "nve": "k_nve"}
     peak, peak_kind = _peak_gbs()
     ach = alg[dom] / (stage_ms[dom] * 1e-3) / 1e9
@@ -547,9 +572,14 @@ def run_ours(args):
 
         def plain_round():
             for c, (p, v, qq, h, n_, l_, f, e, w) in zip(ctxs, views):
-                c.build_nlist(p, RCUT + SKIN, CAP, h, n_, l_)
-                c.compute(p, qq, f, e, w, nlist=(h, n_, l_), flags=ESP_ALL)
-                c.md_run(p, v, qq, f, e, None, (h, n_, l_), MD_STEPS, DT, use_graph=False)
+                if args.hoomd_list:
+                    c.build_nlist(p, RCUT + SKIN, CAP, h, n_, l_)
+                    nlist = (h, n_, l_)
+                else:
+                    c.build_pairlist(p, RCUT + SKIN, CAP)
+                    nlist = None
+                c.compute(p, qq, f, e, w, nlist=nlist, flags=ESP_ALL)
+                c.md_run(p, v, qq, f, e, None, nlist, MD_STEPS, DT, use_graph=False)
 
         plain_round()
         torch.cuda.synchronize(dev)
@@ -639,12 +669,14 @@ def run_ours(args):
                                 "buffer sets, step k+1 uploads and step k-1 downloads on a copy stream "
                                 "during step k"},
                 "autotune": tuned,
-                "gpu_launches": int(args.steps * (K_NLIST + k_eval + MD_STEPS * (k_eval + K_NVE))),
+                "gpu_launches": int(args.steps * ((K_NLIST - 1 if args.hoomd_list else K_NLIST) + k_eval +
+                                                  MD_STEPS * (k_eval + K_NVE))),
+                "pair_list": "HOOMD-layout rows (k_pair)" if args.hoomd_list else "cell-staged (k_pair_cells)",
                 "clocks": clk.summary()}
         line["fft"] = {"ours_ms": stage_ms.get("fft")}
         line["fft"].update(cufft_leg(b, N.size, dev))
         if not args.no_accuracy:
-            line["accuracy"] = accuracy_leg(b, sl, pos_h, q, (head, nn, nl), dev)
+            line["accuracy"] = accuracy_leg(b, sl, pos_h, q, (head, nn, nl) if args.hoomd_list else None, dev)
         if not args.no_cpu:
             from oracle import esp_port as EP
             threads = EP.max_threads()
@@ -691,6 +723,8 @@ def main():
                     help="scaleup: the plain path on one 10^6-particle system (a second measurement)")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default plan)")
+    ap.add_argument("--hoomd-list", action="store_true",
+                    help="short-range term over HOOMD-layout neighbour rows instead of the cell-staged pair list")
     ap.add_argument("--serve-requests", type=int, default=1000, help="requests per arrival rate")
     ap.add_argument("--serve-rates", type=lambda v: [float(x) for x in v.split(",")], default=[100.0, 200.0, 400.0],
                     help="comma-separated arrival rates (requests/s)")

@@ -29,7 +29,7 @@ EXPORTS = [
     "esp_server_create", "esp_server_submit", "esp_server_start", "esp_server_status", "esp_server_wait_all",
     "esp_server_get_stats", "esp_server_destroy", "esp_set_exclusions", "esp_batch_set_exclusions",
     "esp_compute_f64", "esp_batch_compute_f64", "esp_batch_autotune", "esp_batch_lj", "esp_batch_lj_f64",
-    "esp_batch_nve_step1_f64", "esp_batch_nve_step2_f64",
+    "esp_batch_nve_step1_f64", "esp_batch_nve_step2_f64", "esp_batch_build_pairlist", "esp_batch_pairlist_check",
 ]
 
 ESP_FP32 = 0
@@ -143,6 +143,8 @@ def get_lib() -> ctypes.CDLL:
         lib.esp_batch_nve_step2_f64.argtypes = [P, P, P, P, D]
         lib.esp_batch_autotune.argtypes = [P, P, P, P, P, P, P, I, I, ctypes.POINTER(EspParams), P, I]
         lib.esp_spread_noalloc.argtypes = [P, ctypes.POINTER(EspParams), D, D, D, P, P, I, P]
+        lib.esp_batch_build_pairlist.argtypes = [P, P, P, D, I]
+        lib.esp_batch_pairlist_check.argtypes = [P, ctypes.POINTER(ctypes.c_int)]
         for name in EXPORTS:
             if name != "esp_last_error":
                 getattr(lib, name).restype = ctypes.c_int

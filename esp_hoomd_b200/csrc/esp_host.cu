@@ -7,6 +7,7 @@
 // launches over. A single-system context (esp_ctx) is a batch of one: the
 // reference's ESPForceComputeGPU (src/ESPForceComputeGPU.cc:47-448) maps to
 // esp_create + esp_compute.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -239,15 +240,36 @@ struct esp_batch {
     int2 *d_p = nullptr, *d_s = nullptr;
     int n_p = 0, n_s = 0, smem_plane = 0, smem_slab = 0;
     double *d_acc = nullptr, *d_energy = nullptr, *d_virial = nullptr;
-    // neighbour-list harness (allocated on first use)
-    DevAlloc nlmem;
-    double nl_rlist = -1;
-    int n_cells = 0;
-    CellDev* d_cells = nullptr;
-    int* d_cell_sys = nullptr;
-    uint32_t *d_ckey = nullptr, *d_ccount = nullptr, *d_cstart = nullptr, *d_cperm = nullptr;
-    float4 *d_wpos = nullptr, *d_cpos = nullptr;
-    int* d_overflow = nullptr;
+    // cell grids of the neighbour-list builds (allocated on first use): one
+    // for HOOMD-layout lists, one for the library's cell-staged pair list
+    // (whose kernel reads the cell structures of its own build)
+    struct CellGrid {
+        DevAlloc mem;
+        double rlist = -1;
+        int n_cells = 0, cap = -1;  // cap: row capacity the rows' offsets (nl_off) were laid out for
+        std::vector<CellDev> h_cells;
+        CellDev* d_cells = nullptr;
+        int* d_cell_sys = nullptr;
+        uint32_t *d_ckey = nullptr, *d_ccount = nullptr, *d_cstart = nullptr, *d_cperm = nullptr,
+                 *d_slot2idx = nullptr;
+        float4 *d_wpos = nullptr, *d_cpos = nullptr;
+        int* d_overflow = nullptr;  // [flag, largest row] of the last build
+    } cg_nl, cg_pl;
+    int setup_cells(CellGrid& g, double rlist, int cap);
+    NlistArgs nlist_args(CellGrid& g, const float* pos4, double rlist, int cap) const;
+    // the cell-staged pair list (esp_pairlist.cu): rows by cell-sorted slot
+    DevAlloc plmem;
+    uint16_t* d_pl16 = nullptr;
+    uint32_t* d_pl_nn = nullptr;
+    int pl_cap = 0, pl_stage_cap = 0;
+    bool pl_ready = false, pl_pending = false, pl_overflow = false;
+    int* h_pl_ovf = nullptr;  // page-locked copy of the last build's [flag, largest row]
+    cudaEvent_t pl_ev = nullptr;
+    PairList pl{};
+    int build_pairlist(cudaStream_t st, const float* pos4, double rlist, int cap);
+    // ESP_ERR_OVERFLOW when the last pair-list build overflowed; without
+    // `wait` an unfinished build counts as fine (checked again next time)
+    int pairlist_check(bool wait, int* needed);
     // second stream for the concurrent pair term, its force array and the
     // fork/join events (created at plan time, kept across re-plans)
     cudaStream_t st2 = nullptr;
@@ -307,6 +329,11 @@ struct esp_batch {
         }
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
+        if (pl_ev) {
+            cudaEventSynchronize(pl_ev);
+            cudaEventDestroy(pl_ev);
+        }
+        if (h_pl_ovf) cudaFreeHost(h_pl_ovf);
     }
 
     LaunchArgs args() const;
@@ -332,8 +359,21 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
     mem64.release();
     f64 = false;
     if (p.precision != ESP_FP32 && p.precision != ESP_FP64) return fail(ESP_ERR_INVALID, "precision must be ESP_FP32 or ESP_FP64");
-    nlmem.release();
-    nl_rlist = -1;
+    // the neighbour-list cell grids and the pair list depend only on the
+    // systems (particle counts, boxes): a re-plan of the same systems (the
+    // autotuner's candidates) keeps them
+    const bool same_systems = ns == nsys && std::equal(N_, N_ + ns, N.begin()) &&
+                              std::equal(boxes, boxes + 3 * ns, box.begin());
+    if (!same_systems) {
+        cg_nl.mem.release();
+        cg_nl.rlist = -1;
+        cg_pl.mem.release();
+        cg_pl.rlist = -1;
+        plmem.release();
+        pl_cap = 0;
+        pl_stage_cap = 0;
+        pl_ready = pl_pending = pl_overflow = false;
+    }
     prm = p;
     if (ns <= 0) return fail(ESP_ERR_INVALID, "number of systems must be positive");
     if (p.order < 2 || p.order > MAX_P) return fail(ESP_ERR_UNSUPPORTED, "order must be in [2, 12]");
@@ -764,9 +804,14 @@ int esp_batch::compute(cudaStream_t st, const float* pos4, const float* q, const
     if (f64) return fail(ESP_ERR_UNSUPPORTED, "context planned for FP64: use esp_compute_f64");
     if (!pos4 || !q || !force4) return fail(ESP_ERR_INVALID, "null position, charge or force pointer");
     if (!(flags & ESP_ALL)) return fail(ESP_ERR_INVALID, "flags select no term");
-    if ((flags & ESP_SHORT_RANGE) && (!head || !nn || !nl))
-        return fail(ESP_ERR_INVALID, "short-range term needs the neighbour list");
+    // no neighbour list given: the short-range term runs over the library's pair list
+    const bool use_pl = !head && !nn && !nl;
+    if ((flags & ESP_SHORT_RANGE) && !use_pl && (!head || !nn || !nl))
+        return fail(ESP_ERR_INVALID, "short-range term needs the neighbour list (head, n_neigh, nlist)");
+    if ((flags & ESP_SHORT_RANGE) && use_pl && !pl_ready)
+        return fail(ESP_ERR_INVALID, "no neighbour list given and no pair list built (esp_batch_build_pairlist)");
     LaunchArgs a = args();
+    if ((flags & ESP_SHORT_RANGE) && use_pl) a.plist = &pl;
     a.pos_in = reinterpret_cast<const float4*>(pos4);
     a.q_in = q;
     a.force = reinterpret_cast<float4*>(force4);
@@ -838,7 +883,13 @@ int esp_batch::md_run(cudaStream_t st, float* pos4, float* vel4, const float* q,
                       const unsigned* nn, const unsigned* nl, float* force4, double* energy, double* virial, int nsteps,
                       double dt, int use_graph) {
     if (nsteps < 0) return fail(ESP_ERR_INVALID, "negative step count");
-    if (!pos4 || !vel4 || !q || !force4 || !head || !nn || !nl) return fail(ESP_ERR_INVALID, "null pointer");
+    if (!pos4 || !vel4 || !q || !force4) return fail(ESP_ERR_INVALID, "null pointer");
+    if (!(head && nn && nl) && (head || nn || nl || !pl_ready))
+        return fail(ESP_ERR_INVALID, "md_run needs the neighbour list (head, n_neigh, nlist) or a built pair list");
+    if (!head) {
+        int rc = pairlist_check(false, nullptr);
+        if (rc) return rc;
+    }
     // Every step overwrites the energies (force.w, energy) of the previous
     // one, so only the last step evaluates the pair energies.
     auto step = [&](bool with_energy) -> int {
@@ -934,76 +985,189 @@ int esp_batch::spread_only(cudaStream_t st, const float* pos4, const float* q, d
     return 0;
 }
 
-int esp_batch::build_nlist(cudaStream_t st, const float* pos4, double rlist, int cap, unsigned* head, unsigned* nn,
-                           unsigned* nl) {
-    if (!(rlist > 0) || cap <= 0) return fail(ESP_ERR_INVALID, "rlist and cap must be positive");
-    if (!pos4 || !head || !nn || !nl) return fail(ESP_ERR_INVALID, "null pointer");
-    if (rlist != nl_rlist) {
-        nlmem.release();
-        std::vector<CellDev> cells(nsys);
-        std::vector<int> cell_sys;
-        int c_off = 0;
-        long long nl_off = 0;
-        for (int s = 0; s < nsys; ++s) {
-            CellDev& C = cells[s];
-            int nc[3];
-            for (int d = 0; d < 3; ++d) {
-                if (2.0 * rlist > box[3 * s + d]) return fail(ESP_ERR_INVALID, "rlist must not exceed half the box");
-                nc[d] = std::max(1, (int)std::floor(box[3 * s + d] / rlist));
-            }
-            C.ncx = nc[0];
-            C.ncy = nc[1];
-            C.ncz = nc[2];
-            C.inv_wx = (float)(nc[0] / box[3 * s]);
-            C.inv_wy = (float)(nc[1] / box[3 * s + 1]);
-            C.inv_wz = (float)(nc[2] / box[3 * s + 2]);
-            C.c_off = c_off;
-            C.nl_off = nl_off;
-            for (int c = 0; c < nc[0] * nc[1] * nc[2]; ++c) cell_sys.push_back(s);
-            c_off += nc[0] * nc[1] * nc[2];
-            nl_off += (long long)N[s] * cap;
-        }
-        n_cells = c_off;
-        int rc = 0;
-        if ((rc = nlmem.get(d_cells, nsys)) || (rc = nlmem.get(d_cell_sys, n_cells)) ||
-            (rc = nlmem.get(d_ckey, totN)) || (rc = nlmem.get(d_ccount, n_cells)) ||
-            (rc = nlmem.get(d_cstart, n_cells + 1)) || (rc = nlmem.get(d_cperm, totN)) ||
-            (rc = nlmem.get(d_wpos, totN)) || (rc = nlmem.get(d_cpos, totN)) ||
-            (rc = nlmem.get(d_overflow, 1)))
-            return rc;
-        ESPB_CK(cudaMemcpy(d_cells, cells.data(), nsys * sizeof(CellDev), cudaMemcpyHostToDevice));
-        ESPB_CK(cudaMemcpy(d_cell_sys, cell_sys.data(), n_cells * sizeof(int), cudaMemcpyHostToDevice));
-        ESPB_CK(cudaMemset(d_ccount, 0, n_cells * sizeof(uint32_t)));
-        nl_rlist = rlist;
+int esp_batch::setup_cells(CellGrid& g, double rlist, int cap) {
+    if (rlist == g.rlist) {
+        if (cap == g.cap) return 0;
+        // same cells, new row capacity: HOOMD-layout rows of system s start at p_off * cap
+        for (int s = 0; s < nsys; ++s) g.h_cells[s].nl_off = (long long)sd[s].p_off * cap;
+        ESPB_CK(cudaMemcpy(g.d_cells, g.h_cells.data(), nsys * sizeof(CellDev), cudaMemcpyHostToDevice));
+        g.cap = cap;
+        return 0;
     }
+    g.mem.release();
+    g.rlist = -1;
+    g.cap = -1;
+    g.h_cells.assign(nsys, CellDev{});
+    std::vector<int> cell_sys;
+    int c_off = 0;
+    long long nl_off = 0;
+    for (int s = 0; s < nsys; ++s) {
+        CellDev& C = g.h_cells[s];
+        int nc[3];
+        for (int d = 0; d < 3; ++d) {
+            if (2.0 * rlist > box[3 * s + d]) return fail(ESP_ERR_INVALID, "rlist must not exceed half the box");
+            nc[d] = std::max(1, (int)std::floor(box[3 * s + d] / rlist));
+        }
+        C.ncx = nc[0];
+        C.ncy = nc[1];
+        C.ncz = nc[2];
+        C.inv_wx = (float)(nc[0] / box[3 * s]);
+        C.inv_wy = (float)(nc[1] / box[3 * s + 1]);
+        C.inv_wz = (float)(nc[2] / box[3 * s + 2]);
+        C.c_off = c_off;
+        C.nl_off = nl_off;
+        for (int c = 0; c < nc[0] * nc[1] * nc[2]; ++c) cell_sys.push_back(s);
+        c_off += nc[0] * nc[1] * nc[2];
+        nl_off += (long long)N[s] * cap;
+    }
+    g.n_cells = c_off;
+    int rc = 0;
+    if ((rc = g.mem.get(g.d_cells, nsys)) || (rc = g.mem.get(g.d_cell_sys, g.n_cells)) ||
+        (rc = g.mem.get(g.d_ckey, totN)) || (rc = g.mem.get(g.d_ccount, g.n_cells)) ||
+        (rc = g.mem.get(g.d_cstart, g.n_cells + 1)) || (rc = g.mem.get(g.d_cperm, totN)) ||
+        (rc = g.mem.get(g.d_slot2idx, totN)) || (rc = g.mem.get(g.d_wpos, totN)) ||
+        (rc = g.mem.get(g.d_cpos, totN)) || (rc = g.mem.get(g.d_overflow, 2)))
+        return rc;
+    ESPB_CK(cudaMemcpy(g.d_cells, g.h_cells.data(), nsys * sizeof(CellDev), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(g.d_cell_sys, cell_sys.data(), g.n_cells * sizeof(int), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemset(g.d_ccount, 0, g.n_cells * sizeof(uint32_t)));
+    g.rlist = rlist;
+    g.cap = cap;
+    return 0;
+}
+
+NlistArgs esp_batch::nlist_args(CellGrid& g, const float* pos4, double rlist, int cap) const {
     NlistArgs a;
     a.chunks = d_chunks;
     a.n_chunks = n_chunks;
     a.sys = d_sys;
-    a.cells = d_cells;
-    a.cell_sys = d_cell_sys;
-    a.n_cells = n_cells;
+    a.cells = g.d_cells;
+    a.cell_sys = g.d_cell_sys;
+    a.n_cells = g.n_cells;
     a.total = totN;
     a.pos = reinterpret_cast<const float4*>(pos4);
-    a.ckey = d_ckey;
-    a.ccount = d_ccount;
-    a.cstart = d_cstart;
-    a.perm_u = d_cperm;
-    a.wpos = d_wpos;
-    a.cpos = d_cpos;
+    a.ckey = g.d_ckey;
+    a.ccount = g.d_ccount;
+    a.cstart = g.d_cstart;
+    a.perm_u = g.d_cperm;
+    a.slot2idx = g.d_slot2idx;
+    a.wpos = g.d_wpos;
+    a.cpos = g.d_cpos;
     a.rlist2 = (float)(rlist * rlist);
     a.cap = cap;
+    a.overflow = g.d_overflow;
+    return a;
+}
+
+int esp_batch::build_nlist(cudaStream_t st, const float* pos4, double rlist, int cap, unsigned* head, unsigned* nn,
+                           unsigned* nl) {
+    if (!(rlist > 0) || cap <= 0) return fail(ESP_ERR_INVALID, "rlist and cap must be positive");
+    if (!pos4 || !head || !nn || !nl) return fail(ESP_ERR_INVALID, "null pointer");
+    int rc = setup_cells(cg_nl, rlist, cap);
+    if (rc) return rc;
+    NlistArgs a = nlist_args(cg_nl, pos4, rlist, cap);
     a.head = head;
     a.nn = nn;
     a.nl = nl;
-    a.overflow = d_overflow;
+    // HOOMD-layout rows: head[i] = first entry of system s + local i * cap
     timer.begin(ESP_STAGE_NLIST, st);
     ESPB_CK(launch_nlist(a, st));
     timer.end(st);
     int ovf = 0;
-    ESPB_CK(cudaMemcpyAsync(&ovf, d_overflow, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ESPB_CK(cudaMemcpyAsync(&ovf, cg_nl.d_overflow, sizeof(int), cudaMemcpyDeviceToHost, st));
     ESPB_CK(cudaStreamSynchronize(st));
     if (ovf) return fail(ESP_ERR_OVERFLOW, "neighbour-list row capacity exceeded; n_neigh holds the needed counts");
+    return 0;
+}
+
+// Staging capacity of the pair kernel: 1.25 x the mean neighbourhood (the
+// particles of the surrounding cells at each system's mean density) + 64,
+// at most what one CTA's shared memory holds. Denser neighbourhoods are
+// staged in windows (slower, same results).
+static int pair_stage_capacity(const std::vector<CellDev>& cells, const std::vector<int>& N,
+                               const std::vector<double>& box) {
+    double est = 0;
+    for (size_t s = 0; s < cells.size(); ++s) {
+        const CellDev& C = cells[s];
+        const double V = box[3 * s] * box[3 * s + 1] * box[3 * s + 2];
+        const double w3 = V / ((double)C.ncx * C.ncy * C.ncz);
+        const int visited = std::min(C.ncx, 3) * std::min(C.ncy, 3) * std::min(C.ncz, 3);
+        est = std::max(est, visited * w3 * N[s] / V);
+    }
+    const int max_cap = (int)((227 * 1024 - pair_cells_smem(0)) / 16) & ~7;
+    int c = (int)std::ceil(1.25 * est + 64.0);
+    c = ((c + 7) & ~7);
+    c = std::max(64, std::min(c, max_cap));
+    return c - 1;  // stage_cap + 1 (with the padding particle) is a multiple of 8
+}
+
+int esp_batch::build_pairlist(cudaStream_t st, const float* pos4, double rlist, int cap) {
+    if (!(rlist > 0) || cap <= 0) return fail(ESP_ERR_INVALID, "rlist and cap must be positive");
+    if (cap % 8 != 0 || cap > 1024)
+        return fail(ESP_ERR_UNSUPPORTED, "pair-list row capacity must be a multiple of 8, at most 1024");
+    if (!pos4) return fail(ESP_ERR_INVALID, "null position pointer");
+    if (f64) return fail(ESP_ERR_UNSUPPORTED, "the cell-staged pair list serves the FP32 path");
+    int rc = setup_cells(cg_pl, rlist, cap);
+    if (rc) return rc;
+    if (pl_cap != cap) {
+        plmem.release();
+        pl_cap = 0;
+        if ((rc = plmem.get(d_pl16, (size_t)totN * cap)) || (rc = plmem.get(d_pl_nn, totN))) return rc;
+        pl_cap = cap;
+        drop_graphs();  // captured steps hold the previous arrays
+    }
+    const int scap = pair_stage_capacity(cg_pl.h_cells, N, box);
+    if (scap != pl_stage_cap) {
+        ESPB_CK(configure_pair_cells(scap));
+        pl_stage_cap = scap;
+        drop_graphs();
+    }
+    if (!h_pl_ovf) ESPB_CK(cudaHostAlloc((void**)&h_pl_ovf, 2 * sizeof(int), cudaHostAllocDefault));
+    if (!pl_ev) ESPB_CK(cudaEventCreateWithFlags(&pl_ev, cudaEventDisableTiming));
+    NlistArgs a = nlist_args(cg_pl, pos4, rlist, cap);
+    a.nn = d_pl_nn;
+    a.nl16 = d_pl16;
+    timer.begin(ESP_STAGE_NLIST, st);
+    ESPB_CK(launch_nlist(a, st));
+    ESPB_CK(launch_pairlist_pack(totN, d_pl_nn, d_pl16, cap, st));
+    timer.end(st);
+    // the overflow flag is read lazily: no host synchronisation here
+    ESPB_CK(cudaMemcpyAsync(h_pl_ovf, cg_pl.d_overflow, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    ESPB_CK(cudaEventRecord(pl_ev, st));
+    pl.cell_sys = cg_pl.d_cell_sys;
+    pl.cells = cg_pl.d_cells;
+    pl.cstart = cg_pl.d_cstart;
+    pl.slot2idx = cg_pl.d_slot2idx;
+    pl.nn = d_pl_nn;
+    pl.nl16 = d_pl16;
+    pl.n_cells = cg_pl.n_cells;
+    pl.cap = cap;
+    pl.stage_cap = pl_stage_cap;
+    pl_ready = true;
+    pl_pending = true;
+    pl_overflow = false;
+    return 0;
+}
+
+int esp_batch::pairlist_check(bool wait, int* needed) {
+    if (!pl_ready) return fail(ESP_ERR_INVALID, "no pair list has been built (esp_batch_build_pairlist)");
+    if (pl_pending) {
+        if (wait) {
+            ESPB_CK(cudaEventSynchronize(pl_ev));
+        } else {
+            const cudaError_t q = cudaEventQuery(pl_ev);
+            if (q == cudaErrorNotReady) return 0;
+            if (q != cudaSuccess) return fail(ESP_ERR_CUDA, std::string("pair-list build: ") + cudaGetErrorString(q));
+        }
+        pl_pending = false;
+        pl_overflow = h_pl_ovf[0] != 0;
+        if (needed) *needed = h_pl_ovf[1];
+    }
+    if (pl_overflow) {
+        if (needed) *needed = h_pl_ovf[1];
+        return fail(ESP_ERR_OVERFLOW, "pair-list row capacity exceeded (largest row " + std::to_string(h_pl_ovf[1]) +
+                                          "); rebuild with a larger cap");
+    }
     return 0;
 }
 
@@ -1112,7 +1276,7 @@ int esp_batch::info(int s, esp_info* out) const {
     out->m2 = h.split.m2;
     out->split_fit_err = h.split.fit_err;
     out->window_fit_err = h.win.fit_err;
-    out->device_bytes = mem.bytes + nlmem.bytes;
+    out->device_bytes = mem.bytes + cg_nl.mem.bytes + cg_pl.mem.bytes + plmem.bytes;
     return 0;
 }
 
@@ -1276,7 +1440,21 @@ int esp_batch_compute(esp_batch* b, void* stream, const float* pos4, const float
                       const unsigned* n_neigh, const unsigned* nlist, float* force4, double* energy, double* virial6,
                       int flags) {
     if (!b) return fail(ESP_ERR_INVALID, "null batch");
+    if ((flags & ESP_SHORT_RANGE) && !head && !n_neigh && !nlist && b->pl_ready) {
+        int rc = b->pairlist_check(false, nullptr);
+        if (rc) return rc;
+    }
     return b->compute((cudaStream_t)stream, pos4, charge, head, n_neigh, nlist, force4, energy, virial6, flags);
+}
+
+int esp_batch_build_pairlist(esp_batch* b, void* stream, const float* pos4, double rlist, int cap) {
+    if (!b) return fail(ESP_ERR_INVALID, "null batch");
+    return b->build_pairlist((cudaStream_t)stream, pos4, rlist, cap);
+}
+
+int esp_batch_pairlist_check(esp_batch* b, int* needed_cap) {
+    if (!b) return fail(ESP_ERR_INVALID, "null batch");
+    return b->pairlist_check(true, needed_cap);
 }
 
 int esp_batch_compute_f64(esp_batch* b, void* stream, const double* pos4, const double* charge, const unsigned* head,

@@ -2,6 +2,7 @@
 // These stand in for the HOOMD-blue pieces the reference relies on
 // (NeighborList and the integrator; not vendored in the reference) so the
 // ESP path can run standalone.
+#include "esp_cells.cuh"
 #include "esp_common.cuh"
 #include "esp_kernels.h"
 #include "esp_md.h"
@@ -41,7 +42,8 @@ __global__ void k_cell_bin(const int2* __restrict__ chunks, const SysDev* __rest
 // Deterministic order inside each cell (ascending particle index) and the
 // cell-sorted positions.
 __global__ void k_cell_sort(const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm_u,
-                            const float4* __restrict__ wpos, float4* __restrict__ cpos) {
+                            const float4* __restrict__ wpos, float4* __restrict__ cpos,
+                            uint32_t* __restrict__ slot2idx) {
     __shared__ __align__(16) uint32_t sm[1024];
     const uint32_t s0 = start[blockIdx.x];
     const uint32_t n = start[blockIdx.x + 1] - s0;
@@ -68,6 +70,7 @@ __global__ void k_cell_sort(const uint32_t* __restrict__ start, const uint32_t* 
             for (uint32_t j = 0; j < n; ++j) r += (src[j] < v) ? 1u : 0u;
         }
         cpos[s0 + r] = wpos[v];
+        if (slot2idx) slot2idx[s0 + r] = v;
     }
 }
 
@@ -88,6 +91,13 @@ __device__ __forceinline__ void store_if(bool ok, uint32_t* p, uint32_t v) {
     asm volatile(
         "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q st.global.u32 [%0], %1;\n\t}" ::"l"(p), "r"(v),
         "r"((uint32_t)ok)
+        : "memory");
+}
+
+__device__ __forceinline__ void store_if16(bool ok, uint16_t* p, uint32_t v) {
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q st.global.u16 [%0], %1;\n\t}" ::"l"(p),
+        "h"((unsigned short)v), "r"((uint32_t)ok)
         : "memory");
 }
 
@@ -113,73 +123,65 @@ __device__ __forceinline__ uint32_t nl_scan(const float4* __restrict__ cand, int
     return cnt;
 }
 
+// As nl_scan, for the cell-staged pair list: the entry is the candidate's
+// staged index (its position in the cell's neighbourhood enumeration).
+template <bool MINIMG>
+__device__ __forceinline__ uint32_t nl_scan_staged(const float4* __restrict__ cand, int n, float4 pi, int i,
+                                                   const SysDev& S, float rlist2, uint32_t cap,
+                                                   uint16_t* __restrict__ row, uint32_t cnt, uint32_t base) {
+#pragma unroll 4
+    for (int k = 0; k < n; ++k) {
+        const float4 pj = cand[k];
+        float ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
+        if (MINIMG) {
+            ddx -= S.Lx * rintf(ddx * S.inv_Lx);
+            ddy -= S.Ly * rintf(ddy * S.inv_Ly);
+            ddz -= S.Lz * rintf(ddz * S.inv_Lz);
+        }
+        const bool hit = ddx * ddx + ddy * ddy + ddz * ddz < rlist2 && __float_as_int(pj.w) != i;
+        store_if16(hit && cnt < cap, row + cnt, base + (uint32_t)k);
+        cnt += hit ? 1u : 0u;
+    }
+    return cnt;
+}
+
+// STAGED = false: HOOMD-layout rows (row of particle i at nl_off + local i *
+// cap, entries local particle indices). STAGED = true: the cell-staged pair
+// list -- the row of cell-sorted slot s at s * cap (u16), entries staged
+// indices, each row padded to a multiple of 8 entries with the cell's
+// sentinel index (its neighbourhood total, a zero-charge dummy in the pair
+// kernel); rows that exceed cap, or neighbourhoods of more than 65,534
+// particles, set the overflow flag.
+template <bool STAGED>
 __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ cell_sys, const SysDev* __restrict__ sys,
                                                       const CellDev* __restrict__ cells,
                                                       const uint32_t* __restrict__ cstart,
                                                       const float4* __restrict__ cpos, float rlist2, int cap,
                                                       uint32_t* __restrict__ head, uint32_t* __restrict__ nn,
-                                                      uint32_t* __restrict__ nl, int* __restrict__ overflow) {
+                                                      uint32_t* __restrict__ nl, uint16_t* __restrict__ nl16,
+                                                      int* __restrict__ overflow) {
     __shared__ float4 cand[NL_STAGE];
-    __shared__ uint32_t seg_src[27];   // first slot of each surrounding cell
-    __shared__ uint32_t seg_off[28];   // exclusive prefix of their counts
-    __shared__ float seg_shift[27][3];
+    __shared__ CellNbhd nb;
     const uint32_t cidx = blockIdx.x;
     const uint32_t c0 = cstart[cidx], c1 = cstart[cidx + 1];
     if (c0 == c1) return;
     const int si = cell_sys[cidx];
     const SysDev& S = sys[si];
     const CellDev& C = cells[si];
-    const int lc = (int)cidx - C.c_off;
-    const int cx = lc % C.ncx, cy = (lc / C.ncx) % C.ncy, cz = lc / (C.ncx * C.ncy);
-    const bool minimg = C.ncx < 3 || C.ncy < 3 || C.ncz < 3;
     const int tid = threadIdx.x;
-    if (tid < 32) {
-        // surrounding cell t = (iz * 3 + iy) * 3 + ix; with fewer than 3
-        // cells on an axis the -1/+1 neighbours coincide, so only the
-        // distinct ones ({0, 1} for 2 cells, {0} for 1) are visited
-        uint32_t n = 0;
-        if (tid < 27) {
-            const int ix = tid % 3, iy = (tid / 3) % 3, iz = tid / 9;
-            const int dx = (C.ncx >= 3 ? -1 : 0) + ix, dy = (C.ncy >= 3 ? -1 : 0) + iy,
-                      dz = (C.ncz >= 3 ? -1 : 0) + iz;
-            const bool ok = dx <= (C.ncx >= 3 ? 1 : C.ncx - 1) && dy <= (C.ncy >= 3 ? 1 : C.ncy - 1) &&
-                            dz <= (C.ncz >= 3 ? 1 : C.ncz - 1);
-            int xx = cx + dx, yy = cy + dy, zz = cz + dz;
-            float sx = 0.f, sy = 0.f, sz = 0.f;
-            if (xx < 0) { xx += C.ncx; sx = -S.Lx; } else if (xx >= C.ncx) { xx -= C.ncx; sx = S.Lx; }
-            if (yy < 0) { yy += C.ncy; sy = -S.Ly; } else if (yy >= C.ncy) { yy -= C.ncy; sy = S.Ly; }
-            if (zz < 0) { zz += C.ncz; sz = -S.Lz; } else if (zz >= C.ncz) { zz -= C.ncz; sz = S.Lz; }
-            uint32_t b = 0;
-            if (ok) {
-                const uint32_t c = (uint32_t)(C.c_off + (zz * C.ncy + yy) * C.ncx + xx);
-                b = cstart[c];
-                n = cstart[c + 1] - b;
-            }
-            seg_src[tid] = b;
-            seg_shift[tid][0] = minimg ? 0.f : sx;
-            seg_shift[tid][1] = minimg ? 0.f : sy;
-            seg_shift[tid][2] = minimg ? 0.f : sz;
-        }
-        uint32_t inc = n;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
-            if (tid >= o) inc += v;
-        }
-        if (tid < 27) seg_off[tid] = inc - n;
-        if (tid == 26) seg_off[27] = inc;
-    }
+    if (tid < 32) cell_nbhd_warp((int)cidx - C.c_off, C, S, cstart, nb);
     __syncthreads();
-    const uint32_t total = seg_off[27];
+    const bool minimg = nb.minimg != 0;
+    const uint32_t total = nb.off[27];
     auto stage = [&](uint32_t base) {
         const uint32_t top = min(total, base + (uint32_t)NL_STAGE);
         for (int s = 0; s < 27; ++s) {
-            const uint32_t lo = max(seg_off[s], base), hi = min(seg_off[s + 1], top);
+            const uint32_t lo = max(nb.off[s], base), hi = min(nb.off[s + 1], top);
             for (uint32_t g = lo + tid; g < hi; g += NL_THREADS) {
-                float4 p = cpos[seg_src[s] + (g - seg_off[s])];
-                p.x += seg_shift[s][0];
-                p.y += seg_shift[s][1];
-                p.z += seg_shift[s][2];
+                float4 p = cpos[nb.src[s] + (g - nb.off[s])];
+                p.x += nb.shift[s][0];
+                p.y += nb.shift[s][1];
+                p.z += nb.shift[s][2];
                 cand[g - base] = p;
             }
         }
@@ -189,13 +191,15 @@ __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ ce
         stage(0);
         __syncthreads();
     }
+    if (STAGED && total > 65534u && tid == 0) atomicOr(overflow, 2);  // staged indices must fit 16 bits
     for (uint32_t p0 = c0; p0 < c1; p0 += NL_THREADS) {
         const uint32_t slot = p0 + tid;
         const bool active = slot < c1;
         const float4 pi = active ? cpos[slot] : make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, __int_as_float(-1));
         const int i = __float_as_int(pi.w);
-        const long long hrow = (long long)C.nl_off + (long long)(i - S.p_off) * cap;
-        uint32_t* row = nl + (active ? hrow : 0);
+        const long long hrow = STAGED ? (long long)slot * cap : (long long)C.nl_off + (long long)(i - S.p_off) * cap;
+        uint32_t* row = nl + (active && !STAGED ? hrow : 0);
+        uint16_t* row16 = nl16 + (active && STAGED ? hrow : 0);
         uint32_t cnt = 0;
         for (uint32_t base = 0; base < total; base += NL_STAGE) {
             if (!one_stage) {
@@ -204,13 +208,26 @@ __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ ce
                 __syncthreads();
             }
             const int n = (int)min((uint32_t)NL_STAGE, total - base);
-            cnt = minimg ? nl_scan<true>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row, cnt)
-                         : nl_scan<false>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row, cnt);
+            if (STAGED)
+                cnt = minimg ? nl_scan_staged<true>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row16, cnt, base)
+                             : nl_scan_staged<false>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row16, cnt, base);
+            else
+                cnt = minimg ? nl_scan<true>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row, cnt)
+                             : nl_scan<false>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row, cnt);
         }
         if (active) {
-            head[i] = (uint32_t)hrow;
-            nn[i] = cnt;
-            if (cnt > (uint32_t)cap) atomicOr(overflow, 1);
+            if (STAGED) {
+                nn[slot] = cnt;
+                // pad to whole groups of 8 with the sentinel
+                for (uint32_t k = cnt; k < ((cnt + 7u) & ~7u) && k < (uint32_t)cap; ++k) row16[k] = (uint16_t)total;
+            } else {
+                head[i] = (uint32_t)hrow;
+                nn[i] = cnt;
+            }
+            if (cnt > (uint32_t)cap) {
+                atomicOr(overflow, 1);
+                if (STAGED) atomicMax(overflow + 1, (int)cnt);
+            }
         }
     }
 }
@@ -363,15 +380,19 @@ cudaError_t launch_nve64(int half, const int2* chunks, int n_chunks, const SysDe
 
 cudaError_t launch_nlist(const NlistArgs& a, cudaStream_t st) {
     if (a.n_chunks == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(a.overflow, 0, sizeof(int), st);
+    cudaError_t e = cudaMemsetAsync(a.overflow, 0, (a.nl16 ? 2 : 1) * sizeof(int), st);
     if (e != cudaSuccess) return e;
     k_cell_bin<<<a.n_chunks, 256, 0, st>>>(a.chunks, a.sys, a.cells, a.pos, a.ckey, a.ccount, a.wpos);
     if ((e = launch_scan(a.ccount, a.cstart, a.n_cells, st)) != cudaSuccess) return e;
     if ((e = launch_scatter(a.chunks, a.n_chunks, a.sys, a.ckey, a.cstart, a.ccount, a.perm_u, st)) != cudaSuccess)
         return e;
-    k_cell_sort<<<a.n_cells, 256, 0, st>>>(a.cstart, a.perm_u, a.wpos, a.cpos);
-    k_nlist<<<a.n_cells, NL_THREADS, 0, st>>>(a.cell_sys, a.sys, a.cells, a.cstart, a.cpos, a.rlist2, a.cap,
-                                              a.head, a.nn, a.nl, a.overflow);
+    k_cell_sort<<<a.n_cells, 256, 0, st>>>(a.cstart, a.perm_u, a.wpos, a.cpos, a.slot2idx);
+    if (a.nl16)
+        k_nlist<true><<<a.n_cells, NL_THREADS, 0, st>>>(a.cell_sys, a.sys, a.cells, a.cstart, a.cpos, a.rlist2,
+                                                        a.cap, nullptr, a.nn, nullptr, a.nl16, a.overflow);
+    else
+        k_nlist<false><<<a.n_cells, NL_THREADS, 0, st>>>(a.cell_sys, a.sys, a.cells, a.cstart, a.cpos, a.rlist2,
+                                                         a.cap, a.head, a.nn, a.nl, nullptr, a.overflow);
     return cudaGetLastError();
 }
 

@@ -11,7 +11,7 @@ namespace espb {
 struct CellDev {
     int ncx, ncy, ncz, c_off;  // cell grid and first cell
     float inv_wx, inv_wy, inv_wz;
-    long long nl_off;          // first neighbour-list entry of this system
+    long long nl_off;          // first neighbour-list entry of this system (HOOMD-layout rows)
 };
 
 struct NlistArgs {
@@ -35,6 +35,8 @@ struct NlistArgs {
     uint32_t* nn = nullptr;
     uint32_t* nl = nullptr;
     int* overflow = nullptr;
+    uint32_t* slot2idx = nullptr;  // cell-sorted slot -> particle (written by the cell sort)
+    uint16_t* nl16 = nullptr;      // non-null: build the cell-staged pair list instead of HOOMD rows
 };
 
 cudaError_t launch_nlist(const NlistArgs& a, cudaStream_t st);

@@ -172,6 +172,21 @@ class Batch:
         check(self._lib.esp_batch_build_nlist(self._h, _stream(stream), _ptr(pos4), float(rlist), int(cap),
                                               _ptr(head), _ptr(nn), _ptr(nl)), "esp_batch_build_nlist")
 
+    def build_pairlist(self, pos4, rlist: float, cap: int = 256, stream=None) -> None:
+        """Builds the library-owned cell-staged pair list (all pairs with
+        r < rlist); compute / md_run without a neighbour list use it. Does not
+        synchronise: a row overflow is reported by a later call."""
+        check(self._lib.esp_batch_build_pairlist(self._h, _stream(stream), _ptr(pos4), float(rlist), int(cap)),
+              "esp_batch_build_pairlist")
+
+    def pairlist_check(self) -> int:
+        """Waits for the last pair-list build; raises EspError (ESP_ERR_OVERFLOW)
+        if a row exceeded its capacity. Returns the largest row length seen
+        in an overflowing build (0 otherwise)."""
+        need = ctypes.c_int(0)
+        check(self._lib.esp_batch_pairlist_check(self._h, ctypes.byref(need)), "esp_batch_pairlist_check")
+        return int(need.value)
+
     def nve_step1(self, pos4, vel4, force4, dt: float, stream=None) -> None:
         check(self._lib.esp_batch_nve_step1(self._h, _stream(stream), _ptr(pos4), _ptr(vel4), _ptr(force4),
                                             float(dt)), "esp_batch_nve_step1")
@@ -182,7 +197,8 @@ class Batch:
 
     def md_run(self, pos4, vel4, q, force4, energy, virial, nlist, nsteps: int, dt: float, use_graph: bool = True,
                stream=None) -> None:
-        head, nn, nl = nlist
+        """nlist = (head, n_neigh, nlist) or None for the library's pair list."""
+        head, nn, nl = nlist if nlist is not None else (None, None, None)
         check(self._lib.esp_batch_md_run(self._h, _stream(stream), _ptr(pos4), _ptr(vel4), _ptr(q), _ptr(head),
                                          _ptr(nn), _ptr(nl), _ptr(force4), _ptr(energy), _ptr(virial), int(nsteps),
                                          float(dt), int(bool(use_graph))), "esp_batch_md_run")

@@ -239,6 +239,23 @@ int esp_pswf_eval_pairs(void* stream, int n, const double* rsq, const double* qi
 int esp_batch_build_nlist(esp_batch* b, void* stream, const float* pos4, double rlist, int cap, unsigned* head,
                           unsigned* n_neigh, unsigned* nlist);
 
+/* Cell-staged pair list owned by the library: the short-range term's
+ * neighbour list when the library builds it (the reference takes HOOMD's
+ * NeighborList, src/module.cc:73-79; this replaces that list for standalone
+ * and batched runs). Lists all pairs with r < rlist of pos4 (rlist at most
+ * half the smallest box edge) on a cell grid of edge >= rlist; rows are kept
+ * in cell order with 16-bit indices into each cell's neighbourhood.
+ * esp_batch_compute and esp_batch_md_run called with head = n_neigh = nlist
+ * = NULL run the short-range term over the last list built. `cap` is the row
+ * capacity: a multiple of 8, at most 1024. Does not synchronise: a row longer
+ * than cap is detected on the device and reported (ESP_ERR_OVERFLOW) by the
+ * first esp_batch_compute / esp_batch_md_run that finds the build finished,
+ * and by esp_batch_pairlist_check, which waits for the build and writes the
+ * longest row to *needed_cap (may be NULL). Results computed over an
+ * overflowed list are invalid; rebuild with a larger cap. */
+int esp_batch_build_pairlist(esp_batch* b, void* stream, const float* pos4, double rlist, int cap);
+int esp_batch_pairlist_check(esp_batch* b, int* needed_cap);
+
 /* Velocity-Verlet halves on the concatenated arrays: vel4 = (vx, vy, vz,
  * mass). step1: v += dt/2 F/m; x += dt v (wrapped into the box).
  * step2: v += dt/2 F/m. */
@@ -269,7 +286,8 @@ int esp_batch_lj_f64(esp_batch* b, void* stream, const double* pos4, const unsig
  * With use_graph != 0 one step is captured in a CUDA graph on first use
  * (and whenever a pointer or dt changes; one graph per pointer set, a few
  * sets kept) and replayed. The neighbour list is used as given (no
- * rebuild). */
+ * rebuild). head = n_neigh = nlist = NULL: the library's pair list
+ * (esp_batch_build_pairlist). */
 int esp_batch_md_run(esp_batch* b, void* stream, float* pos4, float* vel4, const float* charge, const unsigned* head,
                      const unsigned* n_neigh, const unsigned* nlist, float* force4, double* energy, double* virial6,
                      int nsteps, double dt, int use_graph);
