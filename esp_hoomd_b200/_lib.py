@@ -30,6 +30,7 @@ EXPORTS = [
     "esp_server_get_stats", "esp_server_destroy", "esp_set_exclusions", "esp_batch_set_exclusions",
     "esp_compute_f64", "esp_batch_compute_f64", "esp_batch_autotune", "esp_batch_lj", "esp_batch_lj_f64",
     "esp_batch_nve_step1_f64", "esp_batch_nve_step2_f64", "esp_batch_build_pairlist", "esp_batch_pairlist_check",
+    "esp_compute_hoomd",
 ]
 
 ESP_FP32 = 0
@@ -144,6 +145,7 @@ def get_lib() -> ctypes.CDLL:
         lib.esp_batch_autotune.argtypes = [P, P, P, P, P, P, P, I, I, ctypes.POINTER(EspParams), P, I]
         lib.esp_spread_noalloc.argtypes = [P, ctypes.POINTER(EspParams), D, D, D, P, P, I, P]
         lib.esp_batch_build_pairlist.argtypes = [P, P, P, D, I]
+        lib.esp_compute_hoomd.argtypes = [P, P, P, P, I, P, P, P, P, P, I, P, I]
         lib.esp_batch_pairlist_check.argtypes = [P, ctypes.POINTER(ctypes.c_int)]
         for name in EXPORTS:
             if name != "esp_last_error":

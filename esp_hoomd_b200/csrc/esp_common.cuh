@@ -14,7 +14,7 @@ namespace espb {
 constexpr int MAX_P = 12;      // ESP_MAX_ORDER (src/ESPForceCompute.h:63)
 constexpr int MAX_D = 15;      // window polynomial degree limit
 constexpr int MAX_QC = 32;     // split polynomial coefficients
-constexpr int ACC_STRIDE = 16; // doubles of per-system accumulators
+constexpr int ACC_STRIDE = 24; // doubles of per-system accumulators
 constexpr int FFT_MAX_N = 256; // longest 1D transform (2/3/5-smooth)
 constexpr int FFT_B_YZ = 16;   // columns per CTA in the y/z passes
 constexpr int FFT_B_X = 8;     // row pairs per CTA in the x passes
@@ -30,6 +30,7 @@ enum AccSlot {
     ACC_EK = 3,     // k-space energy (diagnostic, with the virial; equals the mesh energy)
     ACC_WK = 4,     // k-space virial xx,xy,xz,yy,yz,zz (4..9)
     ACC_WP = 10,    // pair virial (10..15)
+    ACC_WX = 16,    // exclusion-correction virial (16..21)
 };
 
 struct SysDev {

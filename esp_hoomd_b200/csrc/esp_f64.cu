@@ -537,7 +537,7 @@ __global__ void k64_exclusions(const int2* __restrict__ chunks, const SysDev* __
     block_sum_f64<7>(e, red);
     if (threadIdx.x == 0) {
         atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_E], e[0]);
-        for (int k = 0; k < 6; ++k) atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_WK + k], e[1 + k]);
+        for (int k = 0; k < 6; ++k) atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_WX + k], e[1 + k]);
     }
 }
 

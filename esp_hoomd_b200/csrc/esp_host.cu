@@ -343,9 +343,12 @@ struct esp_batch {
                int use_graph);
     // want_energy = false (MD steps whose energies are overwritten by the
     // next step) leaves the pair energies out of force.w and energy
+    // virial_pp / external: HOOMD's per-particle virial (6 x pitch floats)
+    // and the terms no particle owns (7 doubles per system), both optional
     int compute(cudaStream_t st, const float* pos4, const float* q, const unsigned* head, const unsigned* nn,
                 const unsigned* nl, float* force4, double* energy, double* virial, int flags,
-                bool want_energy = true);
+                bool want_energy = true, float* virial_pp = nullptr, int vpp_pitch = 0,
+                double* external = nullptr);
     int spread_only(cudaStream_t st, const float* pos4, const float* q, double* rho_out);
     int build_nlist(cudaStream_t st, const float* pos4, double rlist, int cap, unsigned* head, unsigned* nn,
                     unsigned* nl);
@@ -800,7 +803,7 @@ LaunchArgs esp_batch::args() const {
 
 int esp_batch::compute(cudaStream_t st, const float* pos4, const float* q, const unsigned* head, const unsigned* nn,
                        const unsigned* nl, float* force4, double* energy, double* virial, int flags,
-                       bool want_energy) {
+                       bool want_energy, float* virial_pp, int vpp_pitch, double* external) {
     if (f64) return fail(ESP_ERR_UNSUPPORTED, "context planned for FP64: use esp_compute_f64");
     if (!pos4 || !q || !force4) return fail(ESP_ERR_INVALID, "null position, charge or force pointer");
     if (!(flags & ESP_ALL)) return fail(ESP_ERR_INVALID, "flags select no term");
@@ -817,8 +820,13 @@ int esp_batch::compute(cudaStream_t st, const float* pos4, const float* q, const
     a.force = reinterpret_cast<float4*>(force4);
     if (energy) a.energy = energy;
     if (virial) a.virial = virial;
-    a.want_virial = virial != nullptr;
+    if (virial_pp && vpp_pitch < totN) return fail(ESP_ERR_INVALID, "virial pitch below the particle count");
+    a.want_virial = virial != nullptr || virial_pp != nullptr || external != nullptr;
     a.want_energy = (want_energy || a.want_virial) ? 1 : 0;
+    a.virial_pp = virial_pp;
+    a.vpp_pitch = vpp_pitch;
+    a.external = external;
+    if (virial_pp) ESPB_CK(cudaMemsetAsync(virial_pp, 0, (size_t)6 * vpp_pitch * sizeof(float), st));
     a.nl_head = head;
     a.nl_n = nn;
     a.nl_list = nl;
@@ -834,7 +842,8 @@ int esp_batch::compute(cudaStream_t st, const float* pos4, const float* q, const
     // array, concurrently with spread -> FFT -> interpolation (whose kernels
     // leave issue slots idle), and is added before the totals. Stage timing
     // keeps the sequential order so that per-stage times stay separable.
-    const bool fork = lr && sr && !timer.on && d_fsr;
+    // (not with a per-particle virial: the pair and exclusion kernels both add to it)
+    const bool fork = lr && sr && !timer.on && d_fsr && !virial_pp;
     if (fork) {
         ESPB_CK(cudaEventRecord(ev_fork, st));
         ESPB_CK(cudaStreamWaitEvent(st2, ev_fork, 0));
@@ -1361,6 +1370,22 @@ int esp_compute(esp_ctx* c, void* stream, const float* pos4, const float* charge
         return 0;
     }
     return c->b.compute((cudaStream_t)stream, pos4, charge, head, n_neigh, nlist, force4, energy, virial6, flags);
+}
+
+int esp_compute_hoomd(esp_ctx* c, void* stream, const float* pos4, const float* charge, int N, const unsigned* head,
+                      const unsigned* n_neigh, const unsigned* nlist, float* force4, float* virial_pp,
+                      int virial_pitch, double* external7, int flags) {
+    if (!c) return fail(ESP_ERR_INVALID, "null context");
+    if (N <= 0) return fail(ESP_ERR_INVALID, "particle count must be positive");
+    if (!virial_pp || !external7) return fail(ESP_ERR_INVALID, "null virial or external-term pointer");
+    if (N != c->N || c->dirty) {
+        c->N = N;
+        int rc = c->b.plan(c->prm, 1, &c->N, c->L, nullptr);
+        if (rc) return rc;
+        c->dirty = false;
+    }
+    return c->b.compute((cudaStream_t)stream, pos4, charge, head, n_neigh, nlist, force4, nullptr, nullptr, flags,
+                        true, virial_pp, virial_pitch, external7);
 }
 
 int esp_compute_f64(esp_ctx* c, void* stream, const double* pos4, const double* charge, int N, const unsigned* head,

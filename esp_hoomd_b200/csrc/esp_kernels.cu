@@ -1426,7 +1426,7 @@ __global__ void __launch_bounds__(256, EN ? 5 : 6)
     k_pair(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
            const float4* __restrict__ posq, const uint32_t* __restrict__ head, const uint32_t* __restrict__ nn,
            const uint32_t* __restrict__ nlist, float4* __restrict__ force, double* __restrict__ acc, int accumulate,
-           const PairCoef pc) {
+           const PairCoef pc, float* __restrict__ vpp, int vpitch) {
     __shared__ double red[32 * 7];
     const int2 ch = chunks[blockIdx.x];
     const SysDev S = sys[ch.x];
@@ -1514,6 +1514,17 @@ __global__ void __launch_bounds__(256, EN ? 5 : 6)
         f.w += 0.5f * en;
         force[i] = f;
     }
+    if (VIR && vpp) {
+        // this particle's half of its pairs' virial (HOOMD's per-particle virial)
+        float v[6] = {ev.vxx, ev.vxy, ev.vxz, ev.vyy, ev.vyz, ev.vzz};
+#pragma unroll
+        for (int o = TPP / 2; o > 0; o >>= 1)
+#pragma unroll
+            for (int k = 0; k < 6; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+        if (valid && sub == 0)
+#pragma unroll
+            for (int k = 0; k < 6; ++k) vpp[(size_t)k * vpitch + i] += 0.5f * v[k];
+    }
     if (VIR) {
         double e[7] = {sub == 0 ? 0.5 * (double)en : 0.0, 0.5 * (double)ev.vxx, 0.5 * (double)ev.vxy,
                        0.5 * (double)ev.vxz, 0.5 * (double)ev.vyy, 0.5 * (double)ev.vyz, 0.5 * (double)ev.vzz};
@@ -1531,19 +1542,24 @@ __global__ void __launch_bounds__(256, EN ? 5 : 6)
 }
 
 // Energy and virial per system: E = sum_i e_i + E_bg; W = W_k + W_pair + E_bg I.
+// external (may be NULL): the terms no particle owns, {E_bg, W_k + E_bg I}.
 __global__ void k_finalize(const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets, int nsys,
                            const double* __restrict__ acc, double* __restrict__ energy, double* __restrict__ virial,
-                           int add_bg) {
+                           int add_bg, double* __restrict__ external) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nsys) return;
     const SysDev S = sys[s];
     const double* a = acc + s * ACC_STRIDE;
     const double Q = a[ACC_QSUM];
     const double ebg = add_bg ? psets[S.pset].bg_coef * Q * Q / S.V : 0.0;
+    const int diag[6] = {1, 0, 0, 1, 0, 1};
     if (energy) energy[s] = a[ACC_E] + ebg;
-    if (virial) {
-        const int diag[6] = {1, 0, 0, 1, 0, 1};
-        for (int k = 0; k < 6; ++k) virial[s * 6 + k] = a[ACC_WK + k] + a[ACC_WP + k] + (diag[k] ? ebg : 0.0);
+    if (virial)
+        for (int k = 0; k < 6; ++k)
+            virial[s * 6 + k] = a[ACC_WK + k] + a[ACC_WP + k] + a[ACC_WX + k] + (diag[k] ? ebg : 0.0);
+    if (external) {
+        external[7 * s] = ebg;
+        for (int k = 0; k < 6; ++k) external[7 * s + 1 + k] = a[ACC_WK + k] + (diag[k] ? ebg : 0.0);
     }
 }
 
@@ -1741,7 +1757,8 @@ template <int TPP, bool VIR, bool EN>
 static cudaError_t launch_pair_t(const LaunchArgs& a, cudaStream_t st) {
 #define ESPB_PAIR(NQ)                                                                                        \
     k_pair<TPP, NQ, VIR, EN><<<a.n_pchunks, 256, 0, st>>>(a.pchunks, a.sys, a.psets, a.posq, a.nl_head, a.nl_n, \
-                                                          a.nl_list, a.force, a.acc, a.accumulate, a.pc)
+                                                          a.nl_list, a.force, a.acc, a.accumulate, a.pc,    \
+                                                          a.virial_pp, a.vpp_pitch)
     if (a.nq <= 8) ESPB_PAIR(8);
     else if (a.nq <= 10) ESPB_PAIR(10);
     else if (a.nq <= 11) ESPB_PAIR(11);
@@ -1799,7 +1816,8 @@ cudaError_t launch_pair(const LaunchArgs& a, cudaStream_t st) {
 __global__ void k_exclusions(const int2* __restrict__ chunks, const SysDev* __restrict__ sys,
                              const ParamSet* __restrict__ psets, const float4* __restrict__ posq,
                              const uint32_t* __restrict__ n_ex, const uint32_t* __restrict__ ex_list, int ex_pitch,
-                             float4* __restrict__ force, double* __restrict__ acc) {
+                             float4* __restrict__ force, double* __restrict__ acc, float* __restrict__ vpp,
+                             int vpitch) {
     __shared__ double red[32 * 7];
     const int2 ch = chunks[blockIdx.x];
     const SysDev S = sys[ch.x];
@@ -1853,13 +1871,16 @@ __global__ void k_exclusions(const int2* __restrict__ chunks, const SysDev* __re
         fo.z += fz;
         fo.w += en;
         force[i] = fo;
+        if (vpp)
+#pragma unroll
+            for (int k = 0; k < 6; ++k) vpp[(size_t)k * vpitch + i] += 0.5f * v[k];
     }
     double e[7] = {(double)en, 0.5 * v[0], 0.5 * v[1], 0.5 * v[2], 0.5 * v[3], 0.5 * v[4], 0.5 * v[5]};
     block_sum_f64<7>(e, red);
     if (threadIdx.x == 0) {
         atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_E], e[0]);
 #pragma unroll
-        for (int k = 0; k < 6; ++k) atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_WK + k], e[1 + k]);
+        for (int k = 0; k < 6; ++k) atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_WX + k], e[1 + k]);
     }
 }
 
@@ -1887,12 +1908,13 @@ cudaError_t launch_add_forces(const int2* chunks, int n_chunks, const SysDev* sy
 cudaError_t launch_exclusions(const LaunchArgs& a, cudaStream_t st) {
     if (a.n_chunks == 0 || !a.ex_n) return cudaSuccess;
     k_exclusions<<<a.n_chunks, 256, 0, st>>>(a.chunks, a.sys, a.psets, a.posq, a.ex_n, a.ex_list, a.ex_pitch,
-                                             a.force, a.acc);
+                                             a.force, a.acc, a.virial_pp, a.vpp_pitch);
     return cudaGetLastError();
 }
 
 cudaError_t launch_finalize(const LaunchArgs& a, cudaStream_t st) {
-    k_finalize<<<(a.nsys + 127) / 128, 128, 0, st>>>(a.sys, a.psets, a.nsys, a.acc, a.energy, a.virial, a.add_bg);
+    k_finalize<<<(a.nsys + 127) / 128, 128, 0, st>>>(a.sys, a.psets, a.nsys, a.acc, a.energy, a.virial, a.add_bg,
+                                                     a.external);
     return cudaGetLastError();
 }
 

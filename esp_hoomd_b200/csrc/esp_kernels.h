@@ -99,6 +99,13 @@ struct LaunchArgs {
     const uint32_t* nl_head = nullptr;
     const uint32_t* nl_n = nullptr;
     const uint32_t* nl_list = nullptr;
+    // HOOMD ForceCompute outputs: per-particle virial virial_pp[k * vpp_pitch + i]
+    // (k = xx, xy, xz, yy, yz, zz; pair and exclusion terms, cleared by the
+    // host first) and per system the terms no particle owns,
+    // external[7 s] = {E_bg, W_k + E_bg I (6)}
+    float* virial_pp = nullptr;
+    int vpp_pitch = 0;
+    double* external = nullptr;
     const uint32_t* ex_n = nullptr;     // exclusions: row i holds ex_list[i * ex_pitch + k], k < ex_n[i]
     const uint32_t* ex_list = nullptr;
     int ex_pitch = 0;

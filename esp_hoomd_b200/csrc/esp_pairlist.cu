@@ -138,7 +138,8 @@ __global__ void __launch_bounds__(PC_THREADS)
                  const ParamSet* __restrict__ psets, const uint32_t* __restrict__ cstart,
                  const uint32_t* __restrict__ slot2idx, const float4* __restrict__ posq,
                  const uint32_t* __restrict__ nn, const uint16_t* __restrict__ nl16, int cap, int stage_cap,
-                 float4* __restrict__ force, double* __restrict__ acc, int accumulate, const PairCoef pc) {
+                 float4* __restrict__ force, double* __restrict__ acc, int accumulate, const PairCoef pc,
+                 float* __restrict__ vpp, int vpitch) {
     extern __shared__ __align__(128) unsigned char pc_smem[];
     float4* stg = reinterpret_cast<float4*>(pc_smem);
     CellNbhd& nb = *reinterpret_cast<CellNbhd*>(pc_smem + (size_t)(stage_cap + 1) * 16);
@@ -197,6 +198,7 @@ __global__ void __launch_bounds__(PC_THREADS)
     ev.iLz = S.inv_Lz;
     const uint32_t sub = (uint32_t)tid & (PC_LANES - 1);
     double en_sys = 0.0;
+    float vt[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // this lane's pair virial over all its particles
     for (uint32_t p0 = c0; p0 < c1; p0 += PC_THREADS / PC_LANES) {
         const uint32_t slot = p0 + (uint32_t)tid / PC_LANES;
         const bool valid = slot < c1;
@@ -237,10 +239,28 @@ __global__ void __launch_bounds__(PC_THREADS)
             force[i] = f;
             if (EN) en_sys += 0.5 * (double)e;
         }
+        if (VIR) {
+            float v[6] = {ev.vxx, ev.vxy, ev.vxz, ev.vyy, ev.vyz, ev.vzz};
+#pragma unroll
+            for (int k = 0; k < 6; ++k) vt[k] += v[k];
+            ev.vxx = ev.vxy = ev.vxz = ev.vyy = ev.vyz = ev.vzz = 0.f;
+            if (vpp) {
+                // this particle's half of its pairs' virial (HOOMD's per-particle virial)
+#pragma unroll
+                for (int o = PC_LANES / 2; o > 0; o >>= 1)
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+                if (valid && sub == 0) {
+                    const uint32_t i = slot2idx[slot];
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) vpp[(size_t)k * vpitch + i] += 0.5f * v[k];
+                }
+            }
+        }
     }
     if (VIR) {
-        double v[7] = {en_sys, 0.5 * (double)ev.vxx, 0.5 * (double)ev.vxy, 0.5 * (double)ev.vxz,
-                       0.5 * (double)ev.vyy, 0.5 * (double)ev.vyz, 0.5 * (double)ev.vzz};
+        double v[7] = {en_sys, 0.5 * (double)vt[0], 0.5 * (double)vt[1], 0.5 * (double)vt[2],
+                       0.5 * (double)vt[3], 0.5 * (double)vt[4], 0.5 * (double)vt[5]};
         block_sum_f64<7>(v, red);
         if (tid == 0) {
             atomicAdd(&acc[si * ACC_STRIDE + ACC_E], v[0]);
@@ -264,7 +284,7 @@ static cudaError_t launch_pc_t(const LaunchArgs& a, cudaStream_t st) {
     if (a.nq <= NQ) {                                                                                              \
         k_pair_cells<NQ, VIR, EN><<<L.n_cells, PC_THREADS, smem, st>>>(                                            \
             L.cell_sys, a.sys, L.cells, a.psets, L.cstart, L.slot2idx, a.posq, L.nn, L.nl16, L.cap, L.stage_cap, \
-            a.force, a.acc, a.accumulate, a.pc);                                                                   \
+            a.force, a.acc, a.accumulate, a.pc, a.virial_pp, a.vpp_pitch);                                         \
         return cudaGetLastError();                                                                                 \
     }
     ESPB_PC_NQ(ESPB_PC_LAUNCH)

@@ -71,6 +71,18 @@ class Context:
                                     _ptr(nn), _ptr(nl), _ptr(force4), _ptr(energy), _ptr(virial), int(flags)),
               "esp_compute")
 
+    def compute_hoomd(self, pos4: torch.Tensor, q: torch.Tensor, force4: torch.Tensor, virial_pp: torch.Tensor,
+                      external: torch.Tensor, nlist=None, flags: int = _lib.ESP_ALL, stream=None) -> None:
+        """HOOMD ForceCompute outputs: force4 (m_force), virial_pp [6, pitch]
+        float32 (m_virial), external [7] float64 (m_external_energy, then
+        m_external_virial)."""
+        head, nn, nl = nlist if nlist is not None else (None, None, None)
+        if virial_pp.dim() != 2 or virial_pp.shape[0] != 6 or virial_pp.dtype != torch.float32:
+            raise ValueError("virial_pp: float32 tensor of shape [6, pitch] expected")
+        check(self._lib.esp_compute_hoomd(self._h, _stream(stream), _ptr(pos4), _ptr(q), int(pos4.shape[0]),
+                                          _ptr(head), _ptr(nn), _ptr(nl), _ptr(force4), _ptr(virial_pp),
+                                          int(virial_pp.shape[1]), _ptr(external), int(flags)), "esp_compute_hoomd")
+
     def compute_f64(self, pos4: torch.Tensor, q: torch.Tensor, force4: torch.Tensor,
                     energy: Optional[torch.Tensor] = None, virial: Optional[torch.Tensor] = None, nlist=None,
                     flags: int = _lib.ESP_ALL, stream=None) -> None:

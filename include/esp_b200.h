@@ -111,6 +111,21 @@ int esp_compute(esp_ctx* ctx, void* stream, const float* pos4, const float* char
                 const unsigned* head, const unsigned* n_neigh, const unsigned* nlist,
                 float* force4, double* energy, double* virial6, int flags);
 
+/* One evaluation written in the output contract of HOOMD's ForceCompute, as
+ * the reference's ESPForceCompute fills it (src/ESPForceCompute.cc:96-127):
+ * force4 as esp_compute (m_force: force and per-particle energy, the mesh,
+ * self and pair terms); virial_pp[k * virial_pitch + i], k = xx, xy, xz, yy,
+ * yz, zz (m_virial, device floats, virial_pitch >= N): particle i's half of
+ * the virial of its pairs (short-range term and exclusion corrections);
+ * external7 (device doubles) = {E_ext, W_ext xx, xy, xz, yy, yz, zz}
+ * (m_external_energy, m_external_virial): the terms no particle owns -- the
+ * neutralising background energy and the k-space virial plus the
+ * background's. Sum_i force4[i].w + E_ext and sum_i virial_pp + W_ext are the
+ * totals esp_compute returns. */
+int esp_compute_hoomd(esp_ctx* ctx, void* stream, const float* pos4, const float* charge, int N,
+                      const unsigned* head, const unsigned* n_neigh, const unsigned* nlist, float* force4,
+                      float* virial_pp, int virial_pitch, double* external7, int flags);
+
 /* FP64 evaluation (contexts created with precision ESP_FP64), for HOOMD
  * double builds: positions and forces are 4 doubles per particle (Scalar4 =
  * double4), charges doubles; otherwise as esp_compute. Every stage runs in

@@ -210,7 +210,17 @@ def kspace_virial(rk, params, G=None, B=None):
         float(np.sum(Ek))
 
 
-def pair_forces(pos, q, box, split, rcut, nl_head, nl_count, nl_list):
+def _per_particle_virial(N, i_idx, f, d):
+    """HOOMD's per-particle virial: half of each listed pair's r_a F_b on
+    the listing particle, [N, 6] in the order xx, xy, xz, yy, yz, zz."""
+    comps = [(0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2)]
+    Wpp = np.zeros((N, 6))
+    for k, (a, b) in enumerate(comps):
+        np.add.at(Wpp[:, k], i_idx, 0.5 * f * d[:, a] * d[:, b])
+    return Wpp
+
+
+def pair_forces(pos, q, box, split, rcut, nl_head, nl_count, nl_list, per_particle=False):
     """Short-range term over a full CSR neighbour list (HOOMD layout:
     neighbours of i are nl_list[nl_head[i] : nl_head[i] + nl_count[i]]).
 
@@ -218,7 +228,8 @@ def pair_forces(pos, q, box, split, rcut, nl_head, nl_count, nl_list):
     ``src/EvaluatorPairPSWF.h:274-295``): ``pair_eng = qiqj L(r)``,
     ``force_divr = qiqj (-dL/dr) / r`` with
     ``4 pi L = 1/r - Q(r^2/r_c^2)/r_c``.  Energy is split half per particle
-    as HOOMD does. Returns (F[N,3], e[N], virial[6]).
+    as HOOMD does. Returns (F[N,3], e[N], virial[6]) and, with
+    per_particle, the per-particle virial [N, 6] as a fourth value.
     """
     pos = np.asarray(pos, dtype=np.float64)
     L = np.asarray(box, dtype=np.float64)
@@ -245,10 +256,12 @@ def pair_forces(pos, q, box, split, rcut, nl_head, nl_count, nl_list):
     np.add.at(en, i_idx, 0.5 * e)
     W = 0.5 * np.einsum("p,pa,pb->ab", f, d, d)
     vir = np.array([W[0, 0], W[0, 1], W[0, 2], W[1, 1], W[1, 2], W[2, 2]])
+    if per_particle:
+        return F, en, vir, _per_particle_virial(N, i_idx, f, d)
     return F, en, vir
 
 
-def exclusion_correction(pos, q, box, split, rcut, n_ex, ex_list, ex_pitch):
+def exclusion_correction(pos, q, box, split, rcut, n_ex, ex_list, ex_pitch, per_particle=False):
     """Removes the mesh's long-range interaction of excluded pairs
     (``gpu_esp_fix_exclusions_kernel``, ``src/ESPForceComputeGPU.cu:391-471``).
 
@@ -257,7 +270,8 @@ def exclusion_correction(pos, q, box, split, rcut, n_ex, ex_list, ex_pitch):
     cutoff, the bare ``1/(4 pi r)`` beyond it (the reference skips excluded
     pairs beyond r_c). Exclusions of particle i are
     ``ex_list[i * ex_pitch + k], k < n_ex[i]``, listed from both sides; each
-    side takes half of the pair energy. Returns (F[N,3], e[N], virial[6]).
+    side takes half of the pair energy. Returns (F[N,3], e[N], virial[6])
+    and, with per_particle, the per-particle virial [N, 6].
     """
     pos = np.asarray(pos, dtype=np.float64)
     L = np.asarray(box, dtype=np.float64)
@@ -283,6 +297,8 @@ def exclusion_correction(pos, q, box, split, rcut, n_ex, ex_list, ex_pitch):
     np.add.at(en, i_idx, -0.5 * qq * phi)
     W = 0.5 * np.einsum("p,pa,pb->ab", f, d, d)
     vir = np.array([W[0, 0], W[0, 1], W[0, 2], W[1, 1], W[1, 2], W[2, 2]])
+    if per_particle:
+        return F, en, vir, _per_particle_virial(N, i_idx, f, d)
     return F, en, vir
 
 

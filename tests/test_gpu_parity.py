@@ -451,3 +451,48 @@ def test_nlist_row_overflow_is_reported():
     for i in range(0, s.N, 97):
         row = set(l[h[i]:h[i] + cap].tolist())
         assert row <= set(rl[rh[i]:rh[i] + rc[i]].tolist())
+
+
+def test_hoomd_forcecompute_contract():
+    """esp_compute_hoomd fills HOOMD's ForceCompute arrays: m_force as
+    esp_compute, m_virial per particle (pair + exclusion halves) against the
+    oracle's per-particle virial, and the terms no particle owns (background
+    energy; k-space + background virial) in the external slots, with
+    per-particle sums + external = esp_compute's totals."""
+    w = systems.water(216, seed=77)
+    w.pos = w.pos.astype(np.float32).astype(np.float64)
+    excl = R.molecule_exclusions(216, 3)
+    nlh = R.remove_pairs(R.neighbor_list(w.pos, w.box, 0.9), *excl)
+    ctx = native.Context(native.make_params(rcut=0.9, mesh=(24, 24, 24)), w.box, w.N)
+    n_ex = torch.as_tensor(excl[0].astype(np.int32), device="cuda")
+    ex = torch.as_tensor(excl[1].astype(np.int32), device="cuda")
+    ctx.set_exclusions(n_ex, ex, excl[2])
+    pos4, q = _upload(w)
+    nl = _nlist_dev(*nlh)
+    f_tot = torch.zeros((w.N, 4), dtype=torch.float32, device="cuda")
+    e_tot = torch.zeros(1, dtype=torch.float64, device="cuda")
+    v_tot = torch.zeros(6, dtype=torch.float64, device="cuda")
+    ctx.compute(pos4, q, f_tot, e_tot, v_tot, nlist=nl)
+    pitch = w.N + 13  # HOOMD pads m_virial rows to a pitch
+    f = torch.zeros((w.N, 4), dtype=torch.float32, device="cuda")
+    vpp = torch.full((6, pitch), 7.0, dtype=torch.float32, device="cuda")  # must be overwritten
+    ext = torch.zeros(7, dtype=torch.float64, device="cuda")
+    ctx.compute_hoomd(pos4, q, f, vpp, ext, nlist=nl)
+    torch.cuda.synchronize()
+    fa, fb = f.double().cpu().numpy(), f_tot.double().cpu().numpy()
+    assert R.rel_rms(fa[:, :3], fb[:, :3]) <= 1e-6
+    W = v_tot.cpu().numpy()
+    V = vpp.double().cpu().numpy()[:, :w.N]
+    X = ext.cpu().numpy()
+    assert np.abs(V.sum(1) + X[1:] - W).max() <= 1e-5 * np.abs(W).max()
+    assert abs(fa[:, 3].sum() + X[0] - e_tot.item()) <= 1e-5 * R.INV_4PI * np.sum(w.q ** 2) / 0.9
+    # against the oracle: per-particle virial of the pair and exclusion terms,
+    # the background energy and the k-space + background virial
+    prm = _oracle_params(ctx.info(), w.box)
+    _, _, _, Wp = R.pair_forces(w.pos, w.q, w.box, prm.split, prm.rcut, *nlh, per_particle=True)
+    _, _, _, Wx = R.exclusion_correction(w.pos, w.q, w.box, prm.split, prm.rcut, *excl, per_particle=True)
+    Wpp = (Wp + Wx).T
+    assert np.abs(V - Wpp).max() <= 1e-5 * np.abs(Wpp).max()
+    E, F, Wt, parts = R.esp(w.pos, w.q, prm, nlist=nlh, exclusions=excl, return_parts=True)
+    assert abs(X[0] - parts["E_bg"]) <= 1e-6 * abs(parts["E_bg"]) + 1e-12
+    assert np.abs(X[1:] - parts["W_k"]).max() <= 1e-5 * np.abs(parts["W_k"]).max()
