@@ -30,7 +30,7 @@ EXPORTS = [
     "esp_server_get_stats", "esp_server_destroy", "esp_set_exclusions", "esp_batch_set_exclusions",
     "esp_compute_f64", "esp_batch_compute_f64", "esp_batch_autotune", "esp_batch_lj", "esp_batch_lj_f64",
     "esp_batch_nve_step1_f64", "esp_batch_nve_step2_f64", "esp_batch_build_pairlist", "esp_batch_pairlist_check",
-    "esp_compute_hoomd",
+    "esp_compute_hoomd", "esp_batch_set_rigid_water",
 ]
 
 ESP_FP32 = 0
@@ -120,7 +120,7 @@ def get_lib() -> ctypes.CDLL:
         lib.esp_pswf_eval_pairs.argtypes = [P, I, P, P, D, I, P, P, P, P, P, P, P]
         lib.esp_batch_build_nlist.argtypes = [P, P, P, D, I, P, P, P]
         lib.esp_batch_nve_step1.argtypes = [P, P, P, P, P, D]
-        lib.esp_batch_nve_step2.argtypes = [P, P, P, P, D]
+        lib.esp_batch_nve_step2.argtypes = [P, P, P, P, P, D]
         lib.esp_spread.argtypes = [P, P, P, P, I, P]
         lib.esp_get_sort.argtypes = [P, P, P, P]
         lib.esp_get_potential.argtypes = [P, P, P]
@@ -141,7 +141,8 @@ def get_lib() -> ctypes.CDLL:
         lib.esp_batch_lj.argtypes = [P, P, P, P, P, P, D, D, D, P, P]
         lib.esp_batch_lj_f64.argtypes = [P, P, P, P, P, P, D, D, D, P, P]
         lib.esp_batch_nve_step1_f64.argtypes = [P, P, P, P, P, D]
-        lib.esp_batch_nve_step2_f64.argtypes = [P, P, P, P, D]
+        lib.esp_batch_nve_step2_f64.argtypes = [P, P, P, P, P, D]
+        lib.esp_batch_set_rigid_water.argtypes = [P, P, P, D, D]
         lib.esp_batch_autotune.argtypes = [P, P, P, P, P, P, P, I, I, ctypes.POINTER(EspParams), P, I]
         lib.esp_spread_noalloc.argtypes = [P, ctypes.POINTER(EspParams), D, D, D, P, P, I, P]
         lib.esp_batch_build_pairlist.argtypes = [P, P, P, D, I]

@@ -286,6 +286,15 @@ struct esp_batch {
     int plan64(const std::vector<float2>& tw, long long g_total);
     int compute_f64(cudaStream_t st, const double* pos4, const double* q, const unsigned* head, const unsigned* nn,
                     const unsigned* nl, double* force4, double* energy, double* virial, int flags);
+    // rigid (O, H, H) molecules of the MD harness (SETTLE / RATTLE)
+    DevAlloc rgmem;
+    int2* d_mols = nullptr;   // {system, first atom}
+    int2* d_rskip = nullptr;  // per system: local range of the molecules' atoms
+    int n_mols = 0;
+    double r_doh = 0, r_dhh = 0;
+    int set_rigid(const int* first, const int* count, double d_oh, double d_hh);
+    int nve1(cudaStream_t st, void* pos4, void* vel4, const void* force4, double dt, bool f64);
+    int nve2(cudaStream_t st, const void* pos4, void* vel4, const void* force4, double dt, bool f64);
     // excluded pairs (caller-owned device arrays), applied by every
     // long-range evaluation
     const uint32_t* ex_n = nullptr;
@@ -368,6 +377,10 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
     const bool same_systems = ns == nsys && std::equal(N_, N_ + ns, N.begin()) &&
                               std::equal(boxes, boxes + 3 * ns, box.begin());
     if (!same_systems) {
+        rgmem.release();
+        n_mols = 0;
+        d_mols = nullptr;
+        d_rskip = nullptr;
         cg_nl.mem.release();
         cg_nl.rlist = -1;
         cg_pl.mem.release();
@@ -903,16 +916,15 @@ int esp_batch::md_run(cudaStream_t st, float* pos4, float* vel4, const float* q,
     // one, so only the last step evaluates the pair energies.
     auto step = [&](bool with_energy) -> int {
         timer.begin(ESP_STAGE_NVE, st);
-        ESPB_CK(launch_nve1(d_chunks, n_chunks, d_sys, reinterpret_cast<float4*>(pos4),
-                            reinterpret_cast<float4*>(vel4), reinterpret_cast<const float4*>(force4), (float)dt, st));
+        int rc = nve1(st, pos4, vel4, force4, dt, false);
         timer.end(st);
-        int rc = compute(st, pos4, q, head, nn, nl, force4, energy, virial, ESP_ALL, with_energy);
+        if (rc) return rc;
+        rc = compute(st, pos4, q, head, nn, nl, force4, energy, virial, ESP_ALL, with_energy);
         if (rc) return rc;
         timer.begin(ESP_STAGE_NVE, st);
-        ESPB_CK(launch_nve2(d_chunks, n_chunks, d_sys, reinterpret_cast<float4*>(vel4),
-                            reinterpret_cast<const float4*>(force4), (float)dt, st));
+        rc = nve2(st, pos4, vel4, force4, dt, false);
         timer.end(st);
-        return 0;
+        return rc;
     };
     if (!use_graph || timer.on) {
         for (int k = 0; k < nsteps; ++k) {
@@ -1177,6 +1189,55 @@ int esp_batch::pairlist_check(bool wait, int* needed) {
         return fail(ESP_ERR_OVERFLOW, "pair-list row capacity exceeded (largest row " + std::to_string(h_pl_ovf[1]) +
                                           "); rebuild with a larger cap");
     }
+    return 0;
+}
+
+int esp_batch::set_rigid(const int* first, const int* count, double d_oh, double d_hh) {
+    rgmem.release();
+    n_mols = 0;
+    d_mols = nullptr;
+    d_rskip = nullptr;
+    drop_graphs();  // captured steps hold the previous molecule list
+    if (!first || !count) return 0;
+    if (!(d_oh > 0) || !(d_hh > 0) || d_hh >= 2.0 * d_oh)
+        return fail(ESP_ERR_INVALID, "rigid water needs 0 < d_hh < 2 d_oh");
+    std::vector<int2> mols, skip(nsys);
+    for (int s = 0; s < nsys; ++s) {
+        if (count[s] < 0 || first[s] < 0 || (long long)first[s] + 3LL * count[s] > N[s])
+            return fail(ESP_ERR_INVALID, "rigid molecules outside system " + std::to_string(s));
+        for (int m = 0; m < count[s]; ++m) mols.push_back(make_int2(s, sd[s].p_off + first[s] + 3 * m));
+        skip[s] = make_int2(first[s], first[s] + 3 * count[s]);
+    }
+    int rc = 0;
+    if ((rc = rgmem.get(d_mols, mols.size())) || (rc = rgmem.get(d_rskip, nsys))) return rc;
+    if (!mols.empty()) ESPB_CK(cudaMemcpy(d_mols, mols.data(), mols.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    ESPB_CK(cudaMemcpy(d_rskip, skip.data(), nsys * sizeof(int2), cudaMemcpyHostToDevice));
+    n_mols = (int)mols.size();
+    r_doh = d_oh;
+    r_dhh = d_hh;
+    return 0;
+}
+
+int esp_batch::nve1(cudaStream_t st, void* pos4, void* vel4, const void* force4, double dt, bool is64) {
+    const int2* skip = n_mols ? d_rskip : nullptr;
+    if (is64)
+        ESPB_CK(launch_nve64(1, d_chunks, n_chunks, d_sys, reinterpret_cast<double4*>(pos4),
+                             reinterpret_cast<double4*>(vel4), reinterpret_cast<const double4*>(force4), dt, st, skip));
+    else
+        ESPB_CK(launch_nve1(d_chunks, n_chunks, d_sys, reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4),
+                            reinterpret_cast<const float4*>(force4), (float)dt, st, skip));
+    if (n_mols) ESPB_CK(launch_settle1(d_mols, n_mols, d_sys, pos4, vel4, force4, dt, r_doh, r_dhh, is64, st));
+    return 0;
+}
+
+int esp_batch::nve2(cudaStream_t st, const void* pos4, void* vel4, const void* force4, double dt, bool is64) {
+    if (is64)
+        ESPB_CK(launch_nve64(2, d_chunks, n_chunks, d_sys, nullptr, reinterpret_cast<double4*>(vel4),
+                             reinterpret_cast<const double4*>(force4), dt, st));
+    else
+        ESPB_CK(launch_nve2(d_chunks, n_chunks, d_sys, reinterpret_cast<float4*>(vel4),
+                            reinterpret_cast<const float4*>(force4), (float)dt, st));
+    if (n_mols) ESPB_CK(launch_settle2(d_mols, n_mols, d_sys, pos4, vel4, is64, st));
     return 0;
 }
 
@@ -1570,10 +1631,7 @@ int esp_batch_build_nlist(esp_batch* b, void* stream, const float* pos4, double 
 
 int esp_batch_nve_step1(esp_batch* b, void* stream, float* pos4, float* vel4, const float* force4, double dt) {
     if (!b || !pos4 || !vel4 || !force4) return fail(ESP_ERR_INVALID, "null argument");
-    ESPB_CK(launch_nve1(b->d_chunks, b->n_chunks, b->d_sys, reinterpret_cast<float4*>(pos4),
-                        reinterpret_cast<float4*>(vel4), reinterpret_cast<const float4*>(force4), (float)dt,
-                        (cudaStream_t)stream));
-    return 0;
+    return b->nve1((cudaStream_t)stream, pos4, vel4, force4, dt, false);
 }
 
 int esp_batch_lj(esp_batch* b, void* stream, const float* pos4, const unsigned* head, const unsigned* n_neigh,
@@ -1597,24 +1655,25 @@ int esp_batch_lj_f64(esp_batch* b, void* stream, const double* pos4, const unsig
 
 int esp_batch_nve_step1_f64(esp_batch* b, void* stream, double* pos4, double* vel4, const double* force4, double dt) {
     if (!b || !pos4 || !vel4 || !force4) return fail(ESP_ERR_INVALID, "null argument");
-    ESPB_CK(launch_nve64(1, b->d_chunks, b->n_chunks, b->d_sys, reinterpret_cast<double4*>(pos4),
-                         reinterpret_cast<double4*>(vel4), reinterpret_cast<const double4*>(force4), dt,
-                         (cudaStream_t)stream));
-    return 0;
+    return b->nve1((cudaStream_t)stream, pos4, vel4, force4, dt, true);
 }
 
-int esp_batch_nve_step2_f64(esp_batch* b, void* stream, double* vel4, const double* force4, double dt) {
+int esp_batch_nve_step2_f64(esp_batch* b, void* stream, const double* pos4, double* vel4, const double* force4,
+                            double dt) {
     if (!b || !vel4 || !force4) return fail(ESP_ERR_INVALID, "null argument");
-    ESPB_CK(launch_nve64(2, b->d_chunks, b->n_chunks, b->d_sys, nullptr, reinterpret_cast<double4*>(vel4),
-                         reinterpret_cast<const double4*>(force4), dt, (cudaStream_t)stream));
-    return 0;
+    if (b->n_mols && !pos4) return fail(ESP_ERR_INVALID, "rigid molecules need the positions");
+    return b->nve2((cudaStream_t)stream, pos4, vel4, force4, dt, true);
 }
 
-int esp_batch_nve_step2(esp_batch* b, void* stream, float* vel4, const float* force4, double dt) {
+int esp_batch_nve_step2(esp_batch* b, void* stream, const float* pos4, float* vel4, const float* force4, double dt) {
     if (!b || !vel4 || !force4) return fail(ESP_ERR_INVALID, "null argument");
-    ESPB_CK(launch_nve2(b->d_chunks, b->n_chunks, b->d_sys, reinterpret_cast<float4*>(vel4),
-                        reinterpret_cast<const float4*>(force4), (float)dt, (cudaStream_t)stream));
-    return 0;
+    if (b->n_mols && !pos4) return fail(ESP_ERR_INVALID, "rigid molecules need the positions");
+    return b->nve2((cudaStream_t)stream, pos4, vel4, force4, dt, false);
+}
+
+int esp_batch_set_rigid_water(esp_batch* b, const int* first, const int* count, double d_oh, double d_hh) {
+    if (!b) return fail(ESP_ERR_INVALID, "null batch");
+    return b->set_rigid(first, count, d_oh, d_hh);
 }
 
 }  // extern "C"

@@ -232,12 +232,19 @@ __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ ce
     }
 }
 
+// skip (may be NULL): per system, the local particle range [x, y) of rigid
+// molecules, which the constraint kernels integrate instead
 __global__ void k_nve1(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, float4* __restrict__ pos,
-                       float4* __restrict__ vel, const float4* __restrict__ force, float dt) {
+                       float4* __restrict__ vel, const float4* __restrict__ force, float dt,
+                       const int2* __restrict__ skip) {
     const int2 ch = chunks[blockIdx.x];
     const SysDev& S = sys[ch.x];
     const int i = ch.y + threadIdx.x;
     if (i >= S.p_off + S.N) return;
+    if (skip) {
+        const int2 r = skip[ch.x];
+        if (i - S.p_off >= r.x && i - S.p_off < r.y) return;
+    }
     float4 v = vel[i];
     const float4 f = force[i];
     const float h = 0.5f * dt / v.w;
@@ -318,11 +325,16 @@ __global__ void k_lj(const int2* __restrict__ chunks, const SysDev* __restrict__
 }
 
 __global__ void k64_nve1(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, double4* __restrict__ pos,
-                         double4* __restrict__ vel, const double4* __restrict__ force, double dt) {
+                         double4* __restrict__ vel, const double4* __restrict__ force, double dt,
+                         const int2* __restrict__ skip) {
     const int2 ch = chunks[blockIdx.x];
     const SysDev& S = sys[ch.x];
     const int i = ch.y + threadIdx.x;
     if (i >= S.p_off + S.N) return;
+    if (skip) {
+        const int2 r = skip[ch.x];
+        if (i - S.p_off >= r.x && i - S.p_off < r.y) return;
+    }
     double4 v = vel[i];
     const double4 f = force[i];
     const double h = 0.5 * dt / v.w;
@@ -371,9 +383,9 @@ cudaError_t launch_lj(const int2* chunks, int n_chunks, const SysDev* sys, const
 }
 
 cudaError_t launch_nve64(int half, const int2* chunks, int n_chunks, const SysDev* sys, double4* pos, double4* vel,
-                         const double4* force, double dt, cudaStream_t st) {
+                         const double4* force, double dt, cudaStream_t st, const int2* skip) {
     if (n_chunks == 0) return cudaSuccess;
-    if (half == 1) k64_nve1<<<n_chunks, 256, 0, st>>>(chunks, sys, pos, vel, force, dt);
+    if (half == 1) k64_nve1<<<n_chunks, 256, 0, st>>>(chunks, sys, pos, vel, force, dt, skip);
     else k64_nve2<<<n_chunks, 256, 0, st>>>(chunks, sys, vel, force, dt);
     return cudaGetLastError();
 }
@@ -397,9 +409,9 @@ cudaError_t launch_nlist(const NlistArgs& a, cudaStream_t st) {
 }
 
 cudaError_t launch_nve1(const int2* chunks, int n_chunks, const SysDev* sys, float4* pos, float4* vel,
-                        const float4* force, float dt, cudaStream_t st) {
+                        const float4* force, float dt, cudaStream_t st, const int2* skip) {
     if (n_chunks == 0) return cudaSuccess;
-    k_nve1<<<n_chunks, 256, 0, st>>>(chunks, sys, pos, vel, force, dt);
+    k_nve1<<<n_chunks, 256, 0, st>>>(chunks, sys, pos, vel, force, dt, skip);
     return cudaGetLastError();
 }
 

@@ -40,14 +40,23 @@ struct NlistArgs {
 };
 
 cudaError_t launch_nlist(const NlistArgs& a, cudaStream_t st);
+// skip: per-system local ranges of rigid molecules left to launch_settle1 (may be NULL)
 cudaError_t launch_nve1(const int2* chunks, int n_chunks, const SysDev* sys, float4* pos, float4* vel,
-                        const float4* force, float dt, cudaStream_t st);
+                        const float4* force, float dt, cudaStream_t st, const int2* skip = nullptr);
 cudaError_t launch_nve2(const int2* chunks, int n_chunks, const SysDev* sys, float4* vel, const float4* force,
                         float dt, cudaStream_t st);
 cudaError_t launch_lj(const int2* chunks, int n_chunks, const SysDev* sys, const void* pos, const uint32_t* head,
                       const uint32_t* nn, const uint32_t* nl, double eps, double sigma, double rcut, void* force,
                       double* energy, bool f64, cudaStream_t st);
 cudaError_t launch_nve64(int half, const int2* chunks, int n_chunks, const SysDev* sys, double4* pos, double4* vel,
-                         const double4* force, double dt, cudaStream_t st);
+                         const double4* force, double dt, cudaStream_t st, const int2* skip = nullptr);
+// Rigid (O, H, H) molecules (esp_settle.cu): mols[t] = {system, first atom
+// (concatenated index)}; f64 selects double4 arrays. settle1: first
+// velocity-Verlet half with SETTLE; settle2: RATTLE velocity constraint
+// after the second half kick.
+cudaError_t launch_settle1(const int2* mols, int n_mols, const SysDev* sys, void* pos, void* vel, const void* force,
+                           double dt, double d_oh, double d_hh, bool f64, cudaStream_t st);
+cudaError_t launch_settle2(const int2* mols, int n_mols, const SysDev* sys, const void* pos, void* vel, bool f64,
+                           cudaStream_t st);
 
 }  // namespace espb

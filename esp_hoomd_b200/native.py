@@ -203,9 +203,22 @@ class Batch:
         check(self._lib.esp_batch_nve_step1(self._h, _stream(stream), _ptr(pos4), _ptr(vel4), _ptr(force4),
                                             float(dt)), "esp_batch_nve_step1")
 
-    def nve_step2(self, vel4, force4, dt: float, stream=None) -> None:
-        check(self._lib.esp_batch_nve_step2(self._h, _stream(stream), _ptr(vel4), _ptr(force4), float(dt)),
-              "esp_batch_nve_step2")
+    def nve_step2(self, vel4, force4, dt: float, pos4=None, stream=None) -> None:
+        """Second half kick; pos4 (the current positions) is needed with rigid molecules."""
+        check(self._lib.esp_batch_nve_step2(self._h, _stream(stream), _ptr(pos4), _ptr(vel4), _ptr(force4),
+                                            float(dt)), "esp_batch_nve_step2")
+
+    def set_rigid_water(self, first, count, d_oh: float, d_hh: float) -> None:
+        """Rigid (O, H, H) molecules: system s has count[s] consecutive triples
+        from local particle first[s]; None clears."""
+        if first is None:
+            check(self._lib.esp_batch_set_rigid_water(self._h, None, None, 0.0, 0.0), "esp_batch_set_rigid_water")
+            return
+        f = np.ascontiguousarray(np.asarray(first, dtype=np.int32))
+        c = np.ascontiguousarray(np.asarray(count, dtype=np.int32))
+        check(self._lib.esp_batch_set_rigid_water(self._h, f.ctypes.data_as(ctypes.c_void_p),
+                                                  c.ctypes.data_as(ctypes.c_void_p), float(d_oh), float(d_hh)),
+              "esp_batch_set_rigid_water")
 
     def md_run(self, pos4, vel4, q, force4, energy, virial, nlist, nsteps: int, dt: float, use_graph: bool = True,
                stream=None) -> None:
@@ -255,9 +268,9 @@ class Batch:
         check(self._lib.esp_batch_nve_step1_f64(self._h, _stream(stream), _ptr(pos4), _ptr(vel4), _ptr(force4),
                                                 float(dt)), "esp_batch_nve_step1_f64")
 
-    def nve_step2_f64(self, vel4, force4, dt: float, stream=None) -> None:
-        check(self._lib.esp_batch_nve_step2_f64(self._h, _stream(stream), _ptr(vel4), _ptr(force4), float(dt)),
-              "esp_batch_nve_step2_f64")
+    def nve_step2_f64(self, vel4, force4, dt: float, pos4=None, stream=None) -> None:
+        check(self._lib.esp_batch_nve_step2_f64(self._h, _stream(stream), _ptr(pos4), _ptr(vel4), _ptr(force4),
+                                                float(dt)), "esp_batch_nve_step2_f64")
 
     def set_timing(self, on: bool) -> None:
         check(self._lib.esp_batch_set_timing(self._h, int(bool(on))), "esp_batch_set_timing")

@@ -273,14 +273,30 @@ int esp_batch_pairlist_check(esp_batch* b, int* needed_cap);
 
 /* Velocity-Verlet halves on the concatenated arrays: vel4 = (vx, vy, vz,
  * mass). step1: v += dt/2 F/m; x += dt v (wrapped into the box).
- * step2: v += dt/2 F/m. */
+ * step2: v += dt/2 F/m. With rigid molecules set (esp_batch_set_rigid_water)
+ * step1 constrains their positions (SETTLE) and step2 their velocities
+ * (RATTLE), which needs pos4 (the positions after step1); pos4 may be NULL
+ * otherwise. */
 int esp_batch_nve_step1(esp_batch* b, void* stream, float* pos4, float* vel4, const float* force4, double dt);
-int esp_batch_nve_step2(esp_batch* b, void* stream, float* vel4, const float* force4, double dt);
+int esp_batch_nve_step2(esp_batch* b, void* stream, const float* pos4, float* vel4, const float* force4, double dt);
 
 /* FP64 velocity-Verlet halves (double4 positions, velocities with mass in
  * w, forces), as esp_batch_nve_step1/2. */
 int esp_batch_nve_step1_f64(esp_batch* b, void* stream, double* pos4, double* vel4, const double* force4, double dt);
-int esp_batch_nve_step2_f64(esp_batch* b, void* stream, double* vel4, const double* force4, double dt);
+int esp_batch_nve_step2_f64(esp_batch* b, void* stream, const double* pos4, double* vel4, const double* force4,
+                            double dt);
+
+/* Rigid three-site molecules (no reference counterpart: HOOMD supplies the
+ * constraints the reference's users would run; the water workloads are rigid
+ * O-H-H molecules). System s holds count[s] molecules as consecutive (O, H,
+ * H) triples from its local particle first[s] on, with O-H distance d_oh and
+ * H-H distance d_hh (the two H of a molecule of equal mass; masses from
+ * vel4.w). The velocity-Verlet steps (esp_batch_nve_step1/2 and their FP64
+ * forms, esp_batch_md_run) keep them rigid: SETTLE (Miyamoto & Kollman 1992)
+ * for positions, RATTLE for velocities. The initial positions must satisfy
+ * the constraints and velocities have no bond-stretching components.
+ * first = count = NULL clears. Host arrays of nsys ints. */
+int esp_batch_set_rigid_water(esp_batch* b, const int* first, const int* count, double d_oh, double d_hh);
 
 /* Lennard-Jones core repulsion of the harness, 4 eps ((sigma/r)^12 -
  * (sigma/r)^6) for r < r_cut (no shift), over the full neighbour list:
