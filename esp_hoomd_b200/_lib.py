@@ -66,7 +66,7 @@ class EspRequest(ctypes.Structure):
                 ("nsteps", ctypes.c_int), ("dt", ctypes.c_double), ("arrival", ctypes.c_double),
                 ("pos4", ctypes.c_void_p), ("vel4", ctypes.c_void_p), ("charge", ctypes.c_void_p),
                 ("out_pos4", ctypes.c_void_p), ("out_vel4", ctypes.c_void_p), ("out_force4", ctypes.c_void_p),
-                ("out_energy", ctypes.c_void_p)]
+                ("out_energy", ctypes.c_void_p), ("rigid_doh", ctypes.c_double), ("rigid_dhh", ctypes.c_double)]
 
 
 class EspRequestStatus(ctypes.Structure):

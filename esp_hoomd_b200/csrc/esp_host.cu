@@ -288,9 +288,10 @@ struct esp_batch {
                     const unsigned* nl, double* force4, double* energy, double* virial, int flags);
     // rigid (O, H, H) molecules of the MD harness (SETTLE / RATTLE)
     DevAlloc rgmem;
-    int2* d_mols = nullptr;   // {system, first atom}
+    int4* d_mols = nullptr;   // {system, first atom, molecules} per SETTLE_CHUNK molecules
     int2* d_rskip = nullptr;  // per system: local range of the molecules' atoms
-    int n_mols = 0;
+    double2* d_geo = nullptr; // (d_OH, d_HH)
+    int n_mols = 0;           // work items
     double r_doh = 0, r_dhh = 0;
     int set_rigid(const int* first, const int* count, double d_oh, double d_hh);
     int nve1(cudaStream_t st, void* pos4, void* vel4, const void* force4, double dt, bool f64);
@@ -1201,16 +1202,21 @@ int esp_batch::set_rigid(const int* first, const int* count, double d_oh, double
     if (!first || !count) return 0;
     if (!(d_oh > 0) || !(d_hh > 0) || d_hh >= 2.0 * d_oh)
         return fail(ESP_ERR_INVALID, "rigid water needs 0 < d_hh < 2 d_oh");
-    std::vector<int2> mols, skip(nsys);
+    std::vector<int4> mols;
+    std::vector<int2> skip(nsys);
     for (int s = 0; s < nsys; ++s) {
         if (count[s] < 0 || first[s] < 0 || (long long)first[s] + 3LL * count[s] > N[s])
             return fail(ESP_ERR_INVALID, "rigid molecules outside system " + std::to_string(s));
-        for (int m = 0; m < count[s]; ++m) mols.push_back(make_int2(s, sd[s].p_off + first[s] + 3 * m));
+        for (int m = 0; m < count[s]; m += SETTLE_CHUNK)
+            mols.push_back(make_int4(s, sd[s].p_off + first[s] + 3 * m, std::min(SETTLE_CHUNK, count[s] - m), 0));
         skip[s] = make_int2(first[s], first[s] + 3 * count[s]);
     }
     int rc = 0;
-    if ((rc = rgmem.get(d_mols, mols.size())) || (rc = rgmem.get(d_rskip, nsys))) return rc;
-    if (!mols.empty()) ESPB_CK(cudaMemcpy(d_mols, mols.data(), mols.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    if ((rc = rgmem.get(d_mols, mols.size())) || (rc = rgmem.get(d_rskip, nsys)) || (rc = rgmem.get(d_geo, 1)))
+        return rc;
+    const double2 geo = make_double2(d_oh, d_hh);
+    ESPB_CK(cudaMemcpy(d_geo, &geo, sizeof(double2), cudaMemcpyHostToDevice));
+    if (!mols.empty()) ESPB_CK(cudaMemcpy(d_mols, mols.data(), mols.size() * sizeof(int4), cudaMemcpyHostToDevice));
     ESPB_CK(cudaMemcpy(d_rskip, skip.data(), nsys * sizeof(int2), cudaMemcpyHostToDevice));
     n_mols = (int)mols.size();
     r_doh = d_oh;
@@ -1226,7 +1232,7 @@ int esp_batch::nve1(cudaStream_t st, void* pos4, void* vel4, const void* force4,
     else
         ESPB_CK(launch_nve1(d_chunks, n_chunks, d_sys, reinterpret_cast<float4*>(pos4), reinterpret_cast<float4*>(vel4),
                             reinterpret_cast<const float4*>(force4), (float)dt, st, skip));
-    if (n_mols) ESPB_CK(launch_settle1(d_mols, n_mols, d_sys, pos4, vel4, force4, dt, r_doh, r_dhh, is64, st));
+    if (n_mols) ESPB_CK(launch_settle1(d_mols, n_mols, d_sys, pos4, vel4, force4, dt, d_geo, is64, st));
     return 0;
 }
 

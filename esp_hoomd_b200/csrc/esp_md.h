@@ -50,13 +50,15 @@ cudaError_t launch_lj(const int2* chunks, int n_chunks, const SysDev* sys, const
                       double* energy, bool f64, cudaStream_t st);
 cudaError_t launch_nve64(int half, const int2* chunks, int n_chunks, const SysDev* sys, double4* pos, double4* vel,
                          const double4* force, double dt, cudaStream_t st, const int2* skip = nullptr);
-// Rigid (O, H, H) molecules (esp_settle.cu): mols[t] = {system, first atom
-// (concatenated index)}; f64 selects double4 arrays. settle1: first
-// velocity-Verlet half with SETTLE; settle2: RATTLE velocity constraint
-// after the second half kick.
-cudaError_t launch_settle1(const int2* mols, int n_mols, const SysDev* sys, void* pos, void* vel, const void* force,
-                           double dt, double d_oh, double d_hh, bool f64, cudaStream_t st);
-cudaError_t launch_settle2(const int2* mols, int n_mols, const SysDev* sys, const void* pos, void* vel, bool f64,
+// Rigid (O, H, H) molecules (esp_settle.cu): work items {system, first atom
+// (concatenated index), molecules <= SETTLE_CHUNK, geometry index into geo
+// = (d_OH, d_HH)}, one CTA each; f64 selects double4 arrays. settle1: first
+// velocity-Verlet half with SETTLE; settle2: RATTLE velocity constraint after
+// the second half kick.
+constexpr int SETTLE_CHUNK = 128;
+cudaError_t launch_settle1(const int4* items, int n_items, const SysDev* sys, void* pos, void* vel,
+                           const void* force, double dt, const double2* geo, bool f64, cudaStream_t st);
+cudaError_t launch_settle2(const int4* items, int n_items, const SysDev* sys, const void* pos, void* vel, bool f64,
                            cudaStream_t st);
 
 }  // namespace espb

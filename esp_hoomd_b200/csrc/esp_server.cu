@@ -119,6 +119,7 @@ struct Request {
     int mesh[3] = {0, 0, 0};
     int ntile[3] = {0, 0, 0};
     int cap = 0, pset = 0;
+    int geo = -1;  // rigid water: index into the geometry table, else -1
     int steps_done = 0;
     bool evaluated = false;
     long long footprint = 0;
@@ -186,6 +187,14 @@ struct esp_server {
     int2 *d_chunks = nullptr, *d_pchunks = nullptr, *d_mdchunks = nullptr, *d_nlchunks = nullptr;
     int2 *d_pitems = nullptr, *d_sitems = nullptr;
     int4 *d_xitems = nullptr, *d_yitems = nullptr, *d_zitems = nullptr;
+    // rigid water (SETTLE): per-slot atom range the plain integrator skips,
+    // per-round work items, and the (d_OH, d_HH) geometries seen so far
+    int2* d_rskip = nullptr;
+    int4* d_ritems = nullptr;
+    double2* d_geo = nullptr;
+    std::vector<double2> geos;
+    static constexpr int MAX_GEOS = 16;
+    long long ritem_cap = 0;
     long long chunk_cap = 0, pchunk_cap = 0;
     static constexpr long long ITEM_CAP = 1 << 20;
 
@@ -287,6 +296,7 @@ int esp_server::init(const esp_server_config& cfg) {
     }
     chunk_cap = P_cap / 256 + max_slots + 16;
     pchunk_cap = P_cap / 8 + max_slots + 16;  // 256 / tpp >= 8 particles per chunk
+    ritem_cap = P_cap / (3 * SETTLE_CHUNK) + max_slots + 16;
     int rc = 0;
     if ((rc = mem.get(d_sys, max_slots)) || (rc = mem.get(d_pset, MAX_PSETS)) || (rc = mem.get(d_cells, max_slots)) ||
         (rc = mem.get(d_cell_sys, C_cap)) || (rc = mem.get(d_pos, P_cap)) || (rc = mem.get(d_vel, P_cap)) ||
@@ -305,7 +315,8 @@ int esp_server::init(const esp_server_config& cfg) {
         (rc = mem.get(d_chunks, chunk_cap)) || (rc = mem.get(d_pchunks, pchunk_cap)) ||
         (rc = mem.get(d_mdchunks, chunk_cap)) || (rc = mem.get(d_nlchunks, (max_particles + 255) / 256)) ||
         (rc = mem.get(d_pitems, ITEM_CAP)) || (rc = mem.get(d_sitems, ITEM_CAP)) || (rc = mem.get(d_xitems, ITEM_CAP)) ||
-        (rc = mem.get(d_yitems, ITEM_CAP)) || (rc = mem.get(d_zitems, ITEM_CAP)))
+        (rc = mem.get(d_yitems, ITEM_CAP)) || (rc = mem.get(d_zitems, ITEM_CAP)) ||
+        (rc = mem.get(d_rskip, max_slots)) || (rc = mem.get(d_ritems, ritem_cap)) || (rc = mem.get(d_geo, MAX_GEOS)))
         return rc;
     stats.arena_bytes = mem.bytes;
     ESPB_CK(cudaMemcpy(d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice));
@@ -531,6 +542,20 @@ int esp_server::admit(Request* q, Staging& sg) {
     S.radz = radix_plan(S.nz);
     int rc = upload(sg, d_sys + q->slot, &S, sizeof(SysDev));
     if (rc) return rc;
+    // rigid water: geometry index and the atoms the plain integrator skips
+    q->geo = -1;
+    if (r.rigid_doh > 0) {
+        for (size_t g = 0; g < geos.size(); ++g)
+            if (geos[g].x == r.rigid_doh && geos[g].y == r.rigid_dhh) q->geo = (int)g;
+        if (q->geo < 0) {
+            if ((int)geos.size() >= MAX_GEOS) return fail(ESP_ERR_UNSUPPORTED, "more than 16 rigid-water geometries");
+            q->geo = (int)geos.size();
+            geos.push_back(make_double2(r.rigid_doh, r.rigid_dhh));
+            if ((rc = upload(sg, d_geo + q->geo, &geos.back(), sizeof(double2)))) return rc;
+        }
+    }
+    const int2 skip = make_int2(0, q->geo >= 0 ? r.N : 0);
+    if ((rc = upload(sg, d_rskip + q->slot, &skip, sizeof(int2)))) return rc;
     // inputs (caller's host memory) and tile owner table
     ESPB_CK(cudaMemcpyAsync(d_pos + q->p_off, r.pos4, (size_t)r.N * 16, cudaMemcpyHostToDevice, st));
     ESPB_CK(cudaMemcpyAsync(d_q + q->p_off, r.charge, (size_t)r.N * 4, cudaMemcpyHostToDevice, st));
@@ -610,7 +635,7 @@ void esp_server::release(Request* q) {
 // ---------------------------------------------------------------------------
 int esp_server::launch_round(Staging& sg) {
     std::vector<int2> chunks, pchunks, mdchunks, pit, sit;
-    std::vector<int4> xit, yit, zit;
+    std::vector<int4> xit, yit, zit, ritems;
     const int ppb = 256 / tpp;
     int nmax[3] = {4, 4, 4};
     int smem_plane = 0, smem_slab = 0;
@@ -618,8 +643,12 @@ int esp_server::launch_round(Staging& sg) {
         const int s = q->slot, N = q->r.N, po = (int)q->p_off;
         for (int i = 0; i < N; i += 256) chunks.push_back(make_int2(s, po + i));
         for (int i = 0; i < N; i += ppb) pchunks.push_back(make_int2(s, po + i));
-        if (q->evaluated)
+        if (q->evaluated) {
             for (int i = 0; i < N; i += 256) mdchunks.push_back(make_int2(s, po + i));
+            if (q->geo >= 0)
+                for (int m = 0; m < N / 3; m += SETTLE_CHUNK)
+                    ritems.push_back(make_int4(s, po + 3 * m, std::min(SETTLE_CHUNK, N / 3 - m), q->geo));
+        }
         const int nx = q->mesh[0], ny = q->mesh[1], nz = q->mesh[2], nxh = nx / 2 + 1;
         nmax[0] = std::max(nmax[0], nx);
         nmax[1] = std::max(nmax[1], ny);
@@ -644,7 +673,7 @@ int esp_server::launch_round(Staging& sg) {
     }
     if ((long long)chunks.size() > chunk_cap || (long long)pchunks.size() > pchunk_cap ||
         (long long)pit.size() > ITEM_CAP || (long long)sit.size() > ITEM_CAP || (long long)xit.size() > ITEM_CAP ||
-        (long long)yit.size() > ITEM_CAP || (long long)zit.size() > ITEM_CAP)
+        (long long)yit.size() > ITEM_CAP || (long long)zit.size() > ITEM_CAP || (long long)ritems.size() > ritem_cap)
         return fail(ESP_ERR_UNSUPPORTED, "work lists exceed their buffers");
     int rc = 0;
     if ((rc = upload(sg, d_chunks, chunks.data(), chunks.size() * sizeof(int2))) ||
@@ -654,7 +683,8 @@ int esp_server::launch_round(Staging& sg) {
         (rc = upload(sg, d_sitems, sit.data(), sit.size() * sizeof(int2))) ||
         (rc = upload(sg, d_xitems, xit.data(), xit.size() * sizeof(int4))) ||
         (rc = upload(sg, d_yitems, yit.data(), yit.size() * sizeof(int4))) ||
-        (rc = upload(sg, d_zitems, zit.data(), zit.size() * sizeof(int4))))
+        (rc = upload(sg, d_zitems, zit.data(), zit.size() * sizeof(int4))) ||
+        (rc = upload(sg, d_ritems, ritems.data(), ritems.size() * sizeof(int4))))
         return rc;
     LaunchArgs a;
     a.pc = pc;
@@ -719,7 +749,8 @@ int esp_server::launch_round(Staging& sg) {
     const float dt = active.empty() ? 0.f : (float)active[0]->r.dt;
     // NVE first half for the systems past their first evaluation; systems
     // of one round share dt (checked at submit)
-    ESPB_CK(launch_nve1(d_mdchunks, (int)mdchunks.size(), d_sys, d_pos, d_vel, d_force, dt, st));
+    ESPB_CK(launch_nve1(d_mdchunks, (int)mdchunks.size(), d_sys, d_pos, d_vel, d_force, dt, st, d_rskip));
+    ESPB_CK(launch_settle1(d_ritems, (int)ritems.size(), d_sys, d_pos, d_vel, d_force, dt, d_geo, false, st));
     ESPB_CK(cudaMemsetAsync(d_acc, 0, (size_t)max_slots * ACC_STRIDE * sizeof(double), st));
     ESPB_CK(launch_bin(a, st));
     ESPB_CK(launch_sort(a, st));
@@ -729,6 +760,7 @@ int esp_server::launch_round(Staging& sg) {
     ESPB_CK(launch_pair(a, st));
     ESPB_CK(launch_finalize(a, st));
     ESPB_CK(launch_nve2(d_mdchunks, (int)mdchunks.size(), d_sys, d_vel, d_force, dt, st));
+    ESPB_CK(launch_settle2(d_ritems, (int)ritems.size(), d_sys, d_pos, d_vel, false, st));
     n_rounds++;
 
     Round rd;
@@ -924,6 +956,8 @@ int esp_server_submit(esp_server* s, const esp_request* r, long long* id) {
     if (r->nsteps < 0) return fail(ESP_ERR_INVALID, "negative step count");
     if (r->nsteps > 0 && (!r->vel4 || !(r->dt > 0))) return fail(ESP_ERR_INVALID, "NVE steps need velocities and dt > 0");
     if (!r->pos4 || !r->charge) return fail(ESP_ERR_INVALID, "null input pointer");
+    if (r->rigid_doh > 0 && (r->N % 3 != 0 || !(r->rigid_dhh > 0) || r->rigid_dhh >= 2.0 * r->rigid_doh))
+        return fail(ESP_ERR_INVALID, "rigid water needs N = 3 x molecules and 0 < d_hh < 2 d_oh");
     std::lock_guard<std::mutex> lk(s->mu);
     if (!s->pending.empty() && r->arrival < s->pending.back()->t_arrival)
         return fail(ESP_ERR_INVALID, "arrival times must not decrease");

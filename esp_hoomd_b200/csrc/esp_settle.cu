@@ -3,8 +3,11 @@
 // (1992)). The reference plugin has no constraint code -- HOOMD supplies the
 // integrators -- but the water workloads are rigid (O, H, H) molecules.
 //
-// One thread per molecule, FP64 arithmetic relative to the molecule's oxygen
-// (one periodic image per molecule), masses from the velocity arrays' w.
+// One thread per molecule over work items {system, first atom, molecules,
+// geometry} of up to SETTLE_CHUNK consecutive (O, H, H) triples, the
+// geometry an index into a table of (d_OH, d_HH); FP64 arithmetic
+// relative to the molecule's oxygen (one periodic image per molecule),
+// masses from the velocity arrays' w.
 //
 // Positions: the unconstrained velocity-Verlet update x0 -> x1 is corrected
 // to x3 = x1 + Delta with m_i Delta_i a combination of the old bond vectors.
@@ -94,14 +97,14 @@ __device__ void settle_one(D3 b0, D3 c0, D3 a1, D3 b1, D3 c1, double mo, double 
 // Velocity-Verlet first half for the atoms of rigid molecules (k_nve1 skips
 // them): v += dt/2 F/m, unconstrained x1 = x0 + dt v, SETTLE, v = (x3 - x0)/dt.
 template <typename T4>
-__global__ void k_settle1(const int2* __restrict__ mols, int n_mols, const SysDev* __restrict__ sys,
-                          T4* __restrict__ pos, T4* __restrict__ vel, const T4* __restrict__ force, double dt,
-                          double d_oh, double d_hh) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_mols) return;
-    const int2 mo = mols[t];
-    const SysDev& S = sys[mo.x];
-    const int i = mo.y;
+__global__ void __launch_bounds__(SETTLE_CHUNK)
+    k_settle1(const int4* __restrict__ items, const SysDev* __restrict__ sys, T4* __restrict__ pos,
+              T4* __restrict__ vel, const T4* __restrict__ force, double dt, const double2* __restrict__ geo) {
+    const int4 it = items[blockIdx.x];
+    if ((int)threadIdx.x >= it.z) return;
+    const double d_oh = geo[it.w].x, d_hh = geo[it.w].y;
+    const SysDev& S = sys[it.x];
+    const int i = it.y + 3 * (int)threadIdx.x;
     T4 p[3], v[3];
     D3 x0[3], x1[3], vh[3];
     double m[3];
@@ -141,13 +144,13 @@ __global__ void k_settle1(const int2* __restrict__ mols, int n_mols, const SysDe
 
 // RATTLE velocity constraint after the second half kick.
 template <typename T4>
-__global__ void k_settle2(const int2* __restrict__ mols, int n_mols, const SysDev* __restrict__ sys,
-                          const T4* __restrict__ pos, T4* __restrict__ vel) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_mols) return;
-    const int2 mo = mols[t];
-    const SysDev& S = sys[mo.x];
-    const int i = mo.y;
+__global__ void __launch_bounds__(SETTLE_CHUNK)
+    k_settle2(const int4* __restrict__ items, const SysDev* __restrict__ sys, const T4* __restrict__ pos,
+              T4* __restrict__ vel) {
+    const int4 it = items[blockIdx.x];
+    if ((int)threadIdx.x >= it.z) return;
+    const SysDev& S = sys[it.x];
+    const int i = it.y + 3 * (int)threadIdx.x;
     T4 v[3];
     D3 x[3], u[3];
     double im[3];
@@ -182,27 +185,25 @@ __global__ void k_settle2(const int2* __restrict__ mols, int n_mols, const SysDe
     }
 }
 
-cudaError_t launch_settle1(const int2* mols, int n_mols, const SysDev* sys, void* pos, void* vel, const void* force,
-                           double dt, double d_oh, double d_hh, bool f64, cudaStream_t st) {
-    if (n_mols == 0) return cudaSuccess;
-    const int nb = (n_mols + 127) / 128;
+cudaError_t launch_settle1(const int4* items, int n_items, const SysDev* sys, void* pos, void* vel,
+                           const void* force, double dt, const double2* geo, bool f64, cudaStream_t st) {
+    if (n_items == 0) return cudaSuccess;
     if (f64)
-        k_settle1<double4><<<nb, 128, 0, st>>>(mols, n_mols, sys, (double4*)pos, (double4*)vel,
-                                               (const double4*)force, dt, d_oh, d_hh);
+        k_settle1<double4><<<n_items, SETTLE_CHUNK, 0, st>>>(items, sys, (double4*)pos, (double4*)vel,
+                                                             (const double4*)force, dt, geo);
     else
-        k_settle1<float4><<<nb, 128, 0, st>>>(mols, n_mols, sys, (float4*)pos, (float4*)vel, (const float4*)force,
-                                              dt, d_oh, d_hh);
+        k_settle1<float4><<<n_items, SETTLE_CHUNK, 0, st>>>(items, sys, (float4*)pos, (float4*)vel,
+                                                            (const float4*)force, dt, geo);
     return cudaGetLastError();
 }
 
-cudaError_t launch_settle2(const int2* mols, int n_mols, const SysDev* sys, const void* pos, void* vel, bool f64,
+cudaError_t launch_settle2(const int4* items, int n_items, const SysDev* sys, const void* pos, void* vel, bool f64,
                            cudaStream_t st) {
-    if (n_mols == 0) return cudaSuccess;
-    const int nb = (n_mols + 127) / 128;
+    if (n_items == 0) return cudaSuccess;
     if (f64)
-        k_settle2<double4><<<nb, 128, 0, st>>>(mols, n_mols, sys, (const double4*)pos, (double4*)vel);
+        k_settle2<double4><<<n_items, SETTLE_CHUNK, 0, st>>>(items, sys, (const double4*)pos, (double4*)vel);
     else
-        k_settle2<float4><<<nb, 128, 0, st>>>(mols, n_mols, sys, (const float4*)pos, (float4*)vel);
+        k_settle2<float4><<<n_items, SETTLE_CHUNK, 0, st>>>(items, sys, (const float4*)pos, (float4*)vel);
     return cudaGetLastError();
 }
 

@@ -331,7 +331,8 @@ class Server:
 
     def submit(self, pos4, charge, box: Sequence[float], rcut: float, vel4=None, nsteps: int = 10,
                dt: float = 0.002, skin: float = 0.4, arrival: float = 0.0, nlist_cap: int = 0, out_pos4=None,
-               out_vel4=None, out_force4=None, out_energy=None) -> int:
+               out_vel4=None, out_force4=None, out_energy=None, rigid_water=None) -> int:
+        """rigid_water = (d_oh, d_hh): the system is (O, H, H) triples kept rigid."""
         N = int(len(charge))
         r = _lib.EspRequest()
         r.N = N
@@ -349,6 +350,8 @@ class Server:
         r.out_vel4 = _host_ptr(out_vel4, np.float32, 4 * N, "out_vel4")
         r.out_force4 = _host_ptr(out_force4, np.float32, 4 * N, "out_force4")
         r.out_energy = _host_ptr(out_energy, np.float64, 1, "out_energy")
+        if rigid_water is not None:
+            r.rigid_doh, r.rigid_dhh = (float(v) for v in rigid_water)
         rid = ctypes.c_longlong()
         check(self._lib.esp_server_submit(self._h, ctypes.byref(r), ctypes.byref(rid)), "esp_server_submit")
         self._keep.append((pos4, vel4, charge, out_pos4, out_vel4, out_force4, out_energy))

@@ -365,6 +365,8 @@ typedef struct esp_request {
     float* out_vel4;
     float* out_force4;        /* forces and per-particle energies of the last evaluation */
     double* out_energy;       /* total energy of the last evaluation */
+    double rigid_doh, rigid_dhh; /* > 0: the system is rigid water -- (O, H, H) triples, O-H and H-H
+                                    distances, kept rigid by SETTLE / RATTLE in the NVE steps */
 } esp_request;
 
 typedef struct esp_request_status {

@@ -31,7 +31,7 @@ def _host(s):
 
 
 class _Req:
-    def __init__(self, srv, s, rcut, skin, nsteps, arrival=0.0):
+    def __init__(self, srv, s, rcut, skin, nsteps, arrival=0.0, rigid=None):
         self.s = s
         self.pos4, self.vel4, self.q = _host(s)
         self.out_pos = np.zeros_like(self.pos4)
@@ -40,7 +40,7 @@ class _Req:
         self.out_e = np.zeros(1, np.float64)
         self.id = srv.submit(self.pos4, self.q, s.box, rcut, vel4=self.vel4, nsteps=nsteps, dt=0.002, skin=skin,
                              arrival=arrival, out_pos4=self.out_pos, out_vel4=self.out_vel,
-                             out_force4=self.out_force, out_energy=self.out_e)
+                             out_force4=self.out_force, out_energy=self.out_e, rigid_water=rigid)
 
 
 def _server(budget=2 << 30, slots=64):
@@ -146,3 +146,53 @@ def test_admission_under_budget_and_oversized_request():
     assert 2 <= stt["max_active"] < 40  # the neighbour-list pool holds about 30 of these systems
     assert stt["peak_bytes"] <= 256 << 20
     assert stt["influence_hits"] >= 39  # one influence table for 40 equal boxes
+
+
+def test_served_rigid_water_equals_batch_path():
+    """A water request served with rigid molecules (SETTLE / RATTLE) keeps
+    its O-H and H-H distances (to the FP32 storage limit) and equals the
+    batch path's md_run with the same rigid geometry, split and mesh."""
+    import math
+    d_oh, d_hh = 0.1, 2 * 0.1 * math.sin(math.radians(109.47 / 2))
+    w = systems.water(729, seed=4300)
+    w.vel = np.random.default_rng(3).normal(0, 0.2, w.pos.shape) / np.sqrt(w.mass)[:, None]
+    from oracle import settle as ST
+    L = np.asarray(w.box)
+    x = w.pos.reshape(-1, 3, 3).copy()
+    d = x[:, 1:] - x[:, :1]
+    x[:, 1:] = x[:, :1] + d - L * np.round(d / L)
+    w.vel = ST.rattle_velocities(x, w.vel.reshape(-1, 3, 3), w.mass[:3]).reshape(-1, 3)
+    srv = _server()
+    r = _Req(srv, w, 0.9, 0.1, 10, rigid=(d_oh, d_hh))
+    srv.start()
+    srv.wait_all(300)
+    st = srv.status(r.id)
+    assert st["state"] == 2
+    mesh = [st[k] for k in ("nx", "ny", "nz")]
+    srv.close()
+    m = r.out_pos[:, :3].astype(np.float64).reshape(-1, 3, 3)
+    dd = m[:, 1:] - m[:, :1]
+    dd -= L * np.round(dd / L)
+    doh = np.linalg.norm(dd, axis=-1)
+    dhh = np.linalg.norm(dd[:, 0] - dd[:, 1], axis=-1)
+    ulp = float(np.spacing(np.float32(L.max())))
+    assert np.abs(doh - d_oh).max() <= 4 * ulp
+    assert np.abs(dhh - d_hh).max() <= 4 * ulp
+    # the batch path with the server's split (c = 17, kappa = c / r_c) and mesh
+    b = native.Batch(native.make_params(order=8, rcut=0.9, kappa=17.0 / 0.9, mesh=mesh), [w.N], [w.box])
+    b.set_rigid_water([0], [w.N // 3], d_oh, d_hh)
+    pos4, vel4, q = (torch.tensor(v, device="cuda") for v in _host(w))
+    N = w.N
+    head = torch.zeros(N, dtype=torch.int32, device="cuda")
+    nn = torch.zeros_like(head)
+    nl = torch.zeros(N * 512, dtype=torch.int32, device="cuda")
+    force = torch.zeros((N, 4), device="cuda")
+    energy = torch.zeros(1, dtype=torch.float64, device="cuda")
+    b.build_nlist(pos4, 1.0, 512, head, nn, nl)
+    b.compute(pos4, q, force, energy, None, nlist=(head, nn, nl), flags=ESP_ALL)
+    b.md_run(pos4, vel4, q, force, energy, None, (head, nn, nl), 10, 0.002, use_graph=False)
+    torch.cuda.synchronize()
+    dp = pos4.cpu().numpy()[:, :3] - r.out_pos[:, :3]
+    dp -= L * np.round(dp / L)
+    assert np.abs(dp).max() <= 1e-5
+    assert abs(energy.item() - r.out_e[0]) <= 1e-6 * abs(r.out_e[0])
