@@ -51,6 +51,31 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+PYEXT = os.path.join(HERE, "pyext")
+
+
+def build_pyext(force: bool = False) -> str:
+    """The `_esp` pybind11 module (pyext/esp_module.cpp, host code over the C
+    ABI), linked against libesp_b200.so next to it."""
+    import sysconfig
+
+    import pybind11
+    out = os.path.join(HERE, "_esp" + sysconfig.get_config_var("EXT_SUFFIX"))
+    srcs = [os.path.join(PYEXT, f) for f in os.listdir(PYEXT)] + [LIB, os.path.join(CSRC, "esp_tables.h"),
+                                                                    os.path.join(INC, "esp_b200.h")]
+    if not force and os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(f) for f in srcs):
+        return out
+    cuda = os.path.dirname(os.path.dirname(NVCC))
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden",
+           "-I" + pybind11.get_include(), "-I" + sysconfig.get_paths()["include"], "-I" + INC, "-I" + CSRC,
+           "-I" + PYEXT, "-I" + os.path.join(cuda, "include"), os.path.join(PYEXT, "esp_module.cpp"), "-o", out,
+           "-L" + HERE, "-lesp_b200", "-L" + os.path.join(cuda, "lib64"), "-lcudart",
+           "-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + os.path.join(cuda, "lib64")]
+    subprocess.run(cmd, check=True)
+    return out
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose="--verbose" in sys.argv)
+    build_pyext(force="--force" in sys.argv)
     print(LIB)
