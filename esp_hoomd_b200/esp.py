@@ -7,8 +7,11 @@ the same constructor arguments, properties and validation errors
 (ValueError / TypeError / RuntimeError, src/esp.py:103-126, 225-241,
 355-359, 523-527). HOOMD-blue is not a dependency: the objects attach to the
 small standalone ``Simulation`` below (a stand-in for ``hoomd.Simulation``
-with a cell neighbour list and an NVE integrator), and every computation
-runs in the sm_100a library through ``native`` -- there is no CPU path.
+with a cell neighbour list and an NVE integrator). As in HOOMD, each force
+attaches by creating its C++ object from the compiled ``_esp`` module
+(``ESPForceComputeGPU``, ``PotentialPairPSWFGPU``, src/esp.py:405-425) over
+the simulation's system definition and neighbour list, and computes through
+it; every computation runs in the sm_100a library -- there is no CPU path.
 
 Differences from the reference, all deliberate:
 * ``MAX_ORDER`` is 12 (the reference's C++ limit, src/ESPForceCompute.h:63;
@@ -94,6 +97,7 @@ class NeighborList:
         self.r_cut = 0.0
         self._lists = None
         self._ref_pos = None
+        self._cpp = None  # _esp.NeighborList bound to the lists
         self.builds = 0
 
     def _require(self, r_cut: float) -> None:
@@ -120,7 +124,19 @@ class NeighborList:
             batch.build_nlist(st.pos4, self.r_cut + self.buffer, self.capacity, *self._lists)
             self._ref_pos = st.pos4[:, :3].clone()
             self.builds += 1
+            self._bind(sim)
         return self._lists
+
+    def _cpp_obj(self, sim: "Simulation"):
+        """The C++ NeighborList the forces are constructed with."""
+        if self._cpp is None:
+            from . import _esp
+            self._cpp = _esp.NeighborList(sim._sysdef(), self.buffer)
+        return self._cpp
+
+    def _bind(self, sim: "Simulation") -> None:
+        head, nn, nl = self._lists
+        self._cpp_obj(sim).bindLists(head.data_ptr(), nn.data_ptr(), nl.data_ptr())
 
 
 class State:
@@ -159,9 +175,10 @@ class Force:
 
     def __init__(self) -> None:
         self._simulation: Optional["Simulation"] = None
-        self._force = None   # [N, 4] float32: fx, fy, fz, per-particle energy
-        self._energy = None  # [1] float64
-        self._virial = None  # [6] float64
+        self._cpp = None     # the _esp ForceCompute object (created at attachment)
+        self._force = None   # [N, 4] float32: fx, fy, fz, per-particle energy (m_force)
+        self._vpp = None     # [6, pitch] float32: per-particle virial (m_virial)
+        self._computed = False
 
     @property
     def _attached(self) -> bool:
@@ -169,12 +186,16 @@ class Force:
 
     def _alloc(self, N: int, device) -> None:
         import torch
+        pitch = (N + 31) // 32 * 32
         self._force = torch.zeros((N, 4), dtype=torch.float32, device=device)
-        self._energy = torch.zeros(1, dtype=torch.float64, device=device)
-        self._virial = torch.zeros(6, dtype=torch.float64, device=device)
+        self._vpp = torch.zeros((6, pitch), dtype=torch.float32, device=device)
+        self._computed = False
+
+    def _bind_outputs(self) -> None:
+        self._cpp.bindOutputs(self._force.data_ptr(), self._vpp.data_ptr(), int(self._vpp.shape[1]))
 
     def _need_results(self) -> None:
-        if self._force is None:
+        if self._force is None or not self._computed:
             raise RuntimeError("ESP: no results before the first compute.")
 
     @property
@@ -189,14 +210,16 @@ class Force:
 
     @property
     def energy(self) -> float:
+        """Per-particle energies plus the external (global) energy."""
         self._need_results()
-        return float(self._energy.item())
+        return float(self._force[:, 3].double().sum().item()) + self._cpp.getExternalEnergy()
 
     @property
     def virial(self) -> np.ndarray:
-        """Total virial (xx, xy, xz, yy, yz, zz)."""
+        """Total virial (xx, xy, xz, yy, yz, zz): per-particle plus external."""
         self._need_results()
-        return self._virial.cpu().numpy()
+        N = self._force.shape[0]
+        return self._vpp[:, :N].double().sum(1).cpu().numpy() + np.asarray(self._cpp.getExternalVirial())
 
 
 class Simulation:
@@ -212,6 +235,30 @@ class Simulation:
         self.forces: List[Force] = []
         self.timestep = 0
         self._total = None
+        self._sysdef_obj = None
+        self._harness_batch = None
+
+    def _sysdef(self):
+        """The C++ system definition over the state's device arrays."""
+        if self._sysdef_obj is None:
+            from . import _esp
+            st = self.state
+            pd = _esp.ParticleData(st.N, _esp.BoxDim(*st.box))
+            pd.bindPositions(st.pos4.data_ptr())
+            pd.bindCharges(st.charge.data_ptr())
+            self._sysdef_obj = _esp.SystemDefinition(pd)
+            self._group = _esp.ParticleGroup(self._sysdef_obj)
+        return self._sysdef_obj
+
+    def _harness(self, r_cut: float):
+        """Batch of this one system for the neighbour-list builds and the
+        velocity-Verlet steps (HOOMD's NeighborList and integrator)."""
+        if self._harness_batch is None:
+            from . import native
+            st = self.state
+            self._harness_batch = native.Batch(native.make_params(rcut=min(float(r_cut), 0.5 * min(st.box))),
+                                               [st.N], [st.box])
+        return self._harness_batch
 
     def add(self, *forces: Force) -> None:
         for f in forces:
@@ -243,13 +290,13 @@ class Simulation:
     def run(self, steps: int) -> None:
         if not self.forces:
             raise RuntimeError("ESP: no forces attached.")
-        batch = self.forces[0]._batch_handle()
+        batch = self._harness_batch
         if self.timestep == 0 or self._total is None:
             self.compute()
         for _ in range(int(steps)):
             batch.nve_step1(self.state.pos4, self.state.vel4, self._total, self.dt)
             self.compute()
-            batch.nve_step2(self.state.vel4, self._total, self.dt)
+            batch.nve_step2(self.state.vel4, self._total, self.dt, pos4=self.state.pos4)
             self.timestep += 1
 
 
@@ -289,7 +336,6 @@ class Spectral(Force):
         self._alpha = float(alpha)
         self._n_table = int(n_table)
         self._nlist_buffer = 0.1 * self._r_cut if nlist_buffer is None else float(nlist_buffer)
-        self._batch = None
         self._pair: Optional["Local"] = None
 
     # -- properties (src/esp.py:266-313)
@@ -297,16 +343,14 @@ class Spectral(Force):
     def kappa(self) -> Optional[float]:
         """Split bandwidth in use (1/length): c / r_cut. Before attachment the
         constructor's value (None when automatic)."""
-        if self._batch is not None:
-            inf = self._batch.info(0)
-            return inf["c_split"] / inf["rcut"]
+        if self._cpp is not None and self._computed:
+            return float(self._cpp.getKappa())
         return self._kappa
 
     @property
     def resolution(self) -> Tuple[int, int, int]:
-        if self._batch is not None:
-            inf = self._batch.info(0)
-            return (inf["nx"], inf["ny"], inf["nz"])
+        if self._cpp is not None:
+            return tuple(int(v) for v in self._cpp.getResolution())
         return self._resolution
 
     @property
@@ -367,48 +411,44 @@ class Spectral(Force):
             new["n_table"] = int(n_table)
         self._resolution, self._order, self._kappa = new["resolution"], new["order"], new["kappa"]
         self._r_cut, self._alpha, self._n_table = new["r_cut"], new["alpha"], new["n_table"]
-        self.invalidate()
+        self._set_cpp_params()
+        self._nlist._require(self._r_cut)
         if self._pair is not None:
             self._pair._sync_params_from_spectral()
 
     def invalidate(self) -> None:
         """Rebuild every table on the next compute (src/esp.py:396-403)."""
-        if self._batch is not None:
-            self._batch.close()
-            self._batch = None
+        if self._cpp is not None:
+            self._cpp.invalidate()
+            self._computed = False
 
-    # -- lifecycle
-    def _params(self):
-        from . import native
-        return native.make_params(order=self._order, rcut=self._r_cut,
-                                  kappa=0.0 if self._kappa is None else self._kappa, mesh=self._resolution,
-                                  alpha=self._alpha, n_table=self._n_table)
-
-    def _batch_handle(self):
-        from . import native
-        if self._batch is None:
-            st = self._simulation.state
-            self._batch = native.Batch(self._params(), [st.N], [st.box])
-            self._nlist._require(self._r_cut)
-        return self._batch
+    # -- lifecycle (src/esp.py:405-440: ESPForceCompute(GPU) + setParams)
+    def _set_cpp_params(self) -> None:
+        nx, ny, nz = self._resolution
+        self._cpp.setParams(nx, ny, nz, self._order, 0.0 if self._kappa is None else self._kappa, self._r_cut,
+                            self._alpha, self._n_table)
+        self._computed = False
 
     def _attach_hook(self) -> None:
-        st = self._simulation.state
+        from . import _esp
+        sim = self._simulation
+        st = sim.state
         if 2.0 * self._r_cut > min(st.box):
             raise ValueError("ESP: 'default_r_cut' must not exceed half the box.")
         self._alloc(st.N, st.pos4.device)
         self._nlist._require(self._r_cut)
-        self._batch_handle()
+        sim._harness(self._r_cut)
+        self._cpp = _esp.ESPForceComputeGPU(sim._sysdef(), self._nlist._cpp_obj(sim), sim._group)
+        self._bind_outputs()
+        self._set_cpp_params()
 
     def _detach_hook(self) -> None:
-        self.invalidate()
+        self._cpp = None
+        self._computed = False
 
-    def _compute(self, flags: Optional[int] = None) -> None:
-        from ._lib import ESP_LONG_RANGE
-        b = self._batch_handle()
-        st = self._simulation.state
-        b.compute(st.pos4, st.charge, self._force, self._energy, self._virial,
-                  flags=ESP_LONG_RANGE if flags is None else flags)
+    def _compute(self) -> None:
+        self._cpp.compute(self._simulation.timestep)
+        self._computed = True
 
     def __repr__(self) -> str:
         k = "auto" if self._kappa is None else "%.4g" % self._kappa
@@ -481,26 +521,37 @@ class Local(Force):
             raise ValueError(f"ESP: default_r_cut {self._default_r_cut} differs from the Spectral cutoff {rc}.")
 
     def _attach_hook(self) -> None:
+        from . import _esp
         if not self._spectral._attached or self._spectral._simulation is not self._simulation:
             raise RuntimeError("ESP: attach the associated Spectral object to the same simulation before Local.")
         self._check_cutoffs()
-        st = self._simulation.state
+        sim = self._simulation
+        st = sim.state
         self._alloc(st.N, st.pos4.device)
         self._sync_params_from_spectral()
+        self._cpp = _esp.PotentialPairPSWFGPU(sim._sysdef(), self._nlist._cpp_obj(sim))
+        self._bind_outputs()
+        self._cpp_params = None
 
     def _detach_hook(self) -> None:
         self._spectral._pair = None
-
-    def _batch_handle(self):
-        return self._spectral._batch_handle()
+        self._cpp = None
+        self._computed = False
 
     def _compute(self) -> None:
-        from ._lib import ESP_SHORT_RANGE
         self._check_cutoffs()
-        b = self._spectral._batch_handle()
-        st = self._simulation.state
-        lists = self._nlist.lists(self._simulation, b)
-        b.compute(st.pos4, st.charge, self._force, self._energy, self._virial, nlist=lists, flags=ESP_SHORT_RANGE)
+        sim = self._simulation
+        self._nlist.lists(sim, sim._harness(self._spectral.r_cut))
+        # the split of the Spectral object in use (c = kappa r_c), as the
+        # reference's Local copies it into every type pair (src/esp.py:569-617)
+        p = dict(kappa=float(self._spectral.kappa or 0.0), alpha=self._spectral.alpha,
+                 rcut=self._spectral.r_cut, V_cut=0.0)
+        if p != self._cpp_params:
+            self._cpp.setParams("A", "A", p)
+            self._cpp_params = p
+        self._sync_params_from_spectral()
+        self._cpp.compute(sim.timestep)
+        self._computed = True
 
     def __repr__(self) -> str:
         s = self._spectral
