@@ -30,7 +30,7 @@ EXPORTS = [
     "esp_server_get_stats", "esp_server_destroy", "esp_set_exclusions", "esp_batch_set_exclusions",
     "esp_compute_f64", "esp_batch_compute_f64", "esp_batch_autotune", "esp_batch_lj", "esp_batch_lj_f64",
     "esp_batch_nve_step1_f64", "esp_batch_nve_step2_f64", "esp_batch_build_pairlist", "esp_batch_pairlist_check",
-    "esp_compute_hoomd", "esp_batch_set_rigid_water",
+    "esp_compute_hoomd", "esp_batch_set_rigid_water", "esp_batch_device_errors",
 ]
 
 ESP_FP32 = 0
@@ -44,7 +44,7 @@ class EspParams(ctypes.Structure):
                 ("kappa", ctypes.c_double), ("rcut", ctypes.c_double), ("alpha", ctypes.c_double),
                 ("n_table", ctypes.c_int), ("target_error", ctypes.c_double), ("window_c", ctypes.c_double),
                 ("window_degree", ctypes.c_int), ("tile", ctypes.c_int), ("threads_per_particle", ctypes.c_int),
-                ("precision", ctypes.c_int), ("fft_mode", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("fft_mode", ctypes.c_int), ("interp_mode", ctypes.c_int)]
 
 
 class EspInfo(ctypes.Structure):
@@ -146,6 +146,7 @@ def get_lib() -> ctypes.CDLL:
         lib.esp_batch_autotune.argtypes = [P, P, P, P, P, P, P, I, I, ctypes.POINTER(EspParams), P, I]
         lib.esp_spread_noalloc.argtypes = [P, ctypes.POINTER(EspParams), D, D, D, P, P, I, P]
         lib.esp_batch_build_pairlist.argtypes = [P, P, P, D, I]
+        lib.esp_batch_device_errors.argtypes = [P, ctypes.POINTER(ctypes.c_int)]
         lib.esp_compute_hoomd.argtypes = [P, P, P, P, I, P, P, P, P, P, I, P, I]
         lib.esp_batch_pairlist_check.argtypes = [P, ctypes.POINTER(ctypes.c_int)]
         for name in EXPORTS:

@@ -49,7 +49,20 @@ struct SysDev {
     int pset;          // parameter-set index
     int twx, twy, twz; // twiddle-table offsets per axis
     uint32_t radx, rady, radz;  // packed radix plans (4 bits per stage)
+    // potential mesh with a periodic halo: nxp x nyp x nzp (x fastest) at
+    // element offset mp_off, point (x, y, z) holding phi(x mod nx, y mod ny,
+    // z mod nz), so every tile's extended region is one box without wrap
+    long long mp_off;
+    int nxp, nyp, nzp;
 };
+
+// Padded extent of the halo potential mesh along an axis of n points with
+// tiles of edge T and support P: every tile's extended region [t T, t T +
+// T + P - 1) lies inside; x rows are rounded up to whole 16-byte groups.
+__host__ __device__ inline int halo_extent(int n, int T, int P, bool x_axis) {
+    const int e = ((n + T - 1) / T) * T + P - 1;
+    return x_axis ? (e + 3) & ~3 : e;
+}
 
 struct ParamSet {
     float wcoef[MAX_P * (MAX_D + 1)];  // window polynomial [a][j] in t

@@ -16,6 +16,8 @@
 #include <tuple>
 #include <vector>
 
+#include <cuda.h>
+
 #include "esp_b200.h"
 #include "esp_host_util.h"
 #include "esp_kernels.h"
@@ -124,6 +126,39 @@ int build_param_set(double c, double cw, int P, int D, double rcut, PsetHost& h,
     d.bg_coef = -0.25 * rcut * rcut * h.split.m2;
     d.rcut_d = rcut;
     return 0;
+}
+
+void interp_box(int E, int& BX, int& BY) {
+    BX = E + 3;
+    while (BX % 8 != 4) ++BX;
+    BY = E | 1;
+}
+
+bool encode_phi_map(void* map, float* base, int nxp, int nyp, int nzp, int BX, int BY, int BZ) {
+    typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static EncodeTiled fn = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(f);
+        looked_up = true;
+    }
+    if (!fn) return false;
+    // 16-byte rules of the tensor map: base, strides and the box's inner extent
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || (nxp & 3) || (BX & 3) || BX > 256 || BY > 256 || BZ > 256)
+        return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)nxp, (cuuint64_t)nyp, (cuuint64_t)nzp};
+    const cuuint64_t strides[2] = {(cuuint64_t)nxp * 4, (cuuint64_t)nxp * nyp * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)BX, (cuuint32_t)BY, (cuuint32_t)BZ};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return fn(reinterpret_cast<CUtensorMap*>(map), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 void influence_inputs(const SysDev& S, const PsetHost& h, double Lx, double Ly, double Lz, double rcut,
@@ -240,6 +275,11 @@ struct esp_batch {
     int2 *d_p = nullptr, *d_s = nullptr;
     int n_p = 0, n_s = 0, smem_plane = 0, smem_slab = 0;
     double *d_acc = nullptr, *d_energy = nullptr, *d_virial = nullptr;
+    // TMA-staged interpolation: tensor maps of the halo-padded potential mesh
+    // (one per system, NULL when unavailable), the box, the kernels' error word
+    CUtensorMap* d_tmaps = nullptr;
+    int tma_bx = 0, tma_by = 0;
+    int* d_kerr = nullptr;
     // cell grids of the neighbour-list builds (allocated on first use): one
     // for HOOMD-layout lists, one for the library's cell-staged pair list
     // (whose kernel reads the cell structures of its own build)
@@ -489,7 +529,7 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
     // system descriptors, influence-table sharing
     sd.assign(ns, SysDev{});
     std::map<std::tuple<int, double, double, double, int, int, int>, long long> gmap;
-    long long m_off = 0, s_off = 0, g_off = 0;
+    long long m_off = 0, s_off = 0, g_off = 0, mp_off = 0;
     int p_off = 0, t_off = 0;
     std::vector<int> g_first;  // system that owns each distinct table
     for (int s = 0; s < ns; ++s) {
@@ -506,6 +546,10 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         S.nty = (S.ny + T - 1) / T;
         S.ntz = (S.nz + T - 1) / T;
         S.t_off = t_off;
+        S.nxp = halo_extent(S.nx, T, P, true);
+        S.nyp = halo_extent(S.ny, T, P, false);
+        S.nzp = halo_extent(S.nz, T, P, false);
+        S.mp_off = mp_off;
         S.Lx = (float)box[3 * s];
         S.Ly = (float)box[3 * s + 1];
         S.Lz = (float)box[3 * s + 2];
@@ -536,6 +580,7 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         S.g_off = it->second;
         p_off += N[s];
         m_off += (long long)S.nx * S.ny * S.nz;
+        mp_off += ((long long)S.nxp * S.nyp * S.nzp + 31) & ~31LL;  // 128-byte aligned systems
         s_off += (long long)S.nz * S.ny * S.nxh;
         t_off += S.ntx * S.nty * S.ntz;
     }
@@ -587,13 +632,30 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         (rc = mem.get(d_tcount, n_tiles)) || (rc = mem.get(d_tstart, n_tiles + 1)) || (rc = mem.get(d_posq, totN)) ||
         (rc = mem.get(d_trec, totN)) || (rc = mem.get(d_srec, totN)) || (rc = mem.get(d_rel, totN)) ||
         (rc = mem.get(d_key, totN)) || (rc = mem.get(d_perm_u, totN)) || (rc = mem.get(d_perm, totN)) ||
-        (rc = mem.get(d_srel, totN)) || (rc = mem.get(d_rho, m_off)) || (rc = mem.get(d_phi, m_off)) ||
+        (rc = mem.get(d_srel, totN)) || (rc = mem.get(d_rho, m_off)) || (rc = mem.get(d_phi, mp_off)) ||
         (rc = mem.get(d_spec, s_off)) || (rc = mem.get(d_gtab, g_off)) || (rc = mem.get(d_tw, tw.size())) ||
         (rc = mem.get(d_x, xi.size())) || (rc = mem.get(d_y, yi.size())) || (rc = mem.get(d_z, zi.size())) ||
         (rc = mem.get(d_p, pi.size())) || (rc = mem.get(d_s, si.size())) ||
         (rc = mem.get(d_acc, (size_t)ns * ACC_STRIDE)) || (rc = mem.get(d_energy, ns)) ||
-        (rc = mem.get(d_virial, (size_t)ns * 6)) || (rc = mem.get(d_fsr, totN)))
+        (rc = mem.get(d_virial, (size_t)ns * 6)) || (rc = mem.get(d_fsr, totN)) || (rc = mem.get(d_kerr, 1)))
         return rc;
+    ESPB_CK(cudaMemset(d_kerr, 0, sizeof(int)));
+    // tensor maps for the TMA-staged interpolation (supports 5..8; the
+    // cp.async form otherwise or when any map cannot be encoded)
+    d_tmaps = nullptr;
+    interp_box(T + P - 1, tma_bx, tma_by);
+    if (p.interp_mode == 0 && P >= 5 && P <= 8) {
+        std::vector<CUtensorMap> maps(ns);
+        bool ok = true;
+        for (int s = 0; s < ns && ok; ++s) {
+            const SysDev& S = sd[s];
+            ok = encode_phi_map(&maps[s], d_phi + S.mp_off, S.nxp, S.nyp, S.nzp, tma_bx, tma_by, T + P - 1);
+        }
+        if (ok) {
+            if ((rc = mem.get(d_tmaps, ns))) return rc;
+            ESPB_CK(cudaMemcpy(d_tmaps, maps.data(), ns * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+        }
+    }
     if (!st2) {
         ESPB_CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
         ESPB_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
@@ -806,6 +868,10 @@ LaunchArgs esp_batch::args() const {
     a.acc = d_acc;
     a.energy = d_energy;
     a.virial = d_virial;
+    a.tmaps = d_tmaps;
+    a.tma_bx = tma_bx;
+    a.tma_by = tma_by;
+    a.kerr = d_kerr;
     a.nmax_x = a.nmax_y = a.nmax_z = 1;
     for (const SysDev& S : sd) {
         a.nmax_x = std::max(a.nmax_x, S.nx);
@@ -1509,8 +1575,11 @@ int esp_get_sort(const esp_ctx* c, void* stream, unsigned* key, unsigned* perm) 
 int esp_get_potential(const esp_ctx* c, void* stream, float* phi) {
     if (!c || !phi) return fail(ESP_ERR_INVALID, "null argument");
     const SysDev& S = c->b.sd[0];
-    ESPB_CK(cudaMemcpyAsync(phi, c->b.d_phi, (size_t)S.nx * S.ny * S.nz * sizeof(float), cudaMemcpyDeviceToDevice,
-                            (cudaStream_t)stream));
+    // the interior of the halo-padded mesh, plane by plane
+    for (int z = 0; z < S.nz; ++z)
+        ESPB_CK(cudaMemcpy2DAsync(phi + (size_t)z * S.ny * S.nx, (size_t)S.nx * sizeof(float),
+                                  c->b.d_phi + S.mp_off + (size_t)z * S.nyp * S.nxp, (size_t)S.nxp * sizeof(float),
+                                  (size_t)S.nx * sizeof(float), S.ny, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
     return 0;
 }
 
@@ -1542,6 +1611,14 @@ int esp_batch_compute(esp_batch* b, void* stream, const float* pos4, const float
 int esp_batch_build_pairlist(esp_batch* b, void* stream, const float* pos4, double rlist, int cap) {
     if (!b) return fail(ESP_ERR_INVALID, "null batch");
     return b->build_pairlist((cudaStream_t)stream, pos4, rlist, cap);
+}
+
+int esp_batch_device_errors(esp_batch* b, int* flags) {
+    if (!b || !flags) return fail(ESP_ERR_INVALID, "null argument");
+    ESPB_CK(cudaDeviceSynchronize());
+    ESPB_CK(cudaMemcpy(flags, b->d_kerr, sizeof(int), cudaMemcpyDeviceToHost));
+    ESPB_CK(cudaMemset(b->d_kerr, 0, sizeof(int)));
+    return 0;
 }
 
 int esp_batch_pairlist_check(esp_batch* b, int* needed_cap) {

@@ -76,6 +76,17 @@ struct PsetHost {
 // the device parameter block for cutoff rcut. Returns 0 or an ESP_ERR_* code.
 int build_param_set(double c, double cw, int P, int D, double rcut, PsetHost& h, ParamSet& d, double tol = 1e-8);
 
+// TMA box of the interpolation tile (extended region E): x extent BX >= E +
+// 3 with BX = 4 (mod 8) and rows BY >= E odd, so that the staged region's
+// plane pitch BX * BY is 4 x odd (mod 32) and the 8 stencil planes a particle
+// group reads fall in 8 distinct banks.
+void interp_box(int E, int& BX, int& BY);
+
+// Tensor map (CUtensorMap, 128 bytes) of a system's halo-padded potential
+// mesh for TMA boxes of BX x BY x BZ floats; false when the driver entry
+// point is unavailable or the encoding fails.
+bool encode_phi_map(void* map, float* base, int nxp, int nyp, int nzp, int BX, int BY, int BZ);
+
 // Inputs of the influence kernel for system S: the window's Fourier
 // transform per axis (w1d, nx + ny + nz values) and the quadrature nodes and
 // pre-scaled weights (tq, wq) for Psi(|k| r_c).

@@ -15,6 +15,8 @@
 //   k_pair     : EvaluatorPairPSWF over a neighbour list,
 //       src/EvaluatorPairPSWF.h:274-295 with the HOOMD PotentialPair loop
 //   k_influence: influence-function build (K1), src/ESPForceComputeGPU.cu:157-201
+#include <cuda.h>
+
 #include "esp_common.cuh"
 #include "esp_kernels.h"
 #include "esp_pair.cuh"
@@ -941,15 +943,27 @@ __global__ void k_fftx_inv(const int4* __restrict__ items, const SysDev* __restr
     for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
         const int b = dn.div(idx), i = idx - b * n, y = y0 + 2 * b;
         if (y < S.ny) {
-            const float2 v = r[i * SB + b];
             const long long g = S.m_off + ((long long)z * S.ny + y) * n + i;
-            phi[g] = v.x;
             rho[g] = 0.0;  // clear the charge mesh for the next spread
-            if (y + 1 < S.ny) {
-                phi[g + n] = v.y;
-                rho[g + n] = 0.0;
-            }
+            if (y + 1 < S.ny) rho[g + n] = 0.0;
         }
+    }
+    // the rows and their periodic copies in the halo-padded potential mesh,
+    // one warp per (row, copy)
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int b = wid; b < 2 * B; b += nw) {
+        const int y = y0 + b;  // source row b / 2 of the pair, real (even b) or imaginary part
+        if (y >= S.ny) continue;
+        for (int zz = z; zz < S.nzp; zz += S.nz)
+            for (int yy = y; yy < S.nyp; yy += S.ny) {
+                float* dst = phi + S.mp_off + ((long long)zz * S.nyp + yy) * S.nxp;
+                for (int x = lane; x < S.nxp; x += 32) {
+                    int xs = x;
+                    while (xs >= n) xs -= n;
+                    const float2 v = r[xs * SB + (b >> 1)];
+                    dst[x] = (b & 1) ? v.y : v.x;
+                }
+            }
     }
 }
 
@@ -1046,16 +1060,24 @@ __global__ void __launch_bounds__(256)
     }
     __syncthreads();
     const float2* r2 = fft_lines<true>(o, r, nx, np, SBx, twx, S.radx);
-    float* dst = phi + S.m_off + (long long)z * ny * nx;
     double* rz = rho + S.m_off + (long long)z * ny * nx;
-    for (int idx = threadIdx.x; idx < np * nx; idx += blockDim.x) {
-        const int b = dnx.div(idx), i = idx - b * nx;
-        const float2 v = r2[i * SBx + b];
-        dst[(2 * b) * nx + i] = v.x;
-        rz[(2 * b) * nx + i] = 0.0;  // clear the charge mesh for the next spread
-        if (2 * b + 1 < ny) {
-            dst[(2 * b + 1) * nx + i] = v.y;
-            rz[(2 * b + 1) * nx + i] = 0.0;
+    for (int idx = threadIdx.x; idx < ny * nx; idx += blockDim.x) rz[idx] = 0.0;  // cleared for the next spread
+    // the plane and its periodic copies in the halo-padded potential mesh,
+    // one warp per padded row
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int zz = z; zz < S.nzp; zz += S.nz) {
+        float* dst = phi + S.mp_off + (long long)zz * S.nyp * S.nxp;
+        for (int y = wid; y < S.nyp; y += nw) {
+            int ys = y;
+            while (ys >= ny) ys -= ny;
+            const int b = ys >> 1;
+            const bool hi = ys & 1;
+            for (int x = lane; x < S.nxp; x += 32) {
+                int xs = x;
+                while (xs >= nx) xs -= nx;
+                const float2 v = r2[xs * SBx + b];
+                dst[(long long)y * S.nxp + x] = hi ? v.y : v.x;
+            }
         }
     }
 }
@@ -1200,15 +1222,38 @@ struct InterpCfg {
     static constexpr int CH = 2 * NG;       // particles staged per round
 };
 
-template <int P>
+// TMA: the extended region arrives as one cp.async.bulk.tensor box of the
+// halo-padded potential mesh (tensor map per system, x rounded down to a
+// 16-byte boundary, box PX x (PP / PX) x E floats); otherwise as 4-byte
+// cp.async copies. A TMA wait that runs out (kTmaWaitLimit polls) sets
+// kerr[0] and skips the tile.
+constexpr int kTmaWaitLimit = 1 << 24;
+
+__device__ __forceinline__ bool tma_wait(uint32_t mbar, uint32_t phase) {
+    for (int it = 0; it < kTmaWaitLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(mbar), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <int P, bool TMA>
 __global__ void __launch_bounds__(128)
     k_interp(const int* __restrict__ tile_sys, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
              int T, int D, int PX, int PP, const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
              const float4* __restrict__ srec, const uint32_t* __restrict__ srel, const float* __restrict__ phi,
-             float4* __restrict__ force, double* __restrict__ acc) {
+             float4* __restrict__ force, double* __restrict__ acc, const CUtensorMap* __restrict__ tmaps,
+             int* __restrict__ kerr) {
     using C = InterpCfg<P>;
     extern __shared__ float4 sm4[];
     __shared__ double red[32];
+    __shared__ __align__(8) uint64_t mbar;
     const int t = blockIdx.x;
     const uint32_t s0 = start[t];
     const int np = (int)(start[t + 1] - s0);
@@ -1217,13 +1262,14 @@ __global__ void __launch_bounds__(128)
     const SysDev S = sys[si];
     const ParamSet& ps = psets[S.pset];
     const int E = T + P - 1;
+    // the potential region (128-byte aligned for the TMA box), then the
     // particle records (position/t, origin, output slot) of the current and
     // the next chunk: the next chunk's are prefetched while this one runs
-    float4* crec = sm4;                                                     // [2][CH]
+    float* sm = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm4) + 127) & ~(uintptr_t)127);  // [E*PP]
+    float4* crec = reinterpret_cast<float4*>(sm + ((E * PP + 3) & ~3));    // [2][CH]
     uint32_t* crel = reinterpret_cast<uint32_t*>(crec + 2 * C::CH);         // [2][CH]
     uint32_t* cprm = crel + 2 * C::CH;                                      // [2][CH]
-    float* sm = reinterpret_cast<float*>(cprm + 2 * C::CH);  // [E*PP] potential
-    float* wts = sm + E * PP;                      // [CH][6P] wx dwx wy dwy wz dwz (index tables first)
+    float* wts = reinterpret_cast<float*>(cprm + 2 * C::CH);  // [CH][6P] wx dwx wy dwy wz dwz (index tables first)
     float* qv = wts + interp_stage_words(P, C::CH, E);  // [CH] charges
     int* org = reinterpret_cast<int*>(qv + C::CH); // [CH] packed origins
     int* order = org + C::CH;                      // [CH] processing order of the chunk
@@ -1232,9 +1278,26 @@ __global__ void __launch_bounds__(128)
     constexpr int K = 32 / C::G;                   // particle groups per warp
     const int lt = t - S.t_off;
     const int X0 = (lt % S.ntx) * T, Y0 = ((lt / S.ntx) % S.nty) * T, Z0 = (lt / (S.ntx * S.nty)) * T;
-    // stage the extended region with asynchronous 4-byte copies (every
-    // thread keeps all its loads in flight; periodic wrap per axis)
-    {
+    // TMA boxes start on a 16-byte boundary in x: the region sits xoff floats in
+    const int xoff = TMA ? (X0 & 3) : 0;
+    const uint32_t mbar_a = (uint32_t)__cvta_generic_to_shared(&mbar);
+    if (TMA) {
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mbar_a) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+            const uint32_t bytes = (uint32_t)(E * PP) * 4u;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mbar_a), "r"(bytes)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+                "[%5];\n" ::"r"((uint32_t)__cvta_generic_to_shared(sm)),
+                "l"(reinterpret_cast<uint64_t>(tmaps + si)), "r"(X0 - xoff), "r"(Y0), "r"(Z0), "r"(mbar_a)
+                : "memory");
+        }
+        __syncthreads();  // the barrier is initialised before anyone waits on it
+    } else {
+        // stage the extended region with asynchronous 4-byte copies (every
+        // thread keeps all its loads in flight)
         // wrapped global row offsets and shared row offsets per (Y, Z) row,
         // wrapped x indices, then one 4-byte asynchronous copy per point
         // (all of a thread's copies in flight)
@@ -1243,19 +1306,12 @@ __global__ void __launch_bounds__(128)
         int* xs = srow + E * E;
         for (int i = threadIdx.x; i < E * E; i += blockDim.x) {
             const int Y = i % E, Z = i / E;
-            int gy = Y0 + Y, gz = Z0 + Z;
-            while (gy >= S.ny) gy -= S.ny;
-            while (gz >= S.nz) gz -= S.nz;
-            rowo[i] = (gz * S.ny + gy) * S.nx;
+            rowo[i] = ((Z0 + Z) * S.nyp + (Y0 + Y)) * S.nxp;  // the halo-padded mesh needs no wrap
             srow[i] = Z * PP + Y * PX;
         }
-        for (int i = threadIdx.x; i < E; i += blockDim.x) {
-            int gx = X0 + i;
-            while (gx >= S.nx) gx -= S.nx;
-            xs[i] = gx;
-        }
+        for (int i = threadIdx.x; i < E; i += blockDim.x) xs[i] = X0 + i;
         __syncthreads();
-        const float* base = phi + S.m_off;
+        const float* base = phi + S.mp_off;
         const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
         // rows padded to a power of two wide, so the point index splits by shifts
         int sh = 4;
@@ -1281,7 +1337,17 @@ __global__ void __launch_bounds__(128)
         asm volatile("cp.async.commit_group;\n" ::);
     };
     prefetch(0, 0);
-    asm volatile("cp.async.wait_group 0;\n" ::);  // region and first chunk
+    asm volatile("cp.async.wait_group 0;\n" ::);  // region (cp.async form) and first chunk
+    if (TMA) {
+        const bool ok = tma_wait(mbar_a, 0u);
+        if (__syncthreads_or(!ok)) {
+            // the box did not arrive in time: report, let the copy drain
+            // (bounded), skip the tile (the whole CTA)
+            if (threadIdx.x == 0) atomicOr(kerr, 1);
+            tma_wait(mbar_a, 0u);
+            return;
+        }
+    }
     for (int i = threadIdx.x; i < P * (D + 1); i += blockDim.x)
         wc[i] = ps.wcoef[(i / (D + 1)) * (MAX_D + 1) + (i % (D + 1))];
     const int grp = threadIdx.x / C::G, gl = threadIdx.x % C::G;
@@ -1330,7 +1396,10 @@ __global__ void __launch_bounds__(128)
             const int j = threadIdx.x;
             const unsigned full = 0xffffffffu, lt = (1u << j) - 1u;
             const bool valid = j < nc;
-            const int cls = valid ? (((org[j] & 255) + ((org[j] >> 8) & 255)) & (K - 1)) : -1;
+            // bank class of the particle's rows: (ox + oy) mod K for the padded
+            // cp.async layout; ox + xoff mod K for the TMA box (pitches = 0 mod K)
+            const int cls = valid ? ((TMA ? (org[j] & 255) + xoff : (org[j] & 255) + ((org[j] >> 8) & 255)) & (K - 1))
+                                  : -1;
             int rank = 0, cpos = 0;
             const int pk = j & (K - 1);
 #pragma unroll
@@ -1364,7 +1433,7 @@ __global__ void __launch_bounds__(128)
                 }
                 const int rl = org[p];
                 const int ox = rl & 255, oy = (rl >> 8) & 255, oz = (rl >> 16) & 255;
-                const float* plane = sm + (oz + gl) * PP + oy * PX + ox;
+                const float* plane = sm + (oz + gl) * PP + oy * PX + ox + xoff;
                 float Sv = 0.f, Dv = 0.f, Sy = 0.f;
 #pragma unroll
                 for (int b = 0; b < P; ++b) {
@@ -1649,17 +1718,40 @@ static cudaError_t launch_spread_p(const LaunchArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// shared memory of the interpolation kernel: the (128-byte aligned)
+// potential region E x PP, the staging area, charges, origins, order and
+// window coefficients, and two chunks of particle records
+template <int P>
+static size_t interp_smem(int E, int PP) {
+    using C = InterpCfg<P>;
+    return 128 + (size_t)((E * PP + 3) & ~3) * 4 +
+           ((size_t)interp_stage_words(P, C::CH, E) + 3 * C::CH + P * (MAX_D + 1)) * 4 + 2 * C::CH * 24;
+}
+
 template <int P>
 static cudaError_t launch_interp_p(const LaunchArgs& a, cudaStream_t st) {
     using C = InterpCfg<P>;
     const int E = a.T + P - 1;
-    const size_t smem =
-        ((size_t)E * a.PP + interp_stage_words(P, C::CH, E) + 3 * C::CH + P * (MAX_D + 1)) * 4 + 2 * C::CH * 24;
-    if (a.configure_only)
-        return cudaFuncSetAttribute(k_interp<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    constexpr bool kTmaForm = P >= 5 && P <= 8;  // 8 lanes per particle: the box pitches give distinct banks
+    const bool tma = kTmaForm && a.tmaps != nullptr;
+    const int PX = tma ? a.tma_bx : a.PX, PP = tma ? a.tma_bx * a.tma_by : a.PP;
+    if (a.configure_only) {
+        cudaError_t e = cudaFuncSetAttribute(k_interp<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)interp_smem<P>(E, a.PP));
+        if (e == cudaSuccess && kTmaForm && a.tma_bx > 0)
+            e = cudaFuncSetAttribute(k_interp<P, kTmaForm>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)interp_smem<P>(E, a.tma_bx * a.tma_by));
+        return e;
+    }
     if (a.n_tiles == 0) return cudaSuccess;
-    k_interp<P><<<a.n_tiles, C::THREADS, smem, st>>>(a.tile_sys, a.sys, a.psets, a.T, a.D, a.PX, a.PP, a.tile_start,
-                                                       a.perm, a.srec, a.srel, a.phi, a.force, a.acc);
+    if (tma)
+        k_interp<P, kTmaForm><<<a.n_tiles, C::THREADS, interp_smem<P>(E, PP), st>>>(
+            a.tile_sys, a.sys, a.psets, a.T, a.D, PX, PP, a.tile_start, a.perm, a.srec, a.srel, a.phi, a.force, a.acc,
+            reinterpret_cast<const CUtensorMap*>(a.tmaps), a.kerr);
+    else
+        k_interp<P, false><<<a.n_tiles, C::THREADS, interp_smem<P>(E, PP), st>>>(
+            a.tile_sys, a.sys, a.psets, a.T, a.D, PX, PP, a.tile_start, a.perm, a.srec, a.srel, a.phi, a.force, a.acc,
+            nullptr, a.kerr);
     return cudaGetLastError();
 }
 

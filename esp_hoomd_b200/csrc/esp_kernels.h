@@ -106,6 +106,13 @@ struct LaunchArgs {
     float* virial_pp = nullptr;
     int vpp_pitch = 0;
     double* external = nullptr;
+    // TMA-staged interpolation: per-system tensor maps of the halo-padded
+    // potential mesh (CUtensorMap[nsys], NULL: cp.async staging), the box's
+    // x extent and rows (pitches of the staged region), and the kernels'
+    // error word (bit 0: a TMA wait ran out)
+    const void* tmaps = nullptr;
+    int tma_bx = 0, tma_by = 0;
+    int* kerr = nullptr;
     const uint32_t* ex_n = nullptr;     // exclusions: row i holds ex_list[i * ex_pitch + k], k < ex_n[i]
     const uint32_t* ex_list = nullptr;
     int ex_pitch = 0;

@@ -27,6 +27,8 @@
 #include <tuple>
 #include <vector>
 
+#include <cuda.h>
+
 #include "esp_b200.h"
 #include "esp_host_util.h"
 #include "esp_kernels.h"
@@ -191,6 +193,12 @@ struct esp_server {
     // per-round work items, and the (d_OH, d_HH) geometries seen so far
     int2* d_rskip = nullptr;
     int4* d_ritems = nullptr;
+    // TMA-staged interpolation: one tensor map per slot (its halo-padded
+    // potential range), the box, the kernels' error word
+    CUtensorMap* d_tmaps = nullptr;
+    bool use_tma = false;
+    int tma_bx = 0, tma_by = 0;
+    int* d_kerr = nullptr;
     double2* d_geo = nullptr;
     std::vector<double2> geos;
     static constexpr int MAX_GEOS = 16;
@@ -316,8 +324,12 @@ int esp_server::init(const esp_server_config& cfg) {
         (rc = mem.get(d_mdchunks, chunk_cap)) || (rc = mem.get(d_nlchunks, (max_particles + 255) / 256)) ||
         (rc = mem.get(d_pitems, ITEM_CAP)) || (rc = mem.get(d_sitems, ITEM_CAP)) || (rc = mem.get(d_xitems, ITEM_CAP)) ||
         (rc = mem.get(d_yitems, ITEM_CAP)) || (rc = mem.get(d_zitems, ITEM_CAP)) ||
-        (rc = mem.get(d_rskip, max_slots)) || (rc = mem.get(d_ritems, ritem_cap)) || (rc = mem.get(d_geo, MAX_GEOS)))
+        (rc = mem.get(d_rskip, max_slots)) || (rc = mem.get(d_ritems, ritem_cap)) || (rc = mem.get(d_geo, MAX_GEOS)) ||
+        (rc = mem.get(d_tmaps, max_slots)) || (rc = mem.get(d_kerr, 1)))
         return rc;
+    ESPB_CK(cudaMemset(d_kerr, 0, sizeof(int)));
+    interp_box(T + P - 1, tma_bx, tma_by);
+    use_tma = prm.interp_mode == 0 && P >= 5 && P <= 8;
     stats.arena_bytes = mem.bytes;
     ESPB_CK(cudaMemcpy(d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice));
     // counters that the kernels leave at zero, and meshes the inverse FFT pass
@@ -339,6 +351,8 @@ int esp_server::init(const esp_server_config& cfg) {
         a.D = D;
         a.PX = PX;
         a.PP = PP;
+        a.tma_bx = tma_bx;
+        a.tma_by = tma_by;
         ESPB_CK(launch_spread(a, 0));
         ESPB_CK(launch_interp(a, 0));
         ESPB_CK(launch_fft(a, 0));
@@ -448,6 +462,10 @@ int esp_server::admit(Request* q, Staging& sg) {
         ntiles *= q->ntile[d];
     }
     const long long G = (long long)q->mesh[2] * q->mesh[1] * (q->mesh[0] / 2 + 1);
+    // mesh arena units: the halo-padded potential mesh is the largest of the
+    // three arrays sharing the range (charge mesh, potential, half spectrum)
+    const long long Mp = std::max(M, (long long)halo_extent(q->mesh[0], T, P, true) * halo_extent(q->mesh[1], T, P, false) *
+                                         halo_extent(q->mesh[2], T, P, false));
     const double rlist = r.rcut + r.skin;
     int cap = r.nlist_cap;
     if (cap <= 0) {
@@ -457,7 +475,7 @@ int esp_server::admit(Request* q, Staging& sg) {
     cap = (cap + 3) & ~3;
     q->cap = cap;
     const long long NL = (long long)r.N * cap;
-    if (r.N > P_cap / 2 || M > M_cap || ntiles > T_cap || NL > NL_cap || G > G_cap)
+    if (r.N > P_cap / 2 || Mp > M_cap || ntiles > T_cap || NL > NL_cap || G > G_cap)
         return fail(ESP_ERR_UNSUPPORTED, "request larger than the server arenas");
     if (free_slots.empty()) return 1;
     // influence table: shared with earlier requests of the same box and mesh
@@ -485,7 +503,7 @@ int esp_server::admit(Request* q, Staging& sg) {
         build_g = true;
     }
     q->p_off = palloc.alloc(r.N, 256);
-    q->m_off = q->p_off >= 0 ? malloc_.alloc(M, 64) : -1;
+    q->m_off = q->p_off >= 0 ? malloc_.alloc(Mp, 64) : -1;
     q->t_off = q->m_off >= 0 ? talloc.alloc(ntiles, 1) : -1;
     q->nl_off = q->t_off >= 0 ? nlalloc.alloc(NL, 64) : -1;
     if (q->nl_off < 0) {
@@ -503,7 +521,7 @@ int esp_server::admit(Request* q, Staging& sg) {
     git->second.last_use = ++gclock;
     q->slot = free_slots.back();
     free_slots.pop_back();
-    q->footprint = (long long)r.N * PARTICLE_BYTES + M * MESH_BYTES + ntiles * 12 + NL * 4 + (build_g ? G * 8 : 0);
+    q->footprint = (long long)r.N * PARTICLE_BYTES + Mp * MESH_BYTES + ntiles * 12 + NL * 4 + (build_g ? G * 8 : 0);
 
     // system descriptor
     SysDev S{};
@@ -520,6 +538,19 @@ int esp_server::admit(Request* q, Staging& sg) {
     S.nty = q->ntile[1];
     S.ntz = q->ntile[2];
     S.t_off = (int)q->t_off;
+    S.nxp = halo_extent(S.nx, T, P, true);
+    S.nyp = halo_extent(S.ny, T, P, false);
+    S.nzp = halo_extent(S.nz, T, P, false);
+    S.mp_off = q->m_off;
+    if (use_tma) {
+        CUtensorMap map;
+        if (!encode_phi_map(&map, d_phi + S.mp_off, S.nxp, S.nyp, S.nzp, tma_bx, tma_by, T + P - 1))
+            use_tma = false;  // the cp.async staging from now on
+        else {
+            int rcm = upload(sg, d_tmaps + q->slot, &map, sizeof(CUtensorMap));
+            if (rcm) return rcm;
+        }
+    }
     S.Lx = (float)r.Lx;
     S.Ly = (float)r.Ly;
     S.Lz = (float)r.Lz;
@@ -741,6 +772,10 @@ int esp_server::launch_round(Staging& sg) {
     a.acc = d_acc;
     a.energy = d_energy;
     a.virial = nullptr;
+    a.tmaps = use_tma ? d_tmaps : nullptr;
+    a.tma_bx = tma_bx;
+    a.tma_by = tma_by;
+    a.kerr = d_kerr;
     a.want_virial = 0;
     a.add_bg = 1;
     a.nl_head = d_head;

@@ -15,7 +15,7 @@ from ._lib import EspInfo, EspParams, check, get_lib
 def make_params(order: int = 8, rcut: float = 3.0, kappa: float = 0.0, mesh: Optional[Sequence[int]] = None,
                 target_error: float = 1e-5, window_c: float = 0.0, window_degree: int = 0, tile: int = 0,
                 threads_per_particle: int = 0, alpha: float = 0.0, n_table: int = 512,
-                precision: int = 0, fft_mode: int = 0) -> EspParams:
+                precision: int = 0, fft_mode: int = 0, interp_mode: int = 0) -> EspParams:
     p = EspParams()
     check(get_lib().esp_params_default(ctypes.byref(p)), "esp_params_default")
     p.order = int(order)
@@ -32,6 +32,7 @@ def make_params(order: int = 8, rcut: float = 3.0, kappa: float = 0.0, mesh: Opt
     p.threads_per_particle = int(threads_per_particle)
     p.precision = int(precision)
     p.fft_mode = int(fft_mode)
+    p.interp_mode = int(interp_mode)
     return p
 
 
@@ -190,6 +191,13 @@ class Batch:
         synchronise: a row overflow is reported by a later call."""
         check(self._lib.esp_batch_build_pairlist(self._h, _stream(stream), _ptr(pos4), float(rlist), int(cap)),
               "esp_batch_build_pairlist")
+
+    def device_errors(self) -> int:
+        """Error word of the batch's kernels since the last call (bit 0: a
+        TMA-staged interpolation tile timed out); synchronises."""
+        f = ctypes.c_int(0)
+        check(self._lib.esp_batch_device_errors(self._h, ctypes.byref(f)), "esp_batch_device_errors")
+        return int(f.value)
 
     def pairlist_check(self) -> int:
         """Waits for the last pair-list build; raises EspError (ESP_ERR_OVERFLOW)

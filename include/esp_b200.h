@@ -66,6 +66,7 @@ typedef struct esp_params {
     int threads_per_particle; /* pair kernel lanes per particle: 4, 8, 16, 32; 0 = 4 */
     int precision;       /* ESP_FP32 (default) or ESP_FP64 */
     int fft_mode;        /* 0: whole planes/slabs in shared memory where they fit; 1: per-line passes */
+    int interp_mode;     /* 0: the potential tile staged by TMA (supports 5..8); 1: cp.async staging */
 } esp_params;
 
 /* Resolved configuration of a context or of one system of a batch. */
@@ -227,6 +228,11 @@ int esp_batch_autotune(esp_batch* b, void* stream, const float* pos4, const floa
                        const unsigned* n_neigh, const unsigned* nlist, int flags, int reps, esp_params* chosen,
                        double* trial_ms, int max_trials);
 int esp_batch_get_info(const esp_batch* b, int sys, esp_info* info);
+/* Error word of the batch's kernels since the last call (no reference
+ * counterpart): bit 0 -- a TMA-staged interpolation tile waited longer than
+ * its bound for its potential box and was skipped (results invalid).
+ * Synchronises the device, then clears the word. */
+int esp_batch_device_errors(esp_batch* b, int* flags);
 int esp_batch_total_particles(const esp_batch* b);
 int esp_batch_destroy(esp_batch* b);
 /* Exclusions of a batch, as esp_set_exclusions: rows by the particle's index
