@@ -617,6 +617,16 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
                 for (int k0 = 0; k0 < S.nxh; k0 += FFT_B_YZ) zi.push_back(make_int4(s, y, k0, 0));
         }
     }
+    // FFT work in decreasing size (longest processing time first): the
+    // largest planes and slabs of an uneven batch start first instead of
+    // forming the launch's tail
+    auto plane_cost = [&](const int2& it) { return (long long)sd[it.x].nx * sd[it.x].ny; };
+    auto slab_cost = [&](const int2& it) { return (long long)sd[it.x].nx * sd[it.x].nz; };
+    std::stable_sort(pi.begin(), pi.end(), [&](const int2& a, const int2& b) { return plane_cost(a) > plane_cost(b); });
+    std::stable_sort(si.begin(), si.end(), [&](const int2& a, const int2& b) { return slab_cost(a) > slab_cost(b); });
+    auto line_cost = [&](const int4& it) { return (long long)std::max({sd[it.x].nx, sd[it.x].ny, sd[it.x].nz}); };
+    for (auto* v : {&xi, &yi, &zi})
+        std::stable_sort(v->begin(), v->end(), [&](const int4& a, const int4& b) { return line_cost(a) > line_cost(b); });
     n_p = (int)pi.size();
     n_s = (int)si.size();
     n_chunks = (int)chunks.size();
