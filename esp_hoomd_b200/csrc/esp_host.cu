@@ -454,6 +454,7 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
     totN = 0;
     for (int s = 0; s < ns; ++s) {
         if (N[s] < 0) return fail(ESP_ERR_INVALID, "negative particle count");
+        if (N[s] >= (1 << 26)) return fail(ESP_ERR_UNSUPPORTED, "at most 2^26 - 1 particles per system");
         for (int d = 0; d < 3; ++d) {
             const double L = box[3 * s + d];
             if (!(L > 0)) return fail(ESP_ERR_INVALID, "box lengths must be positive");

@@ -176,37 +176,46 @@ __global__ void k_scatter(const int2* __restrict__ chunks, const SysDev* __restr
     if (valid) perm_u[start[k] + top - 1u - (uint32_t)__popc(grp & ((1u << lane) - 1u))] = (uint32_t)i;
 }
 
-// Deterministic per-tile order: particles of one tile sorted by index, so
-// the permutation equals a stable sort on (key, index). Also gathers the
-// sorted particle records.
+// Deterministic per-tile order: the particles of one tile sorted by (y
+// origin of the stencil inside the tile, index), so the permutation equals a
+// stable sort on (key, y origin, index). Grouping equal y origins lets the
+// spreading kernel's warps skip the k-steps whose stencil rows miss theirs.
+// The composite rank key is (oy << 26) | (index - system's first particle).
+// Also gathers the sorted particle records.
+__device__ __forceinline__ uint32_t sort_key(uint32_t v, const uint32_t* __restrict__ rel, int p_off) {
+    return (((rel[v] >> 8) & 255u) << 26) | (v - (uint32_t)p_off);
+}
+
 __global__ void k_tile_sort(const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm_u,
                             uint32_t* __restrict__ perm, const float4* __restrict__ trec,
                             const uint32_t* __restrict__ rel, float4* __restrict__ srec,
-                            uint32_t* __restrict__ srel) {
+                            uint32_t* __restrict__ srel, const int* __restrict__ tile_sys,
+                            const SysDev* __restrict__ sys) {
     __shared__ __align__(16) uint32_t sm[SORT_CAP];
     const uint32_t s0 = start[blockIdx.x];
     const uint32_t n = start[blockIdx.x + 1] - s0;
     if (n == 0) return;
+    const int p_off = sys[tile_sys[blockIdx.x]].p_off;
     const bool cached = n <= (uint32_t)SORT_CAP;
     const uint32_t n4 = (n + 3u) >> 2;
     if (cached) {
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sm[i] = perm_u[s0 + i];
-        // pad to whole 16-byte groups with a value no index is above
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sm[i] = sort_key(perm_u[s0 + i], rel, p_off);
+        // pad to whole 16-byte groups with a value no key is above
         if (threadIdx.x < 4u * n4 - n) sm[n + threadIdx.x] = 0xffffffffu;
     }
     __syncthreads();
-    const uint32_t* src = cached ? sm : perm_u + s0;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-        const uint32_t v = src[i];
+        const uint32_t v = perm_u[s0 + i];
+        const uint32_t kv = cached ? sm[i] : sort_key(v, rel, p_off);
         uint32_t r = 0;
         if (cached) {
-            // rank = number of smaller indices, four per shared load
+            // rank = number of smaller keys, four per shared load
             for (uint32_t j = 0; j < n4; ++j) {
                 const uint4 u = reinterpret_cast<const uint4*>(sm)[j];
-                r += (u.x < v ? 1u : 0u) + (u.y < v ? 1u : 0u) + (u.z < v ? 1u : 0u) + (u.w < v ? 1u : 0u);
+                r += (u.x < kv ? 1u : 0u) + (u.y < kv ? 1u : 0u) + (u.z < kv ? 1u : 0u) + (u.w < kv ? 1u : 0u);
             }
         } else {
-            for (uint32_t j = 0; j < n; ++j) r += (src[j] < v) ? 1u : 0u;
+            for (uint32_t j = 0; j < n; ++j) r += (sort_key(perm_u[s0 + j], rel, p_off) < kv) ? 1u : 0u;
         }
         perm[s0 + r] = v;
         srec[s0 + r] = trec[v];
@@ -506,6 +515,10 @@ __global__ void __launch_bounds__(256, 3)
                  int T, int D, const uint32_t* __restrict__ start, const float4* __restrict__ srec,
                  const uint32_t* __restrict__ srel, double* __restrict__ rho) {
     extern __shared__ float4 smm4[];
+    // per k-step of the chunk: the tile rows Y that carry stencil weight
+    // (particles are sorted by y origin inside a tile, so most k-steps touch
+    // half of the 16 rows; a warp skips the k-steps that miss its two rows)
+    __shared__ int ks_lo[SPREAD_CHM / 8], ks_hi[SPREAD_CHM / 8];
     const int t = blockIdx.x;
     const uint32_t s0 = start[t];
     const int np = (int)(start[t + 1] - s0);
@@ -592,9 +605,24 @@ __global__ void __launch_bounds__(256, 3)
                     }
                 }
             }
+            if (tid < ncp / 8) {
+                int lo = 1 << 30, hi = -1;
+                for (int j = 0; j < 8; ++j) {
+                    const int p = tid * 8 + j;
+                    if (p < nc) {
+                        const int oy = (int)((crel[cb * SPREAD_CHM + p] >> 8) & 255u);
+                        lo = min(lo, oy);
+                        hi = max(hi, oy);
+                    }
+                }
+                ks_lo[tid] = lo;
+                ks_hi[tid] = hi + P - 1;
+            }
         }
         __syncthreads();
         for (int k0 = 0; k0 < ncp; k0 += 8) {
+            const int klo = ks_lo[k0 >> 3], khi = ks_hi[k0 >> 3];
+            if (2 * warp + 1 < klo || 2 * warp > khi) continue;  // warp-uniform: only zero rows here
             const int r1 = (k0 + tg) * SPREAD_MS, r2 = r1 + 4 * SPREAD_MS;  // particles k0 + tg, k0 + tg + 4
             // B fragments: b0 = wz_{p1}[Z], b1 = wz_{p2}[Z], Z = 8 nt + g
             uint32_t bh[2][2], bl[2][2];
@@ -609,6 +637,7 @@ __global__ void __launch_bounds__(256, 3)
 #pragma unroll
             for (int mt = 0; mt < 2; ++mt) {
                 const int Y = 2 * warp + mt;
+                if (Y < klo || Y > khi) continue;
                 const float wy1 = wys[r1 + Y], wy2 = wys[r2 + Y];
                 uint32_t ah0, al0, ah1, al1, ah2, al2, ah3, al3;
                 split_tf32(wx1 * wy1, ah0, al0);   // row X = g,     particle p1
@@ -1792,7 +1821,9 @@ cudaError_t launch_bin(const LaunchArgs& a, cudaStream_t st) {
 cudaError_t launch_sort(const LaunchArgs& a, cudaStream_t st) {
     k_scan<<<1, 1024, 0, st>>>(a.tile_count, a.tile_start, a.n_tiles);
     if (a.n_chunks) k_scatter<<<a.n_chunks, 256, 0, st>>>(a.chunks, a.sys, a.key, a.tile_start, a.tile_count, a.perm_u);
-    if (a.n_tiles) k_tile_sort<<<a.n_tiles, 128, 0, st>>>(a.tile_start, a.perm_u, a.perm, a.trec, a.rel, a.srec, a.srel);
+    if (a.n_tiles)
+        k_tile_sort<<<a.n_tiles, 128, 0, st>>>(a.tile_start, a.perm_u, a.perm, a.trec, a.rel, a.srec, a.srel,
+                                               a.tile_sys, a.sys);
     return cudaGetLastError();
 }
 

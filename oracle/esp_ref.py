@@ -64,10 +64,13 @@ def stencil_origin(g, P):
 
 
 def bin_sort(pos, box, mesh, P, tile):
-    """Tile key of each particle and the stable permutation (key, index).
+    """Tile key of each particle and the stable permutation by (key, y origin
+    inside the tile, index).
 
     key = linear tile index (x-fastest) of the tile holding the particle's
-    first stencil point i0 (mod n); tiles are ``tile^3`` mesh cells.
+    first stencil point i0 (mod n); tiles are ``tile^3`` mesh cells. Inside a
+    tile particles are ordered by the y coordinate of their first stencil
+    point relative to the tile, then by index.
     Returns (key uint32[N], perm uint32[N]).
     """
     g = grid_coords(pos, box, mesh)
@@ -77,7 +80,8 @@ def bin_sort(pos, box, mesh, P, tile):
     nt = (n + tile - 1) // tile
     tc = c // tile
     key = ((tc[:, 2] * nt[1] + tc[:, 1]) * nt[0] + tc[:, 0]).astype(np.uint32)
-    perm = np.argsort(key, kind="stable").astype(np.uint32)
+    oy = c[:, 1] - tc[:, 1] * tile
+    perm = np.lexsort((np.arange(key.size), oy, key)).astype(np.uint32)
     return key, perm
 
 

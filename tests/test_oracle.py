@@ -152,12 +152,16 @@ def test_esp_oracle_gradient_and_accuracy():
 
 
 def test_bin_sort_is_stable():
+    # tiles in key order; inside a tile by the stencil's y origin, then index
     s = systems.rocksalt(6, seed=2)
     key, perm = R.bin_sort(s.pos, s.box, (16, 16, 16), 8, 8)
     assert np.all(np.diff(key[perm].astype(np.int64)) >= 0)
+    i0, _ = R.stencil_origin(R.grid_coords(s.pos, s.box, (16, 16, 16)), 8)
+    oy = np.mod(i0[:, 1], 16) % 8
     for k in np.unique(key):
-        idx = perm[key[perm] == k]
-        assert np.all(np.diff(idx.astype(np.int64)) > 0)
+        idx = perm[key[perm] == k].astype(np.int64)
+        comp = oy[idx] * (1 << 26) + idx
+        assert np.all(np.diff(comp) > 0)
 
 
 def test_neighbor_list_matches_brute_force():
