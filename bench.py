@@ -341,7 +341,9 @@ def run_serving(args, pool):
     base = max(srv.status(i)["t_done"] for i in warm) + 0.05
     out = []
     for rate in args.serve_rates:
-        gaps = rng.exponential(1.0 / rate, size=args.serve_requests)
+        # rate 0: every request arrives at once (a saturating burst: the
+        # server's own throughput, the queue never empties)
+        gaps = rng.exponential(1.0 / rate, size=args.serve_requests) if rate > 0 else np.zeros(args.serve_requests)
         arr = base + np.cumsum(gaps)
         kinds = rng.random(args.serve_requests) < 0.5
         ids, nsum = [], 0
@@ -355,7 +357,7 @@ def run_serving(args, pool):
         ok = [s for s in st if s["state"] == 2]
         lat = np.array([s["t_done"] - s["t_arrival"] for s in ok]) * 1e3
         span = max(s["t_done"] for s in ok) - arr[0]
-        out.append({"rate_per_s": rate, "requests": len(ids), "completed": len(ok),
+        out.append({"rate_per_s": rate if rate > 0 else "burst", "requests": len(ids), "completed": len(ok),
                     "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                     "mean_ms": float(lat.mean()), "throughput": nsum * SERVE_STEPS / span,
                     "requests_per_s": len(ok) / span})
@@ -694,13 +696,16 @@ def run_ours(args):
             b.close()
             torch.cuda.empty_cache()
             rates, sst = run_serving(args, _serve_pool(SEED + 6))
-            mid = rates[len(rates) // 2]
+            mid = rates[0]
+            sat = max(rates, key=lambda r: r["throughput"])
             line["serving"] = {
                 "workload": "Poisson arrivals, 50/50 rock-salt n even ~U{8..64} (r_c 3.0) / rigid water 1,000-32,768 "
                             "molecules (r_c 0.9 nm, SETTLE); each request = nlist + 1 evaluation + 10 NVE steps; "
                             "64 GB HBM budget; latency = completion - arrival (host clock)",
                 "unit": UNIT, "rates": rates, "p50_ms": mid["p50_ms"], "p99_ms": mid["p99_ms"],
                 "at_rate_per_s": mid["rate_per_s"],
+                "saturated_throughput": sat["throughput"],
+                "saturated_over_batched": sat["throughput"] / value if value else None,
                 "server": {k: sst[k] for k in ("rounds", "max_active", "peak_bytes", "arena_bytes",
                                                "influence_builds", "influence_hits", "failed")}}
         print(json.dumps(line), flush=True)
@@ -727,9 +732,9 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default plan)")
     ap.add_argument("--hoomd-list", action="store_true",
                     help="short-range term over HOOMD-layout neighbour rows instead of the cell-staged pair list")
-    ap.add_argument("--serve-requests", type=int, default=1000, help="requests per arrival rate")
-    ap.add_argument("--serve-rates", type=lambda v: [float(x) for x in v.split(",")], default=[100.0, 200.0, 400.0],
-                    help="comma-separated arrival rates (requests/s)")
+    ap.add_argument("--serve-requests", type=int, default=10000, help="requests per arrival rate")
+    ap.add_argument("--serve-rates", type=lambda v: [float(x) for x in v.split(",")], default=[200.0, 800.0, 0.0],
+                    help="comma-separated arrival rates (requests/s); 0 = all requests at once (saturation)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
