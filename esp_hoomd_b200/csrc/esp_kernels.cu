@@ -1765,11 +1765,20 @@ static cudaError_t launch_interp_p(const LaunchArgs& a, cudaStream_t st) {
     const bool tma = kTmaForm && a.tmaps != nullptr;
     const int PX = tma ? a.tma_bx : a.PX, PP = tma ? a.tma_bx * a.tma_by : a.PP;
     if (a.configure_only) {
-        cudaError_t e = cudaFuncSetAttribute(k_interp<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)interp_smem<P>(E, a.PP));
-        if (e == cudaSuccess && kTmaForm && a.tma_bx > 0)
-            e = cudaFuncSetAttribute(k_interp<P, kTmaForm>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)interp_smem<P>(E, a.tma_bx * a.tma_by));
+        // per-function limits shared by every batch of the process: raised
+        // only, so a later plan with a smaller tile cannot lower them
+        static int configured[2] = {0, 0};
+        cudaError_t e = cudaSuccess;
+        const int s0 = (int)interp_smem<P>(E, a.PP);
+        if (s0 > configured[0]) {
+            e = cudaFuncSetAttribute(k_interp<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s0);
+            if (e == cudaSuccess) configured[0] = s0;
+        }
+        const int s1 = (int)interp_smem<P>(E, a.tma_bx * a.tma_by);
+        if (e == cudaSuccess && kTmaForm && a.tma_bx > 0 && s1 > configured[1]) {
+            e = cudaFuncSetAttribute(k_interp<P, kTmaForm>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1);
+            if (e == cudaSuccess) configured[1] = s1;
+        }
         return e;
     }
     if (a.n_tiles == 0) return cudaSuccess;

@@ -299,8 +299,14 @@ cudaError_t launch_pair_cells(const LaunchArgs& a, cudaStream_t st) {
     return launch_pc_t<false, false>(a, st);
 }
 
+// The shared-memory limit is a property of each kernel function, shared by
+// every batch in the process: it is only ever raised, so a batch planned
+// later with a smaller staging capacity cannot lower it below the launch
+// size of one planned earlier.
 cudaError_t configure_pair_cells(int stage_cap) {
+    static int configured = 0;
     const int smem = (int)pair_cells_smem(stage_cap);
+    if (smem <= configured) return cudaSuccess;
     cudaError_t e = cudaSuccess;
 #define ESPB_PC_CONF(NQ)                                                                                    \
     if (e == cudaSuccess)                                                                                   \
@@ -311,6 +317,7 @@ cudaError_t configure_pair_cells(int stage_cap) {
         e = cudaFuncSetAttribute(k_pair_cells<NQ, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     ESPB_PC_NQ(ESPB_PC_CONF)
 #undef ESPB_PC_CONF
+    if (e == cudaSuccess) configured = smem;
     return e;
 }
 

@@ -270,10 +270,11 @@ class PotentialPairPSWF : public ForceCompute {
         if (!(p.rcut > 0)) throw std::invalid_argument("ESP: pair parameter 'rcut' must be positive");
         if (p.alpha != 0) throw std::invalid_argument("ESP: Debye screening (alpha != 0) is not supported");
         if (p.V_cut != 0) throw std::invalid_argument("ESP: the split energy vanishes at r_c; V_cut must be 0");
+        const std::string k = key(a, b);
         for (const auto& kv : m_params)
-            if (kv.second.rcut != p.rcut || kv.second.kappa != p.kappa)
+            if (kv.first != k && (kv.second.rcut != p.rcut || kv.second.kappa != p.kappa))
                 throw std::invalid_argument("ESP: every type pair shares one split (kappa, rcut)");
-        m_params[key(a, b)] = p;
+        m_params[k] = p;
         m_nlist->setRCutPair((Scalar)p.rcut);
         m_ctx.reset();
     }

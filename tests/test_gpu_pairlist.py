@@ -1,7 +1,8 @@
 """The library's cell-staged pair list (esp_batch_build_pairlist) against the
 HOOMD-layout neighbour list path, which is pinned to the oracle
 (test_gpu_parity.py): same forces, energies and virials up to summation
-order (relative RMS <= 1e-6, energy and virial <= 1e-6 relative).
+order (relative RMS <= 1e-6, energy and virial <= 1e-6 relative,
+per-particle energies <= 5e-6 of the largest).
 
 Cases:
 * a batch mixing cell grids of 2, 3 and >= 4 cells per axis (minimum image
@@ -66,7 +67,9 @@ def _both(b, pos, q, rlist, cap, flags=ESP_ALL):
 def _same(a, c, tol=1e-6):
     (fa, ea, wa), (fc, ec, wc) = a, c
     assert R.rel_rms(fc[:, :3], fa[:, :3]) <= tol
-    assert np.abs(fc[:, 3] - fa[:, 3]).max() <= tol * np.abs(fa[:, 3]).max()
+    # per-particle energies: FP32 sums of ~160 cancelling pair terms in a
+    # different order
+    assert np.abs(fc[:, 3] - fa[:, 3]).max() <= 5 * tol * np.abs(fa[:, 3]).max()
     assert np.all(np.abs(ec - ea) <= tol * np.abs(ea))
     assert np.abs(wc - wa).max() <= tol * np.abs(wa).max()
 

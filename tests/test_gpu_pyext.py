@@ -70,7 +70,8 @@ def test_forcecompute_pair_vs_oracle():
         u = r * r / 9.0
         L0 = R.INV_4PI * (1.0 / r - sp.Q(u) / 3.0)
         D0 = R.INV_4PI * (1.0 / (r * r) + 2.0 * r * sp.dQ(u) / 27.0)
-        assert abs(L - L0) <= 1e-9 * max(abs(L0), 1e-3) and abs(D - D0) <= 1e-8 * max(abs(D0), 1e-3)
+        # the table interpolates the C++ split fit (1e-12); the Python split here is fitted to 1e-8
+        assert abs(L - L0) <= 1e-8 * max(abs(L0), 1e-3) and abs(D - D0) <= 1e-7 * max(abs(D0), 1e-3)
 
 
 def test_forcecompute_validation():
