@@ -994,13 +994,16 @@ int esp_server_submit(esp_server* s, const esp_request* r, long long* id) {
     if (r->rigid_doh > 0 && (r->N % 3 != 0 || !(r->rigid_dhh > 0) || r->rigid_dhh >= 2.0 * r->rigid_doh))
         return fail(ESP_ERR_INVALID, "rigid water needs N = 3 x molecules and 0 < d_hh < 2 d_oh");
     std::lock_guard<std::mutex> lk(s->mu);
-    if (!s->pending.empty() && r->arrival < s->pending.back()->t_arrival)
+    // an arrival already in the past counts from now; the queue stays in
+    // arrival order because the clock only moves forward
+    double t_arr = std::max(0.0, r->arrival);
+    if (s->started) t_arr = std::max(t_arr, s->now());
+    if (!s->pending.empty() && t_arr < s->pending.back()->t_arrival)
         return fail(ESP_ERR_INVALID, "arrival times must not decrease");
     auto q = std::make_unique<Request>();
     q->r = *r;
     q->id = (long long)s->reqs.size();
-    q->t_arrival = std::max(0.0, r->arrival);
-    if (s->started) q->t_arrival = std::max(q->t_arrival, s->now());
+    q->t_arrival = t_arr;
     s->pending.push_back(q.get());
     s->reqs.push_back(std::move(q));
     s->stats.submitted++;

@@ -71,7 +71,9 @@ def test_forcecompute_pair_vs_oracle():
         L0 = R.INV_4PI * (1.0 / r - sp.Q(u) / 3.0)
         D0 = R.INV_4PI * (1.0 / (r * r) + 2.0 * r * sp.dQ(u) / 27.0)
         # the table interpolates the C++ split fit (1e-12); the Python split here is fitted to 1e-8
-        assert abs(L - L0) <= 1e-8 * max(abs(L0), 1e-3) and abs(D - D0) <= 1e-7 * max(abs(D0), 1e-3)
+        # of its scale, 1/(4 pi r_c) for L and 1/(4 pi r_c^2) for D (near r_c both values vanish)
+        lsc, dsc = R.INV_4PI / 3.0, R.INV_4PI / 9.0
+        assert abs(L - L0) <= 1e-8 * max(abs(L0), lsc) and abs(D - D0) <= 1e-7 * max(abs(D0), dsc)
 
 
 def test_forcecompute_validation():
