@@ -50,7 +50,7 @@ MD_STEPS = 10
 # passes: 3 whole-plane/slab kernels (fft_mode 0) or 5 per-line kernels
 K_EVAL_BASE = 9
 K_FFT = {0: 3, 1: 5}
-K_NLIST = 6      # cell_bin, scan, scatter, cell_sort, nlist, pack (cell-staged pair list; 5 for HOOMD rows)
+K_NLIST = 5      # cell_bin, scan, scatter, cell_sort, nlist
 K_NVE = 2
 
 
@@ -428,7 +428,7 @@ def run_scaleup(args):
         b.pairlist_check()
         b.build_nlist(pos, RCUT + SKIN, CAP, head, nn, nl)  # neighbour counts for the byte model
     mean_nn = float(nn.double().mean().item())
-    alg = {"pair": (4.0 if args.hoomd_list else 2.0) * N * mean_nn + 32.0 * N, "spread": 20.0 * N + 4.0 * M, "interp": 36.0 * N + 4.0 * M,
+    alg = {"pair": 4.0 * N * mean_nn + 32.0 * N, "spread": 20.0 * N + 4.0 * M, "interp": 36.0 * N + 4.0 * M,
            "fft": 5 * 2 * 8.0 * M / 2, "sort": 40.0 * N, "bin": 40.0 * N, "nlist": 16.0 * N + 4.0 * N * mean_nn,
            "nve": 48.0 * N}
     peak, peak_kind = _peak_gbs()
@@ -489,8 +489,8 @@ def run_ours(args):
 
     def request(bb, p, v, use_graph=True, qq=q, e=energy):
         # the first evaluation reports energy and virial; the NVE steps need
-        # forces and energies only. Default: the library's cell-staged pair
-        # list; --hoomd-list: HOOMD-layout rows built by the harness
+        # forces and energies only. Default: HOOMD-layout rows built by the
+        # harness; --pair-list: the library's pair list
         if args.hoomd_list:
             bb.build_nlist(p, RCUT + SKIN, CAP, head, nn, nl)
             nlist = (head, nn, nl)
@@ -544,9 +544,8 @@ def run_ours(args):
     mean_nn = float(nn.double().mean().item())
     M = sum(b.info(i)["nx"] * b.info(i)["ny"] * b.info(i)["nz"] for i in range(N.size))
     # algorithmic bytes per launch of each stage (FP32 storage)
-    # pair: index stream (4 B per entry for HOOMD rows, 2 B for the
-    # cell-staged list) + positions in + forces out
-    alg = {"pair": (4.0 if args.hoomd_list else 2.0) * tot * mean_nn + 16.0 * tot + 16.0 * tot,
+    # pair: index stream (4 B per entry) + positions in + forces out
+    alg = {"pair": 4.0 * tot * mean_nn + 16.0 * tot + 16.0 * tot,
            "spread": 20.0 * tot + 4.0 * M,
            "interp": 20.0 * tot + 4.0 * M + 16.0 * tot,
            "fft": 5 * 2 * 8.0 * M / 2,
@@ -554,7 +553,7 @@ def run_ours(args):
            "bin": 40.0 * tot,
            "nlist": 16.0 * tot + 4.0 * tot * mean_nn,
            "nve": 48.0 * tot}
-    kname = {"pair": "k_pair" if args.hoomd_list else "k_pair_cells", "spread": "k_spread", "interp": "k_interp", "fft": "k_fft", "nlist": "k_nlist",
+    kname = {"pair": "k_pair", "spread": "k_spread", "interp": "k_interp", "fft": "k_fft", "nlist": "k_nlist",
              "sort": "k_tile_sort", "bin": "k_bin", "nve": "k_nve"}
     peak, peak_kind = _peak_gbs()
     ach = alg[dom] / (stage_ms[dom] * 1e-3) / 1e9
@@ -673,9 +672,9 @@ def run_ours(args):
                                 "buffer sets, step k+1 uploads and step k-1 downloads on a copy stream "
                                 "during step k"},
                 "autotune": tuned,
-                "gpu_launches": int(args.steps * ((K_NLIST - 1 if args.hoomd_list else K_NLIST) + k_eval +
+                "gpu_launches": int(args.steps * (K_NLIST + k_eval +
                                                   MD_STEPS * (k_eval + K_NVE))),
-                "pair_list": "HOOMD-layout rows (k_pair)" if args.hoomd_list else "cell-staged (k_pair_cells)",
+                "pair_list": "HOOMD-layout rows" if args.hoomd_list else "the library's pair list (rows in cell order)",
                 "clocks": clk.summary()}
         line["fft"] = {"ours_ms": stage_ms.get("fft")}
         try:
@@ -741,8 +740,9 @@ def main():
                     help="scaleup: the plain path on one 10^6-particle system (a second measurement)")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default plan)")
-    ap.add_argument("--hoomd-list", action="store_true",
-                    help="short-range term over HOOMD-layout neighbour rows instead of the cell-staged pair list")
+    ap.add_argument("--pair-list", dest="hoomd_list", action="store_false",
+                    help="short-range term over the library's pair list (rows in cell order) instead of HOOMD-layout "
+                         "neighbour rows (the default)")
     ap.add_argument("--serve-requests", type=int, default=10000, help="requests per arrival rate")
     ap.add_argument("--serve-rates", type=lambda v: [float(x) for x in v.split(",")], default=[200.0, 800.0, 0.0],
                     help="comma-separated arrival rates (requests/s); 0 = all requests at once (saturation)")

@@ -30,7 +30,7 @@ EXPORTS = [
     "esp_server_get_stats", "esp_server_destroy", "esp_set_exclusions", "esp_batch_set_exclusions",
     "esp_compute_f64", "esp_batch_compute_f64", "esp_batch_autotune", "esp_batch_lj", "esp_batch_lj_f64",
     "esp_batch_nve_step1_f64", "esp_batch_nve_step2_f64", "esp_batch_build_pairlist", "esp_batch_pairlist_check",
-    "esp_compute_hoomd", "esp_batch_set_rigid_water", "esp_batch_device_errors",
+    "esp_compute_hoomd", "esp_batch_set_rigid_water", "esp_batch_device_errors", "esp_batch_nlist_check",
 ]
 
 ESP_FP32 = 0
@@ -149,6 +149,7 @@ def get_lib() -> ctypes.CDLL:
         lib.esp_batch_device_errors.argtypes = [P, ctypes.POINTER(ctypes.c_int)]
         lib.esp_compute_hoomd.argtypes = [P, P, P, P, I, P, P, P, P, P, I, P, I]
         lib.esp_batch_pairlist_check.argtypes = [P, ctypes.POINTER(ctypes.c_int)]
+        lib.esp_batch_nlist_check.argtypes = [P, ctypes.POINTER(ctypes.c_int)]
         for name in EXPORTS:
             if name != "esp_last_error":
                 getattr(lib, name).restype = ctypes.c_int

@@ -1,10 +1,8 @@
-// The 27-cell neighbourhood of a cell list, shared by the neighbour-list
-// builders (esp_md.cu: HOOMD-layout rows; esp_pairlist.cu: the library's
-// cell-staged pair list) and the cell-staged pair kernel, so that every one
-// of them enumerates the surrounding cells' particles in the same order:
-// surrounding cell t = (iz * 3 + iy) * 3 + ix in that order, and inside each
-// cell the cell-sorted slots in ascending order. A particle's "staged index"
-// is its position in that enumeration.
+// The 27-cell neighbourhood of a cell list, used by the neighbour-list
+// builder (esp_md.cu: HOOMD-layout rows and the library's pair list), which
+// enumerates the surrounding cells' particles in a fixed order: surrounding
+// cell t = (iz * 3 + iy) * 3 + ix in that order, and inside each cell the
+// cell-sorted slots in ascending order (so every row is deterministic).
 #pragma once
 
 #include "esp_common.cuh"
@@ -16,7 +14,6 @@ struct CellNbhd {
     uint32_t src[27];       // first cell-sorted slot of each surrounding cell
     uint32_t off[28];       // exclusive prefix of their counts (off[27] = total)
     float shift[27][3];     // periodic image of each surrounding cell (0 with minimg)
-    int center;             // t of the cell itself
     int minimg;             // fewer than 3 cells on an axis: staged without shifts
 };
 
@@ -60,11 +57,7 @@ __device__ __forceinline__ void cell_nbhd_warp(int lc, const CellDev& C, const S
     }
     if (lane < 27) nb.off[lane] = inc - n;
     if (lane == 26) nb.off[27] = inc;
-    if (lane == 0) {
-        const int ix0 = C.ncx >= 3 ? 1 : 0, iy0 = C.ncy >= 3 ? 1 : 0, iz0 = C.ncz >= 3 ? 1 : 0;
-        nb.center = (iz0 * 3 + iy0) * 3 + ix0;
-        nb.minimg = minimg ? 1 : 0;
-    }
+    if (lane == 0) nb.minimg = minimg ? 1 : 0;
 }
 
 }  // namespace espb

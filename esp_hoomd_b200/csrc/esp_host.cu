@@ -281,8 +281,8 @@ struct esp_batch {
     int tma_bx = 0, tma_by = 0;
     int* d_kerr = nullptr;
     // cell grids of the neighbour-list builds (allocated on first use): one
-    // for HOOMD-layout lists, one for the library's cell-staged pair list
-    // (whose kernel reads the cell structures of its own build)
+    // for HOOMD-layout lists, one for the library's pair list (whose rows
+    // are indexed by the slots of its own build)
     struct CellGrid {
         DevAlloc mem;
         double rlist = -1;
@@ -291,22 +291,31 @@ struct esp_batch {
         CellDev* d_cells = nullptr;
         int* d_cell_sys = nullptr;
         uint32_t *d_ckey = nullptr, *d_ccount = nullptr, *d_cstart = nullptr, *d_cperm = nullptr,
-                 *d_slot2idx = nullptr;
+                 *d_slot2idx = nullptr, *d_idx2slot = nullptr;
         float4 *d_wpos = nullptr, *d_cpos = nullptr;
         int* d_overflow = nullptr;  // [flag, largest row] of the last build
     } cg_nl, cg_pl;
     int setup_cells(CellGrid& g, double rlist, int cap);
     NlistArgs nlist_args(CellGrid& g, const float* pos4, double rlist, int cap) const;
-    // the cell-staged pair list (esp_pairlist.cu): rows by cell-sorted slot
+    // the library's pair list: rows by cell-sorted slot, and the
+    // slot-ordered positions the bin stage writes for it
     DevAlloc plmem;
-    uint16_t* d_pl16 = nullptr;
-    uint32_t* d_pl_nn = nullptr;
-    int pl_cap = 0, pl_stage_cap = 0;
+    uint32_t *d_pl_head = nullptr, *d_pl_nn = nullptr, *d_pl_nl = nullptr;
+    float4* d_spos = nullptr;
+    int pl_cap = 0;
     bool pl_ready = false, pl_pending = false, pl_overflow = false;
     int* h_pl_ovf = nullptr;  // page-locked copy of the last build's [flag, largest row]
     cudaEvent_t pl_ev = nullptr;
     PairList pl{};
     int build_pairlist(cudaStream_t st, const float* pos4, double rlist, int cap);
+    // the last HOOMD-layout build: its overflow flag is read lazily as well
+    // (page-locked copy + event); compute and md_run check it when handed
+    // the rows it wrote
+    int* h_nl_ovf = nullptr;
+    cudaEvent_t nl_ev = nullptr;
+    bool nl_pending = false, nl_overflow = false;
+    const unsigned *nl_last_head = nullptr, *nl_last_nl = nullptr;
+    int nlist_check(bool wait, int* needed);
     // ESP_ERR_OVERFLOW when the last pair-list build overflowed; without
     // `wait` an unfinished build counts as fine (checked again next time)
     int pairlist_check(bool wait, int* needed);
@@ -384,6 +393,11 @@ struct esp_batch {
             cudaEventDestroy(pl_ev);
         }
         if (h_pl_ovf) cudaFreeHost(h_pl_ovf);
+        if (nl_ev) {
+            cudaEventSynchronize(nl_ev);
+            cudaEventDestroy(nl_ev);
+        }
+        if (h_nl_ovf) cudaFreeHost(h_nl_ovf);
     }
 
     LaunchArgs args() const;
@@ -428,8 +442,9 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         cg_pl.rlist = -1;
         plmem.release();
         pl_cap = 0;
-        pl_stage_cap = 0;
         pl_ready = pl_pending = pl_overflow = false;
+        nl_last_head = nl_last_nl = nullptr;
+        nl_pending = nl_overflow = false;
     }
     prm = p;
     if (ns <= 0) return fail(ESP_ERR_INVALID, "number of systems must be positive");
@@ -986,8 +1001,9 @@ int esp_batch::md_run(cudaStream_t st, float* pos4, float* vel4, const float* q,
     if (!pos4 || !vel4 || !q || !force4) return fail(ESP_ERR_INVALID, "null pointer");
     if (!(head && nn && nl) && (head || nn || nl || !pl_ready))
         return fail(ESP_ERR_INVALID, "md_run needs the neighbour list (head, n_neigh, nlist) or a built pair list");
-    if (!head) {
-        int rc = pairlist_check(false, nullptr);
+    {
+        int rc = !head ? pairlist_check(false, nullptr)
+                       : (head == nl_last_head && nl == nl_last_nl ? nlist_check(false, nullptr) : 0);
         if (rc) return rc;
     }
     // Every step overwrites the energies (force.w, energy) of the previous
@@ -1124,7 +1140,8 @@ int esp_batch::setup_cells(CellGrid& g, double rlist, int cap) {
     if ((rc = g.mem.get(g.d_cells, nsys)) || (rc = g.mem.get(g.d_cell_sys, g.n_cells)) ||
         (rc = g.mem.get(g.d_ckey, totN)) || (rc = g.mem.get(g.d_ccount, g.n_cells)) ||
         (rc = g.mem.get(g.d_cstart, g.n_cells + 1)) || (rc = g.mem.get(g.d_cperm, totN)) ||
-        (rc = g.mem.get(g.d_slot2idx, totN)) || (rc = g.mem.get(g.d_wpos, totN)) ||
+        (rc = g.mem.get(g.d_slot2idx, totN)) || (rc = g.mem.get(g.d_idx2slot, totN)) ||
+        (rc = g.mem.get(g.d_wpos, totN)) ||
         (rc = g.mem.get(g.d_cpos, totN)) || (rc = g.mem.get(g.d_overflow, 2)))
         return rc;
     ESPB_CK(cudaMemcpy(g.d_cells, g.h_cells.data(), nsys * sizeof(CellDev), cudaMemcpyHostToDevice));
@@ -1150,6 +1167,7 @@ NlistArgs esp_batch::nlist_args(CellGrid& g, const float* pos4, double rlist, in
     a.cstart = g.d_cstart;
     a.perm_u = g.d_cperm;
     a.slot2idx = g.d_slot2idx;
+    a.idx2slot = g.d_idx2slot;
     a.wpos = g.d_wpos;
     a.cpos = g.d_cpos;
     a.rlist2 = (float)(rlist * rlist);
@@ -1162,86 +1180,88 @@ int esp_batch::build_nlist(cudaStream_t st, const float* pos4, double rlist, int
                            unsigned* nl) {
     if (!(rlist > 0) || cap <= 0) return fail(ESP_ERR_INVALID, "rlist and cap must be positive");
     if (!pos4 || !head || !nn || !nl) return fail(ESP_ERR_INVALID, "null pointer");
+    if ((double)totN * cap >= 4294967296.0)
+        return fail(ESP_ERR_UNSUPPORTED, "HOOMD-layout rows address 32-bit offsets: totN * cap must be below 2^32");
     int rc = setup_cells(cg_nl, rlist, cap);
     if (rc) return rc;
     NlistArgs a = nlist_args(cg_nl, pos4, rlist, cap);
     a.head = head;
     a.nn = nn;
     a.nl = nl;
+    if (!h_nl_ovf) ESPB_CK(cudaHostAlloc((void**)&h_nl_ovf, 2 * sizeof(int), cudaHostAllocDefault));
+    if (!nl_ev) ESPB_CK(cudaEventCreateWithFlags(&nl_ev, cudaEventDisableTiming));
     // HOOMD-layout rows: head[i] = first entry of system s + local i * cap
     timer.begin(ESP_STAGE_NLIST, st);
     ESPB_CK(launch_nlist(a, st));
     timer.end(st);
-    int ovf = 0;
-    ESPB_CK(cudaMemcpyAsync(&ovf, cg_nl.d_overflow, sizeof(int), cudaMemcpyDeviceToHost, st));
-    ESPB_CK(cudaStreamSynchronize(st));
-    if (ovf) return fail(ESP_ERR_OVERFLOW, "neighbour-list row capacity exceeded; n_neigh holds the needed counts");
+    // the overflow flag is read lazily (esp_batch_nlist_check, or the next
+    // compute / md_run over these rows): no host synchronisation here
+    ESPB_CK(cudaMemcpyAsync(h_nl_ovf, cg_nl.d_overflow, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    ESPB_CK(cudaEventRecord(nl_ev, st));
+    nl_last_head = head;
+    nl_last_nl = nl;
+    nl_pending = true;
+    nl_overflow = false;
     return 0;
 }
 
-// Staging capacity of the pair kernel: 1.25 x the mean neighbourhood (the
-// particles of the surrounding cells at each system's mean density) + 64,
-// at most what one CTA's shared memory holds. Denser neighbourhoods are
-// staged in windows (slower, same results).
-static int pair_stage_capacity(const std::vector<CellDev>& cells, const std::vector<int>& N,
-                               const std::vector<double>& box) {
-    double est = 0;
-    for (size_t s = 0; s < cells.size(); ++s) {
-        const CellDev& C = cells[s];
-        const double V = box[3 * s] * box[3 * s + 1] * box[3 * s + 2];
-        const double w3 = V / ((double)C.ncx * C.ncy * C.ncz);
-        const int visited = std::min(C.ncx, 3) * std::min(C.ncy, 3) * std::min(C.ncz, 3);
-        est = std::max(est, visited * w3 * N[s] / V);
+int esp_batch::nlist_check(bool wait, int* needed) {
+    if (!nl_ev || !h_nl_ovf) return fail(ESP_ERR_INVALID, "no neighbour list has been built (esp_batch_build_nlist)");
+    if (nl_pending) {
+        if (wait) {
+            ESPB_CK(cudaEventSynchronize(nl_ev));
+        } else {
+            const cudaError_t q = cudaEventQuery(nl_ev);
+            if (q == cudaErrorNotReady) return 0;
+            if (q != cudaSuccess)
+                return fail(ESP_ERR_CUDA, std::string("neighbour-list build: ") + cudaGetErrorString(q));
+        }
+        nl_pending = false;
+        nl_overflow = h_nl_ovf[0] != 0;
     }
-    const int max_cap = (int)((227 * 1024 - pair_cells_smem(0)) / 16) & ~7;
-    int c = (int)std::ceil(1.25 * est + 64.0);
-    c = ((c + 7) & ~7);
-    c = std::max(64, std::min(c, max_cap));
-    return c - 1;  // stage_cap + 1 (with the padding particle) is a multiple of 8
+    if (needed) *needed = h_nl_ovf[1];
+    if (nl_overflow)
+        return fail(ESP_ERR_OVERFLOW, "neighbour-list row capacity exceeded (largest row " +
+                                          std::to_string(h_nl_ovf[1]) + "); n_neigh holds the needed counts");
+    return 0;
 }
 
 int esp_batch::build_pairlist(cudaStream_t st, const float* pos4, double rlist, int cap) {
     if (!(rlist > 0) || cap <= 0) return fail(ESP_ERR_INVALID, "rlist and cap must be positive");
-    if (cap % 8 != 0 || cap > 1024)
-        return fail(ESP_ERR_UNSUPPORTED, "pair-list row capacity must be a multiple of 8, at most 1024");
     if (!pos4) return fail(ESP_ERR_INVALID, "null position pointer");
-    if (f64) return fail(ESP_ERR_UNSUPPORTED, "the cell-staged pair list serves the FP32 path");
+    if (f64) return fail(ESP_ERR_UNSUPPORTED, "the library's pair list serves the FP32 path");
+    if ((double)totN * cap >= 4294967296.0) return fail(ESP_ERR_UNSUPPORTED, "pair list of 2^32 entries or more");
     int rc = setup_cells(cg_pl, rlist, cap);
     if (rc) return rc;
     if (pl_cap != cap) {
         plmem.release();
         pl_cap = 0;
-        if ((rc = plmem.get(d_pl16, (size_t)totN * cap)) || (rc = plmem.get(d_pl_nn, totN))) return rc;
+        if ((rc = plmem.get(d_pl_nl, (size_t)totN * cap)) || (rc = plmem.get(d_pl_head, totN)) ||
+            (rc = plmem.get(d_pl_nn, totN)) || (rc = plmem.get(d_spos, totN)))
+            return rc;
         pl_cap = cap;
         drop_graphs();  // captured steps hold the previous arrays
-    }
-    const int scap = pair_stage_capacity(cg_pl.h_cells, N, box);
-    if (scap != pl_stage_cap) {
-        ESPB_CK(configure_pair_cells(scap));
-        pl_stage_cap = scap;
-        drop_graphs();
     }
     if (!h_pl_ovf) ESPB_CK(cudaHostAlloc((void**)&h_pl_ovf, 2 * sizeof(int), cudaHostAllocDefault));
     if (!pl_ev) ESPB_CK(cudaEventCreateWithFlags(&pl_ev, cudaEventDisableTiming));
     NlistArgs a = nlist_args(cg_pl, pos4, rlist, cap);
+    a.head = d_pl_head;
     a.nn = d_pl_nn;
-    a.nl16 = d_pl16;
+    a.nl = d_pl_nl;
+    a.sorted = true;
     timer.begin(ESP_STAGE_NLIST, st);
     ESPB_CK(launch_nlist(a, st));
-    ESPB_CK(launch_pairlist_pack(totN, d_pl_nn, d_pl16, cap, st));
     timer.end(st);
     // the overflow flag is read lazily: no host synchronisation here
     ESPB_CK(cudaMemcpyAsync(h_pl_ovf, cg_pl.d_overflow, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     ESPB_CK(cudaEventRecord(pl_ev, st));
-    pl.cell_sys = cg_pl.d_cell_sys;
-    pl.cells = cg_pl.d_cells;
-    pl.cstart = cg_pl.d_cstart;
     pl.slot2idx = cg_pl.d_slot2idx;
+    pl.idx2slot = cg_pl.d_idx2slot;
+    pl.spos = d_spos;
+    pl.head = d_pl_head;
     pl.nn = d_pl_nn;
-    pl.nl16 = d_pl16;
-    pl.n_cells = cg_pl.n_cells;
+    pl.nl = d_pl_nl;
     pl.cap = cap;
-    pl.stage_cap = pl_stage_cap;
     pl_ready = true;
     pl_pending = true;
     pl_overflow = false;
@@ -1260,10 +1280,9 @@ int esp_batch::pairlist_check(bool wait, int* needed) {
         }
         pl_pending = false;
         pl_overflow = h_pl_ovf[0] != 0;
-        if (needed) *needed = h_pl_ovf[1];
     }
+    if (needed) *needed = h_pl_ovf[1];
     if (pl_overflow) {
-        if (needed) *needed = h_pl_ovf[1];
         return fail(ESP_ERR_OVERFLOW, "pair-list row capacity exceeded (largest row " + std::to_string(h_pl_ovf[1]) +
                                           "); rebuild with a larger cap");
     }
@@ -1616,6 +1635,10 @@ int esp_batch_compute(esp_batch* b, void* stream, const float* pos4, const float
         int rc = b->pairlist_check(false, nullptr);
         if (rc) return rc;
     }
+    if ((flags & ESP_SHORT_RANGE) && head && head == b->nl_last_head && nlist == b->nl_last_nl) {
+        int rc = b->nlist_check(false, nullptr);
+        if (rc) return rc;
+    }
     return b->compute((cudaStream_t)stream, pos4, charge, head, n_neigh, nlist, force4, energy, virial6, flags);
 }
 
@@ -1721,6 +1744,11 @@ int esp_batch_build_nlist(esp_batch* b, void* stream, const float* pos4, double 
                           unsigned* n_neigh, unsigned* nlist) {
     if (!b) return fail(ESP_ERR_INVALID, "null batch");
     return b->build_nlist((cudaStream_t)stream, pos4, rlist, cap, head, n_neigh, nlist);
+}
+
+int esp_batch_nlist_check(esp_batch* b, int* needed_cap) {
+    if (!b) return fail(ESP_ERR_INVALID, "null batch");
+    return b->nlist_check(true, needed_cap);
 }
 
 int esp_batch_nve_step1(esp_batch* b, void* stream, float* pos4, float* vel4, const float* force4, double dt) {

@@ -30,7 +30,8 @@ namespace espb {
 __global__ void k_bin(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, int P, int T,
                       const float4* __restrict__ pos_in, const float* __restrict__ q_in,
                       float4* __restrict__ posq, float4* __restrict__ trec, uint32_t* __restrict__ rel,
-                      uint32_t* __restrict__ key, uint32_t* __restrict__ tile_count, double* __restrict__ acc) {
+                      uint32_t* __restrict__ key, uint32_t* __restrict__ tile_count, double* __restrict__ acc,
+                      const uint32_t* __restrict__ idx2slot, float4* __restrict__ spos) {
     __shared__ double red[32 * 2];
     const int2 ch = chunks[blockIdx.x];
     const SysDev S = sys[ch.x];
@@ -68,6 +69,8 @@ __global__ void k_bin(const int2* __restrict__ chunks, const SysDev* __restrict_
         key[i] = k;
         kk = k;
         posq[i] = make_float4(x, y, z, q);
+        // the pair list's slot-ordered copy (rows of that list index it)
+        if (spos) spos[idx2slot[i]] = make_float4(x, y, z, q);
         trec[i] = make_float4(tt[0], tt[1], tt[2], q);
         rel[i] = (uint32_t)(i0m[0] - tx * T) | ((uint32_t)(i0m[1] - ty * T) << 8) |
                  ((uint32_t)(i0m[2] - tz * T) << 16);
@@ -1524,7 +1527,7 @@ __global__ void __launch_bounds__(256, EN ? 5 : 6)
     k_pair(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
            const float4* __restrict__ posq, const uint32_t* __restrict__ head, const uint32_t* __restrict__ nn,
            const uint32_t* __restrict__ nlist, float4* __restrict__ force, double* __restrict__ acc, int accumulate,
-           const PairCoef pc, float* __restrict__ vpp, int vpitch) {
+           const PairCoef pc, float* __restrict__ vpp, int vpitch, const uint32_t* __restrict__ outidx) {
     __shared__ double red[32 * 7];
     const int2 ch = chunks[blockIdx.x];
     const SysDev S = sys[ch.x];
@@ -1604,13 +1607,15 @@ __global__ void __launch_bounds__(256, EN ? 5 : 6)
         fz += __shfl_xor_sync(0xffffffffu, fz, o);
         en += __shfl_xor_sync(0xffffffffu, en, o);
     }
+    // rows by slot (the library's pair list): results go to the particle of the slot
+    const int oi = (outidx && valid) ? (int)outidx[i] : i;
     if (valid && sub == 0) {
-        float4 f = accumulate ? force[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 f = accumulate ? force[oi] : make_float4(0.f, 0.f, 0.f, 0.f);
         f.x += fx;
         f.y += fy;
         f.z += fz;
         f.w += 0.5f * en;
-        force[i] = f;
+        force[oi] = f;
     }
     if (VIR && vpp) {
         // this particle's half of its pairs' virial (HOOMD's per-particle virial)
@@ -1621,7 +1626,7 @@ __global__ void __launch_bounds__(256, EN ? 5 : 6)
             for (int k = 0; k < 6; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
         if (valid && sub == 0)
 #pragma unroll
-            for (int k = 0; k < 6; ++k) vpp[(size_t)k * vpitch + i] += 0.5f * v[k];
+            for (int k = 0; k < 6; ++k) vpp[(size_t)k * vpitch + oi] += 0.5f * v[k];
     }
     if (VIR) {
         double e[7] = {sub == 0 ? 0.5 * (double)en : 0.0, 0.5 * (double)ev.vxx, 0.5 * (double)ev.vxy,
@@ -1823,7 +1828,8 @@ cudaError_t launch_scatter(const int2* chunks, int n_chunks, const SysDev* sys, 
 cudaError_t launch_bin(const LaunchArgs& a, cudaStream_t st) {
     if (a.n_chunks == 0) return cudaSuccess;
     k_bin<<<a.n_chunks, 256, 0, st>>>(a.chunks, a.sys, a.P, a.T, a.pos_in, a.q_in, a.posq, a.trec, a.rel, a.key,
-                                      a.tile_count, a.acc);
+                                      a.tile_count, a.acc, a.plist ? a.plist->idx2slot : nullptr,
+                                      a.plist ? a.plist->spos : nullptr);
     return cudaGetLastError();
 }
 
@@ -1887,10 +1893,17 @@ cudaError_t launch_fft(const LaunchArgs& a, cudaStream_t st) {
 
 template <int TPP, bool VIR, bool EN>
 static cudaError_t launch_pair_t(const LaunchArgs& a, cudaStream_t st) {
-#define ESPB_PAIR(NQ)                                                                                        \
-    k_pair<TPP, NQ, VIR, EN><<<a.n_pchunks, 256, 0, st>>>(a.pchunks, a.sys, a.psets, a.posq, a.nl_head, a.nl_n, \
-                                                          a.nl_list, a.force, a.acc, a.accumulate, a.pc,    \
-                                                          a.virial_pp, a.vpp_pitch)
+    // the library's pair list: rows by slot over the slot-ordered positions
+    const PairList* pl = a.plist;
+    const float4* posq = pl ? pl->spos : a.posq;
+    const uint32_t* head = pl ? pl->head : a.nl_head;
+    const uint32_t* nn = pl ? pl->nn : a.nl_n;
+    const uint32_t* nl = pl ? pl->nl : a.nl_list;
+    const uint32_t* outidx = pl ? pl->slot2idx : nullptr;
+#define ESPB_PAIR(NQ)                                                                                          \
+    k_pair<TPP, NQ, VIR, EN><<<a.n_pchunks, 256, 0, st>>>(a.pchunks, a.sys, a.psets, posq, head, nn, nl, a.force, \
+                                                          a.acc, a.accumulate, a.pc, a.virial_pp, a.vpp_pitch,    \
+                                                          outidx)
     if (a.nq <= 8) ESPB_PAIR(8);
     else if (a.nq <= 10) ESPB_PAIR(10);
     else if (a.nq <= 11) ESPB_PAIR(11);
@@ -1906,7 +1919,6 @@ static cudaError_t launch_pair_t(const LaunchArgs& a, cudaStream_t st) {
 }
 
 cudaError_t launch_pair(const LaunchArgs& a, cudaStream_t st) {
-    if (a.plist) return launch_pair_cells(a, st);
     if (a.n_pchunks == 0) return cudaSuccess;
     if (a.want_virial) {
         switch (a.tpp) {

@@ -31,24 +31,24 @@ struct PairCoef {
     float d[MAX_QC];  // dQ/du in v
 };
 
-struct CellDev;
-
-// The library's cell-staged pair list (esp_pairlist.cu): rows by cell-sorted
-// slot, entries u16 staged indices into the slot's cell neighbourhood, plus
-// the cell structures of the build that defined those indices.
+// The library's pair list: rows indexed by the cell-sorted slot of its
+// build (head/nn/nl in the HOOMD layout, entries local slots), the slot <->
+// particle maps of that build, and the slot-ordered copy of the wrapped
+// positions and charges that the bin stage writes every evaluation (so that
+// a row's neighbours are neighbours in memory too).
 struct PairList {
-    const int* cell_sys = nullptr;      // system of each cell
-    const CellDev* cells = nullptr;     // per-system cell grid
-    const uint32_t* cstart = nullptr;   // first slot of each cell (n_cells + 1)
-    const uint32_t* slot2idx = nullptr; // slot -> particle (concatenated index)
-    const uint32_t* nn = nullptr;       // entries per row
-    const uint16_t* nl16 = nullptr;     // rows of `cap` entries
-    int n_cells = 0, cap = 0, stage_cap = 0;
+    const uint32_t* slot2idx = nullptr;  // slot -> particle (concatenated index)
+    const uint32_t* idx2slot = nullptr;  // particle -> slot
+    float4* spos = nullptr;              // {x, y, z, q} by slot
+    const uint32_t* head = nullptr;
+    const uint32_t* nn = nullptr;
+    const uint32_t* nl = nullptr;
+    int cap = 0;
 };
 
 struct LaunchArgs {
     PairCoef pc{};
-    const PairList* plist = nullptr;  // non-null: short-range term over the cell-staged pair list
+    const PairList* plist = nullptr;  // non-null: short-range term over the library's pair list
     const SysDev* sys = nullptr;
     const ParamSet* psets = nullptr;
     int nsys = 0, P = 8, T = 8, D = 10, PX = 0, PP = 0, tpp = 8, accumulate = 0, nq = 16;
@@ -127,12 +127,6 @@ cudaError_t launch_spread(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_fft(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_interp(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_pair(const LaunchArgs& a, cudaStream_t st);
-// cell-staged pair list: row packing after a build, the pair kernel, and the
-// kernels' shared-memory attributes (plan time)
-cudaError_t launch_pairlist_pack(int rows, const uint32_t* nn, uint16_t* nl16, int cap, cudaStream_t st);
-cudaError_t launch_pair_cells(const LaunchArgs& a, cudaStream_t st);
-cudaError_t configure_pair_cells(int stage_cap);
-size_t pair_cells_smem(int stage_cap);
 cudaError_t launch_exclusions(const LaunchArgs& a, cudaStream_t st);
 cudaError_t launch_add_forces(const int2* chunks, int n_chunks, const SysDev* sys, const float4* add, float4* force,
                               cudaStream_t st);

@@ -43,7 +43,7 @@ __global__ void k_cell_bin(const int2* __restrict__ chunks, const SysDev* __rest
 // cell-sorted positions.
 __global__ void k_cell_sort(const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm_u,
                             const float4* __restrict__ wpos, float4* __restrict__ cpos,
-                            uint32_t* __restrict__ slot2idx) {
+                            uint32_t* __restrict__ slot2idx, uint32_t* __restrict__ idx2slot) {
     __shared__ __align__(16) uint32_t sm[1024];
     const uint32_t s0 = start[blockIdx.x];
     const uint32_t n = start[blockIdx.x + 1] - s0;
@@ -71,95 +71,67 @@ __global__ void k_cell_sort(const uint32_t* __restrict__ start, const uint32_t* 
         }
         cpos[s0 + r] = wpos[v];
         if (slot2idx) slot2idx[s0 + r] = v;
+        if (idx2slot) idx2slot[v] = s0 + r;
     }
 }
 
-// One CTA per cell, one thread per particle of the cell (passes of
-// NL_THREADS). The particles of the 27 surrounding cells are staged in
+// One CTA per cell. The particles of the 27 surrounding cells are staged in
 // shared memory, in the fixed (dz, dy, dx) order and ascending slot inside
-// each cell, so every row is deterministic; each thread scans them with
-// broadcast shared loads. With at least 3 cells on every axis each
-// surrounding cell is a distinct periodic image and its particles are
-// staged already shifted by that image, so the test needs no wrap; smaller
-// cell grids take the minimum-image test.
-constexpr int NL_THREADS = 64;
+// each cell (in windows of NL_STAGE when there are more), so every row is
+// deterministic. One warp per particle of the cell: lane k tests candidate
+// base + k and the hits are appended in candidate order (ballot and prefix
+// count), up to 32 consecutive entries per store. With at least 3 cells on
+// every axis each surrounding cell is a distinct periodic image and its
+// particles are staged already shifted by that image, so the test needs no
+// wrap; smaller cell grids take the minimum-image test.
+constexpr int NL_WARPS = 4;
+constexpr int NL_THREADS = 32 * NL_WARPS;
 constexpr int NL_STAGE = 1024;
 
-// store v at p when ok, as one predicated store (the candidate loop has no
-// per-candidate branch)
-__device__ __forceinline__ void store_if(bool ok, uint32_t* p, uint32_t v) {
-    asm volatile(
-        "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q st.global.u32 [%0], %1;\n\t}" ::"l"(p), "r"(v),
-        "r"((uint32_t)ok)
-        : "memory");
-}
-
-__device__ __forceinline__ void store_if16(bool ok, uint16_t* p, uint32_t v) {
-    asm volatile(
-        "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q st.global.u16 [%0], %1;\n\t}" ::"l"(p),
-        "h"((unsigned short)v), "r"((uint32_t)ok)
-        : "memory");
-}
-
-// Appends the staged candidates within rlist of pi to row (threads without a
-// particle carry a NaN position, which tests false against everything).
+// Appends the staged candidates within rlist of pi (other than `self`) to
+// row, entries w - base_id with w the candidate's staged value; returns the
+// new count (entries past cap are counted, not stored).
 template <bool MINIMG>
-__device__ __forceinline__ uint32_t nl_scan(const float4* __restrict__ cand, int n, float4 pi, int i, const SysDev& S,
-                                            float rlist2, uint32_t cap, uint32_t* __restrict__ row, uint32_t cnt) {
-#pragma unroll 4
-    for (int k = 0; k < n; ++k) {
-        const float4 pj = cand[k];
-        float ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
-        if (MINIMG) {
-            ddx -= S.Lx * rintf(ddx * S.inv_Lx);
-            ddy -= S.Ly * rintf(ddy * S.inv_Ly);
-            ddz -= S.Lz * rintf(ddz * S.inv_Lz);
+__device__ __forceinline__ uint32_t nl_scan_warp(const float4* __restrict__ cand, int n, float4 pi, int self,
+                                                 const SysDev& S, float rlist2, uint32_t cap,
+                                                 uint32_t* __restrict__ row, uint32_t cnt, int base_id) {
+    const unsigned lt = (1u << (threadIdx.x & 31)) - 1u;
+    for (int k0 = 0; k0 < n; k0 += 32) {
+        const int k = k0 + (int)(threadIdx.x & 31);
+        bool hit = false;
+        int w = 0;
+        if (k < n) {
+            const float4 pj = cand[k];
+            float ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
+            if (MINIMG) {
+                ddx -= S.Lx * rintf(ddx * S.inv_Lx);
+                ddy -= S.Ly * rintf(ddy * S.inv_Ly);
+                ddz -= S.Lz * rintf(ddz * S.inv_Lz);
+            }
+            w = __float_as_int(pj.w);
+            hit = ddx * ddx + ddy * ddy + ddz * ddz < rlist2 && w != self;
         }
-        const int j = __float_as_int(pj.w);
-        const bool hit = ddx * ddx + ddy * ddy + ddz * ddz < rlist2 && j != i;
-        store_if(hit && cnt < cap, row + cnt, (uint32_t)(j - S.p_off));
-        cnt += hit ? 1u : 0u;
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        const uint32_t at = cnt + (uint32_t)__popc(m & lt);
+        if (hit && at < cap) row[at] = (uint32_t)(w - base_id);
+        cnt += (uint32_t)__popc(m);
     }
     return cnt;
 }
 
-// As nl_scan, for the cell-staged pair list: the entry is the candidate's
-// staged index (its position in the cell's neighbourhood enumeration).
-template <bool MINIMG>
-__device__ __forceinline__ uint32_t nl_scan_staged(const float4* __restrict__ cand, int n, float4 pi, int i,
-                                                   const SysDev& S, float rlist2, uint32_t cap,
-                                                   uint16_t* __restrict__ row, uint32_t cnt, uint32_t base) {
-#pragma unroll 4
-    for (int k = 0; k < n; ++k) {
-        const float4 pj = cand[k];
-        float ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
-        if (MINIMG) {
-            ddx -= S.Lx * rintf(ddx * S.inv_Lx);
-            ddy -= S.Ly * rintf(ddy * S.inv_Ly);
-            ddz -= S.Lz * rintf(ddz * S.inv_Lz);
-        }
-        const bool hit = ddx * ddx + ddy * ddy + ddz * ddz < rlist2 && __float_as_int(pj.w) != i;
-        store_if16(hit && cnt < cap, row + cnt, base + (uint32_t)k);
-        cnt += hit ? 1u : 0u;
-    }
-    return cnt;
-}
-
-// STAGED = false: HOOMD-layout rows (row of particle i at nl_off + local i *
-// cap, entries local particle indices). STAGED = true: the cell-staged pair
-// list -- the row of cell-sorted slot s at s * cap (u16), entries staged
-// indices, each row padded to a multiple of 8 entries with the cell's
-// sentinel index (its neighbourhood total, a zero-charge dummy in the pair
-// kernel); rows that exceed cap, or neighbourhoods of more than 65,534
-// particles, set the overflow flag.
-template <bool STAGED>
+// SORTED = false: HOOMD-layout rows -- the row of particle i at nl_off +
+// local i * cap, entries local particle indices, head/nn indexed by
+// particle. SORTED = true: the library's pair list -- the same layout indexed
+// by the cell-sorted slot (row of slot s at nl_off + local s * cap, head and
+// nn by slot), entries local slots. Rows longer than cap keep their first cap
+// entries and set the overflow flag; overflow[1] receives the longest row.
+template <bool SORTED>
 __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ cell_sys, const SysDev* __restrict__ sys,
                                                       const CellDev* __restrict__ cells,
                                                       const uint32_t* __restrict__ cstart,
                                                       const float4* __restrict__ cpos, float rlist2, int cap,
                                                       uint32_t* __restrict__ head, uint32_t* __restrict__ nn,
-                                                      uint32_t* __restrict__ nl, uint16_t* __restrict__ nl16,
-                                                      int* __restrict__ overflow) {
+                                                      uint32_t* __restrict__ nl, int* __restrict__ overflow) {
     __shared__ float4 cand[NL_STAGE];
     __shared__ CellNbhd nb;
     const uint32_t cidx = blockIdx.x;
@@ -168,65 +140,54 @@ __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ ce
     const int si = cell_sys[cidx];
     const SysDev& S = sys[si];
     const CellDev& C = cells[si];
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid < 32) cell_nbhd_warp((int)cidx - C.c_off, C, S, cstart, nb);
     __syncthreads();
     const bool minimg = nb.minimg != 0;
     const uint32_t total = nb.off[27];
+    // staged value: the candidate's particle index (HOOMD rows, as the
+    // cell-sorted positions carry it) or its slot (pair list)
     auto stage = [&](uint32_t base) {
         const uint32_t top = min(total, base + (uint32_t)NL_STAGE);
         for (int s = 0; s < 27; ++s) {
             const uint32_t lo = max(nb.off[s], base), hi = min(nb.off[s + 1], top);
             for (uint32_t g = lo + tid; g < hi; g += NL_THREADS) {
-                float4 p = cpos[nb.src[s] + (g - nb.off[s])];
+                const uint32_t slot = nb.src[s] + (g - nb.off[s]);
+                float4 p = cpos[slot];
                 p.x += nb.shift[s][0];
                 p.y += nb.shift[s][1];
                 p.z += nb.shift[s][2];
+                if (SORTED) p.w = __int_as_float((int)slot);
                 cand[g - base] = p;
             }
         }
     };
-    const bool one_stage = total <= (uint32_t)NL_STAGE;
-    if (one_stage) {
-        stage(0);
-        __syncthreads();
-    }
-    if (STAGED && total > 65534u && tid == 0) atomicOr(overflow, 2);  // staged indices must fit 16 bits
-    for (uint32_t p0 = c0; p0 < c1; p0 += NL_THREADS) {
-        const uint32_t slot = p0 + tid;
-        const bool active = slot < c1;
-        const float4 pi = active ? cpos[slot] : make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, __int_as_float(-1));
-        const int i = __float_as_int(pi.w);
-        const long long hrow = STAGED ? (long long)slot * cap : (long long)C.nl_off + (long long)(i - S.p_off) * cap;
-        uint32_t* row = nl + (active && !STAGED ? hrow : 0);
-        uint16_t* row16 = nl16 + (active && STAGED ? hrow : 0);
-        uint32_t cnt = 0;
-        for (uint32_t base = 0; base < total; base += NL_STAGE) {
-            if (!one_stage) {
-                __syncthreads();
-                stage(base);
-                __syncthreads();
-            }
-            const int n = (int)min((uint32_t)NL_STAGE, total - base);
-            if (STAGED)
-                cnt = minimg ? nl_scan_staged<true>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row16, cnt, base)
-                             : nl_scan_staged<false>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row16, cnt, base);
-            else
-                cnt = minimg ? nl_scan<true>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row, cnt)
-                             : nl_scan<false>(cand, n, pi, i, S, rlist2, (uint32_t)cap, row, cnt);
-        }
-        if (active) {
-            if (STAGED) {
-                nn[slot] = cnt;
-                // pad to whole groups of 8 with the sentinel
-                for (uint32_t k = cnt; k < ((cnt + 7u) & ~7u) && k < (uint32_t)cap; ++k) row16[k] = (uint16_t)total;
-            } else {
-                head[i] = (uint32_t)hrow;
-                nn[i] = cnt;
-            }
-            if (cnt > (uint32_t)cap) {
-                atomicOr(overflow, 1);
-                if (STAGED) atomicMax(overflow + 1, (int)cnt);
+    const uint32_t nwin = (total + NL_STAGE - 1) / NL_STAGE;
+    const uint32_t np = c1 - c0;
+    for (uint32_t w = 0; w < nwin; ++w) {
+        const uint32_t base = w * NL_STAGE;
+        if (w) __syncthreads();  // the previous window is consumed
+        stage(base);
+        __syncthreads();  // also makes the previous window's counts visible
+        const int n = (int)min((uint32_t)NL_STAGE, total - base);
+        for (uint32_t p = warp; p < np; p += NL_WARPS) {
+            const uint32_t slot = c0 + p;
+            const float4 pi = cpos[slot];
+            const int idx = __float_as_int(pi.w);
+            const uint32_t key = SORTED ? slot : (uint32_t)idx;  // owner of the row
+            const long long hrow = C.nl_off + (long long)(key - (uint32_t)S.p_off) * cap;
+            uint32_t cnt = w ? nn[key] : 0u;
+            cnt = minimg ? nl_scan_warp<true>(cand, n, pi, SORTED ? (int)slot : idx, S, rlist2, (uint32_t)cap,
+                                              nl + hrow, cnt, S.p_off)
+                         : nl_scan_warp<false>(cand, n, pi, SORTED ? (int)slot : idx, S, rlist2, (uint32_t)cap,
+                                               nl + hrow, cnt, S.p_off);
+            if (lane == 0) {
+                nn[key] = cnt;
+                if (w == 0) head[key] = (uint32_t)hrow;
+                if (w + 1 == nwin && cnt > (uint32_t)cap) {
+                    atomicOr(overflow, 1);
+                    atomicMax(overflow + 1, (int)cnt);
+                }
             }
         }
     }
@@ -392,19 +353,19 @@ cudaError_t launch_nve64(int half, const int2* chunks, int n_chunks, const SysDe
 
 cudaError_t launch_nlist(const NlistArgs& a, cudaStream_t st) {
     if (a.n_chunks == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(a.overflow, 0, (a.nl16 ? 2 : 1) * sizeof(int), st);
+    cudaError_t e = cudaMemsetAsync(a.overflow, 0, 2 * sizeof(int), st);
     if (e != cudaSuccess) return e;
     k_cell_bin<<<a.n_chunks, 256, 0, st>>>(a.chunks, a.sys, a.cells, a.pos, a.ckey, a.ccount, a.wpos);
     if ((e = launch_scan(a.ccount, a.cstart, a.n_cells, st)) != cudaSuccess) return e;
     if ((e = launch_scatter(a.chunks, a.n_chunks, a.sys, a.ckey, a.cstart, a.ccount, a.perm_u, st)) != cudaSuccess)
         return e;
-    k_cell_sort<<<a.n_cells, 256, 0, st>>>(a.cstart, a.perm_u, a.wpos, a.cpos, a.slot2idx);
-    if (a.nl16)
+    k_cell_sort<<<a.n_cells, 256, 0, st>>>(a.cstart, a.perm_u, a.wpos, a.cpos, a.slot2idx, a.idx2slot);
+    if (a.sorted)
         k_nlist<true><<<a.n_cells, NL_THREADS, 0, st>>>(a.cell_sys, a.sys, a.cells, a.cstart, a.cpos, a.rlist2,
-                                                        a.cap, nullptr, a.nn, nullptr, a.nl16, a.overflow);
+                                                        a.cap, a.head, a.nn, a.nl, a.overflow);
     else
         k_nlist<false><<<a.n_cells, NL_THREADS, 0, st>>>(a.cell_sys, a.sys, a.cells, a.cstart, a.cpos, a.rlist2,
-                                                         a.cap, a.head, a.nn, a.nl, nullptr, a.overflow);
+                                                         a.cap, a.head, a.nn, a.nl, a.overflow);
     return cudaGetLastError();
 }
 

@@ -36,7 +36,11 @@ struct NlistArgs {
     uint32_t* nl = nullptr;
     int* overflow = nullptr;
     uint32_t* slot2idx = nullptr;  // cell-sorted slot -> particle (written by the cell sort)
-    uint16_t* nl16 = nullptr;      // non-null: build the cell-staged pair list instead of HOOMD rows
+    uint32_t* idx2slot = nullptr;  // particle -> cell-sorted slot (may be NULL)
+    // true: the library's pair list -- rows, head and counts indexed by the
+    // cell-sorted slot, entries local slots; false: HOOMD-layout rows
+    // (indexed by particle, entries local particle indices)
+    bool sorted = false;
 };
 
 cudaError_t launch_nlist(const NlistArgs& a, cudaStream_t st);

@@ -1,6 +1,4 @@
-// Pair arithmetic of the short-range term, shared by the HOOMD-list pair
-// kernel (esp_kernels.cu) and the cell-staged pair kernel (esp_pairlist.cu):
-// per pair
+// Pair arithmetic of the short-range term (k_pair, esp_kernels.cu): per pair
 //   pair_eng   = qiqj/(4 pi) (1/r - Q(u)/r_c),  u = r^2/r_c^2
 //   force_divr = qiqj/(4 pi) (1/r^3 + 2 Q'(u)/r_c^3)
 // (the split form of EvaluatorPairPSWF::evalForceAndEnergy,

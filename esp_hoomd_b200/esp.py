@@ -122,6 +122,7 @@ class NeighborList:
                                torch.zeros(N, dtype=torch.int32, device=dev),
                                torch.zeros(N * self.capacity, dtype=torch.int32, device=dev))
             batch.build_nlist(st.pos4, self.r_cut + self.buffer, self.capacity, *self._lists)
+            batch.nlist_check()  # a row past the capacity raises here, as HOOMD's list would
             self._ref_pos = st.pos4[:, :3].clone()
             self.builds += 1
             self._bind(sim)

@@ -182,13 +182,24 @@ class Batch:
               "esp_batch_compute")
 
     def build_nlist(self, pos4, rlist: float, cap: int, head, nn, nl, stream=None) -> None:
+        """HOOMD-layout neighbour rows into the caller's arrays. Does not
+        synchronise: a row overflow is reported by nlist_check and by the
+        next compute / md_run over these rows."""
         check(self._lib.esp_batch_build_nlist(self._h, _stream(stream), _ptr(pos4), float(rlist), int(cap),
                                               _ptr(head), _ptr(nn), _ptr(nl)), "esp_batch_build_nlist")
 
+    def nlist_check(self) -> int:
+        """Waits for the last build_nlist; raises EspError (ESP_ERR_OVERFLOW)
+        if a row exceeded its capacity (then n_neigh holds the needed counts);
+        returns 0."""
+        need = ctypes.c_int(0)
+        check(self._lib.esp_batch_nlist_check(self._h, ctypes.byref(need)), "esp_batch_nlist_check")
+        return int(need.value)
+
     def build_pairlist(self, pos4, rlist: float, cap: int = 256, stream=None) -> None:
-        """Builds the library-owned cell-staged pair list (all pairs with
-        r < rlist); compute / md_run without a neighbour list use it. Does not
-        synchronise: a row overflow is reported by a later call."""
+        """Builds the library-owned pair list (all pairs with r < rlist, rows
+        in cell order); compute / md_run without a neighbour list use it.
+        Does not synchronise: a row overflow is reported by a later call."""
         check(self._lib.esp_batch_build_pairlist(self._h, _stream(stream), _ptr(pos4), float(rlist), int(cap)),
               "esp_batch_build_pairlist")
 
@@ -201,8 +212,7 @@ class Batch:
 
     def pairlist_check(self) -> int:
         """Waits for the last pair-list build; raises EspError (ESP_ERR_OVERFLOW)
-        if a row exceeded its capacity. Returns the largest row length seen
-        in an overflowing build (0 otherwise)."""
+        if a row exceeded its capacity; returns 0."""
         need = ctypes.c_int(0)
         check(self._lib.esp_batch_pairlist_check(self._h, ctypes.byref(need)), "esp_batch_pairlist_check")
         return int(need.value)

@@ -218,10 +218,12 @@ class NeighborList {
         }
         for (;;) {
             if (m_nl.size() < (size_t)N * m_cap) m_nl.allocate((size_t)N * m_cap);
-            const int rc = esp_batch_build_nlist(m_batch, nullptr, &pdata->getPositions()->x, m_r_cut + m_r_buff,
-                                                 m_cap, m_head.get(), m_nn.get(), m_nl.get());
+            int rc = esp_batch_build_nlist(m_batch, nullptr, &pdata->getPositions()->x, m_r_cut + m_r_buff, m_cap,
+                                           m_head.get(), m_nn.get(), m_nl.get());
+            int need = 0;
+            if (rc == ESP_OK) rc = esp_batch_nlist_check(m_batch, &need);  // waits for the build
             if (rc == ESP_ERR_OVERFLOW && m_cap < 65536) {
-                m_cap *= 2;  // HOOMD grows its list the same way
+                while (m_cap < need && m_cap < 65536) m_cap *= 2;  // HOOMD grows its list the same way
                 continue;
             }
             esp_check(rc, "neighbour-list build");

@@ -253,27 +253,34 @@ int esp_pswf_eval_pairs(void* stream, int n, const double* rsq, const double* qi
 /* ---------------------------------------------------------------- MD harness
  * The pieces HOOMD would supply (neighbour list, NVE integrator), for
  * standalone runs and benchmarks. Neighbour list: cell list from the
- * particle positions, full list of all pairs with r < rlist, fixed row
- * capacity `cap` (head[i] = offset of system s + local i * cap); returns
- * ESP_ERR_OVERFLOW when a row exceeds cap (n_neigh then holds the true
- * counts). Synchronises `stream` to read the overflow flag. */
+ * particle positions, full list of all pairs with r < rlist (rlist at most
+ * half the smallest box edge), fixed row capacity `cap` (head[i] = offset of
+ * system s + local i * cap; totN * cap below 2^32). Does not synchronise: a
+ * row longer than cap keeps its first cap entries, n_neigh holds the true
+ * counts, and the overflow is reported (ESP_ERR_OVERFLOW) by
+ * esp_batch_nlist_check, which waits for the build and writes the longest
+ * row of an overflowing build to *needed_cap (0 when no row overflowed; may
+ * be NULL), and by the first esp_batch_compute /
+ * esp_batch_md_run over these rows that finds the build finished. Results
+ * computed over an overflowed list are invalid; rebuild with a larger cap. */
 int esp_batch_build_nlist(esp_batch* b, void* stream, const float* pos4, double rlist, int cap, unsigned* head,
                           unsigned* n_neigh, unsigned* nlist);
+int esp_batch_nlist_check(esp_batch* b, int* needed_cap);
 
-/* Cell-staged pair list owned by the library: the short-range term's
- * neighbour list when the library builds it (the reference takes HOOMD's
- * NeighborList, src/module.cc:73-79; this replaces that list for standalone
- * and batched runs). Lists all pairs with r < rlist of pos4 (rlist at most
- * half the smallest box edge) on a cell grid of edge >= rlist; rows are kept
- * in cell order with 16-bit indices into each cell's neighbourhood.
- * esp_batch_compute and esp_batch_md_run called with head = n_neigh = nlist
- * = NULL run the short-range term over the last list built. `cap` is the row
- * capacity: a multiple of 8, at most 1024. Does not synchronise: a row longer
- * than cap is detected on the device and reported (ESP_ERR_OVERFLOW) by the
- * first esp_batch_compute / esp_batch_md_run that finds the build finished,
- * and by esp_batch_pairlist_check, which waits for the build and writes the
- * longest row to *needed_cap (may be NULL). Results computed over an
- * overflowed list are invalid; rebuild with a larger cap. */
+/* Pair list owned by the library: the short-range term's neighbour list
+ * when the library builds it (the reference takes HOOMD's NeighborList,
+ * src/module.cc:73-79; this replaces that list for standalone and batched
+ * runs). Lists all pairs with r < rlist of pos4 (rlist at most half the
+ * smallest box edge) on a cell grid of edge >= rlist, in cell order: rows
+ * indexed by the build's cell-sorted slot, entries slots, so that a row's
+ * neighbours are neighbours in memory (each evaluation's bin stage writes
+ * the slot-ordered positions they are read from). esp_batch_compute and
+ * esp_batch_md_run called with head = n_neigh = nlist = NULL run the
+ * short-range term over the last list built. `cap` is the row capacity
+ * (totN * cap below 2^32). Does not synchronise: overflow is reported as for
+ * esp_batch_build_nlist, by esp_batch_pairlist_check and by the first
+ * esp_batch_compute / esp_batch_md_run over the list that finds the build
+ * finished. */
 int esp_batch_build_pairlist(esp_batch* b, void* stream, const float* pos4, double rlist, int cap);
 int esp_batch_pairlist_check(esp_batch* b, int* needed_cap);
 

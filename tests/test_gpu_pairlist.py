@@ -1,17 +1,18 @@
-"""The library's cell-staged pair list (esp_batch_build_pairlist) against the
-HOOMD-layout neighbour list path, which is pinned to the oracle
+"""The library's pair list (esp_batch_build_pairlist: rows in cell order,
+entries cell-sorted slots, read from the slot-ordered positions) against
+the HOOMD-layout neighbour list path, which is pinned to the oracle
 (test_gpu_parity.py): same forces, energies and virials up to summation
 order (relative RMS <= 1e-6, energy and virial <= 1e-6 relative,
 per-particle energies <= 5e-6 of the largest).
 
 Cases:
 * a batch mixing cell grids of 2, 3 and >= 4 cells per axis (minimum image
-  per pair vs staged nearest images), positions given in other periodic
-  images than the box;
+  in the builder vs staged periodic images), positions given in other
+  periodic images than the box;
 * MD: 10 velocity-Verlet steps from the same state over both lists (the
   pair list is built once, particles cross the box faces);
-* a clustered system whose dense cells hold more particles than the staging
-  capacity (staged in windows);
+* a clustered system whose dense cells' neighbourhoods exceed the builder's
+  shared-memory stage (scanned in windows);
 * a row capacity too small: ESP_ERR_OVERFLOW from the check and from the
   next evaluation, with the longest row reported.
 """
@@ -146,10 +147,12 @@ def test_pairlist_overflow_is_reported():
     with pytest.raises(EspError) as ei:
         b.compute(pos, q, f, None, None, nlist=None, flags=ESP_SHORT_RANGE)
     assert ei.value.code == -5
-    # the longest row, and a rebuild with room for it clears the error
+    # the longest row is reported, and a rebuild with room for it clears the error
     counts = R.neighbor_list(s.pos.astype(np.float32).astype(np.float64), s.box, 3.4)[1]
+    b.build_pairlist(pos, 3.4, 64)
+    with pytest.raises(EspError):
+        b.pairlist_check()
+    assert counts.max() > 64
     b.build_pairlist(pos, 3.4, 256)
     assert b.pairlist_check() == 0
-    with pytest.raises(EspError):
-        b.build_pairlist(pos, 3.4, 60)  # not a multiple of 8
-    assert counts.max() > 64
+    b.compute(pos, q, f, None, None, nlist=None, flags=ESP_SHORT_RANGE)

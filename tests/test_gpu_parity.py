@@ -430,8 +430,10 @@ def test_empty_system_in_batch():
 
 
 def test_nlist_row_overflow_is_reported():
-    """Rows longer than the capacity fail with ESP_ERR_OVERFLOW; n_neigh then
-    holds the counts the caller needs, and rows keep their first cap entries."""
+    """Rows longer than the capacity are reported with ESP_ERR_OVERFLOW (the
+    build does not synchronise: nlist_check waits for it, and the next
+    evaluation over those rows fails); n_neigh then holds the counts the
+    caller needs, and rows keep their first cap entries."""
     s = systems.rocksalt(12, seed=973)
     b = native.Batch(native.make_params(), [s.N], [s.box])
     p4 = np.zeros((s.N, 4), np.float32)
@@ -441,8 +443,14 @@ def test_nlist_row_overflow_is_reported():
     head = torch.zeros(s.N, dtype=torch.int32, device="cuda")
     nn = torch.zeros_like(head)
     nl = torch.zeros(s.N * cap, dtype=torch.int32, device="cuda")
+    b.build_nlist(pos, 3.4, cap, head, nn, nl)
     with pytest.raises(EspError) as ei:
-        b.build_nlist(pos, 3.4, cap, head, nn, nl)
+        b.nlist_check()
+    assert ei.value.code == -5
+    q = torch.tensor(s.q.astype(np.float32), device="cuda")
+    f = torch.zeros((s.N, 4), device="cuda")
+    with pytest.raises(EspError) as ei:
+        b.compute(pos, q, f, None, None, nlist=(head, nn, nl))
     assert ei.value.code == -5
     rh, rc, rl = R.neighbor_list(s.pos.astype(np.float32).astype(np.float64), s.box, 3.4)
     c = nn.cpu().numpy()
