@@ -489,8 +489,8 @@ def run_ours(args):
 
     def request(bb, p, v, use_graph=True, qq=q, e=energy):
         # the first evaluation reports energy and virial; the NVE steps need
-        # forces and energies only. Default: HOOMD-layout rows built by the
-        # harness; --pair-list: the library's pair list
+        # forces and energies only. Default: the library's pair list (rows in
+        # cell order); --hoomd-list: HOOMD-layout rows built by the harness
         if args.hoomd_list:
             bb.build_nlist(p, RCUT + SKIN, CAP, head, nn, nl)
             nlist = (head, nn, nl)
@@ -740,9 +740,9 @@ def main():
                     help="scaleup: the plain path on one 10^6-particle system (a second measurement)")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default plan)")
-    ap.add_argument("--pair-list", dest="hoomd_list", action="store_false",
-                    help="short-range term over the library's pair list (rows in cell order) instead of HOOMD-layout "
-                         "neighbour rows (the default)")
+    ap.add_argument("--hoomd-list", action="store_true",
+                    help="short-range term over HOOMD-layout neighbour rows built by the harness instead of the "
+                         "library's pair list (rows in cell order, the default)")
     ap.add_argument("--serve-requests", type=int, default=10000, help="requests per arrival rate")
     ap.add_argument("--serve-rates", type=lambda v: [float(x) for x in v.split(",")], default=[200.0, 800.0, 0.0],
                     help="comma-separated arrival rates (requests/s); 0 = all requests at once (saturation)")

@@ -574,37 +574,51 @@ __global__ void __launch_bounds__(256, 3)
         if (base + SPREAD_CHM < np) prefetch(base + SPREAD_CHM, cb ^ 1);
         else asm volatile("cp.async.commit_group;\n" ::);
         asm volatile("cp.async.wait_group 1;\n" ::);  // this chunk's records have landed
-        for (int k = tid; k < ncp * SPREAD_MS / 4; k += blockDim.x) {
-            const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-            reinterpret_cast<float4*>(wxs)[k] = z;
-            reinterpret_cast<float4*>(wys)[k] = z;
-            reinterpret_cast<float4*>(wzh)[k] = z;
-            reinterpret_cast<float4*>(wzl)[k] = z;
-        }
-        __syncthreads();
+        __syncthreads();  // (every thread's copies)
         {
-            // thread (a, j0) evaluates window segment a for items j0, j0 + nla, ...
+            // thread (a, p0) evaluates window segment a on all three axes of
+            // particles p0, p0 + nla, ... and writes both the stencil point o + a
+            // and the zero points (o + a + P), (o + a + 2P), ... mod 16 of each
+            // 16-point row, so every row is written whole (padding particles
+            // get zero rows)
             constexpr int DD = default_window_degree<P>();
-            const int nla = blockDim.x / P, a = tid % P, j0 = tid / P;
-            if (j0 < nla) {
+            const int nla = blockDim.x / P, a = tid % P, p0 = tid / P;
+            if (p0 < nla) {
                 SegPoly<DD> sp;
                 if (D == DD) sp.load(&wc[a * (D + 1)]);
-                for (int j = j0; j < nc * 3; j += nla) {
-                    const int p = j / 3, ax = j - 3 * p;
-                    const float4 rec = crec[cb * SPREAD_CHM + p];
-                    const int o = (int)((crel[cb * SPREAD_CHM + p] >> (8 * ax)) & 255u);
-                    const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
-                    const float w = D == DD ? sp.w(tt) : horner_w(&wc[a * (D + 1)], D, tt);
-                    const int k = p * SPREAD_MS + o + a;
-                    if (ax == 0) {
-                        wxs[k] = w * rec.w;
-                    } else if (ax == 1) {
-                        wys[k] = w;
-                    } else {
+                for (int p = p0; p < ncp; p += nla) {
+                    float* rx = wxs + p * SPREAD_MS;
+                    float* ry = wys + p * SPREAD_MS;
+                    uint32_t* rzh = wzh + p * SPREAD_MS;
+                    uint32_t* rzl = wzl + p * SPREAD_MS;
+                    if (p < nc) {
+                        const float4 rec = crec[cb * SPREAD_CHM + p];
+                        const uint32_t rl = crel[cb * SPREAD_CHM + p];
+                        const int ox = (int)(rl & 255u), oy = (int)((rl >> 8) & 255u), oz = (int)((rl >> 16) & 255u);
+                        const float w0 = D == DD ? sp.w(rec.x) : horner_w(&wc[a * (D + 1)], D, rec.x);
+                        const float w1 = D == DD ? sp.w(rec.y) : horner_w(&wc[a * (D + 1)], D, rec.y);
+                        const float w2 = D == DD ? sp.w(rec.z) : horner_w(&wc[a * (D + 1)], D, rec.z);
                         uint32_t h, l;
-                        split_tf32(w, h, l);
-                        wzh[k] = h;
-                        wzl[k] = l;
+                        split_tf32(w2, h, l);
+                        rx[ox + a] = w0 * rec.w;
+                        ry[oy + a] = w1;
+                        rzh[oz + a] = h;
+                        rzl[oz + a] = l;
+#pragma unroll
+                        for (int z = P + a; z < 16; z += P) {
+                            rx[(ox + z) & 15] = 0.f;
+                            ry[(oy + z) & 15] = 0.f;
+                            rzh[(oz + z) & 15] = 0u;
+                            rzl[(oz + z) & 15] = 0u;
+                        }
+                    } else {
+#pragma unroll
+                        for (int z = a; z < 16; z += P) {
+                            rx[z] = 0.f;
+                            ry[z] = 0.f;
+                            rzh[z] = 0u;
+                            rzl[z] = 0u;
+                        }
                     }
                 }
             }
@@ -1391,26 +1405,27 @@ __global__ void __launch_bounds__(128)
         __syncthreads();  // region / coefficients / records staged; previous chunk consumed
         if (base + C::CH < np) prefetch(base + C::CH, cb ^ 1);
         {
-            // thread (a, j0) evaluates window segment a (value and derivative)
+            // thread (a, p0) evaluates window segment a (value and derivative)
+            // on all three axes of particles p0, p0 + nla, ...
             constexpr int DD = default_window_degree<P>();
-            const int nla = blockDim.x / P, a2 = threadIdx.x % P, j0 = threadIdx.x / P;
-            if (j0 < nla) {
+            const int nla = blockDim.x / P, a2 = threadIdx.x % P, p0 = threadIdx.x / P;
+            if (p0 < nla) {
                 SegPoly<DD> sp;
                 if (D == DD) sp.load(&wc[a2 * (D + 1)]);
-                for (int j = j0; j < nc * 3; j += nla) {
-                    const int p = j / 3, ax = j - 3 * p;
+                for (int p = p0; p < nc; p += nla) {
                     const float4 rec = crec[cb * C::CH + p];
-                    const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
-                    float w, dw;
-                    if (D == DD) {
-                        w = sp.w(tt);
-                        dw = sp.dw(tt);
-                    } else {
-                        w = horner_w(&wc[a2 * (D + 1)], D, tt);
-                        dw = horner_dw(&wc[a2 * (D + 1)], D, tt);
+                    float* W = wts + p * WS + a2;
+#pragma unroll
+                    for (int ax = 0; ax < 3; ++ax) {
+                        const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
+                        if (D == DD) {
+                            W[ax * 2 * P] = sp.w(tt);
+                            W[ax * 2 * P + P] = sp.dw(tt);
+                        } else {
+                            W[ax * 2 * P] = horner_w(&wc[a2 * (D + 1)], D, tt);
+                            W[ax * 2 * P + P] = horner_dw(&wc[a2 * (D + 1)], D, tt);
+                        }
                     }
-                    wts[p * WS + ax * 2 * P + a2] = w;
-                    wts[p * WS + ax * 2 * P + P + a2] = dw;
                 }
             }
             for (int p = threadIdx.x; p < nc; p += blockDim.x) {

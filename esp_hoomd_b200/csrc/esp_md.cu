@@ -75,46 +75,48 @@ __global__ void k_cell_sort(const uint32_t* __restrict__ start, const uint32_t* 
     }
 }
 
-// One CTA per cell. The particles of the 27 surrounding cells are staged in
+// One CTA per cell, one thread per particle of the cell (passes of
+// NL_THREADS). The particles of the 27 surrounding cells are staged in
 // shared memory, in the fixed (dz, dy, dx) order and ascending slot inside
 // each cell (in windows of NL_STAGE when there are more), so every row is
-// deterministic. One warp per particle of the cell: lane k tests candidate
-// base + k and the hits are appended in candidate order (ballot and prefix
-// count), up to 32 consecutive entries per store. With at least 3 cells on
-// every axis each surrounding cell is a distinct periodic image and its
-// particles are staged already shifted by that image, so the test needs no
-// wrap; smaller cell grids take the minimum-image test.
-constexpr int NL_WARPS = 4;
-constexpr int NL_THREADS = 32 * NL_WARPS;
+// deterministic; each thread scans them with broadcast shared loads (one
+// wavefront serves the whole warp). With at least 3 cells on every axis each
+// surrounding cell is a distinct periodic image and its particles are staged
+// already shifted by that image, so the test needs no wrap; smaller cell
+// grids take the minimum-image test.
+constexpr int NL_THREADS = 64;
 constexpr int NL_STAGE = 1024;
 
-// Appends the staged candidates within rlist of pi (other than `self`) to
-// row, entries w - base_id with w the candidate's staged value; returns the
-// new count (entries past cap are counted, not stored).
+// store v at p when ok, as one predicated store (the candidate loop has no
+// per-candidate branch)
+__device__ __forceinline__ void store_if(bool ok, uint32_t* p, uint32_t v) {
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q st.global.u32 [%0], %1;\n\t}" ::"l"(p), "r"(v),
+        "r"((uint32_t)ok)
+        : "memory");
+}
+
+// Appends the staged candidates within rlist of pi, other than `self`, to
+// row as w - base_id (w: the candidate's staged value); threads without a
+// particle carry a NaN position, which tests false against everything.
+// Entries past cap are counted, not stored.
 template <bool MINIMG>
-__device__ __forceinline__ uint32_t nl_scan_warp(const float4* __restrict__ cand, int n, float4 pi, int self,
-                                                 const SysDev& S, float rlist2, uint32_t cap,
-                                                 uint32_t* __restrict__ row, uint32_t cnt, int base_id) {
-    const unsigned lt = (1u << (threadIdx.x & 31)) - 1u;
-    for (int k0 = 0; k0 < n; k0 += 32) {
-        const int k = k0 + (int)(threadIdx.x & 31);
-        bool hit = false;
-        int w = 0;
-        if (k < n) {
-            const float4 pj = cand[k];
-            float ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
-            if (MINIMG) {
-                ddx -= S.Lx * rintf(ddx * S.inv_Lx);
-                ddy -= S.Ly * rintf(ddy * S.inv_Ly);
-                ddz -= S.Lz * rintf(ddz * S.inv_Lz);
-            }
-            w = __float_as_int(pj.w);
-            hit = ddx * ddx + ddy * ddy + ddz * ddz < rlist2 && w != self;
+__device__ __forceinline__ uint32_t nl_scan(const float4* __restrict__ cand, int n, float4 pi, int self,
+                                            const SysDev& S, float rlist2, uint32_t cap, uint32_t* __restrict__ row,
+                                            uint32_t cnt, int base_id) {
+#pragma unroll 4
+    for (int k = 0; k < n; ++k) {
+        const float4 pj = cand[k];
+        float ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
+        if (MINIMG) {
+            ddx -= S.Lx * rintf(ddx * S.inv_Lx);
+            ddy -= S.Ly * rintf(ddy * S.inv_Ly);
+            ddz -= S.Lz * rintf(ddz * S.inv_Lz);
         }
-        const unsigned m = __ballot_sync(0xffffffffu, hit);
-        const uint32_t at = cnt + (uint32_t)__popc(m & lt);
-        if (hit && at < cap) row[at] = (uint32_t)(w - base_id);
-        cnt += (uint32_t)__popc(m);
+        const int w = __float_as_int(pj.w);
+        const bool hit = ddx * ddx + ddy * ddy + ddz * ddz < rlist2 && w != self;
+        store_if(hit && cnt < cap, row + cnt, (uint32_t)(w - base_id));
+        cnt += hit ? 1u : 0u;
     }
     return cnt;
 }
@@ -140,12 +142,12 @@ __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ ce
     const int si = cell_sys[cidx];
     const SysDev& S = sys[si];
     const CellDev& C = cells[si];
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tid = threadIdx.x;
     if (tid < 32) cell_nbhd_warp((int)cidx - C.c_off, C, S, cstart, nb);
     __syncthreads();
     const bool minimg = nb.minimg != 0;
     const uint32_t total = nb.off[27];
-    // staged value: the candidate's particle index (HOOMD rows, as the
+    // staged value: the candidate's particle index (HOOMD rows; the
     // cell-sorted positions carry it) or its slot (pair list)
     auto stage = [&](uint32_t base) {
         const uint32_t top = min(total, base + (uint32_t)NL_STAGE);
@@ -162,32 +164,37 @@ __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ ce
             }
         }
     };
-    const uint32_t nwin = (total + NL_STAGE - 1) / NL_STAGE;
-    const uint32_t np = c1 - c0;
-    for (uint32_t w = 0; w < nwin; ++w) {
-        const uint32_t base = w * NL_STAGE;
-        if (w) __syncthreads();  // the previous window is consumed
-        stage(base);
-        __syncthreads();  // also makes the previous window's counts visible
-        const int n = (int)min((uint32_t)NL_STAGE, total - base);
-        for (uint32_t p = warp; p < np; p += NL_WARPS) {
-            const uint32_t slot = c0 + p;
-            const float4 pi = cpos[slot];
-            const int idx = __float_as_int(pi.w);
-            const uint32_t key = SORTED ? slot : (uint32_t)idx;  // owner of the row
-            const long long hrow = C.nl_off + (long long)(key - (uint32_t)S.p_off) * cap;
-            uint32_t cnt = w ? nn[key] : 0u;
-            cnt = minimg ? nl_scan_warp<true>(cand, n, pi, SORTED ? (int)slot : idx, S, rlist2, (uint32_t)cap,
-                                              nl + hrow, cnt, S.p_off)
-                         : nl_scan_warp<false>(cand, n, pi, SORTED ? (int)slot : idx, S, rlist2, (uint32_t)cap,
-                                               nl + hrow, cnt, S.p_off);
-            if (lane == 0) {
-                nn[key] = cnt;
-                if (w == 0) head[key] = (uint32_t)hrow;
-                if (w + 1 == nwin && cnt > (uint32_t)cap) {
-                    atomicOr(overflow, 1);
-                    atomicMax(overflow + 1, (int)cnt);
-                }
+    const bool one_stage = total <= (uint32_t)NL_STAGE;
+    if (one_stage) {
+        stage(0);
+        __syncthreads();
+    }
+    for (uint32_t p0 = c0; p0 < c1; p0 += NL_THREADS) {
+        const uint32_t slot = p0 + tid;
+        const bool active = slot < c1;
+        const float4 pi = active ? cpos[slot] : make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, __int_as_float(-1));
+        const int idx = __float_as_int(pi.w);
+        const int self = SORTED ? (int)slot : idx;
+        const uint32_t key = SORTED ? slot : (uint32_t)idx;  // owner of the row
+        const long long hrow = C.nl_off + (long long)((int)key - S.p_off) * cap;
+        uint32_t* row = nl + (active ? hrow : 0);
+        uint32_t cnt = 0;
+        for (uint32_t base = 0; base < total; base += NL_STAGE) {
+            if (!one_stage) {
+                __syncthreads();
+                stage(base);
+                __syncthreads();
+            }
+            const int n = (int)min((uint32_t)NL_STAGE, total - base);
+            cnt = minimg ? nl_scan<true>(cand, n, pi, self, S, rlist2, (uint32_t)cap, row, cnt, S.p_off)
+                         : nl_scan<false>(cand, n, pi, self, S, rlist2, (uint32_t)cap, row, cnt, S.p_off);
+        }
+        if (active) {
+            head[key] = (uint32_t)hrow;
+            nn[key] = cnt;
+            if (cnt > (uint32_t)cap) {
+                atomicOr(overflow, 1);
+                atomicMax(overflow + 1, (int)cnt);
             }
         }
     }
