@@ -279,7 +279,7 @@ struct esp_batch {
     // (one per system, NULL when unavailable), the box, the kernels' error word
     CUtensorMap* d_tmaps = nullptr;
     int tma_bx = 0, tma_by = 0;
-    int* d_kerr = nullptr;
+    int* d_kerr = nullptr;  // [kernel error word, tile-queue counter]
     // cell grids of the neighbour-list builds (allocated on first use): one
     // for HOOMD-layout lists, one for the library's pair list (whose rows
     // are indexed by the slots of its own build)
@@ -663,9 +663,9 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         (rc = mem.get(d_x, xi.size())) || (rc = mem.get(d_y, yi.size())) || (rc = mem.get(d_z, zi.size())) ||
         (rc = mem.get(d_p, pi.size())) || (rc = mem.get(d_s, si.size())) ||
         (rc = mem.get(d_acc, (size_t)ns * ACC_STRIDE)) || (rc = mem.get(d_energy, ns)) ||
-        (rc = mem.get(d_virial, (size_t)ns * 6)) || (rc = mem.get(d_fsr, totN)) || (rc = mem.get(d_kerr, 1)))
+        (rc = mem.get(d_virial, (size_t)ns * 6)) || (rc = mem.get(d_fsr, totN)) || (rc = mem.get(d_kerr, 2)))
         return rc;
-    ESPB_CK(cudaMemset(d_kerr, 0, sizeof(int)));
+    ESPB_CK(cudaMemset(d_kerr, 0, 2 * sizeof(int)));
     // tensor maps for the TMA-staged interpolation (supports 5..8; the
     // cp.async form otherwise or when any map cannot be encoded)
     d_tmaps = nullptr;
@@ -898,6 +898,7 @@ LaunchArgs esp_batch::args() const {
     a.tma_bx = tma_bx;
     a.tma_by = tma_by;
     a.kerr = d_kerr;
+    a.queue = d_kerr + 1;  // the persistent interpolation kernel's tile counter
     a.nmax_x = a.nmax_y = a.nmax_z = 1;
     for (const SysDev& S : sd) {
         a.nmax_x = std::max(a.nmax_x, S.nx);

@@ -1289,8 +1289,141 @@ __device__ __forceinline__ bool tma_wait(uint32_t mbar, uint32_t phase) {
     return false;
 }
 
+// One chunk of a tile's particles (records already in shared memory):
+// window weights and derivatives, the processing order, and the contraction
+// of each particle's stencil with the staged potential region; writes the
+// particles' forces and energies and returns the chunk's energy (FP64).
+// Called by every thread of the CTA (it synchronises).
 template <int P, bool TMA>
-__global__ void __launch_bounds__(128)
+__device__ __forceinline__ double interp_chunk(const float* __restrict__ sm, int PX, int PP, int xoff, int D,
+                                               const float* __restrict__ wc, const float4* __restrict__ crec,
+                                               const uint32_t* __restrict__ crel, const uint32_t* __restrict__ cprm,
+                                               float* __restrict__ wts, float* __restrict__ qv, int* __restrict__ org,
+                                               int* __restrict__ order, int nc, float gxs, float gys, float gzs,
+                                               double self_coef, float4* __restrict__ force) {
+    using C = InterpCfg<P>;
+    constexpr int WS = 6 * P + 1;  // weight row stride (odd: conflict-free broadcasts)
+    constexpr int K = 32 / C::G;   // particle groups per warp
+    const int grp = threadIdx.x / C::G, gl = threadIdx.x % C::G;
+    double esum = 0.0;
+    {
+        // thread (a, p0) evaluates window segment a (value and derivative)
+        // on all three axes of particles p0, p0 + nla, ...
+        constexpr int DD = default_window_degree<P>();
+        const int nla = blockDim.x / P, a2 = threadIdx.x % P, p0 = threadIdx.x / P;
+        if (p0 < nla) {
+            SegPoly<DD> sp;
+            if (D == DD) sp.load(&wc[a2 * (D + 1)]);
+            for (int p = p0; p < nc; p += nla) {
+                const float4 rec = crec[p];
+                float* W = wts + p * WS + a2;
+#pragma unroll
+                for (int ax = 0; ax < 3; ++ax) {
+                    const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
+                    if (D == DD) {
+                        W[ax * 2 * P] = sp.w(tt);
+                        W[ax * 2 * P + P] = sp.dw(tt);
+                    } else {
+                        W[ax * 2 * P] = horner_w(&wc[a2 * (D + 1)], D, tt);
+                        W[ax * 2 * P + P] = horner_dw(&wc[a2 * (D + 1)], D, tt);
+                    }
+                }
+            }
+        }
+        for (int p = threadIdx.x; p < nc; p += blockDim.x) {
+            qv[p] = crec[p].w;
+            org[p] = (int)crel[p];
+        }
+    }
+    __syncthreads();
+    if (C::CH <= 32 && threadIdx.x < 32) {
+        // processing order: queue position q prefers a particle whose
+        // bank class (ox + oy) mod K is q mod K, so the K groups of a warp
+        // read potential rows in disjoint bank classes (plane pitch = K
+        // mod 32, row pitch = 1 mod K); particles left over fill the free
+        // positions in order
+        const int j = threadIdx.x;
+        const unsigned full = 0xffffffffu, lt = (1u << j) - 1u;
+        const bool valid = j < nc;
+        // bank class of the particle's rows: (ox + oy) mod K for the padded
+        // cp.async layout; ox + xoff mod K for the TMA box (pitches = 0 mod K)
+        const int cls = valid ? ((TMA ? (org[j] & 255) + xoff : (org[j] & 255) + ((org[j] >> 8) & 255)) & (K - 1))
+                              : -1;
+        int rank = 0, cpos = 0;
+        const int pk = j & (K - 1);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const unsigned m = __ballot_sync(full, cls == k);
+            if (cls == k) rank = __popc(m & lt);
+            if (pk == k) cpos = __popc(m);
+        }
+        const int slots = valid ? (nc - cls + K - 1) / K : 0;
+        const bool placed = valid && rank < slots;
+        const unsigned fm = __ballot_sync(full, j < nc && j / K >= cpos);
+        const unsigned lm = __ballot_sync(full, valid && !placed);
+        if (placed) order[cls + K * rank] = j;
+        else if (valid) order[__fns(fm, 0, __popc(lm & lt) + 1)] = j;
+    } else if (C::CH > 32) {
+        for (int p = threadIdx.x; p < nc; p += blockDim.x) order[p] = p;
+    }
+    __syncthreads();
+    for (int pp = 0; pp < nc; pp += C::NG) {
+        const int qq = pp + grp;
+        const int p = qq < nc ? order[qq] : qq;
+        const bool act = qq < nc && gl < P;
+        float pot = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+        if (act) {
+            const float* W = wts + p * WS;
+            float wx[P], dwx[P];
+#pragma unroll
+            for (int a2 = 0; a2 < P; ++a2) {
+                wx[a2] = W[a2];
+                dwx[a2] = W[P + a2];
+            }
+            const int rl = org[p];
+            const int ox = rl & 255, oy = (rl >> 8) & 255, oz = (rl >> 16) & 255;
+            const float* plane = sm + (oz + gl) * PP + oy * PX + ox + xoff;
+            float Sv = 0.f, Dv = 0.f, Sy = 0.f;
+#pragma unroll
+            for (int b = 0; b < P; ++b) {
+                const float* row = plane + b * PX;
+                float sr = 0.f, dr = 0.f;
+#pragma unroll
+                for (int a2 = 0; a2 < P; ++a2) {
+                    const float v = row[a2];
+                    sr = fmaf(v, wx[a2], sr);
+                    dr = fmaf(v, dwx[a2], dr);
+                }
+                const float wyb = W[2 * P + b], dwyb = W[3 * P + b];
+                Sv = fmaf(sr, wyb, Sv);
+                Dv = fmaf(dr, wyb, Dv);
+                Sy = fmaf(sr, dwyb, Sy);
+            }
+            const float wzc = W[4 * P + gl], dwzc = W[5 * P + gl];
+            pot = Sv * wzc;
+            gx = Dv * wzc;
+            gy = Sy * wzc;
+            gz = Sv * dwzc;
+        }
+#pragma unroll
+        for (int o = C::G / 2; o > 0; o >>= 1) {
+            pot += __shfl_xor_sync(0xffffffffu, pot, o, C::G);
+            gx += __shfl_xor_sync(0xffffffffu, gx, o, C::G);
+            gy += __shfl_xor_sync(0xffffffffu, gy, o, C::G);
+            gz += __shfl_xor_sync(0xffffffffu, gz, o, C::G);
+        }
+        if (qq < nc && gl == 0) {
+            const float q = qv[p];
+            const double e_i = 0.5 * (double)q * pot + self_coef * (double)q * q;
+            force[cprm[p]] = make_float4(q * gxs * gx, q * gys * gy, q * gzs * gz, (float)e_i);
+            esum += e_i;
+        }
+    }
+    return esum;
+}
+
+template <int P, bool TMA>
+__global__ void __launch_bounds__(128, 6)
     k_interp(const int* __restrict__ tile_sys, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
              int T, int D, int PX, int PP, const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
              const float4* __restrict__ srec, const uint32_t* __restrict__ srel, const float* __restrict__ phi,
@@ -1320,8 +1453,6 @@ __global__ void __launch_bounds__(128)
     int* org = reinterpret_cast<int*>(qv + C::CH); // [CH] packed origins
     int* order = org + C::CH;                      // [CH] processing order of the chunk
     float* wc = reinterpret_cast<float*>(order + C::CH);  // [P][D+1]
-    constexpr int WS = 6 * P + 1;                  // weight row stride (odd: conflict-free broadcasts)
-    constexpr int K = 32 / C::G;                   // particle groups per warp
     const int lt = t - S.t_off;
     const int X0 = (lt % S.ntx) * T, Y0 = ((lt / S.ntx) % S.nty) * T, Z0 = (lt / (S.ntx * S.nty)) * T;
     // TMA boxes start on a 16-byte boundary in x: the region sits xoff floats in
@@ -1396,7 +1527,6 @@ __global__ void __launch_bounds__(128)
     }
     for (int i = threadIdx.x; i < P * (D + 1); i += blockDim.x)
         wc[i] = ps.wcoef[(i / (D + 1)) * (MAX_D + 1) + (i % (D + 1))];
-    const int grp = threadIdx.x / C::G, gl = threadIdx.x % C::G;
     const float gxs = (float)S.gxd, gys = (float)S.gyd, gzs = (float)S.gzd;
     const double self_coef = ps.self_coef;
     double esum = 0.0;
@@ -1404,124 +1534,185 @@ __global__ void __launch_bounds__(128)
         const int nc = min(C::CH, np - base);
         __syncthreads();  // region / coefficients / records staged; previous chunk consumed
         if (base + C::CH < np) prefetch(base + C::CH, cb ^ 1);
-        {
-            // thread (a, p0) evaluates window segment a (value and derivative)
-            // on all three axes of particles p0, p0 + nla, ...
-            constexpr int DD = default_window_degree<P>();
-            const int nla = blockDim.x / P, a2 = threadIdx.x % P, p0 = threadIdx.x / P;
-            if (p0 < nla) {
-                SegPoly<DD> sp;
-                if (D == DD) sp.load(&wc[a2 * (D + 1)]);
-                for (int p = p0; p < nc; p += nla) {
-                    const float4 rec = crec[cb * C::CH + p];
-                    float* W = wts + p * WS + a2;
-#pragma unroll
-                    for (int ax = 0; ax < 3; ++ax) {
-                        const float tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
-                        if (D == DD) {
-                            W[ax * 2 * P] = sp.w(tt);
-                            W[ax * 2 * P + P] = sp.dw(tt);
-                        } else {
-                            W[ax * 2 * P] = horner_w(&wc[a2 * (D + 1)], D, tt);
-                            W[ax * 2 * P + P] = horner_dw(&wc[a2 * (D + 1)], D, tt);
-                        }
-                    }
-                }
-            }
-            for (int p = threadIdx.x; p < nc; p += blockDim.x) {
-                qv[p] = crec[cb * C::CH + p].w;
-                org[p] = (int)crel[cb * C::CH + p];
-            }
-        }
-        __syncthreads();
-        if (C::CH <= 32 && threadIdx.x < 32) {
-            // processing order: queue position q prefers a particle whose
-            // bank class (ox + oy) mod K is q mod K, so the K groups of a warp
-            // read potential rows in disjoint bank classes (plane pitch = K
-            // mod 32, row pitch = 1 mod K); particles left over fill the free
-            // positions in order
-            const int j = threadIdx.x;
-            const unsigned full = 0xffffffffu, lt = (1u << j) - 1u;
-            const bool valid = j < nc;
-            // bank class of the particle's rows: (ox + oy) mod K for the padded
-            // cp.async layout; ox + xoff mod K for the TMA box (pitches = 0 mod K)
-            const int cls = valid ? ((TMA ? (org[j] & 255) + xoff : (org[j] & 255) + ((org[j] >> 8) & 255)) & (K - 1))
-                                  : -1;
-            int rank = 0, cpos = 0;
-            const int pk = j & (K - 1);
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                const unsigned m = __ballot_sync(full, cls == k);
-                if (cls == k) rank = __popc(m & lt);
-                if (pk == k) cpos = __popc(m);
-            }
-            const int slots = valid ? (nc - cls + K - 1) / K : 0;
-            const bool placed = valid && rank < slots;
-            const unsigned fm = __ballot_sync(full, j < nc && j / K >= cpos);
-            const unsigned lm = __ballot_sync(full, valid && !placed);
-            if (placed) order[cls + K * rank] = j;
-            else if (valid) order[__fns(fm, 0, __popc(lm & lt) + 1)] = j;
-        } else if (C::CH > 32) {
-            for (int p = threadIdx.x; p < nc; p += blockDim.x) order[p] = p;
-        }
-        __syncthreads();
-        for (int pp = 0; pp < nc; pp += C::NG) {
-            const int qq = pp + grp;
-            const int p = qq < nc ? order[qq] : qq;
-            const bool act = qq < nc && gl < P;
-            float pot = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-            if (act) {
-                const float* W = wts + p * WS;
-                float wx[P], dwx[P];
-#pragma unroll
-                for (int a2 = 0; a2 < P; ++a2) {
-                    wx[a2] = W[a2];
-                    dwx[a2] = W[P + a2];
-                }
-                const int rl = org[p];
-                const int ox = rl & 255, oy = (rl >> 8) & 255, oz = (rl >> 16) & 255;
-                const float* plane = sm + (oz + gl) * PP + oy * PX + ox + xoff;
-                float Sv = 0.f, Dv = 0.f, Sy = 0.f;
-#pragma unroll
-                for (int b = 0; b < P; ++b) {
-                    const float* row = plane + b * PX;
-                    float sr = 0.f, dr = 0.f;
-#pragma unroll
-                    for (int a2 = 0; a2 < P; ++a2) {
-                        const float v = row[a2];
-                        sr = fmaf(v, wx[a2], sr);
-                        dr = fmaf(v, dwx[a2], dr);
-                    }
-                    const float wyb = W[2 * P + b], dwyb = W[3 * P + b];
-                    Sv = fmaf(sr, wyb, Sv);
-                    Dv = fmaf(dr, wyb, Dv);
-                    Sy = fmaf(sr, dwyb, Sy);
-                }
-                const float wzc = W[4 * P + gl], dwzc = W[5 * P + gl];
-                pot = Sv * wzc;
-                gx = Dv * wzc;
-                gy = Sy * wzc;
-                gz = Sv * dwzc;
-            }
-#pragma unroll
-            for (int o = C::G / 2; o > 0; o >>= 1) {
-                pot += __shfl_xor_sync(0xffffffffu, pot, o, C::G);
-                gx += __shfl_xor_sync(0xffffffffu, gx, o, C::G);
-                gy += __shfl_xor_sync(0xffffffffu, gy, o, C::G);
-                gz += __shfl_xor_sync(0xffffffffu, gz, o, C::G);
-            }
-            if (qq < nc && gl == 0) {
-                const float q = qv[p];
-                const double e_i = 0.5 * (double)q * pot + self_coef * (double)q * q;
-                force[cprm[cb * C::CH + p]] = make_float4(q * gxs * gx, q * gys * gy, q * gzs * gz, (float)e_i);
-                esum += e_i;
-            }
-        }
+        esum += interp_chunk<P, TMA>(sm, PX, PP, xoff, D, wc, crec + cb * C::CH, crel + cb * C::CH,
+                                     cprm + cb * C::CH, wts, qv, org, order, nc, gxs, gys, gzs, self_coef, force);
         asm volatile("cp.async.wait_group 0;\n" ::);  // next chunk's records (made visible by the top barrier)
     }
     double ev[1] = {esum};
     block_sum_f64<1>(ev, red);
     if (threadIdx.x == 0) atomicAdd(&acc[si * ACC_STRIDE + ACC_E], ev[0]);
+}
+
+// Persistent TMA form, fed from a tile queue: a grid of resident CTAs takes
+// tiles from one counter (cleared by the host before the launch). Each CTA
+// keeps two potential-region buffers: while it interpolates tile t, the box
+// of the tile it takes next is already in flight into the other buffer, and
+// that tile's first chunk of particle records is prefetched during t's last
+// chunk. Thread 0 runs the queue three tiles ahead (counter, then the tile's
+// system and record range, then the system's tile grid), one stage per tile,
+// so none of those dependent loads is waited for. A box wait that runs out
+// sets kerr[0]; the CTA then drains its copies (bounded) and leaves the rest
+// of the queue to the other CTAs.
+__host__ __device__ inline int interp_q_region_words(int E, int PP) {
+    return (E * PP + 31) & ~31;  // 128-byte multiple
+}
+
+template <int P>
+__host__ __device__ inline int interp_q_smem(int E, int PP) {
+    using C = InterpCfg<P>;
+    return 128 + 4 * (2 * interp_q_region_words(E, PP) + C::CH * (6 * P + 1) + 3 * C::CH + P * (MAX_D + 1)) +
+           2 * C::CH * 24;
+}
+
+template <int P>
+__global__ void __launch_bounds__(128, 5)
+    k_interp_q(const int* __restrict__ tile_sys, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
+               int n_tiles, int T, int D, int PX, int PP, const uint32_t* __restrict__ start,
+               const uint32_t* __restrict__ perm, const float4* __restrict__ srec, const uint32_t* __restrict__ srel,
+               float4* __restrict__ force, double* __restrict__ acc, const CUtensorMap* __restrict__ tmaps,
+               int* __restrict__ kerr, int* __restrict__ queue) {
+    using C = InterpCfg<P>;
+    extern __shared__ float4 sm4[];
+    __shared__ double red[32];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ int s_tile[2], s_first[2], s_np[2];  // tile whose box goes to buffer b (n_tiles: none)
+    const int E = T + P - 1;
+    const int RW = interp_q_region_words(E, PP);
+    float* reg0 = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm4) + 127) & ~(uintptr_t)127);
+    float4* crec = reinterpret_cast<float4*>(reg0 + 2 * RW);       // [2][CH]
+    uint32_t* crel = reinterpret_cast<uint32_t*>(crec + 2 * C::CH);  // [2][CH]
+    uint32_t* cprm = crel + 2 * C::CH;                               // [2][CH]
+    float* wts = reinterpret_cast<float*>(cprm + 2 * C::CH);         // [CH][6P + 1]
+    float* qv = wts + C::CH * (6 * P + 1);                           // [CH]
+    int* org = reinterpret_cast<int*>(qv + C::CH);                   // [CH]
+    int* order = org + C::CH;                                        // [CH]
+    float* wc = reinterpret_cast<float*>(order + C::CH);             // [P][D+1]
+    const int tid = threadIdx.x;
+    const uint32_t mb0 = (uint32_t)__cvta_generic_to_shared(&mbar[0]);
+    const uint32_t box_bytes = (uint32_t)(E * PP) * 4u;
+    // thread 0's queue pipeline: q0 = index from the counter; q1 = + system
+    // and record range; q2 = + the system's tile grid (ready to issue)
+    int q0 = n_tiles, q1 = n_tiles, q1_si = 0, q2 = n_tiles, q2_si = 0, q2_ntx = 1, q2_nty = 1, q2_toff = 0;
+    uint32_t q1_f = 0, q1_e = 0, q2_f = 0, q2_np = 0;
+    // shifts the pipeline by one tile; the tile leaving q2 gets its box
+    // issued into buffer b (or buffer b is marked empty)
+    auto advance = [&](int b) {
+        const int t = q2;
+        s_tile[b] = t;
+        s_first[b] = (int)q2_f;
+        s_np[b] = (int)q2_np;
+        if (t < n_tiles) {
+            const int lt = t - q2_toff;
+            const int X0 = (lt % q2_ntx) * T, Y0 = ((lt / q2_ntx) % q2_nty) * T, Z0 = (lt / (q2_ntx * q2_nty)) * T;
+            const uint32_t mb = mb0 + 8u * (uint32_t)b;
+            // the buffer was last read by generic loads of this CTA
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mb), "r"(box_bytes)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+                "[%5];\n" ::"r"((uint32_t)__cvta_generic_to_shared(reg0 + b * RW)),
+                "l"(reinterpret_cast<uint64_t>(tmaps + q2_si)), "r"(X0 - (X0 & 3)), "r"(Y0), "r"(Z0), "r"(mb)
+                : "memory");
+        }
+        q2 = q1;
+        q2_si = q1_si;
+        q2_f = q1_f;
+        q2_np = q1_e - q1_f;
+        if (q1 < n_tiles) {
+            const SysDev& S = sys[q1_si];
+            q2_ntx = S.ntx;
+            q2_nty = S.nty;
+            q2_toff = S.t_off;
+        }
+        q1 = q0;
+        if (q0 < n_tiles) {
+            q1_si = tile_sys[q0];
+            q1_f = start[q0];
+            q1_e = start[q0 + 1];
+        }
+        q0 = atomicAdd(queue, 1);
+        if (q0 > n_tiles) q0 = n_tiles;
+    };
+    auto prefetch = [&](uint32_t first, int n, int buf) {
+        for (int p = tid; p < n; p += blockDim.x) {
+            const uint32_t d1 = (uint32_t)__cvta_generic_to_shared(&crec[buf * C::CH + p]);
+            const uint32_t d2 = (uint32_t)__cvta_generic_to_shared(&crel[buf * C::CH + p]);
+            const uint32_t d3 = (uint32_t)__cvta_generic_to_shared(&cprm[buf * C::CH + p]);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d1), "l"(srec + first + p));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d2), "l"(srel + first + p));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d3), "l"(perm + first + p));
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb0) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb0 + 8u) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        q0 = min(atomicAdd(queue, 1), n_tiles);
+        advance(1);  // fills the pipeline (buffer 1 marked empty on the way)
+        advance(1);
+        advance(0);  // the first tile's box
+    }
+    __syncthreads();
+    int b = 0, cbuf = 0, cur_pset = -1;
+    uint32_t ph[2] = {0u, 0u};
+    int t = s_tile[0];
+    if (t < n_tiles) prefetch((uint32_t)s_first[0], min(C::CH, s_np[0]), 0);
+    while (t < n_tiles) {
+        const uint32_t s0 = (uint32_t)s_first[b];
+        const int np = s_np[b];
+        const int si = tile_sys[t];
+        const SysDev& S = sys[si];
+        const ParamSet& ps = psets[S.pset];
+        const int xoff = ((t - S.t_off) % S.ntx) * T & 3;
+        if (S.pset != cur_pset) {  // read after the chunk loop's top barrier
+            cur_pset = S.pset;
+            for (int i = tid; i < P * (D + 1); i += blockDim.x)
+                wc[i] = ps.wcoef[(i / (D + 1)) * (MAX_D + 1) + (i % (D + 1))];
+        }
+        const bool ok = tma_wait(mb0 + 8u * (uint32_t)b, ph[b]);
+        ph[b] ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            // the box did not arrive in time: report, drain this CTA's copies
+            // (bounded) and stop taking tiles
+            if (tid == 0) atomicOr(kerr, 1);
+            tma_wait(mb0 + 8u * (uint32_t)b, ph[b] ^ 1u);
+            asm volatile("cp.async.wait_group 0;\n" ::);
+            return;
+        }
+        // this box has arrived and the previous tile is done: start the next one
+        if (tid == 0) advance(b ^ 1);
+        const float gxs = (float)S.gxd, gys = (float)S.gyd, gzs = (float)S.gzd;
+        const double self_coef = ps.self_coef;
+        double esum = 0.0;
+        for (int base = 0; base < np; base += C::CH) {
+            const int nc = min(C::CH, np - base);
+            asm volatile("cp.async.wait_group 0;\n" ::);  // this chunk's records
+            __syncthreads();  // records, coefficients and the next tile's range visible; previous chunk consumed
+            if (base + C::CH < np) {
+                prefetch(s0 + base + C::CH, min(C::CH, np - base - C::CH), cbuf ^ 1);
+            } else if (s_tile[b ^ 1] < n_tiles) {
+                prefetch((uint32_t)s_first[b ^ 1], min(C::CH, s_np[b ^ 1]), cbuf ^ 1);
+            }
+            esum += interp_chunk<P, true>(reg0 + b * RW, PX, PP, xoff, D, wc, crec + cbuf * C::CH,
+                                          crel + cbuf * C::CH, cprm + cbuf * C::CH, wts, qv, org, order, nc, gxs, gys,
+                                          gzs, self_coef, force);
+            cbuf ^= 1;
+        }
+        if (np == 0) {
+            // an empty tile: its box is not read; the next tile's range
+            // becomes visible here, and its first records are prefetched
+            __syncthreads();
+            if (s_tile[b ^ 1] < n_tiles) prefetch((uint32_t)s_first[b ^ 1], min(C::CH, s_np[b ^ 1]), cbuf);
+        }
+        double ev[1] = {esum};
+        block_sum_f64<1>(ev, red);
+        if (tid == 0 && np > 0) atomicAdd(&acc[si * ACC_STRIDE + ACC_E], ev[0]);
+        t = s_tile[b ^ 1];
+        b ^= 1;
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::);
 }
 
 // ============================================================================
@@ -1787,7 +1978,7 @@ static cudaError_t launch_interp_p(const LaunchArgs& a, cudaStream_t st) {
     if (a.configure_only) {
         // per-function limits shared by every batch of the process: raised
         // only, so a later plan with a smaller tile cannot lower them
-        static int configured[2] = {0, 0};
+        static int configured[3] = {0, 0, 0};
         cudaError_t e = cudaSuccess;
         const int s0 = (int)interp_smem<P>(E, a.PP);
         if (s0 > configured[0]) {
@@ -1799,9 +1990,30 @@ static cudaError_t launch_interp_p(const LaunchArgs& a, cudaStream_t st) {
             e = cudaFuncSetAttribute(k_interp<P, kTmaForm>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1);
             if (e == cudaSuccess) configured[1] = s1;
         }
+        const int s2 = interp_q_smem<P>(E, a.tma_bx * a.tma_by);
+        if (e == cudaSuccess && kTmaForm && a.tma_bx > 0 && s2 > configured[2]) {
+            e = cudaFuncSetAttribute(k_interp_q<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2);
+            if (e == cudaSuccess) configured[2] = s2;
+        }
         return e;
     }
     if (a.n_tiles == 0) return cudaSuccess;
+    if (tma && a.queue) {
+        // persistent CTAs, as many as are resident at once, fed from the queue
+        const int smem = interp_q_smem<P>(E, PP);
+        int per_sm = 0, dev = 0, n_sm = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_interp_q<P>, C::THREADS, smem);
+        if (e != cudaSuccess) return e;
+        const int grid = std::max(1, std::min(a.n_tiles, std::max(per_sm, 1) * n_sm));
+        if ((e = cudaMemsetAsync(a.queue, 0, sizeof(int), st)) != cudaSuccess) return e;
+        k_interp_q<P><<<grid, C::THREADS, smem, st>>>(a.tile_sys, a.sys, a.psets, a.n_tiles, a.T, a.D, PX, PP,
+                                                      a.tile_start, a.perm, a.srec, a.srel, a.force, a.acc,
+                                                      reinterpret_cast<const CUtensorMap*>(a.tmaps), a.kerr, a.queue);
+        return cudaGetLastError();
+    }
     if (tma)
         k_interp<P, kTmaForm><<<a.n_tiles, C::THREADS, interp_smem<P>(E, PP), st>>>(
             a.tile_sys, a.sys, a.psets, a.T, a.D, PX, PP, a.tile_start, a.perm, a.srec, a.srel, a.phi, a.force, a.acc,

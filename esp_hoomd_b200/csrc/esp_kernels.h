@@ -113,6 +113,9 @@ struct LaunchArgs {
     const void* tmaps = nullptr;
     int tma_bx = 0, tma_by = 0;
     int* kerr = nullptr;
+    // tile-queue counter of the persistent interpolation kernel (device int;
+    // NULL: one CTA per tile)
+    int* queue = nullptr;
     const uint32_t* ex_n = nullptr;     // exclusions: row i holds ex_list[i * ex_pitch + k], k < ex_n[i]
     const uint32_t* ex_list = nullptr;
     int ex_pitch = 0;

@@ -198,7 +198,7 @@ struct esp_server {
     CUtensorMap* d_tmaps = nullptr;
     bool use_tma = false;
     int tma_bx = 0, tma_by = 0;
-    int* d_kerr = nullptr;
+    int* d_kerr = nullptr;  // [kernel error word, tile-queue counter]
     double2* d_geo = nullptr;
     std::vector<double2> geos;
     static constexpr int MAX_GEOS = 16;
@@ -325,9 +325,9 @@ int esp_server::init(const esp_server_config& cfg) {
         (rc = mem.get(d_pitems, ITEM_CAP)) || (rc = mem.get(d_sitems, ITEM_CAP)) || (rc = mem.get(d_xitems, ITEM_CAP)) ||
         (rc = mem.get(d_yitems, ITEM_CAP)) || (rc = mem.get(d_zitems, ITEM_CAP)) ||
         (rc = mem.get(d_rskip, max_slots)) || (rc = mem.get(d_ritems, ritem_cap)) || (rc = mem.get(d_geo, MAX_GEOS)) ||
-        (rc = mem.get(d_tmaps, max_slots)) || (rc = mem.get(d_kerr, 1)))
+        (rc = mem.get(d_tmaps, max_slots)) || (rc = mem.get(d_kerr, 2)))
         return rc;
-    ESPB_CK(cudaMemset(d_kerr, 0, sizeof(int)));
+    ESPB_CK(cudaMemset(d_kerr, 0, 2 * sizeof(int)));
     interp_box(T + P - 1, tma_bx, tma_by);
     use_tma = prm.interp_mode == 0 && P >= 5 && P <= 8;
     stats.arena_bytes = mem.bytes;
@@ -776,6 +776,7 @@ int esp_server::launch_round(Staging& sg) {
     a.tma_bx = tma_bx;
     a.tma_by = tma_by;
     a.kerr = d_kerr;
+    a.queue = d_kerr + 1;  // the persistent interpolation kernel's tile counter
     a.want_virial = 0;
     a.add_bg = 1;
     a.nl_head = d_head;

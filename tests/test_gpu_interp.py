@@ -3,9 +3,10 @@ cp.async.bulk.tensor box of the halo-padded potential mesh per tile) against
 the cp.async staging of the same plan: the same forces and per-particle
 energies (each particle's contraction is the same arithmetic on the same
 staged values), for supports 5..8, odd, non-cubic and small meshes (where
-the halo is widest) and the autotuner's smaller tiles; the kernels' error
-word stays clear. The cp.async form itself is pinned to the oracle by
-test_gpu_parity.py."""
+the halo is widest) and the autotuner's smaller tiles, and for a clustered
+system whose empty tiles the persistent tile-queue kernel passes over; the
+kernels' error word stays clear. The cp.async form itself is pinned to the
+oracle by test_gpu_parity.py."""
 import numpy as np
 import pytest
 
@@ -38,5 +39,19 @@ def test_tma_interp_equals_cp_async(order, tile):
     kw = dict(order=order, tile=tile)
     fa, ea = _run(sl, interp_mode=1, **kw)
     fb, eb = _run(sl, interp_mode=0, **kw)
+    assert np.abs(fb - fa).max() <= 1e-6 * np.abs(fa).max()
+    assert np.all(np.abs(eb - ea) <= 1e-9 * np.abs(ea))
+
+
+def test_tma_interp_with_empty_tiles():
+    # every particle in one corner octant: most tiles hold none
+    rng = np.random.default_rng(12)
+    L, n = 24.0, 3000
+    pos = rng.uniform(0.0, 0.45 * L, (n, 3))
+    q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+    s = systems.System(pos=pos, q=q, vel=np.zeros_like(pos), mass=np.ones(n), box=(L, L, L))
+    sl = [systems.rocksalt(10, seed=9201), s, systems.rocksalt(12, seed=9202)]
+    fa, ea = _run(sl, interp_mode=1, order=8)
+    fb, eb = _run(sl, interp_mode=0, order=8)
     assert np.abs(fb - fa).max() <= 1e-6 * np.abs(fa).max()
     assert np.all(np.abs(eb - ea) <= 1e-9 * np.abs(ea))
