@@ -449,6 +449,7 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
     prm = p;
     if (ns <= 0) return fail(ESP_ERR_INVALID, "number of systems must be positive");
     if (p.order < 2 || p.order > MAX_P) return fail(ESP_ERR_UNSUPPORTED, "order must be in [2, 12]");
+    if (p.interp_mode < 0 || p.interp_mode > 2) return fail(ESP_ERR_INVALID, "interp_mode must be 0, 1 or 2");
     if (!(p.rcut > 0)) return fail(ESP_ERR_INVALID, "rcut must be positive");
     if (p.alpha != 0.0) return fail(ESP_ERR_UNSUPPORTED, "Debye screening (alpha != 0) is not supported");
     if (p.kappa < 0 || p.window_c < 0) return fail(ESP_ERR_INVALID, "kappa and window_c must be >= 0");
@@ -670,7 +671,7 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
     // cp.async form otherwise or when any map cannot be encoded)
     d_tmaps = nullptr;
     interp_box(T + P - 1, tma_bx, tma_by);
-    if (p.interp_mode == 0 && P >= 5 && P <= 8) {
+    if ((p.interp_mode == 0 || p.interp_mode == 2) && P >= 5 && P <= 8) {
         std::vector<CUtensorMap> maps(ns);
         bool ok = true;
         for (int s = 0; s < ns && ok; ++s) {
@@ -898,7 +899,8 @@ LaunchArgs esp_batch::args() const {
     a.tma_bx = tma_bx;
     a.tma_by = tma_by;
     a.kerr = d_kerr;
-    a.queue = d_kerr + 1;  // the persistent interpolation kernel's tile counter
+    // interp_mode 2: the persistent TMA kernel fed from a tile queue (its counter)
+    a.queue = prm.interp_mode == 2 ? d_kerr + 1 : nullptr;
     a.nmax_x = a.nmax_y = a.nmax_z = 1;
     for (const SysDev& S : sd) {
         a.nmax_x = std::max(a.nmax_x, S.nx);
@@ -1413,6 +1415,17 @@ int esp_batch::autotune(cudaStream_t st, const float* pos4, const float* q, cons
         {
             esp_params c = best;
             c.fft_mode = best.fft_mode ? 0 : 1;
+            double ms = 0;
+            if ((rc = run(c, ms))) goto done;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = c;
+            }
+        }
+        // TMA interpolation: one CTA per tile, or persistent CTAs on a tile queue
+        if (P >= 5 && P <= 8 && (best.interp_mode == 0 || best.interp_mode == 2)) {
+            esp_params c = best;
+            c.interp_mode = best.interp_mode == 0 ? 2 : 0;
             double ms = 0;
             if ((rc = run(c, ms))) goto done;
             if (ms < best_ms) {

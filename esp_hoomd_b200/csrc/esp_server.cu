@@ -329,7 +329,7 @@ int esp_server::init(const esp_server_config& cfg) {
         return rc;
     ESPB_CK(cudaMemset(d_kerr, 0, 2 * sizeof(int)));
     interp_box(T + P - 1, tma_bx, tma_by);
-    use_tma = prm.interp_mode == 0 && P >= 5 && P <= 8;
+    use_tma = (prm.interp_mode == 0 || prm.interp_mode == 2) && P >= 5 && P <= 8;
     stats.arena_bytes = mem.bytes;
     ESPB_CK(cudaMemcpy(d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice));
     // counters that the kernels leave at zero, and meshes the inverse FFT pass
@@ -776,7 +776,8 @@ int esp_server::launch_round(Staging& sg) {
     a.tma_bx = tma_bx;
     a.tma_by = tma_by;
     a.kerr = d_kerr;
-    a.queue = d_kerr + 1;  // the persistent interpolation kernel's tile counter
+    // interp_mode 2: the persistent TMA kernel fed from a tile queue (its counter)
+    a.queue = prm.interp_mode == 2 ? d_kerr + 1 : nullptr;
     a.want_virial = 0;
     a.add_bg = 1;
     a.nl_head = d_head;

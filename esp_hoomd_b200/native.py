@@ -265,7 +265,8 @@ class Batch:
                                            trials.ctypes.data_as(ctypes.c_void_p), int(trials.size)),
               "esp_batch_autotune")
         return {"tile": chosen.tile, "threads_per_particle": chosen.threads_per_particle,
-                "fft_mode": chosen.fft_mode, "trial_ms": [float(t) for t in trials if t > 0]}
+                "fft_mode": chosen.fft_mode, "interp_mode": chosen.interp_mode,
+                "trial_ms": [float(t) for t in trials if t > 0]}
 
     def compute_f64(self, pos4, q, force4, energy=None, virial=None, nlist=None, flags: int = _lib.ESP_ALL,
                     stream=None) -> None:

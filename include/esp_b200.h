@@ -66,7 +66,9 @@ typedef struct esp_params {
     int threads_per_particle; /* pair kernel lanes per particle: 4, 8, 16, 32; 0 = 4 */
     int precision;       /* ESP_FP32 (default) or ESP_FP64 */
     int fft_mode;        /* 0: whole planes/slabs in shared memory where they fit; 1: per-line passes */
-    int interp_mode;     /* 0: the potential tile staged by TMA (supports 5..8); 1: cp.async staging */
+    int interp_mode;     /* 0: the potential tile staged by TMA, one CTA per tile (supports 5..8);
+                            1: cp.async staging; 2: TMA, persistent CTAs fed from a tile queue with
+                            the next tile's box in flight (supports 5..8) */
 } esp_params;
 
 /* Resolved configuration of a context or of one system of a batch. */

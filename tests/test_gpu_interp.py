@@ -1,5 +1,6 @@
 """Interpolation with the potential tile staged by TMA (one
-cp.async.bulk.tensor box of the halo-padded potential mesh per tile) against
+cp.async.bulk.tensor box of the halo-padded potential mesh per tile; one CTA
+per tile, or persistent CTAs fed from a tile queue) against
 the cp.async staging of the same plan: the same forces and per-particle
 energies (each particle's contraction is the same arithmetic on the same
 staged values), for supports 5..8, odd, non-cubic and small meshes (where
@@ -32,13 +33,14 @@ def _run(sl, **kw):
     return f.double().cpu().numpy(), e.cpu().numpy()
 
 
+@pytest.mark.parametrize("mode", [0, 2])
 @pytest.mark.parametrize("order,tile", [(8, 0), (6, 0), (5, 0), (8, 8), (8, 7)])
-def test_tma_interp_equals_cp_async(order, tile):
+def test_tma_interp_equals_cp_async(order, tile, mode):
     sl = [systems.rocksalt(n, seed=9100 + n) for n in (8, 11, 20)]
     sl.append(systems.rocksalt(0, seed=9199, shape=(13, 22, 9)))
     kw = dict(order=order, tile=tile)
     fa, ea = _run(sl, interp_mode=1, **kw)
-    fb, eb = _run(sl, interp_mode=0, **kw)
+    fb, eb = _run(sl, interp_mode=mode, **kw)
     assert np.abs(fb - fa).max() <= 1e-6 * np.abs(fa).max()
     assert np.all(np.abs(eb - ea) <= 1e-9 * np.abs(ea))
 
@@ -52,6 +54,7 @@ def test_tma_interp_with_empty_tiles():
     s = systems.System(pos=pos, q=q, vel=np.zeros_like(pos), mass=np.ones(n), box=(L, L, L))
     sl = [systems.rocksalt(10, seed=9201), s, systems.rocksalt(12, seed=9202)]
     fa, ea = _run(sl, interp_mode=1, order=8)
-    fb, eb = _run(sl, interp_mode=0, order=8)
-    assert np.abs(fb - fa).max() <= 1e-6 * np.abs(fa).max()
-    assert np.all(np.abs(eb - ea) <= 1e-9 * np.abs(ea))
+    for mode in (0, 2):
+        fb, eb = _run(sl, interp_mode=mode, order=8)
+        assert np.abs(fb - fa).max() <= 1e-6 * np.abs(fa).max()
+        assert np.all(np.abs(eb - ea) <= 1e-9 * np.abs(ea))
