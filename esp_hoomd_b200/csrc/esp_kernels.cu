@@ -509,11 +509,11 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-constexpr int SPREAD_CHM = 64;  // particles staged per round (multiple of 8)
+constexpr int SPREAD_CHM = 48;  // particles staged per round (multiple of 8; 4 CTAs of 256 threads per SM)
 constexpr int SPREAD_MS = 24;   // staged row stride: rows of 4 consecutive particles hit disjoint banks
 
 template <int P>
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 4)
     k_spread_mma(const int* __restrict__ tile_sys, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
                  int T, int D, const uint32_t* __restrict__ start, const float4* __restrict__ srec,
                  const uint32_t* __restrict__ srel, double* __restrict__ rho) {
