@@ -121,42 +121,6 @@ __device__ __forceinline__ uint32_t nl_scan(const float4* __restrict__ cand, int
     return cnt;
 }
 
-// As nl_scan, for a warp that holds fewer than 17 particles of the cell:
-// each particle gets G = 2^lg lanes (lane = particle j * G + sub), lane sub
-// tests candidates sub, sub + G, ...; the G lanes' hits of a step are
-// appended in candidate order (group ballot and prefix count), so the row is
-// the same as one thread's scan. Every lane of the warp calls it.
-template <bool MINIMG>
-__device__ __forceinline__ uint32_t nl_scan_grp(const float4* __restrict__ cand, int n, float4 pi, int self,
-                                                const SysDev& S, float rlist2, uint32_t cap,
-                                                uint32_t* __restrict__ row, uint32_t cnt, int base_id, int lg,
-                                                int j, int sub) {
-    const int G = 1 << lg;
-    const unsigned gmask = lg == 5 ? 0xffffffffu : ((1u << G) - 1u);
-    const unsigned below = (1u << sub) - 1u;
-    for (int k0 = 0; k0 < n; k0 += G) {
-        const int k = k0 + sub;
-        bool hit = false;
-        int w = 0;
-        if (k < n) {
-            const float4 pj = cand[k];
-            float ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
-            if (MINIMG) {
-                ddx -= S.Lx * rintf(ddx * S.inv_Lx);
-                ddy -= S.Ly * rintf(ddy * S.inv_Ly);
-                ddz -= S.Lz * rintf(ddz * S.inv_Lz);
-            }
-            w = __float_as_int(pj.w);
-            hit = ddx * ddx + ddy * ddy + ddz * ddz < rlist2 && w != self;
-        }
-        const unsigned gm = (__ballot_sync(0xffffffffu, hit) >> (j << lg)) & gmask;
-        const uint32_t at = cnt + (uint32_t)__popc(gm & below);
-        if (hit && at < cap) row[at] = (uint32_t)(w - base_id);
-        cnt += (uint32_t)__popc(gm);
-    }
-    return cnt;
-}
-
 // SORTED = false: HOOMD-layout rows -- the row of particle i at nl_off +
 // local i * cap, entries local particle indices, head/nn indexed by
 // particle. SORTED = true: the library's pair list -- the same layout indexed
@@ -205,17 +169,9 @@ __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ ce
         stage(0);
         __syncthreads();
     }
-    const int warp = tid >> 5, lane = tid & 31;
     for (uint32_t p0 = c0; p0 < c1; p0 += NL_THREADS) {
-        // this warp's particles in this pass: with fewer than 17, each one is
-        // scanned by G = 2^lg lanes (a warp with none skips the scan)
-        const int wb = (int)p0 + 32 * warp;
-        const int m = max(0, min(32, (int)c1 - wb));
-        int lg = 0;
-        while (lg < 5 && (m << (lg + 1)) <= 32) ++lg;
-        const int j = lane >> lg, sub = lane & ((1 << lg) - 1);
-        const uint32_t slot = (uint32_t)(wb + j);
-        const bool active = j < m;
+        const uint32_t slot = p0 + tid;
+        const bool active = slot < c1;
         const float4 pi = active ? cpos[slot] : make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, __int_as_float(-1));
         const int idx = __float_as_int(pi.w);
         const int self = SORTED ? (int)slot : idx;
@@ -230,17 +186,10 @@ __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ ce
                 __syncthreads();
             }
             const int n = (int)min((uint32_t)NL_STAGE, total - base);
-            if (m == 0) continue;  // warp-uniform
-            if (lg == 0)
-                cnt = minimg ? nl_scan<true>(cand, n, pi, self, S, rlist2, (uint32_t)cap, row, cnt, S.p_off)
-                             : nl_scan<false>(cand, n, pi, self, S, rlist2, (uint32_t)cap, row, cnt, S.p_off);
-            else
-                cnt = minimg ? nl_scan_grp<true>(cand, n, pi, self, S, rlist2, (uint32_t)cap, row, cnt, S.p_off, lg,
-                                                 j, sub)
-                             : nl_scan_grp<false>(cand, n, pi, self, S, rlist2, (uint32_t)cap, row, cnt, S.p_off,
-                                                  lg, j, sub);
+            cnt = minimg ? nl_scan<true>(cand, n, pi, self, S, rlist2, (uint32_t)cap, row, cnt, S.p_off)
+                         : nl_scan<false>(cand, n, pi, self, S, rlist2, (uint32_t)cap, row, cnt, S.p_off);
         }
-        if (active && sub == 0) {
+        if (active) {
             head[key] = (uint32_t)hrow;
             nn[key] = cnt;
             if (cnt > (uint32_t)cap) {
