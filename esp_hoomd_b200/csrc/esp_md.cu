@@ -87,23 +87,30 @@ __global__ void k_cell_sort(const uint32_t* __restrict__ start, const uint32_t* 
 constexpr int NL_THREADS = 64;
 constexpr int NL_STAGE = 1024;
 
-// store v at p when ok, as one predicated store (the candidate loop has no
-// per-candidate branch)
-__device__ __forceinline__ void store_if(bool ok, uint32_t* p, uint32_t v) {
+// Appends the staged candidates within rlist of pi, other than `self`, to
+// row (staged values are already local indices or slots); threads without a
+// particle carry a NaN position, which tests false against everything. Hits
+// past cap are counted, and stored over the row's last entry (so an
+// overflowing row still holds only neighbours; the build reports it).
+// One candidate's test and append, as straight-line predicated code (no
+// branch per candidate): stores w at p when r2 < rlist2 and w != self, and
+// returns 1 then (0 otherwise).
+__device__ __forceinline__ uint32_t append_if(float r2, float rlist2, int w, int self, uint32_t* p) {
+    uint32_t inc;
     asm volatile(
-        "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q st.global.u32 [%0], %1;\n\t}" ::"l"(p), "r"(v),
-        "r"((uint32_t)ok)
+        "{\n\t.reg .pred q, r;\n\tsetp.lt.f32 q, %1, %2;\n\tsetp.ne.s32 r, %3, %4;\n\tand.pred q, q, r;\n\t"
+        "@q st.global.u32 [%5], %3;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(inc)
+        : "f"(r2), "f"(rlist2), "r"(w), "r"(self), "l"(p)
         : "memory");
+    return inc;
 }
 
-// Appends the staged candidates within rlist of pi, other than `self`, to
-// row as w - base_id (w: the candidate's staged value); threads without a
-// particle carry a NaN position, which tests false against everything.
-// Entries past cap are counted, not stored.
 template <bool MINIMG>
 __device__ __forceinline__ uint32_t nl_scan(const float4* __restrict__ cand, int n, float4 pi, int self,
                                             const SysDev& S, float rlist2, uint32_t cap, uint32_t* __restrict__ row,
-                                            uint32_t cnt, int base_id) {
+                                            uint32_t cnt) {
+    const uint32_t cap1 = cap - 1u;
 #pragma unroll 4
     for (int k = 0; k < n; ++k) {
         const float4 pj = cand[k];
@@ -113,10 +120,7 @@ __device__ __forceinline__ uint32_t nl_scan(const float4* __restrict__ cand, int
             ddy -= S.Ly * rintf(ddy * S.inv_Ly);
             ddz -= S.Lz * rintf(ddz * S.inv_Lz);
         }
-        const int w = __float_as_int(pj.w);
-        const bool hit = ddx * ddx + ddy * ddy + ddz * ddz < rlist2 && w != self;
-        store_if(hit && cnt < cap, row + cnt, (uint32_t)(w - base_id));
-        cnt += hit ? 1u : 0u;
+        cnt += append_if(ddx * ddx + ddy * ddy + ddz * ddz, rlist2, __float_as_int(pj.w), self, row + min(cnt, cap1));
     }
     return cnt;
 }
@@ -147,8 +151,8 @@ __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ ce
     __syncthreads();
     const bool minimg = nb.minimg != 0;
     const uint32_t total = nb.off[27];
-    // staged value: the candidate's particle index (HOOMD rows; the
-    // cell-sorted positions carry it) or its slot (pair list)
+    // staged value: the candidate's local particle index (HOOMD rows; the
+    // cell-sorted positions carry the index) or its local slot (pair list)
     auto stage = [&](uint32_t base) {
         const uint32_t top = min(total, base + (uint32_t)NL_STAGE);
         for (int s = 0; s < 27; ++s) {
@@ -159,7 +163,8 @@ __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ ce
                 p.x += nb.shift[s][0];
                 p.y += nb.shift[s][1];
                 p.z += nb.shift[s][2];
-                if (SORTED) p.w = __int_as_float((int)slot);
+                // local values: the pair list's slot, or the particle index
+                p.w = __int_as_float((SORTED ? (int)slot : __float_as_int(p.w)) - S.p_off);
                 cand[g - base] = p;
             }
         }
@@ -174,7 +179,7 @@ __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ ce
         const bool active = slot < c1;
         const float4 pi = active ? cpos[slot] : make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, __int_as_float(-1));
         const int idx = __float_as_int(pi.w);
-        const int self = SORTED ? (int)slot : idx;
+        const int self = (SORTED ? (int)slot : idx) - S.p_off;
         const uint32_t key = SORTED ? slot : (uint32_t)idx;  // owner of the row
         const long long hrow = C.nl_off + (long long)((int)key - S.p_off) * cap;
         uint32_t* row = nl + (active ? hrow : 0);
@@ -186,8 +191,8 @@ __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ ce
                 __syncthreads();
             }
             const int n = (int)min((uint32_t)NL_STAGE, total - base);
-            cnt = minimg ? nl_scan<true>(cand, n, pi, self, S, rlist2, (uint32_t)cap, row, cnt, S.p_off)
-                         : nl_scan<false>(cand, n, pi, self, S, rlist2, (uint32_t)cap, row, cnt, S.p_off);
+            cnt = minimg ? nl_scan<true>(cand, n, pi, self, S, rlist2, (uint32_t)cap, row, cnt)
+                         : nl_scan<false>(cand, n, pi, self, S, rlist2, (uint32_t)cap, row, cnt);
         }
         if (active) {
             head[key] = (uint32_t)hrow;
