@@ -81,6 +81,36 @@ def _systems(rank: int, count: int = N_SYS):
     return [systems.rocksalt(int(n), seed=SEED * 100000 + rank * N_SYS + i) for i, n in enumerate(ns)]
 
 
+def _smooth235(n: int) -> int:
+    """Smallest 2/3/5-smooth integer >= n."""
+    m = max(int(n), 1)
+    while True:
+        k = m
+        for p in (2, 3, 5):
+            while k % p == 0:
+                k //= p
+        if k == 1:
+            return m
+        m += 1
+
+
+def workload_config(count: int, world: int) -> dict:
+    """The workload's description, the same in both arms: rank 0's batch
+    (the first `count` systems), its particle and mesh-point totals from the
+    mesh rule (h = pi r_c / 18.5 for the 1e-5 target)."""
+    rng = np.random.default_rng(SEED)
+    ns = [int(n) for n in rng.choice(np.arange(8, 41, 2), size=N_SYS)[:count]]
+    h = math.pi * RCUT / 18.5
+    M = sum(_smooth235(max(8, math.ceil(n / h))) ** 3 for n in ns)
+    return {"workload": "batched%d: %d rock-salt systems n^3, n even ~U{8..40} (seed %d), 1 nlist + 1 eval + "
+                        "10 NVE steps per system per step" % (count, count, SEED),
+            "systems_per_gpu": count, "particles_per_gpu": sum(n ** 3 for n in ns), "order": 8, "rcut": RCUT,
+            "skin": SKIN, "mesh_rule": "smallest 2/3/5-smooth >= L/h, h = pi r_c / 18.5 (1e-5 target)",
+            "mesh_points_per_gpu": int(M), "dt": DT,
+            "l2": "inputs larger than L2 (neighbour rows: 4 B x ~164 entries per particle)",
+            "parallelism": "replicas over systems (dp%d)" % world}
+
+
 class Clocks:
     """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
 
@@ -201,8 +231,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "batched256 rock-salt (CPU sample of %d systems)" % len(sl), "rcut": RCUT,
-                       "order": 8},
+            "config": workload_config(args.systems, world),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -652,16 +681,15 @@ def run_ours(args):
     k_eval = K_EVAL_BASE + K_FFT[tuned["fft_mode"] if tuned else 0]
     if rank == 0:
         cores = os.cpu_count() or 1
+        cfg = workload_config(int(N.size), world)
+        if cfg["particles_per_gpu"] != tot or cfg["mesh_points_per_gpu"] != int(M):
+            cfg["note"] = "the planned batch differs from this description (see measured)"
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": max(3, args.warmup), "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "batched%d: %d rock-salt systems n^3, n even ~U{8..40} (seed 1004), "
-                                       "1 nlist + 1 eval + 10 NVE steps per system per step" % (N.size, N.size),
-                           "systems_per_gpu": int(N.size), "particles_per_gpu": tot, "order": 8, "rcut": RCUT,
-                           "mesh_rule": "smallest 2/3/5-smooth >= L/h, h = pi r_c / 18.5 (1e-5 target)",
-                           "mesh_points_per_gpu": int(M), "mean_neighbours": mean_nn, "dt": DT,
-                           "l2": "inputs larger than L2 (neighbour lists %.1f GB)" % (tot * mean_nn * 4 / 1e9),
-                           "parallelism": "replicas over systems (dp%d)" % world},
+                "config": cfg,
+                "measured": {"mean_neighbours": mean_nn, "mesh_points": int(M), "particles": tot,
+                             "neighbour_rows_gb": tot * mean_nn * 4 / 1e9},
                 "plain": {"value": plain_value, "unit": UNIT,
                           "desc": "same systems, one system per launch sequence, no graph"},
                 "batched_over_plain": (value / world / plain_value) if plain_value else None,
