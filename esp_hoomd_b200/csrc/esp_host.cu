@@ -1176,6 +1176,9 @@ NlistArgs esp_batch::nlist_args(CellGrid& g, const float* pos4, double rlist, in
     a.rlist2 = (float)(rlist * rlist);
     a.cap = cap;
     a.overflow = g.d_overflow;
+    a.ex_n = ex_n;
+    a.ex_list = ex_list;
+    a.ex_pitch = ex_pitch;
     return a;
 }
 

@@ -205,6 +205,54 @@ __global__ void __launch_bounds__(NL_THREADS) k_nlist(const int* __restrict__ ce
     }
 }
 
+// Leaves the excluded partners out of the rows just built (HOOMD's lists
+// hold no excluded pairs): one thread per row with exclusions, in place, the
+// kept entries in their order; the count drops by the entries removed from
+// the stored part. Pair-list rows hold slots, so the excluded indices are
+// mapped to slots first.
+constexpr int NL_MAXEX = 8;  // exclusions per particle held in registers
+
+template <bool SORTED>
+__global__ void k_nlist_exclude(const int2* __restrict__ chunks, const SysDev* __restrict__ sys,
+                                const uint32_t* __restrict__ head, uint32_t* __restrict__ nn,
+                                uint32_t* __restrict__ nl, int cap, const uint32_t* __restrict__ ex_n,
+                                const uint32_t* __restrict__ ex_list, int ex_pitch,
+                                const uint32_t* __restrict__ slot2idx, const uint32_t* __restrict__ idx2slot) {
+    const int2 ch = chunks[blockIdx.x];
+    const SysDev& S = sys[ch.x];
+    const int key = ch.y + threadIdx.x;  // the row: a slot (pair list) or a particle
+    if (key >= S.p_off + S.N) return;
+    const int i = SORTED ? (int)slot2idx[key] : key;
+    const int ne = min((int)ex_n[i], ex_pitch);
+    if (ne == 0) return;
+    uint32_t ex[NL_MAXEX];
+#pragma unroll
+    for (int k = 0; k < NL_MAXEX; ++k) {
+        uint32_t v = 0xffffffffu;
+        if (k < ne) {
+            const uint32_t jl = ex_list[(size_t)i * ex_pitch + k];
+            v = SORTED ? idx2slot[S.p_off + jl] - (uint32_t)S.p_off : jl;
+        }
+        ex[k] = v;
+    }
+    uint32_t* row = nl + head[key];
+    const uint32_t cnt = nn[key];
+    const uint32_t n = min(cnt, (uint32_t)cap);
+    uint32_t w = 0;
+    for (uint32_t r = 0; r < n; ++r) {
+        const uint32_t v = row[r];
+        bool drop = false;
+#pragma unroll
+        for (int k = 0; k < NL_MAXEX; ++k) drop |= v == ex[k];
+        for (int k = NL_MAXEX; k < ne; ++k) {  // rows with more exclusions than registers hold
+            const uint32_t jl = ex_list[(size_t)i * ex_pitch + k];
+            drop |= v == (SORTED ? idx2slot[S.p_off + jl] - (uint32_t)S.p_off : jl);
+        }
+        if (!drop) row[w++] = v;
+    }
+    nn[key] = cnt - (n - w);
+}
+
 // skip (may be NULL): per system, the local particle range [x, y) of rigid
 // molecules, which the constraint kernels integrate instead
 __global__ void k_nve1(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, float4* __restrict__ pos,
@@ -378,6 +426,14 @@ cudaError_t launch_nlist(const NlistArgs& a, cudaStream_t st) {
     else
         k_nlist<false><<<a.n_cells, NL_THREADS, 0, st>>>(a.cell_sys, a.sys, a.cells, a.cstart, a.cpos, a.rlist2,
                                                          a.cap, a.head, a.nn, a.nl, a.overflow);
+    if (a.ex_n) {
+        if (a.sorted)
+            k_nlist_exclude<true><<<a.n_chunks, 256, 0, st>>>(a.chunks, a.sys, a.head, a.nn, a.nl, a.cap, a.ex_n,
+                                                               a.ex_list, a.ex_pitch, a.slot2idx, a.idx2slot);
+        else
+            k_nlist_exclude<false><<<a.n_chunks, 256, 0, st>>>(a.chunks, a.sys, a.head, a.nn, a.nl, a.cap, a.ex_n,
+                                                                a.ex_list, a.ex_pitch, a.slot2idx, a.idx2slot);
+    }
     return cudaGetLastError();
 }
 

@@ -41,6 +41,11 @@ struct NlistArgs {
     // cell-sorted slot, entries local slots; false: HOOMD-layout rows
     // (indexed by particle, entries local particle indices)
     bool sorted = false;
+    // exclusions (HOOMD's n_ex / ex_list layout, rows by particle, local
+    // indices): when set, the built rows leave the excluded partners out
+    const uint32_t* ex_n = nullptr;
+    const uint32_t* ex_list = nullptr;
+    int ex_pitch = 0;
 };
 
 cudaError_t launch_nlist(const NlistArgs& a, cudaStream_t st);

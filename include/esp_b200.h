@@ -148,8 +148,10 @@ int esp_destroy(esp_ctx* ctx);
  * indices local to the system, every pair listed from both sides). Every
  * later long-range evaluation removes the mesh's interaction of these pairs
  * (force, energy, virial) at any distance; the neighbour list given to the
- * short-range term must leave them out, as HOOMD's does. The arrays stay
- * owned by the caller and must stay valid while set; n_ex = NULL clears. */
+ * short-range term must leave them out, as HOOMD's does (lists built by
+ * esp_batch_build_nlist / esp_batch_build_pairlist while exclusions are set
+ * do). The arrays stay owned by the caller and must stay valid while set;
+ * n_ex = NULL clears. */
 int esp_set_exclusions(esp_ctx* ctx, const unsigned* n_ex, const unsigned* ex_list, int ex_pitch);
 
 /* Stage outputs, for validation of single stages (no reference

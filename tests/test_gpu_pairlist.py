@@ -14,7 +14,8 @@ Cases:
 * a clustered system whose dense cells' neighbourhoods exceed the builder's
   shared-memory stage (scanned in windows);
 * a row capacity too small: ESP_ERR_OVERFLOW from the check and from the
-  next evaluation, with the longest row reported.
+  next evaluation, with the longest row reported;
+* exclusions set on the batch: both builders leave the excluded pairs out.
 """
 import numpy as np
 import pytest
@@ -156,3 +157,30 @@ def test_pairlist_overflow_is_reported():
     b.build_pairlist(pos, 3.4, 256)
     assert b.pairlist_check() == 0
     b.compute(pos, q, f, None, None, nlist=None, flags=ESP_SHORT_RANGE)
+
+
+def test_lists_leave_exclusions_out():
+    # rigid water with every intramolecular pair excluded, exclusions set on
+    # the batch before the builds: the HOOMD-layout rows are the oracle's list
+    # without the excluded pairs (order kept), and the pair list gives the same
+    # forces, energies and virials
+    w = systems.water(216, seed=71)
+    w.pos = w.pos.astype(np.float32).astype(np.float64)
+    excl = R.molecule_exclusions(216, 3)
+    b = native.Batch(native.make_params(rcut=0.9, mesh=(16, 16, 16)), [w.N], [w.box])
+    pos, _, q = _inputs([w])
+    b.set_exclusions(torch.tensor(excl[0].astype(np.int32), device="cuda"),
+                     torch.tensor(excl[1].astype(np.int32), device="cuda"), excl[2])
+    cap = 512
+    head = torch.zeros(w.N, dtype=torch.int32, device="cuda")
+    nn = torch.zeros_like(head)
+    nl = torch.zeros(w.N * cap, dtype=torch.int32, device="cuda")
+    b.build_nlist(pos, 0.9, cap, head, nn, nl)
+    b.nlist_check()
+    rh, rc, rl = R.remove_pairs(R.neighbor_list(w.pos, w.box, 0.9), *excl)
+    h, c, l = head.cpu().numpy(), nn.cpu().numpy(), nl.cpu().numpy()
+    assert np.array_equal(c, rc.astype(np.int32))
+    for i in range(0, w.N, 7):
+        assert sorted(l[h[i]:h[i] + c[i]].tolist()) == sorted(rl[rh[i]:rh[i] + rc[i]].tolist())
+    a, d = _both(b, pos, q, 0.9, cap, ESP_ALL)
+    _same(a, d)
