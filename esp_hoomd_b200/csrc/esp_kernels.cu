@@ -4,16 +4,20 @@
 //   k_bin / k_scan / k_scatter / k_tile_sort : new particle binning + stable
 //       sort (nearest reference code: makeFraction+floorf in
 //       src/ESPForceComputeGPU.cu:228-236)
-//   k_spread   : charge assignment, src/ESPForceComputeGPU.cu:206-272 (K2)
-//   k_fftx_fwd / k_ffty<false> : forward FFT, src/ESPForceComputeGPU.cc:254-265 (K3)
-//   k_fftz_conv : influence multiply fused into the z pass,
+//   k_spread_mma (tensor-core tiles; default), k_spread_dense, k_spread :
+//       charge assignment, src/ESPForceComputeGPU.cu:206-272 (K2)
+//   k_fft_plane_fwd, or k_fftx_fwd / k_ffty<false> : forward FFT,
+//       src/ESPForceComputeGPU.cc:254-265 (K3)
+//   k_fft_slab_z, or k_fftz_conv : influence multiply fused into the z pass,
 //       src/ESPForceComputeGPU.cu:277-287 (K4), plus the k-space energy and
 //       virial (stubs in src/ESPForceCompute.cc:236-248)
-//   k_ffty<true> / k_fftx_inv : inverse FFT (missing in the reference,
-//       src/ESPForceCompute.cc:225-232)
-//   k_interp   : force interpolation, src/ESPForceComputeGPU.cu:292-373 (K6)
+//   k_fft_plane_inv, or k_ffty<true> / k_fftx_inv : inverse FFT (missing in
+//       the reference, src/ESPForceCompute.cc:225-232)
+//   k_interp (one CTA per tile), k_interp_q (persistent, tile queue) : force
+//       interpolation, src/ESPForceComputeGPU.cu:292-373 (K6)
 //   k_pair     : EvaluatorPairPSWF over a neighbour list,
 //       src/EvaluatorPairPSWF.h:274-295 with the HOOMD PotentialPair loop
+//   k_exclusions : exclusion correction, src/ESPForceComputeGPU.cu:391-471 (K7)
 //   k_influence: influence-function build (K1), src/ESPForceComputeGPU.cu:157-201
 #include <cuda.h>
 
