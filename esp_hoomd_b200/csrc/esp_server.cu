@@ -185,7 +185,7 @@ struct esp_server {
     float* d_phi = nullptr;
     float2 *d_spec = nullptr, *d_gtab = nullptr, *d_tw = nullptr;
     double *d_acc = nullptr, *d_energy = nullptr, *d_infl = nullptr;
-    int* d_ovf = nullptr;
+    int* d_ovf = nullptr;  // per slot: [overflow flag, longest row] of its neighbour-list build
     int2 *d_chunks = nullptr, *d_pchunks = nullptr, *d_mdchunks = nullptr, *d_nlchunks = nullptr;
     int2 *d_pitems = nullptr, *d_sitems = nullptr;
     int4 *d_xitems = nullptr, *d_yitems = nullptr, *d_zitems = nullptr;
@@ -319,7 +319,7 @@ int esp_server::init(const esp_server_config& cfg) {
         (rc = mem.get(d_rho, M_cap)) || (rc = mem.get(d_phi, M_cap)) || (rc = mem.get(d_spec, M_cap)) ||
         (rc = mem.get(d_gtab, G_cap)) || (rc = mem.get(d_tw, tw.size())) ||
         (rc = mem.get(d_acc, (size_t)max_slots * ACC_STRIDE)) || (rc = mem.get(d_energy, max_slots)) ||
-        (rc = mem.get(d_infl, 3 * FFT_MAX_N + 2 * 320)) || (rc = mem.get(d_ovf, max_slots)) ||
+        (rc = mem.get(d_infl, 3 * FFT_MAX_N + 2 * 320)) || (rc = mem.get(d_ovf, 2 * max_slots)) ||
         (rc = mem.get(d_chunks, chunk_cap)) || (rc = mem.get(d_pchunks, pchunk_cap)) ||
         (rc = mem.get(d_mdchunks, chunk_cap)) || (rc = mem.get(d_nlchunks, (max_particles + 255) / 256)) ||
         (rc = mem.get(d_pitems, ITEM_CAP)) || (rc = mem.get(d_sitems, ITEM_CAP)) || (rc = mem.get(d_xitems, ITEM_CAP)) ||
@@ -642,7 +642,7 @@ int esp_server::admit(Request* q, Staging& sg) {
     na.head = d_head;
     na.nn = d_nn;
     na.nl = d_nl;
-    na.overflow = d_ovf + q->slot;
+    na.overflow = d_ovf + 2 * q->slot;  // [flag, longest row] of this slot's build
     ESPB_CK(launch_nlist(na, st));
     q->steps_done = 0;
     q->evaluated = false;
@@ -833,7 +833,7 @@ int esp_server::launch_round(Staging& sg) {
         if (r.out_vel4) ESPB_CK(cudaMemcpyAsync(r.out_vel4, d_vel + q->p_off, n * 16, cudaMemcpyDeviceToHost, st));
         if (r.out_force4) ESPB_CK(cudaMemcpyAsync(r.out_force4, d_force + q->p_off, n * 16, cudaMemcpyDeviceToHost, st));
         if (r.out_energy) ESPB_CK(cudaMemcpyAsync(r.out_energy, d_energy + q->slot, 8, cudaMemcpyDeviceToHost, st));
-        ESPB_CK(cudaMemcpyAsync(rd.ovf + k, d_ovf + q->slot, sizeof(int), cudaMemcpyDeviceToHost, st));
+        ESPB_CK(cudaMemcpyAsync(rd.ovf + k, d_ovf + 2 * q->slot, sizeof(int), cudaMemcpyDeviceToHost, st));
         release(q);  // later uploads into these ranges are stream-ordered after the copies above
     }
     active.swap(keep);
