@@ -248,7 +248,7 @@ class ESPForceCompute : public ForceCompute {
     EspContext m_ctx;
 };
 
-// The GPU class of the reference (every stage of this build runs on the GPU).
+// The GPU class of the reference (every stage of this library runs on the GPU).
 class ESPForceComputeGPU : public ESPForceCompute {
   public:
     using ESPForceCompute::ESPForceCompute;

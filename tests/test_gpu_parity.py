@@ -8,7 +8,7 @@ Tolerances (FP32 bulk arithmetic, FP64 reductions):
 * forces: relative RMS difference <= 5e-6; energy relative <= 2e-6;
   virial max abs <= 1e-5 max |W|;
 * physics: relative RMS force error vs FP64 Ewald <= 1e-5 at the default
-  target (the north-star accuracy bar).
+  target (the accuracy bar of the headline metric).
 """
 import numpy as np
 import pytest
