@@ -397,6 +397,151 @@ def run_serving(args, pool):
 
 
 # ----------------------------------------------------------------------------- scale-up
+def run_c1(args):
+    """The CPU-runnable plain case, timed: N = 1,000 rock-salt ions (10^3
+    lattice, L = 10, seed 1000), mesh 32^3, support 8, r_c 3.0, FP64 mode,
+    Lennard-Jones core repulsion (eps 1, sigma 0.9, r_cut 2.5); a step = one
+    evaluation + 100 NVE steps at dt 0.002 with the neighbour list (r_c + 0.4)
+    rebuilt every 10 steps. One small system: launch-bound by nature."""
+    import torch
+    from esp_hoomd_b200 import native, systems
+    dev = torch.device("cuda", 0)
+    s = systems.rocksalt(10, seed=1000)
+    N = s.N
+    b = native.Batch(native.make_params(order=8, rcut=RCUT, mesh=(32, 32, 32), precision=1), [N], [s.box])
+    b32 = native.Batch(native.make_params(order=8, rcut=RCUT, mesh=(32, 32, 32)), [N], [s.box])  # list builder
+    p4 = np.zeros((N, 4))
+    p4[:, :3] = s.pos
+    v4 = np.zeros((N, 4))
+    v4[:, :3] = s.vel
+    v4[:, 3] = 1.0
+    pos0 = torch.tensor(p4, dtype=torch.float64, device=dev)
+    vel0 = torch.tensor(v4, dtype=torch.float64, device=dev)
+    pos, vel = pos0.clone(), vel0.clone()
+    q = torch.tensor(s.q, dtype=torch.float64, device=dev)
+    force = torch.zeros((N, 4), dtype=torch.float64, device=dev)
+    e_esp = torch.zeros(1, dtype=torch.float64, device=dev)
+    e_lj = torch.zeros(1, dtype=torch.float64, device=dev)
+    head = torch.zeros(N, dtype=torch.int32, device=dev)
+    nn = torch.zeros_like(head)
+    nl = torch.zeros(N * CAP, dtype=torch.int32, device=dev)
+    nlist = (head, nn, nl)
+
+    def evaluate():
+        e_lj.zero_()
+        b.compute_f64(pos, q, force, e_esp, nlist=nlist)
+        b.lj(pos, nlist, 1.0, 0.9, 2.5, force, e_lj)
+
+    def step():
+        pos.copy_(pos0)
+        vel.copy_(vel0)
+        b32.build_nlist(pos.float(), RCUT + SKIN, CAP, head, nn, nl)
+        evaluate()
+        for k in range(100):
+            if k and k % 10 == 0:
+                b32.build_nlist(pos.float(), RCUT + SKIN, CAP, head, nn, nl)
+            b.nve_step1_f64(pos, vel, force, DT)
+            evaluate()
+            b.nve_step2_f64(vel, force, DT)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    b32.nlist_check()
+    torch.cuda.synchronize()
+    st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(0) as clk:
+        st.record()
+        for _ in range(args.steps):
+            step()
+        en.record()
+        torch.cuda.synchronize()
+    ms = st.elapsed_time(en) / args.steps
+    line = {"metric": "particle-steps/s (C1: FP64 ESP + LJ, N = 1,000, 100 NVE steps per step)",
+            "value": N * 100 / (ms * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "c1: rock-salt 10^3 (N = 1,000), L = 10, seed 1000, mesh 32^3, order 8, r_c 3.0, "
+                                   "LJ eps 1 sigma 0.9 r_cut 2.5, 1 eval + 100 NVE steps (dt 0.002), list r_c + 0.4 "
+                                   "rebuilt every 10 steps"},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def run_water(args):
+    """The water-like accuracy sweep (32,768 rigid three-site molecules,
+    98,304 charges, no exclusions, r_c 0.9 nm): for each target (1e-3, 1e-5,
+    1e-7 with supports 6, 8, 10) the planner's mesh, one evaluation timed
+    in FP32 (library pair list) and in FP64 (list from the FP32 builder),
+    and its force and energy error against FP64 Ewald (oracle/ewald_torch.py
+    as the checker, outside the timed region). A step = one evaluation."""
+    import torch
+    from esp_hoomd_b200 import native, systems
+    from esp_hoomd_b200._lib import ESP_ALL
+    from oracle.ewald_torch import ewald_torch
+    dev = torch.device("cuda", 0)
+    w = systems.water(32768, seed=1003)
+    N = w.N
+    posd = w.pos.astype(np.float32).astype(np.float64)
+    E0, F0, _ = ewald_torch(posd, w.q, w.box, device=dev)
+    p4 = np.zeros((N, 4))
+    p4[:, :3] = posd
+    rows = []
+    for target, order in ((1e-3, 6), (1e-5, 8), (1e-7, 10)):
+        for prec in (0, 1):
+            params = native.make_params(order=order, rcut=0.9, target_error=target, precision=prec)
+            b = native.Batch(params, [N], [w.box])
+            if prec == 0:
+                pos = torch.tensor(p4, dtype=torch.float32, device=dev)
+                q = torch.tensor(w.q.astype(np.float32), device=dev)
+                force = torch.zeros((N, 4), device=dev)
+                b.build_pairlist(pos, 0.9, 1024)
+
+                def ev():
+                    b.compute(pos, q, force, energy, None, nlist=None, flags=ESP_ALL)
+            else:
+                b32 = native.Batch(native.make_params(order=order, rcut=0.9, target_error=target), [N], [w.box])
+                pos = torch.tensor(p4, dtype=torch.float64, device=dev)
+                q = torch.tensor(w.q, dtype=torch.float64, device=dev)
+                force = torch.zeros((N, 4), dtype=torch.float64, device=dev)
+                head = torch.zeros(N, dtype=torch.int32, device=dev)
+                nn = torch.zeros_like(head)
+                nl = torch.zeros(N * 1024, dtype=torch.int32, device=dev)
+                b32.build_nlist(pos.float(), 0.9, 1024, head, nn, nl)
+                b32.nlist_check()
+
+                def ev():
+                    b.compute_f64(pos, q, force, energy, None, nlist=(head, nn, nl))
+            energy = torch.zeros(1, dtype=torch.float64, device=dev)
+            # warm-up: at least W evaluations and half a second (clocks settle)
+            t0, k = time.perf_counter(), 0
+            while k < max(3, args.warmup) or time.perf_counter() - t0 < 0.5:
+                ev()
+                torch.cuda.synchronize()
+                k += 1
+            st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            st.record()
+            for _ in range(args.steps):
+                ev()
+            en.record()
+            torch.cuda.synchronize()
+            ms = st.elapsed_time(en) / args.steps
+            f = force.double().cpu().numpy()[:, :3]
+            err = float(np.sqrt(((f - F0) ** 2).sum() / (F0 ** 2).sum()))
+            inf = b.info(0)
+            rows.append({"target": target, "order": order, "precision": "f64" if prec else "f32",
+                         "mesh": [inf["nx"], inf["ny"], inf["nz"]], "ms_per_eval": ms,
+                         "particle_evals_per_s": N / (ms * 1e-3), "force_rel_rms": err,
+                         "energy_rel": abs(energy.item() - E0) / abs(E0)})
+            del b
+    line = {"metric": "particle-evals/s and error vs FP64 Ewald (C3: water accuracy sweep)",
+            "value": rows[2]["particle_evals_per_s"], "unit": "particle-evals/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": max(3, args.warmup), "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "c3: 32,768 rigid three-site molecules (98,304 charges), seed 1003, r_c 0.9 nm, "
+                                   "no exclusions; value = the 1e-5 FP32 row"},
+            "rows": rows}
+    print(json.dumps(line), flush=True)
+
+
 def run_scaleup(args):
     """The plain one-system path at the scale-up size: 10^6 rock-salt ions
     (100^3 lattice, L = 100, mesh 200^3, support 8, r_c 3.0, 1e-5 target).
@@ -764,8 +909,9 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP64 Ewald check of the timed plan")
     ap.add_argument("--systems", type=int, default=N_SYS,
                     help="evaluate only the first S systems of the batch (small cases for profiling)")
-    ap.add_argument("--workload", default="batched256", choices=["batched256", "scaleup"],
-                    help="scaleup: the plain path on one 10^6-particle system (a second measurement)")
+    ap.add_argument("--workload", default="batched256", choices=["batched256", "scaleup", "c1", "water"],
+                    help="second measurements: scaleup (the plain path on one 10^6-particle system), c1 (FP64 "
+                         "plain case with LJ, 100 NVE steps), water (the C3 accuracy sweep)")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default plan)")
     ap.add_argument("--hoomd-list", action="store_true",
@@ -779,6 +925,10 @@ def main():
         run_reference(args)
     elif args.workload == "scaleup":
         run_scaleup(args)
+    elif args.workload == "c1":
+        run_c1(args)
+    elif args.workload == "water":
+        run_water(args)
     else:
         run_ours(args)
 
