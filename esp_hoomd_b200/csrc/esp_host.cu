@@ -250,7 +250,6 @@ struct StageTimer {
 struct esp_batch {
     esp_params prm{};
     int P = 8, T = 8, D = 10, tpp = 8, PX = 0, PP = 0;
-    int n_sm = 0;  // SMs of the device (CTAs per tile: tile_split_for)
     int nsys = 0, totN = 0, n_tiles = 0;
     std::vector<int> N;
     std::vector<double> box;
@@ -423,11 +422,6 @@ struct esp_batch {
 };
 
 int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* boxes, const int* mesh_) {
-    if (n_sm == 0) {
-        int dev = 0;
-        ESPB_CK(cudaGetDevice(&dev));
-        ESPB_CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-    }
     mem.release();
     mem64.release();
     f64 = false;
@@ -871,7 +865,6 @@ LaunchArgs esp_batch::args() const {
     a.n_pchunks = n_pchunks;
     a.tile_sys = d_tile_sys;
     a.n_tiles = n_tiles;
-    a.tile_split = tile_split_for(n_tiles, n_sm);
     a.tile_count = d_tcount;
     a.tile_start = d_tstart;
     a.posq = d_posq;

@@ -27,25 +27,6 @@
 
 namespace espb {
 
-// The particles one CTA of a tile kernel (spreading, interpolation) takes:
-// tile blockIdx.x / split, part blockIdx.x % split of its sorted particles.
-// split > 1 when a plan has too few tiles to fill the GPU (one small mesh):
-// each part is processed as a tile of its own (spreading flushes each part's
-// region separately).
-struct TilePart {
-    int t;
-    uint32_t s0;
-    int np;
-};
-
-__device__ __forceinline__ TilePart tile_part(const uint32_t* __restrict__ start, int split) {
-    const int t = (int)blockIdx.x / split, part = (int)blockIdx.x - t * split;
-    const uint32_t b = start[t], n = start[t + 1] - b;
-    const uint32_t per = (n + (uint32_t)split - 1u) / (uint32_t)split;
-    const uint32_t lo = min(n, (uint32_t)part * per), hi = min(n, lo + per);
-    return {t, b + lo, (int)(hi - lo)};
-}
-
 // ============================================================================
 // a1: bin + stable sort
 // ============================================================================
@@ -276,13 +257,12 @@ template <int P>
 __global__ void __launch_bounds__(SpreadCfg<P>::THREADS)
     k_spread(const int* __restrict__ tile_sys, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
              int T, int D, const uint32_t* __restrict__ start, const float4* __restrict__ srec,
-             const uint32_t* __restrict__ srel, double* __restrict__ rho, int split) {
+             const uint32_t* __restrict__ srel, double* __restrict__ rho) {
     using C = SpreadCfg<P>;
     extern __shared__ float4 smem4[];
-    const TilePart tp = tile_part(start, split);
-    const int t = tp.t;
-    const uint32_t s0 = tp.s0;
-    const int np = tp.np;
+    const int t = blockIdx.x;
+    const uint32_t s0 = start[t];
+    const int np = (int)(start[t + 1] - s0);
     if (np == 0) return;
     const int si = tile_sys[t];
     const SysDev S = sys[si];
@@ -398,13 +378,11 @@ template <int P>
 __global__ void __launch_bounds__(256)
     k_spread_dense(const int* __restrict__ tile_sys, const SysDev* __restrict__ sys,
                    const ParamSet* __restrict__ psets, int T, int D, const uint32_t* __restrict__ start,
-                   const float4* __restrict__ srec, const uint32_t* __restrict__ srel, double* __restrict__ rho,
-                   int split) {
+                   const float4* __restrict__ srec, const uint32_t* __restrict__ srel, double* __restrict__ rho) {
     extern __shared__ float4 smd4[];
-    const TilePart tp = tile_part(start, split);
-    const int t = tp.t;
-    const uint32_t s0 = tp.s0;
-    const int np = tp.np;
+    const int t = blockIdx.x;
+    const uint32_t s0 = start[t];
+    const int np = (int)(start[t + 1] - s0);
     if (np == 0) return;
     const int si = tile_sys[t];
     const SysDev S = sys[si];
@@ -542,16 +520,15 @@ template <int P>
 __global__ void __launch_bounds__(256, 4)
     k_spread_mma(const int* __restrict__ tile_sys, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
                  int T, int D, const uint32_t* __restrict__ start, const float4* __restrict__ srec,
-                 const uint32_t* __restrict__ srel, double* __restrict__ rho, int split) {
+                 const uint32_t* __restrict__ srel, double* __restrict__ rho) {
     extern __shared__ float4 smm4[];
     // per k-step of the chunk: the tile rows Y that carry stencil weight
     // (particles are sorted by y origin inside a tile, so most k-steps touch
     // half of the 16 rows; a warp skips the k-steps that miss its two rows)
     __shared__ int ks_lo[SPREAD_CHM / 8], ks_hi[SPREAD_CHM / 8];
-    const TilePart tp = tile_part(start, split);
-    const int t = tp.t;
-    const uint32_t s0 = tp.s0;
-    const int np = tp.np;
+    const int t = blockIdx.x;
+    const uint32_t s0 = start[t];
+    const int np = (int)(start[t + 1] - s0);
     if (np == 0) return;
     const int si = tile_sys[t];
     const SysDev S = sys[si];
@@ -1455,15 +1432,14 @@ __global__ void __launch_bounds__(128, 6)
              int T, int D, int PX, int PP, const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
              const float4* __restrict__ srec, const uint32_t* __restrict__ srel, const float* __restrict__ phi,
              float4* __restrict__ force, double* __restrict__ acc, const CUtensorMap* __restrict__ tmaps,
-             int* __restrict__ kerr, int split) {
+             int* __restrict__ kerr) {
     using C = InterpCfg<P>;
     extern __shared__ float4 sm4[];
     __shared__ double red[32];
     __shared__ __align__(8) uint64_t mbar;
-    const TilePart tp = tile_part(start, split);
-    const int t = tp.t;
-    const uint32_t s0 = tp.s0;
-    const int np = tp.np;
+    const int t = blockIdx.x;
+    const uint32_t s0 = start[t];
+    const int np = (int)(start[t + 1] - s0);
     if (np == 0) return;
     const int si = tile_sys[t];
     const SysDev S = sys[si];
@@ -1975,17 +1951,14 @@ static cudaError_t launch_spread_p(const LaunchArgs& a, cudaStream_t st) {
     }
     if (a.n_tiles == 0) return cudaSuccess;
     if (mma)
-        k_spread_mma<P><<<a.n_tiles * a.tile_split, 256, smem_m, st>>>(a.tile_sys, a.sys, a.psets, a.T, a.D,
-                                                                       a.tile_start, a.srec, a.srel, a.rho,
-                                                                       a.tile_split);
+        k_spread_mma<P><<<a.n_tiles, 256, smem_m, st>>>(a.tile_sys, a.sys, a.psets, a.T, a.D, a.tile_start, a.srec,
+                                                        a.srel, a.rho);
     else if (dense)
-        k_spread_dense<P><<<a.n_tiles * a.tile_split, 256, smem_d, st>>>(a.tile_sys, a.sys, a.psets, a.T, a.D,
-                                                                         a.tile_start, a.srec, a.srel, a.rho,
-                                                                         a.tile_split);
+        k_spread_dense<P><<<a.n_tiles, 256, smem_d, st>>>(a.tile_sys, a.sys, a.psets, a.T, a.D, a.tile_start, a.srec,
+                                                          a.srel, a.rho);
     else
-        k_spread<P><<<a.n_tiles * a.tile_split, C::THREADS, smem, st>>>(a.tile_sys, a.sys, a.psets, a.T, a.D,
-                                                                         a.tile_start, a.srec, a.srel, a.rho,
-                                                                         a.tile_split);
+        k_spread<P><<<a.n_tiles, C::THREADS, smem, st>>>(a.tile_sys, a.sys, a.psets, a.T, a.D, a.tile_start, a.srec,
+                                                          a.srel, a.rho);
     return cudaGetLastError();
 }
 
@@ -2046,13 +2019,13 @@ static cudaError_t launch_interp_p(const LaunchArgs& a, cudaStream_t st) {
         return cudaGetLastError();
     }
     if (tma)
-        k_interp<P, kTmaForm><<<a.n_tiles * a.tile_split, C::THREADS, interp_smem<P>(E, PP), st>>>(
+        k_interp<P, kTmaForm><<<a.n_tiles, C::THREADS, interp_smem<P>(E, PP), st>>>(
             a.tile_sys, a.sys, a.psets, a.T, a.D, PX, PP, a.tile_start, a.perm, a.srec, a.srel, a.phi, a.force, a.acc,
-            reinterpret_cast<const CUtensorMap*>(a.tmaps), a.kerr, a.tile_split);
+            reinterpret_cast<const CUtensorMap*>(a.tmaps), a.kerr);
     else
-        k_interp<P, false><<<a.n_tiles * a.tile_split, C::THREADS, interp_smem<P>(E, PP), st>>>(
+        k_interp<P, false><<<a.n_tiles, C::THREADS, interp_smem<P>(E, PP), st>>>(
             a.tile_sys, a.sys, a.psets, a.T, a.D, PX, PP, a.tile_start, a.perm, a.srec, a.srel, a.phi, a.force, a.acc,
-            nullptr, a.kerr, a.tile_split);
+            nullptr, a.kerr);
     return cudaGetLastError();
 }
 

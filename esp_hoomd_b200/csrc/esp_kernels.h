@@ -58,9 +58,6 @@ struct LaunchArgs {
     int n_pchunks = 0;
     const int* tile_sys = nullptr;
     int n_tiles = 0;
-    // CTAs per tile in spreading and interpolation (tile_part): > 1 when the
-    // plan has too few tiles to fill the GPU
-    int tile_split = 1;
     uint32_t* tile_count = nullptr;
     uint32_t* tile_start = nullptr;
     const float4* pos_in = nullptr;
@@ -123,14 +120,6 @@ struct LaunchArgs {
     const uint32_t* ex_list = nullptr;
     int ex_pitch = 0;
 };
-
-// CTAs per tile so that spreading and interpolation launch about four CTAs
-// per SM even for a single small mesh (at most 16 parts per tile)
-inline int tile_split_for(int n_tiles, int n_sm) {
-    if (n_tiles <= 0 || n_sm <= 0) return 1;
-    const int s = (4 * n_sm + n_tiles - 1) / n_tiles;
-    return s < 1 ? 1 : (s > 16 ? 16 : s);
-}
 
 cudaError_t launch_scan(const uint32_t* cnt, uint32_t* start, int n, cudaStream_t st);
 cudaError_t launch_scatter(const int2* chunks, int n_chunks, const SysDev* sys, const uint32_t* key,

@@ -203,7 +203,6 @@ struct esp_server {
     std::vector<double2> geos;
     static constexpr int MAX_GEOS = 16;
     long long ritem_cap = 0;
-    int n_sm = 0;  // SMs of the device (CTAs per tile: tile_split_for)
     long long chunk_cap = 0, pchunk_cap = 0;
     static constexpr long long ITEM_CAP = 1 << 20;
 
@@ -259,11 +258,6 @@ int esp_server::init(const esp_server_config& cfg) {
     if (cfg.hbm_budget < (256LL << 20)) return fail(ESP_ERR_INVALID, "hbm_budget must be at least 256 MB");
     max_slots = cfg.max_systems;
     max_particles = cfg.max_particles;
-    {
-        int dev = 0;
-        ESPB_CK(cudaGetDevice(&dev));
-        ESPB_CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-    }
     tpp = prm.threads_per_particle ? prm.threads_per_particle : 4;
     if (tpp != 4 && tpp != 8 && tpp != 16 && tpp != 32)
         return fail(ESP_ERR_UNSUPPORTED, "threads_per_particle must be 4, 8, 16 or 32");
@@ -742,7 +736,6 @@ int esp_server::launch_round(Staging& sg) {
     a.n_pchunks = (int)pchunks.size();
     a.tile_sys = d_tile_sys;
     a.n_tiles = (int)talloc.high();
-    a.tile_split = tile_split_for(a.n_tiles, n_sm);
     a.tile_count = d_tcount;
     a.tile_start = d_tstart;
     a.pos_in = d_pos;
