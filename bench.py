@@ -525,13 +525,21 @@ def run_water(args):
             en.record()
             torch.cuda.synchronize()
             ms = st.elapsed_time(en) / args.steps
+            stages = None
+            if prec == 0:
+                # per-stage times of two more evaluations (stage timer; the pair term not forked)
+                b.set_timing(True)
+                for _ in range(2):
+                    ev()
+                stages = {k: v[0] / v[1] for k, v in b.stage_times().items() if v[1] > 0}
+                b.set_timing(False)
             f = force.double().cpu().numpy()[:, :3]
             err = float(np.sqrt(((f - F0) ** 2).sum() / (F0 ** 2).sum()))
             inf = b.info(0)
             rows.append({"target": target, "order": order, "precision": "f64" if prec else "f32",
                          "mesh": [inf["nx"], inf["ny"], inf["nz"]], "ms_per_eval": ms,
                          "particle_evals_per_s": N / (ms * 1e-3), "force_rel_rms": err,
-                         "energy_rel": abs(energy.item() - E0) / abs(E0)})
+                         "energy_rel": abs(energy.item() - E0) / abs(E0), "stage_ms": stages})
             del b
     line = {"metric": "particle-evals/s and error vs FP64 Ewald (C3: water accuracy sweep)",
             "value": rows[2]["particle_evals_per_s"], "unit": "particle-evals/s", "n_gpus": 1, "steps": args.steps,
