@@ -223,7 +223,8 @@ int esp_batch_compute_f64(esp_batch* b, void* stream, const double* pos4, const 
  * evaluations (flags as esp_batch_compute) of candidate plans on the given
  * inputs with CUDA events on `stream` -- pair lanes per particle (4, 8, 16),
  * tile edge (the 16^3 tensor-core tile and smaller dense tiles), FFT pass form
- * (whole planes/slabs in shared memory or per-line passes) -- by coordinate
+ * (whole planes/slabs in shared memory or per-line passes), TMA interpolation
+ * form (one CTA per tile or persistent CTAs on a tile queue) -- by coordinate
  * descent, keeps the fastest plan (same meshes and accuracy) and writes its
  * parameters to `chosen` (may be NULL) and the per-candidate times (ms per
  * evaluation, up to `max_trials`) to `trial_ms` (may be NULL). Synchronises
