@@ -171,4 +171,21 @@ struct SegPoly {
     }
 };
 
+// Launch FN<P> for a stencil order known at run time (2..ESP_MAX_ORDER).
+#define ESPB_DISPATCH_P(FN, P_, ...)                 \
+    switch (P_) {                                    \
+        case 2: return FN<2>(__VA_ARGS__);           \
+        case 3: return FN<3>(__VA_ARGS__);           \
+        case 4: return FN<4>(__VA_ARGS__);           \
+        case 5: return FN<5>(__VA_ARGS__);           \
+        case 6: return FN<6>(__VA_ARGS__);           \
+        case 7: return FN<7>(__VA_ARGS__);           \
+        case 8: return FN<8>(__VA_ARGS__);           \
+        case 9: return FN<9>(__VA_ARGS__);           \
+        case 10: return FN<10>(__VA_ARGS__);         \
+        case 11: return FN<11>(__VA_ARGS__);         \
+        case 12: return FN<12>(__VA_ARGS__);         \
+        default: return cudaErrorInvalidValue;       \
+    }
+
 }  // namespace espb

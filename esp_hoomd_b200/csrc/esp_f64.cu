@@ -1,18 +1,25 @@
 // FP64 mode of the ESP path: every stage in double precision, for HOOMD
 // double builds (Scalar4 = double4 positions and forces) and for accuracy
-// targets below the FP32 floor (~1e-7). Same algorithm and data layout as
-// the FP32 kernels:
+// targets below the FP32 floor (~1e-7). Same algorithm, tiles and sorted
+// order as the FP32 kernels:
 //   k64_bin / k64_tile_sort : tile keys (shared sort kernels) with FP64
 //                             stencil records;
-//   k64_spread              : one CTA per tile, FP64 accumulation of the
-//                             tile's extended region in shared memory, one
-//                             FP64 atomic per region point into the mesh;
+//   k64_spread              : one CTA per tile, each thread summing one row
+//                             of the tile's extended region in registers over
+//                             the staged particles (no atomics inside the
+//                             tile), one FP64 atomic per region point into the
+//                             mesh;
 //   k64_fft_pass            : one warp per mesh line, mixed-radix Stockham in
 //                             shared memory on the full complex spectrum; the
 //                             z pass multiplies by the influence table and
 //                             accumulates the k-space energy and virial;
-//   k64_interp, k64_pair, k64_exclusions : as the FP32 kernels, in FP64.
+//   k64_interp              : one CTA per tile, the tile's potential region
+//                             staged in shared memory, eight lanes per
+//                             particle over the stencil rows;
+//   k64_pair, k64_exclusions : as the FP32 kernels, in FP64.
 // Reference stages: src/ESPForceComputeGPU.cu:157-471 (K1-K7).
+#include <algorithm>
+
 #include "esp_common.cuh"
 #include "esp_kernels.h"
 
@@ -110,132 +117,235 @@ __device__ __forceinline__ double dhorner64(const double* c, int D, double t) {
 }
 
 // ----------------------------------------------------------------------------
-// spreading: one CTA per tile, shared FP64 region [E]^3 (E = T + P - 1),
-// one warp per particle (lanes over the P^3 stencil), FP64 shared atomics
+// spreading: one CTA per tile (several when the tiles are few, each over a
+// share of the tile's particle chunks); every thread owns one row (z, y) of
+// the tile's extended region [E]^3 (E = T + P - 1) and sums it in registers, 16 points
+// along x at a time. The tile's particles are staged K64S_CH at a time: per
+// particle its x weights times q as a 16-point row segment pre-shifted to its
+// stencil origin (zero elsewhere), its y and z weights and its origin. A
+// thread adds, in particle order, every staged particle whose stencil covers
+// its row: a broadcast read of the segment and 16 FMAs, no atomics, and a
+// CTA's sums are deterministic. Row r = (r / E, r % E), so with E = 16 and 256
+// threads a warp owns two z planes and the coverage test is nearly
+// warp-uniform. The finished rows pass through shared memory (rows padded to
+// an odd stride) so that the flush, one FP64 atomic per nonzero region point,
+// is coalesced along x.
 // ----------------------------------------------------------------------------
-constexpr int K64_WARPS = 8;
+// Mesh offsets of a tile's extended region [E]^3 with the periodic wrap:
+// roff[r] = (gz ny + gy) nx for region row r = (z, y) = (r / E, r % E), xo[x] = gx.
+__device__ __forceinline__ void region_tables(const SysDev& S, int X0, int Y0, int Z0, int E, int* roff, int* xo) {
+    for (int r = threadIdx.x; r < E * E; r += blockDim.x) {
+        int gy = Y0 + r % E, gz = Z0 + r / E;
+        while (gy >= S.ny) gy -= S.ny;
+        while (gz >= S.nz) gz -= S.nz;
+        roff[r] = (gz * S.ny + gy) * S.nx;
+    }
+    for (int x = threadIdx.x; x < E; x += blockDim.x) {
+        int gx = X0 + x;
+        while (gx >= S.nx) gx -= S.nx;
+        xo[x] = gx;
+    }
+}
 
-__global__ void __launch_bounds__(K64_WARPS * 32)
+constexpr int K64S_THREADS = 256;
+constexpr int K64S_CH = 48;   // particles staged per pass
+constexpr int K64S_SEG = 16;  // register row segment along x
+
+__host__ __device__ inline int spread64_stride(int E) { return E | 1; }
+// region doubles, rounded up to an even count so that the x segments after it are 16-byte aligned
+__host__ __device__ inline size_t spread64_region(int E) { return ((size_t)E * E * spread64_stride(E) + 1) & ~(size_t)1; }
+
+__global__ void __launch_bounds__(K64S_THREADS)
     k64_spread(const int* __restrict__ tile_sys, const SysDev* __restrict__ sys, const double* __restrict__ wcoef,
                int P, int T, int D, const uint32_t* __restrict__ start, const double4* __restrict__ srec,
                const uint32_t* __restrict__ srel, double* __restrict__ rho) {
-    extern __shared__ double sreg[];  // [E^3] region, then [K64_WARPS][3 * MAX_P] weights
+    // [E^2][ES] region | [K64S_CH][K64S_SEG] x segments | [K64S_CH][2P] y, z weights | [P][D+1] window
+    // | [K64S_CH] origins | row and column offsets
+    extern __shared__ double sreg[];
     const int t = blockIdx.x;
     const uint32_t s0 = start[t];
     const int np = (int)(start[t + 1] - s0);
     if (np == 0) return;
     const SysDev S = sys[tile_sys[t]];
-    const int E = T + P - 1, E3 = E * E * E;
-    double* wts = sreg + E3;
-    for (int k = threadIdx.x; k < E3; k += blockDim.x) sreg[k] = 0.0;
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double* W = wts + warp * 3 * MAX_P;
-    for (int p = warp; p < np; p += K64_WARPS) {
-        const double4 rec = srec[s0 + p];
-        const uint32_t rl = srel[s0 + p];
-        if (lane < 3 * P) {
-            const int ax = lane / P, a = lane - ax * P;
-            const double tt = ax == 0 ? rec.x : (ax == 1 ? rec.y : rec.z);
-            W[lane] = horner64(wcoef + a * (D + 1), D, tt) * (ax == 0 ? rec.w : 1.0);
+    const int E = T + P - 1, ES = spread64_stride(E), E2 = E * E, D1 = D + 1;
+    double* xs = sreg + spread64_region(E);
+    double* yz = xs + K64S_CH * K64S_SEG;
+    double* wc = yz + K64S_CH * 2 * P;
+    uint32_t* org = reinterpret_cast<uint32_t*>(wc + P * D1);
+    for (int k = threadIdx.x; k < P * D1; k += blockDim.x) wc[k] = wcoef[k];
+    const int nseg = (E + K64S_SEG - 1) / K64S_SEG;
+    for (int rb = 0; rb < E2; rb += blockDim.x) {
+        const int r = rb + threadIdx.x;
+        const bool own = r < E2;
+        const int z = r / E, y = r - z * E;
+        for (int seg = 0; seg < nseg; ++seg) {
+            const int x0 = seg * K64S_SEG;
+            double acc[K64S_SEG];
+#pragma unroll
+            for (int j = 0; j < K64S_SEG; ++j) acc[j] = 0.0;
+            // CTA blockIdx.y of gridDim.y takes every gridDim.y-th chunk
+            for (int p0 = blockIdx.y * K64S_CH; p0 < np; p0 += gridDim.y * K64S_CH) {
+                const int m = min(K64S_CH, np - p0);
+                __syncthreads();  // window staged / previous chunk consumed
+                for (int k = threadIdx.x; k < m * K64S_SEG; k += blockDim.x) {
+                    const int pp = k / K64S_SEG, a = x0 + (k - pp * K64S_SEG) - (int)(srel[s0 + p0 + pp] & 255u);
+                    double v = 0.0;
+                    if ((unsigned)a < (unsigned)P) {
+                        const double4 rec = srec[s0 + p0 + pp];
+                        v = horner64(wc + a * D1, D, rec.x) * rec.w;
+                    }
+                    xs[k] = v;
+                }
+                for (int k = threadIdx.x; k < m * 2 * P; k += blockDim.x) {
+                    const int pp = k / (2 * P), l = k - pp * 2 * P, a = l < P ? l : l - P;
+                    const double4 rec = srec[s0 + p0 + pp];
+                    yz[k] = horner64(wc + a * D1, D, l < P ? rec.y : rec.z);
+                }
+                for (int k = threadIdx.x; k < m; k += blockDim.x) org[k] = srel[s0 + p0 + k];
+                __syncthreads();
+                if (own)
+                    for (int pp = 0; pp < m; ++pp) {
+                        const uint32_t rl = org[pp];
+                        const int b = y - (int)((rl >> 8) & 255u), c = z - (int)((rl >> 16) & 255u);
+                        if ((unsigned)b < (unsigned)P && (unsigned)c < (unsigned)P) {
+                            const double cw = yz[pp * 2 * P + b] * yz[pp * 2 * P + P + c];
+                            const double2* xr = reinterpret_cast<const double2*>(xs + pp * K64S_SEG);
+#pragma unroll
+                            for (int j = 0; j < K64S_SEG / 2; ++j) {
+                                const double2 v = xr[j];
+                                acc[2 * j] = fma(v.x, cw, acc[2 * j]);
+                                acc[2 * j + 1] = fma(v.y, cw, acc[2 * j + 1]);
+                            }
+                        }
+                    }
+            }
+            if (own) {
+                double* row = sreg + (size_t)r * ES + x0;
+#pragma unroll
+                for (int j = 0; j < K64S_SEG; ++j)
+                    if (x0 + j < E) row[j] = acc[j];
+            }
         }
-        __syncwarp();
-        const int ox = rl & 255, oy = (rl >> 8) & 255, oz = (rl >> 16) & 255;
-        const int P3 = P * P * P;
-        for (int k = lane; k < P3; k += 32) {
-            const int a = k % P, b = (k / P) % P, c = k / (P * P);
-            atomicAdd(&sreg[((oz + c) * E + (oy + b)) * E + ox + a], W[a] * W[P + b] * W[2 * P + c]);
-        }
-        __syncwarp();
     }
-    __syncthreads();
     const int lt = t - S.t_off;
     const int X0 = (lt % S.ntx) * T, Y0 = ((lt / S.ntx) % S.nty) * T, Z0 = (lt / (S.ntx * S.nty)) * T;
-    for (int k = threadIdx.x; k < E3; k += blockDim.x) {
-        const double v = sreg[k];
-        if (v == 0.0) continue;
-        int gx = X0 + k % E, gy = Y0 + (k / E) % E, gz = Z0 + k / (E * E);
-        while (gx >= S.nx) gx -= S.nx;
-        while (gy >= S.ny) gy -= S.ny;
-        while (gz >= S.nz) gz -= S.nz;
-        atomicAdd(&rho[S.m_off + ((long long)gz * S.ny + gy) * S.nx + gx], v);
+    int* roff = reinterpret_cast<int*>(org + K64S_CH);
+    int* xo = roff + E2;
+    region_tables(S, X0, Y0, Z0, E, roff, xo);
+    __syncthreads();
+    double* mesh = rho + S.m_off;
+    // element (r, x) stepped by the block size: consecutive threads along x
+    const int dr = blockDim.x / E, dx = blockDim.x - dr * E;
+    for (int x = threadIdx.x % E, r = threadIdx.x / E; r < E2;) {
+        const double v = sreg[(size_t)r * ES + x];
+        if (v != 0.0) atomicAdd(&mesh[roff[r] + xo[x]], v);
+        x += dx;
+        r += dr;
+        if (x >= E) {
+            x -= E;
+            ++r;
+        }
     }
 }
 
 // ----------------------------------------------------------------------------
-// FFT: one warp per line, Stockham autosort, radices 2/3/4/5 from the packed
-// plan; tw = exp(-2 pi i t / n) (the forward sign), conjugated for inverse
+// FFT: one warp per line, Stockham autosort in shared memory, radices
+// 2/3/4/5 from the packed plan (one register-resident butterfly per radix);
+// tw = exp(-2 pi i t / n) (the forward sign), staged in shared memory per CTA
+// and conjugated for the inverse. A CTA transforms F64_WARPS neighbouring
+// lines of one system; the strided (y, z) passes load and store them
+// cooperatively, the F64_WARPS lines' elements adjacent in memory.
 // ----------------------------------------------------------------------------
 __device__ __forceinline__ double2 z_mul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+__device__ __forceinline__ double2 z_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 z_sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+// s * i * a for s = +-1
+__device__ __forceinline__ double2 z_rot(double2 a, double s) { return make_double2(-s * a.y, s * a.x); }
 
-// R-point DFT in place, sign -1 forward / +1 inverse.
-__device__ __forceinline__ void dft_small(double2* v, int R, int sign) {
+// R-point DFT in registers, y_k = sum_r v_r exp(sign 2 pi i r k / R)
+template <int R>
+__device__ __forceinline__ void dft64(double2 (&v)[R], double s);
+template <>
+__device__ __forceinline__ void dft64<2>(double2 (&v)[2], double) {
+    const double2 a = v[0], b = v[1];
+    v[0] = z_add(a, b);
+    v[1] = z_sub(a, b);
+}
+template <>
+__device__ __forceinline__ void dft64<4>(double2 (&v)[4], double s) {
+    const double2 ac = z_add(v[0], v[2]), am = z_sub(v[0], v[2]);
+    const double2 bd = z_add(v[1], v[3]), jb = z_rot(z_sub(v[1], v[3]), s);
+    v[0] = z_add(ac, bd);
+    v[1] = z_add(am, jb);
+    v[2] = z_sub(ac, bd);
+    v[3] = z_sub(am, jb);
+}
+template <>
+__device__ __forceinline__ void dft64<3>(double2 (&v)[3], double s) {
+    constexpr double S3 = 0.86602540378443864676;  // sin(2 pi / 3)
+    const double2 t1 = z_add(v[1], v[2]);
+    const double2 m = make_double2(fma(-0.5, t1.x, v[0].x), fma(-0.5, t1.y, v[0].y));
+    const double2 r = z_rot(z_sub(v[1], v[2]), s * S3);
+    v[0] = z_add(v[0], t1);
+    v[1] = z_add(m, r);
+    v[2] = z_sub(m, r);
+}
+template <>
+__device__ __forceinline__ void dft64<5>(double2 (&v)[5], double s) {
+    constexpr double C1 = 0.30901699437494742410, S1 = 0.95105651629515357212;   // 2 pi / 5
+    constexpr double C2 = -0.80901699437494742410, S2 = 0.58778525229247312917;  // 4 pi / 5
+    const double2 a1 = z_add(v[1], v[4]), b1 = z_sub(v[1], v[4]);
+    const double2 a2 = z_add(v[2], v[3]), b2 = z_sub(v[2], v[3]);
+    const double2 p1 = make_double2(v[0].x + C1 * a1.x + C2 * a2.x, v[0].y + C1 * a1.y + C2 * a2.y);
+    const double2 p2 = make_double2(v[0].x + C2 * a1.x + C1 * a2.x, v[0].y + C2 * a1.y + C1 * a2.y);
+    const double2 q1 = z_rot(make_double2(S1 * b1.x + S2 * b2.x, S1 * b1.y + S2 * b2.y), s);
+    const double2 q2 = z_rot(make_double2(S2 * b1.x - S1 * b2.x, S2 * b1.y - S1 * b2.y), s);
+    v[0] = z_add(v[0], z_add(a1, a2));
+    v[1] = z_add(p1, q1);
+    v[4] = z_sub(p1, q1);
+    v[2] = z_add(p2, q2);
+    v[3] = z_sub(p2, q2);
+}
+
+// One Stockham stage of radix R: the R inputs of butterfly j are j + r n/R;
+// twiddle index r k (n / (Ns R)) < n with k = j mod Ns.
+template <int R>
+__device__ __forceinline__ void stage64(const double2* src, double2* dst, int n, int Ns, const double2* tw,
+                                        int sign, int lane) {
+    const int nb = n / R, step = n / (Ns * R);
     const double s = (double)sign;
-    if (R == 2) {
-        const double2 a = v[0], b = v[1];
-        v[0] = make_double2(a.x + b.x, a.y + b.y);
-        v[1] = make_double2(a.x - b.x, a.y - b.y);
-    } else if (R == 4) {
-        const double2 a = v[0], b = v[1], c = v[2], d = v[3];
-        const double2 ac = make_double2(a.x + c.x, a.y + c.y), am = make_double2(a.x - c.x, a.y - c.y);
-        const double2 bd = make_double2(b.x + d.x, b.y + d.y), bm = make_double2(b.x - d.x, b.y - d.y);
-        // multiply bm by (sign i): forward -i
-        const double2 jb = make_double2(-s * bm.y, s * bm.x);
-        v[0] = make_double2(ac.x + bd.x, ac.y + bd.y);
-        v[1] = make_double2(am.x + jb.x, am.y + jb.y);
-        v[2] = make_double2(ac.x - bd.x, ac.y - bd.y);
-        v[3] = make_double2(am.x - jb.x, am.y - jb.y);
-    } else {
-        // generic O(R^2) for R = 3, 5 with the exact roots of unity
-        const double c1 = R == 3 ? -0.5 : 0.30901699437494742410, s1 = R == 3 ? 0.86602540378443864676 : 0.95105651629515357212;
-        const double c2 = -0.80901699437494742410, s2 = 0.58778525229247312917;
-        double2 out[5];
-        for (int k = 0; k < R; ++k) {
-            double2 acc = make_double2(0.0, 0.0);
-            for (int r = 0; r < R; ++r) {
-                const int m = (r * k) % R;
-                double cr, sr;
-                if (m == 0) { cr = 1.0; sr = 0.0; }
-                else if (R == 3) { cr = c1; sr = m == 1 ? s1 : -s1; }
-                else if (m == 1 || m == 4) { cr = c1; sr = m == 1 ? s1 : -s1; }
-                else { cr = c2; sr = m == 2 ? s2 : -s2; }
-                // exp(sign * 2 pi i m / R) with the forward sign -1
-                const double2 w = make_double2(cr, s * sr);
-                acc.x += v[r].x * w.x - v[r].y * w.y;
-                acc.y += v[r].x * w.y + v[r].y * w.x;
+    for (int j = lane; j < nb; j += 32) {
+        const int k = j % Ns;
+        double2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = src[j + r * nb];
+        if (k > 0) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                double2 w = tw[r * k * step];
+                w.y *= -s;  // tw holds the forward (sign -1) roots
+                v[r] = z_mul(v[r], w);
             }
-            out[k] = acc;
         }
-        for (int k = 0; k < R; ++k) v[k] = out[k];
+        dft64<R>(v, s);
+        const int o = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) dst[o + r * Ns] = v[r];
     }
 }
 
 // Transforms the n points in a (scratch b); returns the buffer holding the result.
-__device__ double2* fft64_line(double2* a, double2* b, int n, uint32_t plan, const double2* __restrict__ tw,
-                               int sign, int lane) {
+__device__ double2* fft64_line(double2* a, double2* b, int n, uint32_t plan, const double2* tw, int sign, int lane) {
     int Ns = 1;
     double2 *src = a, *dst = b;
     for (uint32_t pl = plan; pl; pl >>= 4) {
         const int R = pl & 15;
-        const int nb = n / R;
-        const int step = n / (Ns * R);
-        for (int j = lane; j < nb; j += 32) {
-            const int k = j % Ns;
-            double2 v[5];
-            for (int r = 0; r < R; ++r) {
-                v[r] = src[j + r * nb];
-                if (r > 0 && k > 0) {
-                    double2 w = tw[(r * k * step) % n];
-                    if (sign > 0) w.y = -w.y;
-                    v[r] = z_mul(v[r], w);
-                }
-            }
-            dft_small(v, R, sign);
-            const int idxD = (j / Ns) * Ns * R + k;
-            for (int r = 0; r < R; ++r) dst[idxD + r * Ns] = v[r];
-        }
+        if (R == 4) stage64<4>(src, dst, n, Ns, tw, sign, lane);
+        else if (R == 2) stage64<2>(src, dst, n, Ns, tw, sign, lane);
+        else if (R == 3) stage64<3>(src, dst, n, Ns, tw, sign, lane);
+        else stage64<5>(src, dst, n, Ns, tw, sign, lane);
         __syncwarp();
         double2* x = src;
         src = dst;
@@ -256,6 +366,8 @@ __global__ void __launch_bounds__(F64_WARPS * 32)
                  double2* __restrict__ cbuf, double* __restrict__ rho, double* __restrict__ phi,
                  const double2* __restrict__ gtab, double* __restrict__ acc) {
     __shared__ double2 sb[F64_WARPS][2][FFT_MAX_N];
+    __shared__ double2 stw[FFT_MAX_N];
+    __shared__ long long lbase[F64_WARPS];
     __shared__ double red[32 * 7];
     const int2 it = items[blockIdx.x];
     const SysDev S = sys[it.x];
@@ -263,42 +375,53 @@ __global__ void __launch_bounds__(F64_WARPS * 32)
     constexpr int AX = (MODE == 0 || MODE == 4) ? 0 : (MODE == 1 || MODE == 3) ? 1 : 2;
     const int n = AX == 0 ? S.nx : (AX == 1 ? S.ny : S.nz);
     const long long nlines = AX == 0 ? (long long)S.ny * S.nz : (AX == 1 ? (long long)S.nx * S.nz : (long long)S.nx * S.ny);
-    const long long l = (long long)it.y + warp;
-    double e[7] = {0, 0, 0, 0, 0, 0, 0};
-    if (l < nlines) {
-        long long base, stride;
-        int lx = 0, ly = 0;
-        if (AX == 0) {
-            base = l * S.nx;
-            stride = 1;
-        } else if (AX == 1) {
-            const long long z = l / S.nx, x = l % S.nx;
-            base = z * S.nx * S.ny + x;
-            stride = S.nx;
-        } else {
-            ly = (int)(l / S.nx);
-            lx = (int)(l % S.nx);
-            base = (long long)ly * S.nx + lx;
-            stride = (long long)S.nx * S.ny;
+    const long long stride = AX == 0 ? 1 : (AX == 1 ? (long long)S.nx : (long long)S.nx * S.ny);
+    const uint32_t plan = AX == 0 ? S.radx : (AX == 1 ? S.rady : S.radz);
+    const double2* twa = tw + (AX == 0 ? S.twx : (AX == 1 ? S.twy : S.twz));
+    for (int k = threadIdx.x; k < n; k += blockDim.x) stw[k] = twa[k];
+    if (threadIdx.x < F64_WARPS) {
+        const long long l = (long long)it.y + threadIdx.x;
+        long long base = -1;
+        if (l < nlines) {
+            if (AX == 0) base = l * S.nx;
+            else if (AX == 1) base = (l / S.nx) * S.nx * S.ny + l % S.nx;
+            else base = l;  // (y, x) = (l / nx, l % nx): base y nx + x = l
         }
-        const uint32_t plan = AX == 0 ? S.radx : (AX == 1 ? S.rady : S.radz);
-        const double2* twa = tw + (AX == 0 ? S.twx : (AX == 1 ? S.twy : S.twz));
+        lbase[threadIdx.x] = base;
+    }
+    __syncthreads();
+    const long long l = (long long)it.y + warp;
+    const bool active = l < nlines;
+    // load: x lines one per warp (contiguous); y and z lines cooperatively,
+    // the F64_WARPS lines' elements at one k adjacent in memory
+    if (AX == 0) {
+        if (active)
+            for (int k = lane; k < n; k += 32) {
+                const long long g = S.m_off + lbase[warp] + k;
+                if (MODE == 0) {
+                    sb[warp][0][k] = make_double2(rho[g], 0.0);
+                    rho[g] = 0.0;
+                } else {
+                    sb[warp][0][k] = cbuf[g];
+                }
+            }
+    } else {
+        for (int idx = threadIdx.x; idx < F64_WARPS * n; idx += blockDim.x) {
+            const int w = idx % F64_WARPS, k = idx / F64_WARPS;
+            if (lbase[w] >= 0) sb[w][0][k] = cbuf[S.m_off + lbase[w] + k * stride];
+        }
+    }
+    __syncthreads();
+    double e[7] = {0, 0, 0, 0, 0, 0, 0};
+    double2* res = sb[warp][0];
+    if (active) {
         double2* a = sb[warp][0];
         double2* b = sb[warp][1];
-        for (int k = lane; k < n; k += 32) {
-            const long long g = S.m_off + base + k * stride;
-            if (MODE == 0) {
-                a[k] = make_double2(rho[g], 0.0);
-                rho[g] = 0.0;
-            } else {
-                a[k] = cbuf[g];
-            }
-        }
-        __syncwarp();
-        const int sign = (MODE <= 1) ? -1 : (MODE == 2 ? -1 : 1);
-        double2* r = fft64_line(a, b, n, plan, twa, sign, lane);
+        const int sign = MODE <= 2 ? -1 : 1;
+        res = fft64_line(a, b, n, plan, stw, sign, lane);
         if (MODE == 2) {
             // (kx, ky) = (lx, ly) after the x and y passes; kz along the line
+            const int ly = (int)(l / S.nx), lx = (int)(l % S.nx);
             const int nxh = S.nxh;
             const double tpx = 6.283185307179586 / S.Lxd, tpy = 6.283185307179586 / S.Lyd,
                          tpz = 6.283185307179586 / S.Lzd;
@@ -310,7 +433,7 @@ __global__ void __launch_bounds__(F64_WARPS * 32)
                 if (lx < nxh) gi = ((long long)kz * S.ny + ly) * nxh + lx;
                 else gi = ((long long)((S.nz - kz) % S.nz) * S.ny + (S.ny - ly) % S.ny) * nxh + (S.nx - lx);
                 const double2 g = gtab[S.g_off + gi];
-                const double2 v = r[kz];
+                const double2 v = res[kz];
                 const double a2 = v.x * v.x + v.y * v.y;
                 const double ek = 0.5 * g.x * a2, eb = 0.5 * g.y * a2;
                 const double kxv = tpx * fx, kyv = tpy * fy, kzv = tpz * fz;
@@ -321,16 +444,30 @@ __global__ void __launch_bounds__(F64_WARPS * 32)
                 e[4] += ek + eb * kyv * kyv;
                 e[5] += eb * kyv * kzv;
                 e[6] += ek + eb * kzv * kzv;
-                r[kz] = make_double2(v.x * g.x, v.y * g.x);
+                res[kz] = make_double2(v.x * g.x, v.y * g.x);
             }
             __syncwarp();
-            double2* o = (r == a) ? b : a;
-            r = fft64_line(r, o, n, plan, twa, +1, lane);
+            res = fft64_line(res, res == a ? b : a, n, plan, stw, +1, lane);
         }
-        for (int k = lane; k < n; k += 32) {
-            const long long g = S.m_off + base + k * stride;
-            if (MODE == 4) phi[g] = r[k].x;
-            else cbuf[g] = r[k];
+    }
+    if (AX == 0) {
+        if (active)
+            for (int k = lane; k < n; k += 32) {
+                const long long g = S.m_off + lbase[warp] + k;
+                if (MODE == 4) phi[g] = res[k].x;
+                else cbuf[g] = res[k];
+            }
+    } else {
+        // every line of the CTA has the same length and plan: its result sits
+        // in buffer (stages mod 2) of its warp (buffer 0 after the two
+        // transforms of the z pass)
+        int stages = 0;
+        for (uint32_t pl = plan; pl; pl >>= 4) ++stages;
+        const int rb = MODE == 2 ? 0 : (stages & 1);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < F64_WARPS * n; idx += blockDim.x) {
+            const int w = idx % F64_WARPS, k = idx / F64_WARPS;
+            if (lbase[w] >= 0) cbuf[S.m_off + lbase[w] + k * stride] = sb[w][rb][k];
         }
     }
     if (MODE == 2) {
@@ -341,114 +478,223 @@ __global__ void __launch_bounds__(F64_WARPS * 32)
 }
 
 // ----------------------------------------------------------------------------
-// interpolation: one thread per particle, potential, gradient and energy
+// interpolation: one CTA (or a few) per tile. The tile's extended potential region
+// [E]^3 (E = T + P - 1, periodic wrap) is staged in shared memory with
+// coalesced loads along x (rows padded to an odd stride of doubles), then the
+// tile's particles, in sorted order, are interpolated from it (by several
+// CTAs per tile when the tiles are few): K64I_G lanes
+// per particle (four particles per warp) share the P^2 stencil rows (y, z),
+// each row a run of P values along x read with the x weights held in
+// registers; potential, gradient and energy reduced over the particle's
+// lanes. The stencil records (t, q) and origins come from the sort.
 // ----------------------------------------------------------------------------
-__global__ void k64_interp(const int2* __restrict__ chunks, const SysDev* __restrict__ sys,
-                           const ParamSet* __restrict__ psets, const double* __restrict__ wcoef, int P, int D,
-                           const double4* __restrict__ posq, const double* __restrict__ phi,
-                           double4* __restrict__ force, double* __restrict__ acc) {
+constexpr int K64I_WARPS = 4;
+constexpr int K64I_G = 8;              // lanes per particle
+constexpr int K64I_PPW = 32 / K64I_G;  // particles per warp pass
+
+size_t interp64_smem(int P, int T) {
+    const int E = T + P - 1;
+    return ((size_t)E * E * spread64_stride(E) + (size_t)P * (MAX_D + 1)) * sizeof(double) +
+           (size_t)(E * E + E) * sizeof(int);
+}
+
+template <int P>
+__global__ void __launch_bounds__(K64I_WARPS * 32)
+    k64_interp(const int* __restrict__ tile_sys, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
+               const double* __restrict__ wcoef, int T, int D, const uint32_t* __restrict__ start,
+               const uint32_t* __restrict__ perm, const double4* __restrict__ srec,
+               const uint32_t* __restrict__ srel, const double* __restrict__ phi, double4* __restrict__ force,
+               double* __restrict__ acc) {
+    extern __shared__ double sreg[];  // [E^2][ES] potential region, [P][D+1] window, row and column offsets
     __shared__ double red[32];
-    const int2 ch = chunks[blockIdx.x];
-    const SysDev S = sys[ch.x];
-    const int i = ch.y + threadIdx.x;
-    double e1[1] = {0.0};
-    if (i < S.p_off + S.N) {
-        const double4 p = posq[i];
-        const double x[3] = {p.x, p.y, p.z};
-        const double gd[3] = {S.gxd, S.gyd, S.gzd};
-        const int n[3] = {S.nx, S.ny, S.nz};
-        double W[3][MAX_P], dW[3][MAX_P];
-        int idx[3][MAX_P];
-        for (int d = 0; d < 3; ++d) {
-            double g = x[d] * gd[d];
-            if (g >= n[d]) g -= n[d];
-            const int i0 = (int)floor(g - 0.5 * P) + 1;
-            const double tt = (double)i0 + 0.5 * P - g;
-            int v = i0 < 0 ? i0 + n[d] : (i0 >= n[d] ? i0 - n[d] : i0);
+    __shared__ double wsh[K64I_WARPS * K64I_PPW][6 * P];  // W x | y | z, then dW x | y | z
+    const int t = blockIdx.x;
+    const uint32_t s0 = start[t];
+    const int np = (int)(start[t + 1] - s0);
+    if (np == 0) return;
+    const int sid = tile_sys[t];
+    const SysDev S = sys[sid];
+    const int E = T + P - 1, ES = spread64_stride(E), E2 = E * E, D1 = D + 1;
+    double* wc = sreg + (size_t)E2 * ES;
+    for (int k = threadIdx.x; k < P * D1; k += blockDim.x) wc[k] = wcoef[k];
+    const int lt = t - S.t_off;
+    const int X0 = (lt % S.ntx) * T, Y0 = ((lt / S.ntx) % S.nty) * T, Z0 = (lt / (S.ntx * S.nty)) * T;
+    const double* ph = phi + S.m_off;
+    int* roff = reinterpret_cast<int*>(wc + P * (MAX_D + 1));
+    int* xo = roff + E2;
+    region_tables(S, X0, Y0, Z0, E, roff, xo);
+    __syncthreads();
+    // element (r, x) stepped by the block size: consecutive threads along x
+    const int dr = blockDim.x / E, dx = blockDim.x - dr * E;
+    for (int x = threadIdx.x % E, r = threadIdx.x / E; r < E2;) {
+        sreg[(size_t)r * ES + x] = ph[roff[r] + xo[x]];
+        x += dx;
+        r += dr;
+        if (x >= E) {
+            x -= E;
+            ++r;
+        }
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int sub = lane % K64I_G, slot = lane / K64I_G;
+    const double self = psets[S.pset].self_coef;
+    double* W = wsh[warp * K64I_PPW + slot];
+    double e_acc = 0.0;
+    // CTA blockIdx.y of gridDim.y takes every gridDim.y-th group of K64I_WARPS * K64I_PPW particles
+    for (int pb = (blockIdx.y * K64I_WARPS + warp) * K64I_PPW; pb < np; pb += gridDim.y * K64I_WARPS * K64I_PPW) {
+        const int pp = pb + slot;
+        const bool valid = pp < np;
+        const double4 rec = valid ? srec[s0 + pp] : make_double4(0.0, 0.0, 0.0, 0.0);
+        const uint32_t rl = valid ? srel[s0 + pp] : 0u;
+        if (valid)
+            for (int l = sub; l < 3 * P; l += K64I_G) {
+                const int d = l / P, a = l - d * P;
+                const double tt = d == 0 ? rec.x : (d == 1 ? rec.y : rec.z);
+                W[l] = horner64(wc + a * D1, D, tt);
+                W[3 * P + l] = dhorner64(wc + a * D1, D, tt);
+            }
+        __syncwarp();
+        double pot = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+        if (valid) {
+            double wx[P], dwx[P];
+#pragma unroll
             for (int a = 0; a < P; ++a) {
-                W[d][a] = horner64(wcoef + a * (D + 1), D, tt);
-                dW[d][a] = dhorner64(wcoef + a * (D + 1), D, tt);
-                idx[d][a] = v;
-                if (++v == n[d]) v = 0;
+                wx[a] = W[a];
+                dwx[a] = W[3 * P + a];
+            }
+            const double* base =
+                sreg + ((size_t)((rl >> 16) & 255u) * E + ((rl >> 8) & 255u)) * ES + (rl & 255u);
+            for (int r = sub; r < P * P; r += K64I_G) {
+                const int c = r / P, b = r - c * P;
+                const double* row = base + (size_t)(c * E + b) * ES;
+                double sv = 0.0, sd = 0.0;
+#pragma unroll
+                for (int a = 0; a < P; ++a) {
+                    const double v = row[a];
+                    sv = fma(wx[a], v, sv);
+                    sd = fma(dwx[a], v, sd);
+                }
+                const double wy = W[P + b], dwy = W[4 * P + b], wz = W[2 * P + c], dwz = W[5 * P + c];
+                pot = fma(wz * wy, sv, pot);
+                gx = fma(wz * wy, sd, gx);
+                gy = fma(wz * dwy, sv, gy);
+                gz = fma(dwz * wy, sv, gz);
             }
         }
-        const double* ph = phi + S.m_off;
-        double pot = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
-        for (int c = 0; c < P; ++c)
-            for (int b = 0; b < P; ++b) {
-                const double* row = ph + ((long long)idx[2][c] * S.ny + idx[1][b]) * S.nx;
-                double sv = 0.0, sd = 0.0;
-                for (int a = 0; a < P; ++a) {
-                    const double v = row[idx[0][a]];
-                    sv = fma(W[0][a], v, sv);
-                    sd = fma(dW[0][a], v, sd);
-                }
-                pot = fma(W[2][c] * W[1][b], sv, pot);
-                gx = fma(W[2][c] * W[1][b], sd, gx);
-                gy = fma(W[2][c] * dW[1][b], sv, gy);
-                gz = fma(dW[2][c] * W[1][b], sv, gz);
-            }
-        const double q = p.w;
-        const double e_i = 0.5 * q * pot + psets[S.pset].self_coef * q * q;
-        force[i] = make_double4(q * S.gxd * gx, q * S.gyd * gy, q * S.gzd * gz, e_i);
-        e1[0] = e_i;
+#pragma unroll
+        for (int o = K64I_G / 2; o > 0; o >>= 1) {
+            pot += __shfl_xor_sync(0xffffffffu, pot, o);
+            gx += __shfl_xor_sync(0xffffffffu, gx, o);
+            gy += __shfl_xor_sync(0xffffffffu, gy, o);
+            gz += __shfl_xor_sync(0xffffffffu, gz, o);
+        }
+        if (valid && sub == 0) {
+            const double q = rec.w;
+            const double e_i = 0.5 * q * pot + self * q * q;
+            force[perm[s0 + pp]] = make_double4(q * S.gxd * gx, q * S.gyd * gy, q * S.gzd * gz, e_i);
+            e_acc += e_i;
+        }
+        __syncwarp();  // the weights are rewritten for the next particles
     }
+    double e1[1] = {e_acc};
     block_sum_f64<1>(e1, red);
-    if (threadIdx.x == 0) atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_E], e1[0]);
+    if (threadIdx.x == 0) atomicAdd(&acc[sid * ACC_STRIDE + ACC_E], e1[0]);
+}
+
+// CTAs per tile for the tile kernels when the tiles are fewer than two per SM
+// (coarse meshes, large tiles): about four CTAs per SM, at most 8 per tile.
+// Measured on 98,304 water charges (FP64 evaluation): 125 tiles in 5 CTAs
+// each 0.65 ms against 0.99 unsplit and 0.71 in 3; 512 tiles in 2 CTAs each
+// 4% slower than unsplit.
+static int split64(int n_tiles) {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        sms = 148;
+    if (n_tiles >= 2 * sms) return 1;
+    return std::min(8, std::max(1, (4 * sms + n_tiles - 1) / std::max(1, n_tiles)));
+}
+
+template <int P>
+static cudaError_t configure64_interp_p(int T) {
+    return cudaFuncSetAttribute(k64_interp<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)interp64_smem(P, T));
+}
+
+template <int P>
+static cudaError_t launch64_interp_p(const Launch64& b, cudaStream_t st) {
+    const LaunchArgs& a = b.a;
+    // several CTAs per tile when the tiles are few, each staging the region
+    // and taking a share of its particles
+    k64_interp<P><<<dim3(a.n_tiles, split64(a.n_tiles)), K64I_WARPS * 32, interp64_smem(a.P, a.T), st>>>(
+        a.tile_sys, a.sys, a.psets, b.wcoef, a.T, a.D, a.tile_start, a.perm, b.srec, a.srel, b.phi, b.force, a.acc);
+    return cudaGetLastError();
 }
 
 // ----------------------------------------------------------------------------
 // pair term (EvaluatorPairPSWF, src/EvaluatorPairPSWF.h:274-295) in FP64:
 // 8 lanes per particle over its neighbour row
 // ----------------------------------------------------------------------------
-__global__ void __launch_bounds__(256)
+// without the virial: 64 registers, four CTAs per SM (measured 1-2% faster than 72 and three)
+template <bool VIR>
+__global__ void __launch_bounds__(256, VIR ? 3 : 4)
     k64_pair(const int2* __restrict__ chunks, const SysDev* __restrict__ sys, const ParamSet* __restrict__ psets,
              const double* __restrict__ qv, int nq, const double4* __restrict__ posq,
              const uint32_t* __restrict__ head, const uint32_t* __restrict__ nn, const uint32_t* __restrict__ nlist,
-             double4* __restrict__ force, double* __restrict__ acc, int accumulate, int want_virial) {
+             double4* __restrict__ force, double* __restrict__ acc, int accumulate) {
     __shared__ double red[32 * 7];
+    __shared__ double sq[MAX_QC];  // split coefficients (nq <= MAX_QC, checked by the planner)
     constexpr int TPP = 8;
     const int2 ch = chunks[blockIdx.x];
     const SysDev S = sys[ch.x];
     const ParamSet& ps = psets[S.pset];
     const double rc = ps.rcut_d, rc2 = rc * rc, irc = 1.0 / rc, irc2 = irc * irc, tirc3 = 2.0 * irc2 * irc;
+    const double iLx = 1.0 / S.Lxd, iLy = 1.0 / S.Lyd, iLz = 1.0 / S.Lzd;
+    for (int c = threadIdx.x; c < nq; c += blockDim.x) sq[c] = qv[c];
+    __syncthreads();
     const int i = ch.y + threadIdx.x / TPP;
     const int sub = threadIdx.x % TPP;
     const bool valid = i < S.p_off + S.N;
     double fx = 0, fy = 0, fz = 0, en = 0, v[6] = {0, 0, 0, 0, 0, 0};
-    if (valid) {
-        const double4 pi = posq[i];
-        const uint32_t n = nn[i], h = head[i];
-        for (uint32_t k = sub; k < n; k += TPP) {
-            const double4 pj = posq[S.p_off + (int)nlist[h + k]];
-            double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-            dx -= S.Lxd * rint(dx / S.Lxd);
-            dy -= S.Lyd * rint(dy / S.Lyd);
-            dz -= S.Lzd * rint(dz / S.Lzd);
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 < rc2 && r2 > 0.0) {
-                const double ri = 1.0 / sqrt(r2);
-                const double vv = fma(2.0 * irc2, r2, -1.0);
-                double Q = qv[nq - 1], dQ = (nq - 1) * qv[nq - 1];
-                for (int c = nq - 2; c >= 0; --c) Q = fma(Q, vv, qv[c]);
-                for (int c = nq - 2; c >= 1; --c) dQ = fma(dQ, vv, c * qv[c]);
-                dQ *= 2.0;  // dQ/du = 2 dQ/dv
-                const double qq = pi.w * pj.w * INV_4PI_D;
-                const double fdr = qq * (tirc3 * dQ + ri * ri * ri);
-                en += qq * (ri - Q * irc);
-                fx += fdr * dx;
-                fy += fdr * dy;
-                fz += fdr * dz;
-                if (want_virial) {
-                    v[0] += fdr * dx * dx;
-                    v[1] += fdr * dx * dy;
-                    v[2] += fdr * dx * dz;
-                    v[3] += fdr * dy * dy;
-                    v[4] += fdr * dy * dz;
-                    v[5] += fdr * dz * dz;
-                }
+    const double4 pi = valid ? posq[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+    auto pair = [&](const double4 pj) {
+        double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        // minimum image by the reciprocal box length; a pair that it could image
+        // differently from a division sits at |d| = L/2 > r_c
+        dx -= S.Lxd * rint(dx * iLx);
+        dy -= S.Lyd * rint(dy * iLy);
+        dz -= S.Lzd * rint(dz * iLz);
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 < rc2 && r2 > 0.0) {
+            const double ri = rsqrt(r2);
+            const double vv = fma(2.0 * irc2, r2, -1.0);
+            // Q(v) and dQ/dv in one Horner pass over the staged coefficients
+            double Q = sq[nq - 1], dQ = 0.0;
+            for (int c = nq - 2; c >= 0; --c) {
+                dQ = fma(dQ, vv, Q);
+                Q = fma(Q, vv, sq[c]);
+            }
+            dQ *= 2.0;  // dQ/du = 2 dQ/dv
+            const double qq = pi.w * pj.w * INV_4PI_D;
+            const double fdr = qq * (tirc3 * dQ + ri * ri * ri);
+            en += qq * (ri - Q * irc);
+            fx += fdr * dx;
+            fy += fdr * dy;
+            fz += fdr * dz;
+            if (VIR) {
+                v[0] += fdr * dx * dx;
+                v[1] += fdr * dx * dy;
+                v[2] += fdr * dx * dz;
+                v[3] += fdr * dy * dy;
+                v[4] += fdr * dy * dz;
+                v[5] += fdr * dz * dz;
             }
         }
+    };
+    if (valid) {
+        // one neighbour per lane and step: streaming 16-byte index segments
+        // with four gathers in flight per lane measured 2-6% slower here
+        const uint32_t n = nn[i], h = head[i];
+        for (uint32_t k = sub; k < n; k += TPP) pair(posq[S.p_off + (int)nlist[h + k]]);
     }
 #pragma unroll
     for (int o = TPP / 2; o > 0; o >>= 1) {
@@ -465,11 +711,18 @@ __global__ void __launch_bounds__(256)
         f.w += 0.5 * en;
         force[i] = f;
     }
-    double e[7] = {sub == 0 ? 0.5 * en : 0.0, 0.5 * v[0], 0.5 * v[1], 0.5 * v[2], 0.5 * v[3], 0.5 * v[4], 0.5 * v[5]};
-    block_sum_f64<7>(e, red);
-    if (threadIdx.x == 0) {
-        atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_E], e[0]);
-        for (int k = 0; k < 6; ++k) atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_WP + k], e[1 + k]);
+    if (VIR) {
+        double e[7] = {sub == 0 ? 0.5 * en : 0.0, 0.5 * v[0], 0.5 * v[1], 0.5 * v[2],
+                       0.5 * v[3],                0.5 * v[4], 0.5 * v[5]};
+        block_sum_f64<7>(e, red);
+        if (threadIdx.x == 0) {
+            atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_E], e[0]);
+            for (int k = 0; k < 6; ++k) atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_WP + k], e[1 + k]);
+        }
+    } else {
+        double e[1] = {sub == 0 ? 0.5 * en : 0.0};
+        block_sum_f64<1>(e, red);
+        if (threadIdx.x == 0) atomicAdd(&acc[ch.x * ACC_STRIDE + ACC_E], e[0]);
     }
 }
 
@@ -546,11 +799,16 @@ __global__ void k64_exclusions(const int2* __restrict__ chunks, const SysDev* __
 // ----------------------------------------------------------------------------
 size_t spread64_smem(int P, int T) {
     const int E = T + P - 1;
-    return ((size_t)E * E * E + (size_t)K64_WARPS * 3 * MAX_P) * sizeof(double);
+    return (spread64_region(E) + (size_t)K64S_CH * (K64S_SEG + 2 * P) + (size_t)P * (MAX_D + 1)) *
+               sizeof(double) +
+           (size_t)(K64S_CH + E * E + E) * sizeof(uint32_t);
 }
 
 cudaError_t launch64_configure(int P, int T) {
-    return cudaFuncSetAttribute(k64_spread, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)spread64_smem(P, T));
+    const cudaError_t e =
+        cudaFuncSetAttribute(k64_spread, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)spread64_smem(P, T));
+    if (e != cudaSuccess) return e;
+    ESPB_DISPATCH_P(configure64_interp_p, P, T);
 }
 
 cudaError_t launch64_eval(const Launch64& b, cudaStream_t st) {
@@ -566,7 +824,7 @@ cudaError_t launch64_eval(const Launch64& b, cudaStream_t st) {
         if (e != cudaSuccess) return e;
         if (a.n_tiles) {
             k64_tile_sort<<<a.n_tiles, 256, 0, st>>>(a.tile_start, a.perm_u, a.perm, b.trec, a.rel, b.srec, a.srel);
-            k64_spread<<<a.n_tiles, K64_WARPS * 32, spread64_smem(a.P, a.T), st>>>(
+            k64_spread<<<dim3(a.n_tiles, split64(a.n_tiles)), K64S_THREADS, spread64_smem(a.P, a.T), st>>>(
                 a.tile_sys, a.sys, b.wcoef, a.P, a.T, a.D, a.tile_start, b.srec, a.srel, a.rho);
         }
         if (b.n_xl) k64_fft_pass<0><<<b.n_xl, F64_WARPS * 32, 0, st>>>(b.xl, a.sys, b.tw, b.cbuf, a.rho, b.phi, b.gtab, a.acc);
@@ -574,17 +832,23 @@ cudaError_t launch64_eval(const Launch64& b, cudaStream_t st) {
         if (b.n_zl) k64_fft_pass<2><<<b.n_zl, F64_WARPS * 32, 0, st>>>(b.zl, a.sys, b.tw, b.cbuf, a.rho, b.phi, b.gtab, a.acc);
         if (b.n_yl) k64_fft_pass<3><<<b.n_yl, F64_WARPS * 32, 0, st>>>(b.yl, a.sys, b.tw, b.cbuf, a.rho, b.phi, b.gtab, a.acc);
         if (b.n_xl) k64_fft_pass<4><<<b.n_xl, F64_WARPS * 32, 0, st>>>(b.xl, a.sys, b.tw, b.cbuf, a.rho, b.phi, b.gtab, a.acc);
-        if (a.n_chunks)
-            k64_interp<<<a.n_chunks, 256, 0, st>>>(a.chunks, a.sys, a.psets, b.wcoef, a.P, a.D, b.posq, b.phi, b.force,
-                                                   a.acc);
+        if (a.n_tiles) {
+            e = [&]() -> cudaError_t { ESPB_DISPATCH_P(launch64_interp_p, a.P, b, st); }();
+            if (e != cudaSuccess) return e;
+        }
         if (a.n_chunks && a.ex_n)
             k64_exclusions<<<a.n_chunks, 256, 0, st>>>(a.chunks, a.sys, a.psets, b.qv, b.nq, b.posq, a.ex_n,
                                                        a.ex_list, a.ex_pitch, b.force, a.acc);
     }
     if (sr && b.n_pchunks)
-        k64_pair<<<b.n_pchunks, 256, 0, st>>>(b.pchunks, a.sys, a.psets, b.qv, b.nq, b.posq,
-                                                               a.nl_head, a.nl_n, a.nl_list, b.force, a.acc,
-                                                               lr ? 1 : 0, a.want_virial);
+    {
+        if (a.want_virial)
+            k64_pair<true><<<b.n_pchunks, 256, 0, st>>>(b.pchunks, a.sys, a.psets, b.qv, b.nq, b.posq, a.nl_head,
+                                                        a.nl_n, a.nl_list, b.force, a.acc, lr ? 1 : 0);
+        else
+            k64_pair<false><<<b.n_pchunks, 256, 0, st>>>(b.pchunks, a.sys, a.psets, b.qv, b.nq, b.posq, a.nl_head,
+                                                         a.nl_n, a.nl_list, b.force, a.acc, lr ? 1 : 0);
+    }
     return cudaGetLastError();
 }
 
