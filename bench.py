@@ -486,8 +486,11 @@ def run_water(args):
     p4 = np.zeros((N, 4))
     p4[:, :3] = posd
     rows = []
+    only = {(float(t), p) for t, p in (r.split(":") for r in args.water_rows.split(",") if r)}
     for target, order in ((1e-3, 6), (1e-5, 8), (1e-7, 10)):
         for prec in (0, 1):
+            if only and (target, ("f32", "f64")[prec]) not in only:
+                continue
             params = native.make_params(order=order, rcut=0.9, target_error=target, precision=prec)
             b = native.Batch(params, [N], [w.box])
             if prec == 0:
@@ -541,11 +544,13 @@ def run_water(args):
                          "particle_evals_per_s": N / (ms * 1e-3), "force_rel_rms": err,
                          "energy_rel": abs(energy.item() - E0) / abs(E0), "stage_ms": stages})
             del b
+    head_row = next((r for r in rows if r["target"] == 1e-5 and r["precision"] == "f32"), rows[0])
     line = {"metric": "particle-evals/s and error vs FP64 Ewald (C3: water accuracy sweep)",
-            "value": rows[2]["particle_evals_per_s"], "unit": "particle-evals/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": max(3, args.warmup), "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "value": head_row["particle_evals_per_s"], "unit": "particle-evals/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": max(3, args.warmup), "higher_is_better": True, "dtype": head_row["precision"],
+            "data": "synthetic",
             "config": {"workload": "c3: 32,768 rigid three-site molecules (98,304 charges), seed 1003, r_c 0.9 nm, "
-                                   "no exclusions; value = the 1e-5 FP32 row"},
+                                   "no exclusions; value = the 1e-5 FP32 row (else the first row run)"},
             "rows": rows}
     print(json.dumps(line), flush=True)
 
@@ -610,6 +615,29 @@ def run_scaleup(args):
         b.pairlist_check()
         b.build_nlist(pos, RCUT + SKIN, CAP, head, nn, nl)  # neighbour counts for the byte model
     mean_nn = float(nn.double().mean().item())
+    # single evaluations in both precisions (the configuration's FP64 and FP32
+    # modes), same mesh and target: FP32 over the library's pair list, FP64
+    # over the HOOMD-layout list just built
+    def eval_ms(fn, reps=5):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    b.build_pairlist(pos, RCUT + SKIN, CAP)
+    f32_ms = eval_ms(lambda: b.compute(pos, q, force, energy, virial, nlist=None, flags=ESP_ALL))
+    b64 = native.Batch(native.make_params(order=8, rcut=RCUT, target_error=1e-5, precision=1), [N], [s.box])
+    pos64 = pos.double()
+    q64 = q.double()
+    force64 = torch.zeros((N, 4), dtype=torch.float64, device=dev)
+    f64_ms = eval_ms(lambda: b64.compute_f64(pos64, q64, force64, energy, virial, nlist=(head, nn, nl)))
+    del b64, pos64, q64, force64
     alg = {"pair": 4.0 * N * mean_nn + 32.0 * N, "spread": 20.0 * N + 4.0 * M, "interp": 36.0 * N + 4.0 * M,
            "fft": 5 * 2 * 8.0 * M / 2, "sort": 40.0 * N, "bin": 40.0 * N, "nlist": 16.0 * N + 4.0 * N * mean_nn,
            "nve": 48.0 * N}
@@ -628,7 +656,8 @@ def run_scaleup(args):
                                    "1 nlist + 1 eval + 10 NVE steps per step",
                        "mesh": [inf["nx"], inf["ny"], inf["nz"]], "order": 8, "rcut": RCUT,
                        "mean_neighbours": mean_nn},
-            "peak_gbs": peak, "peak_kind": peak_kind, "stages": stages, "clocks": clk.summary()}
+            "peak_gbs": peak, "peak_kind": peak_kind, "stages": stages, "clocks": clk.summary(),
+            "single_eval_ms": {"f32": f32_ms, "f64": f64_ms}}
     print(json.dumps(line), flush=True)
 
 
@@ -920,6 +949,8 @@ def main():
     ap.add_argument("--workload", default="batched256", choices=["batched256", "scaleup", "c1", "water"],
                     help="second measurements: scaleup (the plain path on one 10^6-particle system), c1 (FP64 "
                          "plain case with LJ, 100 NVE steps), water (the C3 accuracy sweep)")
+    ap.add_argument("--water-rows", default="",
+                    help="water sweep rows to run, comma-separated target:precision (e.g. 1e-5:f64); default all")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default plan)")
     ap.add_argument("--hoomd-list", action="store_true",
