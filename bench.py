@@ -402,7 +402,8 @@ def run_c1(args):
     lattice, L = 10, seed 1000), mesh 32^3, support 8, r_c 3.0, FP64 mode,
     Lennard-Jones core repulsion (eps 1, sigma 0.9, r_cut 2.5); a step = one
     evaluation + 100 NVE steps at dt 0.002 with the neighbour list (r_c + 0.4)
-    rebuilt every 10 steps. One small system: launch-bound by nature."""
+    rebuilt every 10 steps (10 steps per esp_batch_md_run_f64 call, replayed
+    from a captured graph). One small system: launch-bound by nature."""
     import torch
     from esp_hoomd_b200 import native, systems
     dev = torch.device("cuda", 0)
@@ -437,12 +438,12 @@ def run_c1(args):
         vel.copy_(vel0)
         b32.build_nlist(pos.float(), RCUT + SKIN, CAP, head, nn, nl)
         evaluate()
-        for k in range(100):
-            if k and k % 10 == 0:
+        e_esp.add_(e_lj)  # md_run_f64 carries ESP + LJ in one energy
+        for k in range(10):
+            if k:
                 b32.build_nlist(pos.float(), RCUT + SKIN, CAP, head, nn, nl)
-            b.nve_step1_f64(pos, vel, force, DT)
-            evaluate()
-            b.nve_step2_f64(vel, force, DT)
+            # 10 velocity-Verlet steps (ESP + LJ) replayed from a captured graph
+            b.md_run_f64(pos, vel, q, force, e_esp, None, nlist, 10, DT, lj=(1.0, 0.9, 2.5))
 
     for _ in range(max(3, args.warmup)):
         step()

@@ -25,7 +25,7 @@ EXPORTS = [
     "esp_compute", "esp_get_info", "esp_destroy", "esp_batch_create", "esp_batch_compute", "esp_batch_get_info",
     "esp_batch_total_particles", "esp_batch_destroy", "esp_pswf_eval_pairs", "esp_batch_build_nlist",
     "esp_batch_nve_step1", "esp_batch_nve_step2", "esp_spread", "esp_get_sort", "esp_get_potential",
-    "esp_batch_md_run", "esp_batch_set_timing", "esp_batch_stage_times", "esp_spread_noalloc",
+    "esp_batch_md_run", "esp_batch_md_run_f64", "esp_batch_set_timing", "esp_batch_stage_times", "esp_spread_noalloc",
     "esp_server_create", "esp_server_submit", "esp_server_start", "esp_server_status", "esp_server_wait_all",
     "esp_server_get_stats", "esp_server_destroy", "esp_set_exclusions", "esp_batch_set_exclusions",
     "esp_compute_f64", "esp_batch_compute_f64", "esp_batch_autotune", "esp_batch_lj", "esp_batch_lj_f64",
@@ -125,6 +125,7 @@ def get_lib() -> ctypes.CDLL:
         lib.esp_get_sort.argtypes = [P, P, P, P]
         lib.esp_get_potential.argtypes = [P, P, P]
         lib.esp_batch_md_run.argtypes = [P, P, P, P, P, P, P, P, P, P, P, I, D, I]
+        lib.esp_batch_md_run_f64.argtypes = [P, P, P, P, P, P, P, P, P, P, P, I, D, D, D, D, I]
         lib.esp_batch_set_timing.argtypes = [P, I]
         lib.esp_batch_stage_times.argtypes = [P, P, P]
         lib.esp_server_create.argtypes = [ctypes.POINTER(EspServerConfig), ctypes.POINTER(P)]

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <string>
 #include <tuple>
@@ -356,10 +357,13 @@ struct esp_batch {
         const void *pos, *vel, *q, *head, *nn, *nl, *force, *energy, *virial;
         double dt;
         bool with_energy;
+        bool f64 = false;                               // md_run_f64 steps
+        double lj_eps = 0, lj_sigma = 0, lj_rcut = 0;   // md_run_f64's Lennard-Jones term (sigma 0: none)
         bool operator==(const GraphKey& o) const {
             return pos == o.pos && vel == o.vel && q == o.q && head == o.head && nn == o.nn && nl == o.nl &&
                    force == o.force && energy == o.energy && virial == o.virial && dt == o.dt &&
-                   with_energy == o.with_energy;
+                   with_energy == o.with_energy && f64 == o.f64 && lj_eps == o.lj_eps && lj_sigma == o.lj_sigma &&
+                   lj_rcut == o.lj_rcut;
         }
     };
     // captured MD steps, one per distinct set of caller pointers; a few
@@ -405,6 +409,13 @@ struct esp_batch {
     int md_run(cudaStream_t st, float* pos4, float* vel4, const float* q, const unsigned* head, const unsigned* nn,
                const unsigned* nl, float* force4, double* energy, double* virial, int nsteps, double dt,
                int use_graph);
+    int md_run_f64(cudaStream_t st, double* pos4, double* vel4, const double* q, const unsigned* head,
+                   const unsigned* nn, const unsigned* nl, double* force4, double* energy, double* virial, int nsteps,
+                   double dt, double lj_eps, double lj_sigma, double lj_rcut, int use_graph);
+    // nsteps calls of step(with_energy), with_energy on the last; with
+    // use_graph each form is captured once per key (st is swapped for the
+    // capture stream while step runs) and replayed
+    int run_steps(cudaStream_t& st, GraphKey key, const std::function<int(bool)>& step, int nsteps, bool use_graph);
     // want_energy = false (MD steps whose energies are overwritten by the
     // next step) leaves the pair energies out of force.w and energy
     // virial_pp / external: HOOMD's per-particle virial (6 x pitch floats)
@@ -1023,16 +1034,53 @@ int esp_batch::md_run(cudaStream_t st, float* pos4, float* vel4, const float* q,
         timer.end(st);
         return rc;
     };
-    if (!use_graph || timer.on) {
+    const GraphKey key{pos4, vel4, q, head, nn, nl, force4, energy, virial, dt, false};
+    return run_steps(st, key, step, nsteps, use_graph && !timer.on);
+}
+
+int esp_batch::md_run_f64(cudaStream_t st, double* pos4, double* vel4, const double* q, const unsigned* head,
+                          const unsigned* nn, const unsigned* nl, double* force4, double* energy, double* virial,
+                          int nsteps, double dt, double lj_eps, double lj_sigma, double lj_rcut, int use_graph) {
+    if (!f64) return fail(ESP_ERR_UNSUPPORTED, "context planned for FP32: create it with precision ESP_FP64");
+    if (nsteps < 0) return fail(ESP_ERR_INVALID, "negative step count");
+    if (!pos4 || !vel4 || !q || !force4 || !head || !nn || !nl)
+        return fail(ESP_ERR_INVALID, "md_run_f64 needs positions, velocities, charges, forces and the neighbour list");
+    const bool lj = lj_sigma > 0;
+    if (lj && !(lj_rcut > 0)) return fail(ESP_ERR_INVALID, "Lennard-Jones r_cut must be positive");
+    if (head == nl_last_head && nl == nl_last_nl) {
+        const int rc = nlist_check(false, nullptr);
+        if (rc) return rc;
+    }
+    auto step = [&](bool) -> int {
+        int rc = nve1(st, pos4, vel4, force4, dt, true);
+        if (rc) return rc;
+        rc = compute_f64(st, pos4, q, head, nn, nl, force4, energy, virial, ESP_ALL);
+        if (rc) return rc;
+        if (lj)
+            ESPB_CK(launch_lj(d_chunks, n_chunks, d_sys, pos4, head, nn, nl, lj_eps, lj_sigma, lj_rcut, force4, energy,
+                              true, st));
+        return nve2(st, pos4, vel4, force4, dt, true);
+    };
+    GraphKey key{pos4, vel4, q, head, nn, nl, force4, energy, virial, dt, false};
+    key.f64 = true;
+    key.lj_eps = lj ? lj_eps : 0.0;
+    key.lj_sigma = lj ? lj_sigma : 0.0;
+    key.lj_rcut = lj ? lj_rcut : 0.0;
+    return run_steps(st, key, step, nsteps, use_graph != 0);
+}
+
+int esp_batch::run_steps(cudaStream_t& st, GraphKey key, const std::function<int(bool)>& step, int nsteps,
+                         bool use_graph) {
+    if (!use_graph) {
         for (int k = 0; k < nsteps; ++k) {
             int rc = step(k == nsteps - 1);
             if (rc) return rc;
         }
         return 0;
     }
-    // one captured step per (caller pointers, energy or not)
+    // one captured step per (key, energy or not)
     auto graph_for = [&](bool with_energy, cudaGraphExec_t& out) -> int {
-        const GraphKey key{pos4, vel4, q, head, nn, nl, force4, energy, virial, dt, with_energy};
+        key.with_energy = with_energy;
         GraphEntry* ge = nullptr;
         for (GraphEntry& g : graphs)
             if (g.exec && g.key == key) ge = &g;
@@ -1725,6 +1773,15 @@ int esp_batch_md_run(esp_batch* b, void* stream, float* pos4, float* vel4, const
     if (!b) return fail(ESP_ERR_INVALID, "null batch");
     return b->md_run((cudaStream_t)stream, pos4, vel4, charge, head, n_neigh, nlist, force4, energy, virial6, nsteps,
                      dt, use_graph);
+}
+
+int esp_batch_md_run_f64(esp_batch* b, void* stream, double* pos4, double* vel4, const double* charge,
+                         const unsigned* head, const unsigned* n_neigh, const unsigned* nlist, double* force4,
+                         double* energy, double* virial6, int nsteps, double dt, double lj_epsilon, double lj_sigma,
+                         double lj_r_cut, int use_graph) {
+    if (!b) return fail(ESP_ERR_INVALID, "null batch");
+    return b->md_run_f64((cudaStream_t)stream, pos4, vel4, charge, head, n_neigh, nlist, force4, energy, virial6,
+                         nsteps, dt, lj_epsilon, lj_sigma, lj_r_cut, use_graph);
 }
 
 int esp_batch_set_timing(esp_batch* b, int on) {

@@ -3,7 +3,7 @@ CUDA tensors; torch is only the allocator and stream provider here)."""
 from __future__ import annotations
 
 import ctypes
-from typing import Optional, Sequence
+from typing import Optional, Sequence, Tuple
 
 import numpy as np
 import torch
@@ -245,6 +245,18 @@ class Batch:
         check(self._lib.esp_batch_md_run(self._h, _stream(stream), _ptr(pos4), _ptr(vel4), _ptr(q), _ptr(head),
                                          _ptr(nn), _ptr(nl), _ptr(force4), _ptr(energy), _ptr(virial), int(nsteps),
                                          float(dt), int(bool(use_graph))), "esp_batch_md_run")
+
+    def md_run_f64(self, pos4, vel4, q, force4, energy, virial, nlist, nsteps: int, dt: float,
+                   lj: Optional[Tuple[float, float, float]] = None, use_graph: bool = True, stream=None) -> None:
+        """FP64 velocity-Verlet steps (float64 tensors) over nlist = (head,
+        n_neigh, nlist); lj = (epsilon, sigma, r_cut) adds the Lennard-Jones
+        core to every step's forces and energy."""
+        head, nn, nl = nlist
+        eps, sig, rc = lj if lj is not None else (0.0, 0.0, 0.0)
+        check(self._lib.esp_batch_md_run_f64(self._h, _stream(stream), _ptr(pos4), _ptr(vel4), _ptr(q), _ptr(head),
+                                             _ptr(nn), _ptr(nl), _ptr(force4), _ptr(energy), _ptr(virial),
+                                             int(nsteps), float(dt), float(eps), float(sig), float(rc),
+                                             int(bool(use_graph))), "esp_batch_md_run_f64")
 
     def set_exclusions(self, n_ex: Optional[torch.Tensor], ex_list: Optional[torch.Tensor] = None,
                        ex_pitch: int = 0) -> None:

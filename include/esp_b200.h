@@ -341,6 +341,25 @@ int esp_batch_md_run(esp_batch* b, void* stream, float* pos4, float* vel4, const
                      const unsigned* n_neigh, const unsigned* nlist, float* force4, double* energy, double* virial6,
                      int nsteps, double dt, int use_graph);
 
+/* FP64 form of esp_batch_md_run for contexts created with precision
+ * ESP_FP64 (the C1 harness: HOOMD double builds integrating ESP with a
+ * Lennard-Jones core): nsteps velocity-Verlet steps (esp_batch_nve_step1_f64,
+ * a full FP64 evaluation over the caller's HOOMD-layout neighbour list, and,
+ * when lj_sigma > 0, the Lennard-Jones term of esp_batch_lj_f64 added to the
+ * forces, the per-particle energies and energy[s]; esp_batch_nve_step2_f64).
+ * force4 must hold the forces of the current positions on entry (ESP plus
+ * Lennard-Jones when it is on); on return force4, energy (ESP plus
+ * Lennard-Jones) and virial (ESP only) are those of the final positions. Rigid
+ * water set by esp_batch_set_rigid_water is kept rigid. use_graph as in
+ * esp_batch_md_run: one captured step per pointer set, dt and Lennard-Jones
+ * parameters, replayed. The per-step sequence of the integration loop of
+ * HOOMD's TwoStepNVE around ESPForceCompute::computeForces
+ * (src/ESPForceCompute.cc:200-248) in one call. */
+int esp_batch_md_run_f64(esp_batch* b, void* stream, double* pos4, double* vel4, const double* charge,
+                         const unsigned* head, const unsigned* n_neigh, const unsigned* nlist, double* force4,
+                         double* energy, double* virial6, int nsteps, double dt, double lj_epsilon, double lj_sigma,
+                         double lj_r_cut, int use_graph);
+
 /* ---------------------------------------------------------------- serving
  * Continuous-batching request server (no counterpart in the reference, whose
  * ForceCompute serves one HOOMD simulation). A request is one system: a

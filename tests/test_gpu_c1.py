@@ -102,3 +102,50 @@ def test_c1_plain_fp64_with_lj():
     d = pos.cpu().numpy()[:, :3] - po
     d -= L * np.round(d / L)
     assert np.abs(d).max() <= 1e-6
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_md_run_f64_equals_the_step_loop(use_graph):
+    """esp_batch_md_run_f64 (ESP + LJ, 10 steps, eager or replayed from a
+    captured graph) follows the explicit loop of nve_step1_f64 / compute_f64
+    / lj / nve_step2_f64 on the same list: positions to 1e-12, forces and the
+    energy (ESP + LJ) to 1e-10 relative (the mesh flush's FP64 atomics may
+    add in another order)."""
+    s = systems.rocksalt(10, seed=1000)
+    b = native.Batch(native.make_params(order=8, rcut=3.0, mesh=(32, 32, 32), precision=1), [s.N], [s.box])
+    q = torch.as_tensor(s.q, dtype=torch.float64, device="cuda")
+    nl = _nl_dev(R.neighbor_list(s.pos, s.box, 3.4))
+    runs = []
+    for fused in (False, True):
+        pos, vel = _dev4(s.pos, 0.0), _dev4(s.vel, 1.0)
+        force = torch.zeros((s.N, 4), dtype=torch.float64, device="cuda")
+        energy = torch.zeros(1, dtype=torch.float64, device="cuda")
+        b.compute_f64(pos, q, force, energy, nlist=nl)
+        b.lj(pos, nl, EPS, SIG, RLJ, force, energy)
+        if fused:
+            b.md_run_f64(pos, vel, q, force, energy, None, nl, 10, 0.002, lj=(EPS, SIG, RLJ), use_graph=use_graph)
+            if use_graph:  # a second call replays the captured steps
+                b.md_run_f64(pos, vel, q, force, energy, None, nl, 5, 0.002, lj=(EPS, SIG, RLJ), use_graph=True)
+        else:
+            for _ in range(15 if use_graph else 10):
+                b.nve_step1_f64(pos, vel, force, 0.002)
+                b.compute_f64(pos, q, force, energy, nlist=nl)
+                b.lj(pos, nl, EPS, SIG, RLJ, force, energy)
+                b.nve_step2_f64(vel, force, 0.002)
+        torch.cuda.synchronize()
+        runs.append((pos.cpu().numpy(), vel.cpu().numpy(), force.cpu().numpy(), energy.item()))
+    (p0, v0, f0, e0), (p1, v1, f1, e1) = runs
+    assert np.abs(p1[:, :3] - p0[:, :3]).max() <= 1e-12 * 10
+    assert np.abs(v1 - v0).max() <= 1e-10 * np.abs(v0).max()
+    assert R.rel_rms(f1[:, :3], f0[:, :3]) <= 1e-10
+    assert abs(e1 - e0) <= 1e-10 * abs(e0)
+
+
+def test_md_run_f64_rejects_an_fp32_context():
+    s = systems.rocksalt(8, seed=1000)
+    b = native.Batch(native.make_params(order=8, rcut=3.0), [s.N], [s.box])
+    t = torch.zeros((s.N, 4), dtype=torch.float64, device="cuda")
+    q = torch.zeros(s.N, dtype=torch.float64, device="cuda")
+    nl = _nl_dev(R.neighbor_list(s.pos, s.box, 3.4))
+    with pytest.raises(RuntimeError):
+        b.md_run_f64(t, t.clone(), q, t.clone(), None, None, nl, 1, 0.002)
