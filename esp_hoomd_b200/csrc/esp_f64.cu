@@ -395,16 +395,16 @@ __global__ void __launch_bounds__(F64_WARPS * 32)
     // load: x lines one per warp (contiguous); y and z lines cooperatively,
     // the F64_WARPS lines' elements at one k adjacent in memory
     if (AX == 0) {
-        if (active)
+        if (active) {
             for (int k = lane; k < n; k += 32) {
                 const long long g = S.m_off + lbase[warp] + k;
-                if (MODE == 0) {
-                    sb[warp][0][k] = make_double2(rho[g], 0.0);
-                    rho[g] = 0.0;
-                } else {
-                    sb[warp][0][k] = cbuf[g];
-                }
+                sb[warp][0][k] = MODE == 0 ? make_double2(rho[g], 0.0) : cbuf[g];
             }
+            // the charge mesh is cleared for the next spread in a loop of its
+            // own, so that the loads above are not ordered behind the stores
+            if (MODE == 0)
+                for (int k = lane; k < n; k += 32) rho[S.m_off + lbase[warp] + k] = 0.0;
+        }
     } else {
         for (int idx = threadIdx.x; idx < F64_WARPS * n; idx += blockDim.x) {
             const int w = idx % F64_WARPS, k = idx / F64_WARPS;

@@ -717,8 +717,14 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
         // kernel attributes are set here, outside any stream capture
         LaunchArgs a = args();
         a.configure_only = 1;
-        ESPB_CK(launch_spread(a, 0));
-        ESPB_CK(launch_interp(a, 0));
+        // a tile whose kernels need more shared memory than a CTA can have
+        // is refused here (the attribute call fails with an invalid value)
+        if (launch_spread(a, 0) != cudaSuccess || launch_interp(a, 0) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ESP_ERR_UNSUPPORTED, "tile edge " + std::to_string(T) + " with support " + std::to_string(P) +
+                                                 ": its extended region needs more shared memory than a CTA has; "
+                                                 "use a smaller tile");
+        }
         ESPB_CK(launch_fft(a, 0));
     }
     f64 = p.precision == ESP_FP64;
@@ -797,7 +803,12 @@ int esp_batch::plan64(const std::vector<float2>& tw, long long g_total) {
     ESPB_CK(cudaMemcpy(d_xl, xl.data(), xl.size() * sizeof(int2), cudaMemcpyHostToDevice));
     ESPB_CK(cudaMemcpy(d_yl, yl.data(), yl.size() * sizeof(int2), cudaMemcpyHostToDevice));
     ESPB_CK(cudaMemcpy(d_zl, zl.data(), zl.size() * sizeof(int2), cudaMemcpyHostToDevice));
-    ESPB_CK(launch64_configure(P, T));
+    if (launch64_configure(P, T) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ESP_ERR_UNSUPPORTED, "tile edge " + std::to_string(T) + " with support " + std::to_string(P) +
+                                             ": the FP64 tile kernels need more shared memory than a CTA has; "
+                                             "use a smaller tile");
+    }
     return 0;
 }
 

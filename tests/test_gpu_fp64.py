@@ -5,6 +5,8 @@
   its largest component;
 * accuracy below the FP32 floor against FP64 Ewald: <= 1e-7 relative RMS
   force error at the 1e-7 target (rock-salt and water, support 10);
+* other supports and tile edges (regions larger than a CTA's threads, odd
+  supports, split tiles) against the oracle;
 * exclusions in FP64 against the oracle;
 * a context serves only the precision it was created for.
 """
@@ -61,6 +63,26 @@ def test_fp64_matches_oracle():
     assert abs(f[:, 3].sum() - e) <= 1e-10 * abs(E)
 
 
+@pytest.mark.parametrize("order,tile,n", [(8, 10, 32), (4, 20, 24), (5, 0, 24), (7, 5, 24), (12, 0, 24), (4, 0, 16)])
+def test_fp64_tiles_and_orders_match_oracle(order, tile, n):
+    """The FP64 tile kernels at other supports and tile edges: extended
+    regions of 17 and 23 (more rows than threads, two register segments per
+    row), odd supports, a region of 11, support 12 (3P > 32 weights), and
+    the small meshes whose few tiles are split over several CTAs."""
+    s = systems.rocksalt(8, seed=6404 + order)
+    s.pos = s.pos.astype(np.float32).astype(np.float64)
+    nlist = R.neighbor_list(s.pos, s.box, 3.0)
+    ctx, f, e, w = _run(s, native.make_params(order=order, mesh=(n, n, n), tile=tile, precision=1), nlist)
+    prm = _oracle_params(ctx.info(), s.box)
+    E, F, W = R.esp(s.pos, s.q, prm, nlist=nlist)
+    assert R.rel_rms(f[:, :3], F) <= 1e-8
+    assert abs(e - E) <= 1e-10 * abs(E)
+    # the virial comes from the FFT's z pass, not from the tile kernels; the
+    # oracle's virial factor takes Psi' by a finite difference (h = 1e-6),
+    # which on the finer meshes here limits it to ~1e-8 (2e-9 at 32^3)
+    assert np.abs(w - W).max() <= 2e-8 * np.abs(W).max()
+
+
 @pytest.mark.parametrize("kind", ["rocksalt", "water"])
 def test_fp64_accuracy_below_fp32_floor(kind):
     if kind == "rocksalt":
@@ -87,6 +109,14 @@ def test_fp64_exclusions_match_oracle():
     # the oracle's virial factor takes Psi' by a finite difference (h = 1e-6);
     # with the large cancelling intramolecular terms that limits it to ~1e-8
     assert np.abs(wv - W).max() <= 5e-8 * np.abs(W).max()
+
+
+def test_oversized_tile_is_refused():
+    """A tile whose extended region needs more shared memory than a CTA has
+    is refused at create with ESP_ERR_UNSUPPORTED (support 8, tile 20)."""
+    s = systems.rocksalt(8, seed=1)
+    with pytest.raises(EspError, match="tile edge 20"):
+        native.Context(native.make_params(order=8, mesh=(32, 32, 32), tile=20, precision=1), s.box, s.N)
 
 
 def test_precision_is_checked():
