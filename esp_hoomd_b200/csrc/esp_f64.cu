@@ -10,9 +10,10 @@
 //                             tile), one FP64 atomic per region point into the
 //                             mesh;
 //   k64_fft_pass            : one warp per mesh line, mixed-radix Stockham in
-//                             shared memory on the full complex spectrum; the
-//                             z pass multiplies by the influence table and
-//                             accumulates the k-space energy and virial;
+//                             shared memory on the half spectrum (two real x
+//                             rows per complex line); the z pass multiplies by
+//                             the influence table and accumulates the k-space
+//                             energy and virial;
 //   k64_interp              : one CTA per tile, the tile's potential region
 //                             staged in shared memory, eight lanes per
 //                             particle over the stencil rows;
@@ -357,9 +358,14 @@ __device__ double2* fft64_line(double2* a, double2* b, int n, uint32_t plan, con
 
 constexpr int F64_WARPS = 4;
 
-// MODE 0: x forward (real mesh -> spectrum, the mesh is cleared), 1: y
+// Half spectrum, as the FP32 passes: the x passes transform two real rows
+// (y, y + 1) as one complex line and store (or rebuild) their nx/2 + 1
+// Hermitian halves, so the spectrum is [z][y][kx < nxh] and the y and z
+// passes touch nxh of the nx columns.
+// MODE 0: x forward (real mesh -> half spectrum, the mesh is cleared), 1: y
 // forward, 2: z forward + influence multiply + energy/virial + z inverse,
-// 3: y inverse, 4: x inverse (spectrum -> real potential).
+// 3: y inverse, 4: x inverse (half spectrum -> real potential).
+// Lines per system: x: ceil(ny/2) nz row pairs; y: nxh nz; z: nxh ny.
 template <int MODE>
 __global__ void __launch_bounds__(F64_WARPS * 32)
     k64_fft_pass(const int2* __restrict__ items, const SysDev* __restrict__ sys, const double2* __restrict__ tw,
@@ -373,9 +379,11 @@ __global__ void __launch_bounds__(F64_WARPS * 32)
     const SysDev S = sys[it.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int AX = (MODE == 0 || MODE == 4) ? 0 : (MODE == 1 || MODE == 3) ? 1 : 2;
+    const int nxh = S.nxh, nyp = (S.ny + 1) / 2;
     const int n = AX == 0 ? S.nx : (AX == 1 ? S.ny : S.nz);
-    const long long nlines = AX == 0 ? (long long)S.ny * S.nz : (AX == 1 ? (long long)S.nx * S.nz : (long long)S.nx * S.ny);
-    const long long stride = AX == 0 ? 1 : (AX == 1 ? (long long)S.nx : (long long)S.nx * S.ny);
+    const long long nlines =
+        AX == 0 ? (long long)nyp * S.nz : (AX == 1 ? (long long)nxh * S.nz : (long long)nxh * S.ny);
+    const long long stride = AX == 1 ? (long long)nxh : (long long)nxh * S.ny;  // y and z lines
     const uint32_t plan = AX == 0 ? S.radx : (AX == 1 ? S.rady : S.radz);
     const double2* twa = tw + (AX == 0 ? S.twx : (AX == 1 ? S.twy : S.twz));
     for (int k = threadIdx.x; k < n; k += blockDim.x) stw[k] = twa[k];
@@ -383,27 +391,46 @@ __global__ void __launch_bounds__(F64_WARPS * 32)
         const long long l = (long long)it.y + threadIdx.x;
         long long base = -1;
         if (l < nlines) {
-            if (AX == 0) base = l * S.nx;
-            else if (AX == 1) base = (l / S.nx) * S.nx * S.ny + l % S.nx;
-            else base = l;  // (y, x) = (l / nx, l % nx): base y nx + x = l
+            if (AX == 0) base = (l / nyp) * S.ny + 2 * (l % nyp);  // first row (z ny + y) of the pair
+            else if (AX == 1) base = (l / nxh) * nxh * S.ny + l % nxh;
+            else base = l;  // (y, kx) = (l / nxh, l % nxh): base y nxh + kx = l
         }
         lbase[threadIdx.x] = base;
     }
     __syncthreads();
     const long long l = (long long)it.y + warp;
     const bool active = l < nlines;
-    // load: x lines one per warp (contiguous); y and z lines cooperatively,
-    // the F64_WARPS lines' elements at one k adjacent in memory
+    // x row pairs: the pair's second row exists unless ny is odd and y = ny - 1
+    const long long row0 = active && AX == 0 ? lbase[warp] : 0;
+    const bool two = AX == 0 && active && (row0 % S.ny) + 1 < S.ny;
+    double2* a = sb[warp][0];
+    double2* b = sb[warp][1];
+    // load: x row pairs one per warp (contiguous rows); y and z lines
+    // cooperatively, the F64_WARPS lines' elements at one k adjacent in memory
     if (AX == 0) {
         if (active) {
-            for (int k = lane; k < n; k += 32) {
-                const long long g = S.m_off + lbase[warp] + k;
-                sb[warp][0][k] = MODE == 0 ? make_double2(rho[g], 0.0) : cbuf[g];
+            if (MODE == 0) {
+                double* r0 = rho + S.m_off + row0 * S.nx;
+                for (int k = lane; k < n; k += 32) a[k] = make_double2(r0[k], two ? r0[k + S.nx] : 0.0);
+                // cleared in a loop of its own: the loads above are not ordered behind stores
+                for (int k = lane; k < n; k += 32) {
+                    r0[k] = 0.0;
+                    if (two) r0[k + S.nx] = 0.0;
+                }
+            } else {
+                // Z_k = A_k + i B_k, with A_{n-k} = conj(A_k) (and B) for k >= nxh
+                const double2* c0 = cbuf + S.m_off + row0 * nxh;
+                for (int k = lane; k < n; k += 32) {
+                    const bool lo = k < nxh;
+                    const int kk = lo ? k : n - k;
+                    double2 A = c0[kk], B = two ? c0[kk + nxh] : make_double2(0.0, 0.0);
+                    if (!lo) {
+                        A.y = -A.y;
+                        B.y = -B.y;
+                    }
+                    a[k] = make_double2(A.x - B.y, A.y + B.x);
+                }
             }
-            // the charge mesh is cleared for the next spread in a loop of its
-            // own, so that the loads above are not ordered behind the stores
-            if (MODE == 0)
-                for (int k = lane; k < n; k += 32) rho[S.m_off + lbase[warp] + k] = 0.0;
         }
     } else {
         for (int idx = threadIdx.x; idx < F64_WARPS * n; idx += blockDim.x) {
@@ -413,28 +440,24 @@ __global__ void __launch_bounds__(F64_WARPS * 32)
     }
     __syncthreads();
     double e[7] = {0, 0, 0, 0, 0, 0, 0};
-    double2* res = sb[warp][0];
+    double2* res = a;
     if (active) {
-        double2* a = sb[warp][0];
-        double2* b = sb[warp][1];
         const int sign = MODE <= 2 ? -1 : 1;
         res = fft64_line(a, b, n, plan, stw, sign, lane);
         if (MODE == 2) {
-            // (kx, ky) = (lx, ly) after the x and y passes; kz along the line
-            const int ly = (int)(l / S.nx), lx = (int)(l % S.nx);
-            const int nxh = S.nxh;
+            // (kx, ky) = (lx, ly) after the x and y passes; kz along the line;
+            // the columns 0 < kx < nx/2 stand for their conjugates too
+            const int ly = (int)(l / nxh), lx = (int)(l % nxh);
             const double tpx = 6.283185307179586 / S.Lxd, tpy = 6.283185307179586 / S.Lyd,
                          tpz = 6.283185307179586 / S.Lzd;
-            const int fx = lx <= S.nx / 2 ? lx : lx - S.nx;
+            const int fx = lx;
             const int fy = ly <= S.ny / 2 ? ly : ly - S.ny;
+            const double wk = (lx == 0 || 2 * lx == S.nx) ? 1.0 : 2.0;
             for (int kz = lane; kz < n; kz += 32) {
                 const int fz = kz <= S.nz / 2 ? kz : kz - S.nz;
-                long long gi;
-                if (lx < nxh) gi = ((long long)kz * S.ny + ly) * nxh + lx;
-                else gi = ((long long)((S.nz - kz) % S.nz) * S.ny + (S.ny - ly) % S.ny) * nxh + (S.nx - lx);
-                const double2 g = gtab[S.g_off + gi];
+                const double2 g = gtab[S.g_off + ((long long)kz * S.ny + ly) * nxh + lx];
                 const double2 v = res[kz];
-                const double a2 = v.x * v.x + v.y * v.y;
+                const double a2 = wk * (v.x * v.x + v.y * v.y);
                 const double ek = 0.5 * g.x * a2, eb = 0.5 * g.y * a2;
                 const double kxv = tpx * fx, kyv = tpy * fy, kzv = tpz * fz;
                 e[0] += ek;
@@ -451,12 +474,25 @@ __global__ void __launch_bounds__(F64_WARPS * 32)
         }
     }
     if (AX == 0) {
-        if (active)
-            for (int k = lane; k < n; k += 32) {
-                const long long g = S.m_off + lbase[warp] + k;
-                if (MODE == 4) phi[g] = res[k].x;
-                else cbuf[g] = res[k];
+        if (active) {
+            if (MODE == 4) {
+                // the potential rows: real part row y, imaginary part row y + 1
+                double* p0 = phi + S.m_off + row0 * S.nx;
+                for (int k = lane; k < n; k += 32) {
+                    const double2 z = res[k];
+                    p0[k] = z.x;
+                    if (two) p0[k + S.nx] = z.y;
+                }
+            } else {
+                // A_k = (Z_k + conj Z_{n-k}) / 2, B_k = (Z_k - conj Z_{n-k}) / (2i), k < nxh
+                double2* c0 = cbuf + S.m_off + row0 * nxh;
+                for (int k = lane; k < nxh; k += 32) {
+                    const double2 z = res[k], zc = res[k == 0 ? 0 : n - k];
+                    c0[k] = make_double2(0.5 * (z.x + zc.x), 0.5 * (z.y - zc.y));
+                    if (two) c0[k + nxh] = make_double2(0.5 * (z.y + zc.y), -0.5 * (z.x - zc.x));
+                }
             }
+        }
     } else {
         // every line of the CTA has the same length and plan: its result sits
         // in buffer (stages mod 2) of its warp (buffer 0 after the two

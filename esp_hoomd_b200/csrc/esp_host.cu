@@ -758,7 +758,7 @@ int esp_batch::plan(const esp_params& p, int ns, const int* N_, const double* bo
 
 // FP64 tables (window and split coefficients in double, twiddles from FP64
 // angles), FP64 records and spectrum, and the FP64 work lists: 32 particles
-// per pair chunk, four mesh lines per FFT item.
+// per pair chunk, four x row pairs or y/z lines per FFT item.
 int esp_batch::plan64(const std::vector<float2>& tw, long long g_total) {
     const PsetHost& h = psh[0];
     std::vector<double> w64(h.win.coef.begin(), h.win.coef.end());
@@ -779,7 +779,9 @@ int esp_batch::plan64(const std::vector<float2>& tw, long long g_total) {
     for (int s = 0; s < nsys; ++s) {
         const SysDev& S = sd[s];
         for (int i = 0; i < S.N; i += 32) pch.push_back(make_int2(s, S.p_off + i));
-        const long long lx = (long long)S.ny * S.nz, ly = (long long)S.nx * S.nz, lz = (long long)S.nx * S.ny;
+        // half spectrum: x row pairs, then nxh columns for the y and z lines
+        const long long lx = (long long)((S.ny + 1) / 2) * S.nz, ly = (long long)S.nxh * S.nz,
+                        lz = (long long)S.nxh * S.ny;
         for (long long l = 0; l < lx; l += 4) xl.push_back(make_int2(s, (int)l));
         for (long long l = 0; l < ly; l += 4) yl.push_back(make_int2(s, (int)l));
         for (long long l = 0; l < lz; l += 4) zl.push_back(make_int2(s, (int)l));
