@@ -45,6 +45,7 @@ __global__ void k64_bin(const int2* __restrict__ chunks, const SysDev* __restric
     const SysDev S = sys[ch.x];
     const int i = ch.y + threadIdx.x;
     double qs[2] = {0.0, 0.0};
+    uint32_t kk = 0xffffffffu;  // this particle's tile (none: an idle lane)
     if (i < S.p_off + S.N) {
         const double4 p = pos_in[i];
         const double q = q_in[i];
@@ -66,13 +67,19 @@ __global__ void k64_bin(const int2* __restrict__ chunks, const SysDev* __restric
         const int tx = i0m[0] / T, ty = i0m[1] / T, tz = i0m[2] / T;
         const uint32_t k = (uint32_t)(S.t_off + (tz * S.nty + ty) * S.ntx + tx);
         key[i] = k;
-        atomicAdd(&tile_count[k], 1u);
+        kk = k;
         posq[i] = make_double4(x[0], x[1], x[2], q);
         trec[i] = make_double4(tt[0], tt[1], tt[2], q);
         rel[i] = (uint32_t)(i0m[0] - tx * T) | ((uint32_t)(i0m[1] - ty * T) << 8) |
                  ((uint32_t)(i0m[2] - tz * T) << 16);
         qs[0] = q;
         qs[1] = q * q;
+    }
+    {
+        // one atomic per distinct tile of the warp (neighbouring particles
+        // mostly share a tile)
+        const unsigned grp = __match_any_sync(0xffffffffu, kk);
+        if (kk != 0xffffffffu && (threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&tile_count[kk], (uint32_t)__popc(grp));
     }
     block_sum_f64<2>(qs, red);
     if (threadIdx.x == 0) {
@@ -738,10 +745,20 @@ __global__ void __launch_bounds__(256, VIR ? 3 : 4)
         // one neighbour per lane and step: streaming 16-byte index segments
         // with four gathers in flight per lane measured 2-6% slower here
         const uint32_t n = nn[i], h = head[i];
+        // the next neighbour index is loaded one step ahead of its gather
+        uint32_t jn = sub < n ? nlist[h + sub] : 0u;
         if (interior)
-            for (uint32_t k = sub; k < n; k += TPP) pair(posq[S.p_off + (int)nlist[h + k]], false);
+            for (uint32_t k = sub; k < n; k += TPP) {
+                const uint32_t j = jn;
+                if (k + TPP < n) jn = nlist[h + k + TPP];
+                pair(posq[S.p_off + (int)j], false);
+            }
         else
-            for (uint32_t k = sub; k < n; k += TPP) pair(posq[S.p_off + (int)nlist[h + k]], true);
+            for (uint32_t k = sub; k < n; k += TPP) {
+                const uint32_t j = jn;
+                if (k + TPP < n) jn = nlist[h + k + TPP];
+                pair(posq[S.p_off + (int)j], true);
+            }
     }
 #pragma unroll
     for (int o = TPP / 2; o > 0; o >>= 1) {

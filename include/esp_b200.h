@@ -62,7 +62,9 @@ typedef struct esp_params {
     double target_error; /* relative RMS force error the auto choices aim at */
     double window_c;     /* window bandwidth c_w; 0 = auto */
     int window_degree;   /* window polynomial degree; 0 = auto */
-    int tile;            /* tile edge in mesh cells; 0 = auto */
+    int tile;            /* tile edge in mesh cells; 0 = auto (tile + order - 1 = 16); a tile whose
+                            extended region needs more shared memory than a CTA has is refused at
+                            create with ESP_ERR_UNSUPPORTED */
     int threads_per_particle; /* pair kernel lanes per particle: 4, 8, 16, 32; 0 = 4 */
     int precision;       /* ESP_FP32 (default) or ESP_FP64 */
     int fft_mode;        /* 0: whole planes/slabs in shared memory where they fit; 1: per-line passes */
