@@ -124,21 +124,6 @@ __device__ __forceinline__ double dhorner64(const double* c, int D, double t) {
     return v;
 }
 
-// ----------------------------------------------------------------------------
-// spreading: one CTA per tile (several when the tiles are few, each over a
-// share of the tile's particle chunks); every thread owns one row (z, y) of
-// the tile's extended region [E]^3 (E = T + P - 1) and sums it in registers, 16 points
-// along x at a time. The tile's particles are staged K64S_CH at a time: per
-// particle its x weights times q as a 16-point row segment pre-shifted to its
-// stencil origin (zero elsewhere), its y and z weights and its origin. A
-// thread adds, in particle order, every staged particle whose stencil covers
-// its row: a broadcast read of the segment and 16 FMAs, no atomics, and a
-// CTA's sums are deterministic. Row r = (r / E, r % E), so with E = 16 and 256
-// threads a warp owns two z planes and the coverage test is nearly
-// warp-uniform. The finished rows pass through shared memory (rows padded to
-// an odd stride) so that the flush, one FP64 atomic per nonzero region point,
-// is coalesced along x.
-// ----------------------------------------------------------------------------
 // Mesh offsets of a tile's extended region [E]^3 with the periodic wrap:
 // roff[r] = (gz ny + gy) nx for region row r = (z, y) = (r / E, r % E), xo[x] = gx.
 __device__ __forceinline__ void region_tables(const SysDev& S, int X0, int Y0, int Z0, int E, int* roff, int* xo) {
@@ -155,6 +140,21 @@ __device__ __forceinline__ void region_tables(const SysDev& S, int X0, int Y0, i
     }
 }
 
+// ----------------------------------------------------------------------------
+// spreading: one CTA per tile (several when the tiles are few, each over a
+// share of the tile's particle chunks); every thread owns one row (z, y) of
+// the tile's extended region [E]^3 (E = T + P - 1) and sums it in registers,
+// 16 points along x at a time. The tile's particles are staged K64S_CH at a time: per
+// particle its x weights times q as a 16-point row segment pre-shifted to its
+// stencil origin (zero elsewhere), its y and z weights and its origin. A
+// thread adds, in particle order, every staged particle whose stencil covers
+// its row: a broadcast read of the segment and 16 FMAs, no atomics, and a
+// CTA's sums are deterministic. Row r = (r / E, r % E), so with E = 16 and 256
+// threads a warp owns two z planes and the coverage test is nearly
+// warp-uniform. The finished rows pass through shared memory (rows padded to
+// an odd stride) so that the flush, one FP64 atomic per nonzero region point,
+// is coalesced along x.
+// ----------------------------------------------------------------------------
 constexpr int K64S_THREADS = 256;
 constexpr int K64S_CH = 48;   // particles staged per pass
 constexpr int K64S_SEG = 16;  // register row segment along x
