@@ -356,7 +356,7 @@ int esp_batch_md_run(esp_batch* b, void* stream, float* pos4, float* vel4, const
  * esp_batch_md_run: one captured step per pointer set, dt and Lennard-Jones
  * parameters, replayed. The per-step sequence of the integration loop of
  * HOOMD's TwoStepNVE around ESPForceCompute::computeForces
- * (src/ESPForceCompute.cc:200-248) in one call. */
+ * (src/ESPForceCompute.cc:96-127) in one call. */
 int esp_batch_md_run_f64(esp_batch* b, void* stream, double* pos4, double* vel4, const double* charge,
                          const unsigned* head, const unsigned* n_neigh, const unsigned* nlist, double* force4,
                          double* energy, double* virial6, int nsteps, double dt, double lj_epsilon, double lj_sigma,
