@@ -48,3 +48,37 @@ def test_oracle_reference_build_present_or_skipped():
         pytest.skip("reference evaluator not built (needs the reference sources)")
     lib = ctypes.CDLL(path)
     assert hasattr(lib, "ref_eval_pairs") and hasattr(lib, "ref_eval_L")
+
+
+def _prototypes():
+    """name -> parameter count of every entry point in the header."""
+    text = open(os.path.join(ROOT, "include", "esp_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    out = {}
+    for m in re.finditer(r"^\s*(?:int|const char\*)\s+(esp_\w+)\s*\(([^;]*?)\)\s*;", text, re.M):
+        params = " ".join(m.group(2).split())
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_binding_argument_counts_match_the_header():
+    """Every ctypes argtypes list has as many entries as the header's
+    prototype has parameters (a missing or extra argument would pass the
+    wrong values silently)."""
+    lib = _lib.get_lib()
+    protos = _prototypes()
+    assert set(protos) == set(_declared())
+    checked = 0
+    for name, n in protos.items():
+        at = getattr(lib, name).argtypes
+        if at is not None:
+            assert len(at) == n, (name, len(at), n)
+            checked += 1
+    assert checked >= 40
+
+
+def test_md_run_f64_rejects_a_null_batch():
+    lib = _lib.get_lib()
+    assert lib.esp_batch_md_run_f64(None, None, None, None, None, None, None, None, None, None, None, 1, 0.002,
+                                    0.0, 0.0, 0.0, 1) == -1
+    assert b"null" in lib.esp_last_error()
