@@ -468,6 +468,19 @@ def run_c1(args):
     print(json.dumps(line), flush=True)
 
 
+def water_rows(spec: str) -> set:
+    """--water-rows "1e-5:f64,1e-3:f32" -> {(1e-5, "f64"), (1e-3, "f32")}; "" -> all rows."""
+    out = set()
+    for r in spec.split(","):
+        if not r.strip():
+            continue
+        t, p = r.split(":")
+        if p not in ("f32", "f64"):
+            raise ValueError("water row precision must be f32 or f64: " + r)
+        out.add((float(t), p))
+    return out
+
+
 def run_water(args):
     """The water-like accuracy sweep (32,768 rigid three-site molecules,
     98,304 charges, no exclusions, r_c 0.9 nm): for each target (1e-3, 1e-5,
@@ -487,7 +500,7 @@ def run_water(args):
     p4 = np.zeros((N, 4))
     p4[:, :3] = posd
     rows = []
-    only = {(float(t), p) for t, p in (r.split(":") for r in args.water_rows.split(",") if r)}
+    only = water_rows(args.water_rows)
     for target, order in ((1e-3, 6), (1e-5, 8), (1e-7, 10)):
         for prec in (0, 1):
             if only and (target, ("f32", "f64")[prec]) not in only:

@@ -4,6 +4,7 @@ mesh rule, so it must agree with the systems the GPU step builds and with
 the meshes the oracle's planner gives them (the same rule as the library's
 planner)."""
 import numpy as np
+import pytest
 
 import bench
 from esp_hoomd_b200 import systems
@@ -21,3 +22,10 @@ def test_workload_description_matches_the_batch():
     # the batch is the published mixed batch of the systems module
     ref = systems.batched_rocksalt(256, seed=bench.SEED)
     assert bench.workload_config(256, 1)["particles_per_gpu"] == sum(s.N for s in ref)
+
+
+def test_water_row_filter():
+    assert bench.water_rows("") == set()
+    assert bench.water_rows("1e-5:f64, 1e-3:f32") == {(1e-5, "f64"), (1e-3, "f32")}
+    with pytest.raises(ValueError):
+        bench.water_rows("1e-5:f16")
