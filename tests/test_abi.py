@@ -82,3 +82,34 @@ def test_md_run_f64_rejects_a_null_batch():
     assert lib.esp_batch_md_run_f64(None, None, None, None, None, None, None, None, None, None, None, 1, 0.002,
                                     0.0, 0.0, 0.0, 1) == -1
     assert b"null" in lib.esp_last_error()
+
+
+@pytest.mark.parametrize("field,value,code,text", [
+    ("order", 13, -4, b"order must be in [2, 12]"),
+    ("order", 1, -4, b"order must be in [2, 12]"),
+    ("tile", 70, -4, b"tile edge must be <= 64"),
+    ("threads_per_particle", 3, -4, b"threads_per_particle must be 4, 8, 16 or 32"),
+    ("precision", 2, -1, b"precision must be ESP_FP32 or ESP_FP64"),
+    ("interp_mode", 3, -1, b"interp_mode must be 0, 1 or 2"),
+])
+def test_create_validates_parameters_before_any_device_work(field, value, code, text):
+    """Parameter errors are reported by the host with their own status code
+    and message (ESP_ERR_UNSUPPORTED / ESP_ERR_INVALID), before the context
+    touches the device, so they need no GPU."""
+    lib = _lib.get_lib()
+    p = _lib.EspParams()
+    assert lib.esp_params_default(ctypes.byref(p)) == 0
+    setattr(p, field, value)
+    h = ctypes.c_void_p()
+    assert lib.esp_create(ctypes.byref(p), 8.0, 8.0, 8.0, 512, ctypes.byref(h)) == code
+    assert text in lib.esp_last_error()
+    assert not h.value
+
+
+def test_create_rejects_a_negative_particle_count():
+    lib = _lib.get_lib()
+    p = _lib.EspParams()
+    lib.esp_params_default(ctypes.byref(p))
+    h = ctypes.c_void_p()
+    assert lib.esp_create(ctypes.byref(p), 8.0, 8.0, 8.0, -5, ctypes.byref(h)) == -1
+    assert b"negative particle count" in lib.esp_last_error()
