@@ -113,3 +113,19 @@ def test_create_rejects_a_negative_particle_count():
     h = ctypes.c_void_p()
     assert lib.esp_create(ctypes.byref(p), 8.0, 8.0, 8.0, -5, ctypes.byref(h)) == -1
     assert b"negative particle count" in lib.esp_last_error()
+
+
+def test_batch_create_validates_on_the_host():
+    lib = _lib.get_lib()
+    p = _lib.EspParams()
+    lib.esp_params_default(ctypes.byref(p))
+    h = ctypes.c_void_p()
+    n = (ctypes.c_int * 2)(512, 512)
+    boxes = (ctypes.c_double * 6)(8, 8, 8, 8, 8, 8)
+    assert lib.esp_batch_create(ctypes.byref(p), 0, n, boxes, None, ctypes.byref(h)) == -1
+    assert b"number of systems must be positive" in lib.esp_last_error()
+    assert lib.esp_batch_create(ctypes.byref(p), 2, None, boxes, None, ctypes.byref(h)) == -1
+    small = (ctypes.c_double * 6)(8, 8, 8, 1, 8, 8)  # r_c = 3 exceeds half of the second box
+    assert lib.esp_batch_create(ctypes.byref(p), 2, n, small, None, ctypes.byref(h)) == -1
+    assert b"rcut must not exceed half the box" in lib.esp_last_error()
+    assert not h.value
